@@ -1,0 +1,104 @@
+"""ctypes binding of the C ABI in include/rt_b200.h (librt_b200.so, built in-tree).
+
+This is a thin loader: every function here forwards to the CUDA library. There is
+no CPU fallback: if the library is missing, import fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "lib" / "librt_b200.so"
+
+RT_OK = 0
+RT_TRACE_SHADOW = 0x1
+RT_TRACE_FAST = 0x2
+RT_PRIM_SHAPE = 0x40000000
+
+STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID", 2: "RT_ERR_CUDA", 3: "RT_ERR_OOM", 4: "RT_ERR_TIMEOUT",
+                5: "RT_ERR_UNSUPPORTED", 6: "RT_ERR_STATE", 7: "RT_ERR_CAPACITY"}
+
+RAY_DTYPE = np.dtype([("ox", "<f4"), ("oy", "<f4"), ("oz", "<f4"), ("tmax", "<f4"),
+                      ("dx", "<f4"), ("dy", "<f4"), ("dz", "<f4"), ("flags", "<u4")], align=True)
+HIT_DTYPE = np.dtype([("t", "<f4"), ("prim", "<i4"), ("b1", "<f4"), ("b2", "<f4")], align=True)
+
+
+class RtError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class SceneStats(ctypes.Structure):
+    _fields_ = [("triangles", ctypes.c_uint64), ("spheres", ctypes.c_uint64), ("bvh8_nodes", ctypes.c_uint64),
+                ("bvh8_leaf_triangles", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64),
+                ("build_ms", ctypes.c_double)]
+
+
+class TraceStats(ctypes.Structure):
+    _fields_ = [("rays", ctypes.c_uint64), ("exact_fallback_rays", ctypes.c_uint64)]
+
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+_I32 = ctypes.c_int32
+_INT = ctypes.c_int
+_F32 = ctypes.c_float
+
+# name -> argtypes (all return int status)
+SIGNATURES = {
+    "rt_abi_version": [],
+    "rt_last_error": [ctypes.c_char_p, ctypes.c_size_t],
+    "rt_context_create": [_INT, ctypes.POINTER(_P)],
+    "rt_context_destroy": [_P],
+    "rt_context_set_stream": [_P, _P],
+    "rt_context_synchronize": [_P],
+    "rt_scene_create": [_P, ctypes.POINTER(_P)],
+    "rt_scene_destroy": [_P],
+    "rt_scene_add_mesh": [_P, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _I32, _INT, ctypes.POINTER(_U32)],
+    "rt_scene_add_sphere": [_P, _P, _P, _F32, _U32, _I32, _INT, ctypes.POINTER(_U32)],
+    "rt_scene_commit": [_P],
+    "rt_scene_stats_get": [_P, ctypes.POINTER(SceneStats)],
+    "rt_trace_closest": [_P, _P, _U64, _P, _U32],
+    "rt_trace_closest_host": [_P, _P, _U64, _P, _U32],
+    "rt_trace_any": [_P, _P, _U64, _P, _U32],
+    "rt_trace_stats_get": [_P, ctypes.POINTER(TraceStats)],
+}
+
+
+def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(f"CUDA core library not built: {p} (run __graft_entry__.build())")
+    lib = ctypes.CDLL(str(p))
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    return lib
+
+
+_lib: ctypes.CDLL | None = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = load()
+    return _lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    lib().rt_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int):
+    if status != RT_OK:
+        raise RtError(status, last_error())

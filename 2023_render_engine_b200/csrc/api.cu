@@ -1,0 +1,369 @@
+// C ABI entry points (include/rt_b200.h): contexts, scenes, tracing.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "rt_internal.h"
+
+namespace rtb {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int fail(int status, const std::string &msg)
+{
+    set_error(msg);
+    return status;
+}
+
+int cuda_status(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return RT_OK;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? RT_ERR_OOM : RT_ERR_CUDA;
+}
+
+int DevBuf::reserve(size_t n)
+{
+    if (n <= bytes && ptr) return RT_OK;
+    release();
+    if (n == 0) return RT_OK;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return cuda_status(e, "cudaMalloc");
+    }
+    bytes = n;
+    return RT_OK;
+}
+
+int DevBuf::upload(const void *src, size_t n, cudaStream_t s)
+{
+    RTB_CHECK(reserve(n));
+    if (n == 0) return RT_OK;
+    RTB_CUDA(cudaMemcpyAsync(ptr, src, n, cudaMemcpyHostToDevice, s));
+    return RT_OK;
+}
+
+void DevBuf::release()
+{
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+// Status word written by kernels -> rt_status.
+int check_device_status(uint32_t word)
+{
+    switch (word) {
+    case DEV_OK:
+        return RT_OK;
+    case DEV_STACK_OVERFLOW:
+        return fail(RT_ERR_CAPACITY, "traversal stack overflow (a ray was replayed on the reference tree)");
+    case DEV_STEP_CAP:
+        return fail(RT_ERR_TIMEOUT, "traversal exceeded its step cap");
+    case DEV_QUEUE_OVERFLOW:
+        return fail(RT_ERR_CAPACITY, "exact-traversal queue overflow");
+    default:
+        return fail(RT_ERR_CUDA, "unknown device status");
+    }
+}
+
+}  // namespace rtb
+
+using namespace rtb;
+
+rtb::SceneView rt_scene::view() const
+{
+    SceneView v{};
+    v.nodes = d_nodes.as<Bvh8Node>();
+    v.tris = d_tris.as<TriRecord>();
+    v.leafpos = d_leafpos.as<uint32_t>();
+    v.ref_boxes = d_ref_boxes.as<float2>();
+    v.ref_sorted = d_ref_sorted.as<uint32_t>();
+    v.ref_pos = d_ref_pos.as<uint32_t>();
+    v.spheres = d_spheres.as<SphereRecord>();
+    v.ntri = (uint32_t)(tri9.size() / 9);
+    v.nspheres = (uint32_t)spheres.size();
+    v.nnodes = (uint32_t)nnodes;
+    return v;
+}
+
+uint64_t rt_scene::device_bytes() const
+{
+    return d_nodes.bytes + d_tris.bytes + d_leafpos.bytes + d_ref_boxes.bytes + d_ref_sorted.bytes + d_ref_pos.bytes +
+           d_spheres.bytes + scratch.queue.bytes + scratch.counters.bytes;
+}
+
+extern "C" {
+
+int rt_abi_version(void) { return RT_B200_ABI_VERSION; }
+
+int rt_last_error(char *buf, size_t len)
+{
+    if (!buf || len == 0) return RT_ERR_INVALID;
+    size_t n = std::min(len - 1, g_last_error.size());
+    std::memcpy(buf, g_last_error.data(), n);
+    buf[n] = 0;
+    return RT_OK;
+}
+
+int rt_context_create(int device, rt_context **out)
+{
+    if (!out) return fail(RT_ERR_INVALID, "rt_context_create: out is null");
+    int count = 0;
+    RTB_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return fail(RT_ERR_INVALID, "rt_context_create: no such device");
+    RTB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    RTB_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return fail(RT_ERR_UNSUPPORTED, "rt_context_create: sm_100a (B200) required");
+    rt_context *c = new rt_context();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_status(e, "cudaStreamCreate");
+    }
+    c->own_stream = true;
+    *out = c;
+    return RT_OK;
+}
+
+int rt_context_destroy(rt_context *ctx)
+{
+    if (!ctx) return RT_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return RT_OK;
+}
+
+int rt_context_set_stream(rt_context *ctx, void *stream)
+{
+    if (!ctx) return fail(RT_ERR_INVALID, "rt_context_set_stream: null context");
+    if (ctx->own_stream && ctx->stream) {
+        RTB_CUDA(cudaStreamSynchronize(ctx->stream));
+        cudaStreamDestroy(ctx->stream);
+    }
+    ctx->stream = static_cast<cudaStream_t>(stream);
+    ctx->own_stream = false;
+    return RT_OK;
+}
+
+int rt_context_synchronize(rt_context *ctx)
+{
+    if (!ctx) return fail(RT_ERR_INVALID, "rt_context_synchronize: null context");
+    RTB_CUDA(cudaSetDevice(ctx->device));
+    RTB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return RT_OK;
+}
+
+int rt_scene_create(rt_context *ctx, rt_scene **out)
+{
+    if (!ctx || !out) return fail(RT_ERR_INVALID, "rt_scene_create: null argument");
+    rt_scene *s = new rt_scene();
+    s->ctx = ctx;
+    *out = s;
+    return RT_OK;
+}
+
+int rt_scene_destroy(rt_scene *s)
+{
+    if (!s) return RT_OK;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    for (DevBuf *b : {&s->d_nodes, &s->d_tris, &s->d_leafpos, &s->d_ref_boxes, &s->d_ref_sorted, &s->d_ref_pos,
+                      &s->d_spheres, &s->scratch.queue, &s->scratch.counters, &s->h2d_rays, &s->d2h_hits})
+        b->release();
+    delete s;
+    return RT_OK;
+}
+
+int rt_scene_add_mesh(rt_scene *s, const float *xyz, uint32_t nv, const uint32_t *idx, uint32_t ntri,
+                      const float *normals, uint32_t nn, const uint32_t *nidx, uint32_t material, int32_t shape_id,
+                      int transparent, uint32_t *first_tri)
+{
+    if (!s || (!xyz && nv) || (!idx && ntri)) return fail(RT_ERR_INVALID, "rt_scene_add_mesh: null argument");
+    if ((normals == nullptr) != (nidx == nullptr)) return fail(RT_ERR_INVALID, "rt_scene_add_mesh: normals need nidx");
+    uint64_t base = s->tri9.size() / 9;
+    if (base + ntri >= 0x40000000ull) return fail(RT_ERR_CAPACITY, "rt_scene_add_mesh: more than 2^30 triangles");
+    for (uint64_t i = 0; i < 3ull * ntri; i++) {
+        if (idx[i] >= nv) return fail(RT_ERR_INVALID, "rt_scene_add_mesh: vertex index out of range");
+        if (nidx && nidx[i] >= nn) return fail(RT_ERR_INVALID, "rt_scene_add_mesh: normal index out of range");
+    }
+    uint32_t nbase = (uint32_t)(s->normals.size() / 3);
+    if (normals) s->normals.insert(s->normals.end(), normals, normals + 3ull * nn);
+    s->tri9.reserve(s->tri9.size() + 9ull * ntri);
+    for (uint32_t t = 0; t < ntri; t++) {
+        for (int k = 0; k < 3; k++) {
+            const float *p = xyz + 3ull * idx[3ull * t + k];
+            s->tri9.push_back(p[0]);
+            s->tri9.push_back(p[1]);
+            s->tri9.push_back(p[2]);
+            s->tri_normal_idx.push_back(nidx ? (int32_t)(nbase + nidx[3ull * t + k]) : -1);
+        }
+        s->tri_material.push_back(material);
+        s->tri_shape.push_back(shape_id);
+        s->tri_transparent.push_back(transparent ? 1 : 0);
+    }
+    if (first_tri) *first_tri = (uint32_t)base;
+    s->committed = false;
+    return RT_OK;
+}
+
+int rt_scene_add_sphere(rt_scene *s, const float o2w[16], const float w2o[16], float radius, uint32_t material,
+                        int32_t shape_id, int transparent, uint32_t *index)
+{
+    if (!s || !o2w || !w2o) return fail(RT_ERR_INVALID, "rt_scene_add_sphere: null argument");
+    if (!(radius > 0)) return fail(RT_ERR_INVALID, "rt_scene_add_sphere: radius must be positive");
+    SphereRecord r{};
+    std::memcpy(r.w2o, w2o, sizeof(r.w2o));
+    std::memcpy(r.o2w, o2w, sizeof(r.o2w));
+    r.radius = radius;
+    r.material = material;
+    r.shape_id = shape_id;
+    r.flags = transparent ? 1u : 0u;
+    if (index) *index = (uint32_t)s->spheres.size();
+    s->spheres.push_back(r);
+    s->committed = false;
+    return RT_OK;
+}
+
+int rt_scene_commit(rt_scene *s)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_scene_commit: null scene");
+    RTB_CUDA(cudaSetDevice(s->ctx->device));
+    cudaStream_t st = s->ctx->stream;
+    auto t0 = std::chrono::steady_clock::now();
+    const uint32_t n = (uint32_t)(s->tri9.size() / 9);
+    // conservative margin: 1e-5 of the largest coordinate magnitude
+    float maxabs = 0.f;
+    for (float x : s->tri9) maxabs = std::max(maxabs, std::fabs(x));
+    const float margin = std::max(1e-5f * maxabs, 1e-30f);
+    Bvh8Host bvh;
+    RefTreeHost ref;
+    build_bvh8(s->tri9.data(), n, margin, bvh);
+    build_ref_tree(s->tri9.data(), n, ref);
+    std::vector<TriRecord> recs(bvh.leaf_tris.size());
+    std::vector<uint32_t> leafpos(n, 0);
+    for (size_t r = 0; r < bvh.leaf_tris.size(); r++) {
+        uint32_t id = bvh.leaf_tris[r];
+        const float *p = s->tri9.data() + 9ull * id;
+        TriRecord &tr = recs[r];
+        uint32_t rank = ref.rank[id], flags = s->tri_transparent[id];
+        tr.v0 = make_float4(p[0], p[1], p[2], 0.f);
+        tr.v1 = make_float4(p[3], p[4], p[5], 0.f);
+        tr.v2 = make_float4(p[6], p[7], p[8], 0.f);
+        std::memcpy(&tr.v0.w, &rank, 4);
+        std::memcpy(&tr.v1.w, &id, 4);
+        std::memcpy(&tr.v2.w, &flags, 4);
+        leafpos[id] = (uint32_t)r;
+    }
+    if (bvh.nodes.empty()) {
+        bvh.nodes.resize(1);
+        std::memset(bvh.nodes.data(), 0, sizeof(Bvh8Node));
+        std::memset(bvh.nodes[0].meta, 0xFF, 8);
+    }
+    s->nnodes = bvh.nodes.size();
+    RTB_CHECK(s->d_nodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(Bvh8Node), st));
+    RTB_CHECK(s->d_tris.upload(recs.data(), recs.size() * sizeof(TriRecord), st));
+    RTB_CHECK(s->d_leafpos.upload(leafpos.data(), leafpos.size() * 4, st));
+    RTB_CHECK(s->d_ref_boxes.upload(ref.boxes.data(), ref.boxes.size() * 4, st));
+    RTB_CHECK(s->d_ref_sorted.upload(ref.sorted.data(), ref.sorted.size() * 4, st));
+    RTB_CHECK(s->d_ref_pos.upload(ref.pos.data(), ref.pos.size() * 4, st));
+    RTB_CHECK(s->d_spheres.upload(s->spheres.data(), s->spheres.size() * sizeof(SphereRecord), st));
+    RTB_CHECK(s->scratch.counters.reserve(64));
+    RTB_CUDA(cudaStreamSynchronize(st));
+    s->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    s->committed = true;
+    return RT_OK;
+}
+
+int rt_scene_stats_get(rt_scene *s, rt_scene_stats *out)
+{
+    if (!s || !out) return fail(RT_ERR_INVALID, "rt_scene_stats_get: null argument");
+    out->triangles = s->tri9.size() / 9;
+    out->spheres = s->spheres.size();
+    out->bvh8_nodes = s->nnodes;
+    out->bvh8_leaf_triangles = s->d_tris.bytes / sizeof(TriRecord);
+    out->device_bytes = s->device_bytes();
+    out->build_ms = s->build_ms;
+    return RT_OK;
+}
+
+static int trace_common(rt_scene *s, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_trace_closest: null scene");
+    if (!s->committed) return fail(RT_ERR_STATE, "rt_trace_closest: scene not committed");
+    if (n && (!rays || !hits)) return fail(RT_ERR_INVALID, "rt_trace_closest: null buffer");
+    if (n >= 0x80000000ull) return fail(RT_ERR_INVALID, "rt_trace_closest: at most 2^31-1 rays per call");
+    if ((reinterpret_cast<uintptr_t>(rays) | reinterpret_cast<uintptr_t>(hits)) & 15u)
+        return fail(RT_ERR_INVALID, "rt_trace_closest: buffers must be 16-byte aligned");
+    RTB_CUDA(cudaSetDevice(s->ctx->device));
+    RTB_CHECK(s->scratch.queue.reserve(std::max<uint64_t>(n, 1) * 4));
+    RTB_CHECK(launch_trace_closest(s->view(), rays, n, hits, flags, s->scratch.queue.as<uint32_t>(), (uint32_t)n,
+                                   s->scratch.counters.as<uint32_t>(), s->ctx->stream));
+    return RT_OK;
+}
+
+static int finish_trace(rt_scene *s, uint64_t n)
+{
+    uint32_t c[4] = {0, 0, 0, 0};
+    RTB_CUDA(cudaMemcpyAsync(c, s->scratch.counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, s->ctx->stream));
+    RTB_CUDA(cudaStreamSynchronize(s->ctx->stream));
+    s->last_rays = n;
+    s->last_fallback = c[0];
+    return check_device_status(c[1]);
+}
+
+int rt_trace_closest(rt_scene *s, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags)
+{
+    RTB_CHECK(trace_common(s, rays, n, hits, flags));
+    return finish_trace(s, n);
+}
+
+int rt_trace_closest_host(rt_scene *s, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_trace_closest_host: null scene");
+    if (n && (!rays || !hits)) return fail(RT_ERR_INVALID, "rt_trace_closest_host: null buffer");
+    RTB_CUDA(cudaSetDevice(s->ctx->device));
+    cudaStream_t st = s->ctx->stream;
+    RTB_CHECK(s->h2d_rays.reserve(std::max<uint64_t>(n, 1) * sizeof(rt_ray)));
+    RTB_CHECK(s->d2h_hits.reserve(std::max<uint64_t>(n, 1) * sizeof(rt_hit)));
+    RTB_CUDA(cudaMemcpyAsync(s->h2d_rays.ptr, rays, n * sizeof(rt_ray), cudaMemcpyHostToDevice, st));
+    RTB_CHECK(trace_common(s, s->h2d_rays.as<rt_ray>(), n, s->d2h_hits.as<rt_hit>(), flags));
+    RTB_CUDA(cudaMemcpyAsync(hits, s->d2h_hits.ptr, n * sizeof(rt_hit), cudaMemcpyDeviceToHost, st));
+    return finish_trace(s, n);
+}
+
+int rt_trace_any(rt_scene *s, const rt_ray *rays, uint64_t n, uint8_t *occluded, uint32_t flags)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_trace_any: null scene");
+    if (!s->committed) return fail(RT_ERR_STATE, "rt_trace_any: scene not committed");
+    if (n && (!rays || !occluded)) return fail(RT_ERR_INVALID, "rt_trace_any: null buffer");
+    if (reinterpret_cast<uintptr_t>(rays) & 15u) return fail(RT_ERR_INVALID, "rt_trace_any: rays must be 16-byte aligned");
+    RTB_CUDA(cudaSetDevice(s->ctx->device));
+    RTB_CHECK(launch_trace_any(s->view(), rays, n, occluded, flags, s->scratch.counters.as<uint32_t>(), s->ctx->stream));
+    uint32_t c[4] = {0, 0, 0, 0};
+    RTB_CUDA(cudaMemcpyAsync(c, s->scratch.counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, s->ctx->stream));
+    RTB_CUDA(cudaStreamSynchronize(s->ctx->stream));
+    return check_device_status(c[1]);
+}
+
+int rt_trace_stats_get(rt_scene *s, rt_trace_stats *out)
+{
+    if (!s || !out) return fail(RT_ERR_INVALID, "rt_trace_stats_get: null argument");
+    out->rays = s->last_rays;
+    out->exact_fallback_rays = s->last_fallback;
+    return RT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,168 @@
+// Internal declarations shared by the host build code, the kernels and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/rt_b200.h"
+
+namespace rtb {
+
+// ------------------------------------------------------------------ errors
+
+void set_error(const std::string &msg);
+int fail(int status, const std::string &msg);
+// Records a CUDA error (with location) and returns RT_ERR_CUDA, or RT_OK.
+int cuda_status(cudaError_t e, const char *what);
+
+#define RTB_CUDA(call)                                            \
+    do {                                                          \
+        int rtb_s_ = ::rtb::cuda_status((call), #call);           \
+        if (rtb_s_ != RT_OK) return rtb_s_;                       \
+    } while (0)
+
+#define RTB_CHECK(expr)                          \
+    do {                                         \
+        int rtb_s_ = (expr);                     \
+        if (rtb_s_ != RT_OK) return rtb_s_;      \
+    } while (0)
+
+// Device buffer that remembers its size; grows on demand, never shrinks.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t n);  // n bytes at least; contents are not preserved
+    int upload(const void *src, size_t n, cudaStream_t s);
+    void release();
+    template <typename T>
+    T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Error codes written by kernels into the status word (first failure wins).
+enum DevError : uint32_t {
+    DEV_OK = 0,
+    DEV_STACK_OVERFLOW = 1,  // traversal stack would overflow (result of that ray is undefined)
+    DEV_STEP_CAP = 2,        // traversal exceeded its step cap
+    DEV_QUEUE_OVERFLOW = 3,  // a work queue would overflow
+};
+
+// ---------------------------------------------------------- BVH8 layout
+
+// Compressed 8-wide node, 80 bytes (5 x 16 B). Child boxes are quantized to 8 bits per
+// axis on a power-of-two grid anchored at `p`; every quantized box contains the child's
+// exact box enlarged by the scene's conservative margin, so the float slab test never
+// culls a primitive the exact triangle test would hit.
+struct alignas(16) Bvh8Node {
+    float px, py, pz;      // grid origin
+    uint8_t ex, ey, ez;    // biased exponents of the grid step per axis (2^(e-127))
+    uint8_t imask;         // bit k: child slot k is an interior node
+    uint32_t child_base;   // node index of the first interior child
+    uint32_t tri_base;     // record index of the first leaf triangle
+    uint8_t meta[8];       // interior: slot's rank among interior children; leaf: (count-1)<<5 | offset
+    uint8_t qlox[8], qloy[8], qloz[8];
+    uint8_t qhix[8], qhiy[8], qhiz[8];
+};
+static_assert(sizeof(Bvh8Node) == 80, "Bvh8Node must be 80 bytes");
+
+// Triangle record in BVH8 leaf order, 48 bytes: the three world-space vertices in the
+// reference's vertex order with, in the w lanes, the reference traversal rank, the
+// global triangle id and the flags (bit 0: transparent to shadow rays).
+struct alignas(16) TriRecord {
+    float4 v0;  // w: rank (uint bits)
+    float4 v1;  // w: triangle id (uint bits)
+    float4 v2;  // w: flags
+};
+
+// Sphere as the reference stores it: world->object matrix (rows 0..3) and radius.
+struct alignas(16) SphereRecord {
+    float w2o[16];
+    float radius;
+    uint32_t material;
+    int32_t shape_id;
+    uint32_t flags;  // bit 0: transparent to shadow rays
+    float o2w[16];
+};
+
+// Device view used by the kernels.
+struct SceneView {
+    const Bvh8Node *nodes;
+    const TriRecord *tris;       // leaf order
+    const uint32_t *leafpos;     // triangle id -> record index
+    const float2 *ref_boxes;     // reference tree boxes, 3 float2 per node (pMin xyz, pMax xyz)
+    const uint32_t *ref_sorted;  // sorted position -> triangle id
+    const uint32_t *ref_pos;     // triangle id -> sorted position
+    const SphereRecord *spheres;
+    uint32_t ntri;
+    uint32_t nspheres;
+    uint32_t nnodes;
+    uint32_t root_is_leaf;  // scene with a single leaf (ntri <= 3): node 0 still describes it
+};
+
+// ------------------------------------------------------------ host build
+
+struct Bvh8Host {
+    std::vector<Bvh8Node> nodes;
+    std::vector<uint32_t> leaf_tris;  // record index -> triangle id
+};
+
+// Builds the 8-wide BVH over `n` triangles (9 floats each). `margin` enlarges every box.
+void build_bvh8(const float *tri9, uint32_t n, float margin, Bvh8Host &out);
+
+// Reference-order tree (cuda_libraries/BVH.cu:314-341): sorted ids, node boxes and
+// each triangle's rank in the tree's static traversal order.
+struct RefTreeHost {
+    std::vector<uint32_t> codes;
+    std::vector<uint32_t> sorted;  // sorted position -> triangle id
+    std::vector<uint32_t> pos;     // triangle id -> sorted position
+    std::vector<float> boxes;      // (2n-1)*6
+    std::vector<uint32_t> rank;    // triangle id -> traversal rank
+};
+void build_ref_tree(const float *tri9, uint32_t n, RefTreeHost &out);
+
+// ---------------------------------------------------------------- kernels
+
+struct TraceScratch {
+    DevBuf queue;   // ray indices needing the exact path
+    DevBuf counters;  // [0] queue length, [1] status word, [2..] stats
+};
+
+int launch_trace_closest(const SceneView &v, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags,
+                         uint32_t *queue, uint32_t queue_cap, uint32_t *counters, cudaStream_t s);
+int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, uint8_t *occluded, uint32_t flags,
+                     uint32_t *counters, cudaStream_t s);
+
+}  // namespace rtb
+
+// ------------------------------------------------------------- handles
+
+struct rt_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 0;
+};
+
+struct rt_scene {
+    rt_context *ctx = nullptr;
+    // host copies of what was added
+    std::vector<float> tri9;           // 9 floats per triangle
+    std::vector<uint32_t> tri_material;
+    std::vector<int32_t> tri_shape;
+    std::vector<uint8_t> tri_transparent;
+    std::vector<int32_t> tri_normal_idx;  // 3 per triangle into `normals` (-1: none)
+    std::vector<float> normals;
+    std::vector<rtb::SphereRecord> spheres;
+    bool committed = false;
+    double build_ms = 0;
+    uint64_t nnodes = 0;
+    // device
+    rtb::DevBuf d_nodes, d_tris, d_leafpos, d_ref_boxes, d_ref_sorted, d_ref_pos, d_spheres;
+    rtb::TraceScratch scratch;
+    uint64_t last_rays = 0, last_fallback = 0;
+    rtb::DevBuf h2d_rays, d2h_hits;  // device staging for the host-buffer entry points
+    rtb::SceneView view() const;
+    uint64_t device_bytes() const;
+};

@@ -1,0 +1,152 @@
+/*
+ * rt_b200.h — C ABI of the B200 rendering core.
+ *
+ * One GPU (sm_100a). Plain pointers and sizes only; every function returns an
+ * rt_status (0 = RT_OK). rt_last_error() returns the message of the last failure
+ * on the calling host thread. Calls on one rt_context are serialised by the
+ * caller (the reference API is not re-entrant either, cuda_libraries/types.h:20);
+ * work is queued on the context's stream and functions return once it is done
+ * unless stated otherwise.
+ *
+ * Each entry point names the reference interface it replaces
+ * (hsunekichi/2023_render_engine, path:line).
+ */
+#ifndef RT_B200_H
+#define RT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RT_B200_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define RT_API __attribute__((visibility("default")))
+#else
+#define RT_API
+#endif
+
+typedef enum rt_status {
+    RT_OK = 0,
+    RT_ERR_INVALID = 1,     /* bad argument (null pointer, size, index) */
+    RT_ERR_CUDA = 2,        /* CUDA runtime error */
+    RT_ERR_OOM = 3,         /* device allocation failed */
+    RT_ERR_TIMEOUT = 4,     /* a device loop hit its iteration cap */
+    RT_ERR_UNSUPPORTED = 5, /* feature or material not supported */
+    RT_ERR_STATE = 6,       /* wrong call order (e.g. trace before commit) */
+    RT_ERR_CAPACITY = 7     /* a fixed-capacity queue or buffer would overflow */
+} rt_status;
+
+typedef struct rt_context rt_context;
+typedef struct rt_scene rt_scene;
+
+/* ---------------------------------------------------------------- basics */
+
+RT_API int rt_abi_version(void);
+/* Copies the calling thread's last error message (NUL-terminated, truncated). */
+RT_API int rt_last_error(char *buf, size_t len);
+
+/* Selects the device (replaces the bare cudaSetDevice(argv[2]) of the reference
+ * mains, cornellBoxGuion.cu:35-49) and creates the context's stream. */
+RT_API int rt_context_create(int device, rt_context **out);
+RT_API int rt_context_destroy(rt_context *ctx);
+/* Use a caller-owned cudaStream_t (passed as void*) instead of the internal one. */
+RT_API int rt_context_set_stream(rt_context *ctx, void *cuda_stream);
+RT_API int rt_context_synchronize(rt_context *ctx);
+
+/* ----------------------------------------------------------------- scene */
+
+/* Scene container; replaces Scene (integration/Scene.cu:21-95). */
+RT_API int rt_scene_create(rt_context *ctx, rt_scene **out);
+RT_API int rt_scene_destroy(rt_scene *scene);
+
+/* Appends a triangle mesh (world-space vertices). Triangles get consecutive global
+ * ids in call order — the concatenation order of Scene::build / BVH::initializeTriangles
+ * (Scene.cu:64-89, BVH.cu:288-291). `normals`/`nidx` may be NULL (no shading normals);
+ * when given, the reference's interpolated shading normal and its 0.15 hit-point
+ * offset apply (Triangle.cu:379-419). material: index into the material table.
+ * shape_id: the id the reference stores in SurfaceInteraction (meshId, Triangle.cu:427).
+ * transparent: 1 when shadow rays ignore these triangles (Triangle.cu:439-440).
+ * first_tri (out, nullable): global id of the mesh's first triangle. */
+RT_API int rt_scene_add_mesh(rt_scene *scene, const float *xyz, uint32_t nv, const uint32_t *idx, uint32_t ntri,
+                      const float *normals, uint32_t nn, const uint32_t *nidx, uint32_t material,
+                      int32_t shape_id, int transparent, uint32_t *first_tri);
+
+/* Appends a full sphere of `radius` with the reference's object<->world matrices
+ * (row-major 4x4; Sphere(Point3f,Float), shapes/Sphere.cu:233-245). Analytic shapes
+ * are reported as prim = RT_PRIM_SHAPE | index. */
+RT_API int rt_scene_add_sphere(rt_scene *scene, const float object_to_world[16], const float world_to_object[16],
+                        float radius, uint32_t material, int32_t shape_id, int transparent,
+                        uint32_t *index);
+
+/* Builds the acceleration structures: the 8-wide compressed BVH used for traversal
+ * and the reference-order tree (BVH::BVH, cuda_libraries/BVH.cu:314-341) whose
+ * static order breaks exact distance ties like the reference does. */
+RT_API int rt_scene_commit(rt_scene *scene);
+
+typedef struct rt_scene_stats {
+    uint64_t triangles;
+    uint64_t spheres;
+    uint64_t bvh8_nodes;
+    uint64_t bvh8_leaf_triangles; /* triangle records in BVH8 leaf order */
+    uint64_t device_bytes;        /* device memory held by the scene */
+    double build_ms;              /* host build time of the last commit */
+} rt_scene_stats;
+RT_API int rt_scene_stats_get(rt_scene *scene, rt_scene_stats *out);
+
+/* ----------------------------------------------------------------- rays */
+
+#define RT_PRIM_NONE (-1)
+#define RT_PRIM_SHAPE ((int32_t)0x40000000) /* analytic shape flag in rt_hit.prim */
+
+/* 32-byte ray: origin + tmax, direction + flags (read as two 16-byte loads). */
+typedef struct rt_ray {
+    float ox, oy, oz, tmax;
+    float dx, dy, dz;
+    uint32_t flags; /* reserved, 0 */
+} rt_ray;
+
+/* 16-byte hit: distance, primitive (global triangle id, RT_PRIM_SHAPE|shape, or -1),
+ * scaled barycentrics b1, b2 of a triangle hit (0 for shapes). */
+typedef struct rt_hit {
+    float t;
+    int32_t prim;
+    float b1, b2;
+} rt_hit;
+
+/* Trace flags. */
+#define RT_TRACE_SHADOW 0x1u /* checkShadow semantics: skip transparent primitives */
+#define RT_TRACE_FAST 0x2u   /* skip the reference-order exactness checks */
+
+/* Closest hit for n rays, device pointers. Replaces BVH::intersectRays
+ * (cuda_libraries/BVH.cu:541-584) followed by the analytic-shape loop of
+ * Scene::intersects (integration/Scene.cu:108-150): the triangle id equals the one
+ * the reference traversal returns (its distance-tie order and its offset-update
+ * quirk included), unless RT_TRACE_FAST is given. */
+RT_API int rt_trace_closest(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, rt_hit *hits_dev, uint32_t flags);
+
+/* Same with host buffers: copies rays in and hits out inside the call (pinned
+ * staging; the end-to-end form the reference's host-vector API corresponds to). */
+RT_API int rt_trace_closest_host(rt_scene *scene, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags);
+
+/* Occlusion test: occluded[i] = 1 when a primitive is hit at t < rays[i].tmax.
+ * Replaces the shadow-ray use of Scene::intersects in Scene::isVisible
+ * (Scene.cu:238-276). Device pointers. */
+RT_API int rt_trace_any(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, uint8_t *occluded_dev, uint32_t flags);
+
+/* Counters of the last rt_trace_closest call: rays that took the reference-order
+ * exact traversal (distance ties resolved through the reference tree, grazing
+ * rays, near-zero offsets). */
+typedef struct rt_trace_stats {
+    uint64_t rays;
+    uint64_t exact_fallback_rays;
+} rt_trace_stats;
+RT_API int rt_trace_stats_get(rt_scene *scene, rt_trace_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RT_B200_H */

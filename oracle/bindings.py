@@ -1,0 +1,281 @@
+"""Test infrastructure: ctypes bindings of the two checkers.
+
+* RefOracle: the reference renderer's own code compiled from its sources
+  (oracle/_ref/libref_oracle.so, recipe in oracle/Makefile).
+* Restated: the plain-C restatement (oracle/_build/librt_oracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's reference/CPU-baseline legs use
+these. The product never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_SO = HERE / "_ref" / "libref_oracle.so"
+RESTATE_SO = HERE / "_build" / "librt_oracle.so"
+
+P = ctypes.c_void_p
+U32 = ctypes.c_uint32
+U64 = ctypes.c_uint64
+I = ctypes.c_int
+F = ctypes.c_float
+
+
+def build(ref: bool = True):
+    """Builds the restatement (always) and the reference harness when the reference
+    tree is present. Returns the list of targets built."""
+    targets = ["restate"]
+    if ref and Path(os.environ.get("REF_DIR", "/root/reference")).is_dir():
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+    return targets
+
+
+def _np(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class RefOracle:
+    """The reference's own BVH / triangle / sphere / kd-tree code."""
+
+    def __init__(self, path: Path = REF_SO):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+        L = ctypes.CDLL(str(path))
+        L.refo_bvh_build.restype = P
+        L.refo_bvh_build.argtypes = [P, U32, P, U32, P]
+        L.refo_bvh_free.argtypes = [P]
+        L.refo_bvh_root.argtypes = [P]
+        L.refo_bvh_root.restype = U32
+        L.refo_bvh_export.argtypes = [P] * 7
+        L.refo_bvh_intersect.argtypes = [P, P, P, P, U64, I, P, I]
+        L.refo_bvh_brute.argtypes = [P, P, P, P, U64, I, P, I]
+        L.refo_triangle_intersects.argtypes = [P, U32, P, P, F, P, I]
+        L.refo_triangle_intersects.restype = I
+        L.refo_triangle_hit_t.argtypes = [P, P, P, P, U64, P, I]
+        L.refo_spheres_build.restype = P
+        L.refo_spheres_build.argtypes = [P, P, P, U32]
+        L.refo_spheres_free.argtypes = [P]
+        L.refo_sphere_matrices.argtypes = [P, U32, P, P]
+        L.refo_spheres_intersect.argtypes = [P, P, P, U64, I, P, P, I]
+        L.refo_kdtree_build.restype = P
+        L.refo_kdtree_build.argtypes = [P, P, U64]
+        L.refo_kdtree_free.argtypes = [P]
+        L.refo_kdtree_knn.argtypes = [P, P, P, U64, U32, F, P, P, I]
+        self.L = L
+
+    # ---- BVH
+    def bvh(self, verts, idx, transparent=None):
+        v = _np(verts, np.float32).reshape(-1, 3)
+        i = _np(idx, np.uint32).reshape(-1, 3)
+        tr = None if transparent is None else _np(transparent, np.uint8)
+        h = self.L.refo_bvh_build(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0],
+                                  None if tr is None else tr.ctypes.data)
+        if not h:
+            raise ValueError("reference BVH needs at least 2 triangles")
+        return RefBvh(self, h, i.shape[0])
+
+
+class RefBvh:
+    def __init__(self, o: RefOracle, h, ntri):
+        self.o, self.h, self.ntri = o, h, ntri
+
+    def __del__(self):
+        try:
+            self.o.L.refo_bvh_free(self.h)
+        except Exception:
+            pass
+
+    def export(self):
+        nn = 2 * self.ntri - 1
+        boxes = np.zeros((nn, 6), np.float32)
+        oid = np.zeros(nn, np.int32)
+        left = np.zeros(nn, np.uint32)
+        right = np.zeros(nn, np.uint32)
+        codes = np.zeros(self.ntri, np.uint32)
+        srt = np.zeros(self.ntri, np.uint32)
+        self.o.L.refo_bvh_export(self.h, boxes.ctypes.data, oid.ctypes.data, left.ctypes.data, right.ctypes.data,
+                                 codes.ctypes.data, srt.ctypes.data)
+        return dict(boxes=boxes, objectIds=oid, left=left, right=right, codes=codes, sorted=srt,
+                    root=self.o.L.refo_bvh_root(self.h))
+
+    def intersect(self, o, d, tmax=None, shadow=False, threads=8, brute=False):
+        o = _np(o, np.float32)
+        d = _np(d, np.float32)
+        tm = None if tmax is None else _np(tmax, np.float32)
+        out = np.zeros(o.shape[0], np.int32)
+        fn = self.o.L.refo_bvh_brute if brute else self.o.L.refo_bvh_intersect
+        fn(self.h, o.ctypes.data, d.ctypes.data, None if tm is None else tm.ctypes.data, o.shape[0], int(shadow),
+           out.ctypes.data, threads)
+        return out
+
+    def hit_t(self, ids, o, d, threads=8):
+        ids = _np(ids, np.int32)
+        o = _np(o, np.float32)
+        d = _np(d, np.float32)
+        t = np.zeros(o.shape[0], np.float32)
+        self.o.L.refo_triangle_hit_t(self.h, ids.ctypes.data, o.ctypes.data, d.ctypes.data, o.shape[0],
+                                     t.ctypes.data, threads)
+        return t
+
+    def triangle_intersects(self, tri, o, d, tmax=np.inf, hit_offset=np.inf, shadow=False):
+        o = _np(o, np.float32)
+        d = _np(d, np.float32)
+        h = np.array([hit_offset], np.float32)
+        r = self.o.L.refo_triangle_intersects(self.h, tri, o.ctypes.data, d.ctypes.data, float(tmax), h.ctypes.data,
+                                              int(shadow))
+        return bool(r), float(h[0])
+
+
+class RefSpheres:
+    def __init__(self, o: RefOracle, centers, radii, glass):
+        self.o = o
+        c = _np(centers, np.float32).reshape(-1, 3)
+        r = _np(radii, np.float32)
+        g = _np(glass, np.uint8)
+        self.n = c.shape[0]
+        self.h = o.L.refo_spheres_build(c.ctypes.data, r.ctypes.data, g.ctypes.data, self.n)
+
+    def __del__(self):
+        try:
+            self.o.L.refo_spheres_free(self.h)
+        except Exception:
+            pass
+
+    def matrices(self, i):
+        o2w = np.zeros(16, np.float32)
+        w2o = np.zeros(16, np.float32)
+        self.o.L.refo_sphere_matrices(self.h, i, o2w.ctypes.data, w2o.ctypes.data)
+        return o2w.reshape(4, 4), w2o.reshape(4, 4)
+
+    def intersect(self, o, d, shadow=False, threads=8):
+        o = _np(o, np.float32)
+        d = _np(d, np.float32)
+        ids = np.zeros(o.shape[0], np.int32)
+        t = np.zeros(o.shape[0], np.float32)
+        self.o.L.refo_spheres_intersect(self.h, o.ctypes.data, d.ctypes.data, o.shape[0], int(shadow), ids.ctypes.data,
+                                        t.ctypes.data, threads)
+        return ids, t
+
+
+class RefKdTree:
+    def __init__(self, o: RefOracle, pos, shape_ids=None):
+        self.o = o
+        p = _np(pos, np.float32).reshape(-1, 3)
+        s = None if shape_ids is None else _np(shape_ids, np.int32)
+        self.h = o.L.refo_kdtree_build(p.ctypes.data, None if s is None else s.ctypes.data, p.shape[0])
+
+    def __del__(self):
+        try:
+            self.o.L.refo_kdtree_free(self.h)
+        except Exception:
+            pass
+
+    def knn(self, q, k, radius, qshape=None, threads=8):
+        q = _np(q, np.float32).reshape(-1, 3)
+        qs = None if qshape is None else _np(qshape, np.int32)
+        idx = np.zeros((q.shape[0], k), np.int32)
+        cnt = np.zeros(q.shape[0], np.uint32)
+        self.o.L.refo_kdtree_knn(self.h, q.ctypes.data, None if qs is None else qs.ctypes.data, q.shape[0], k,
+                                 float(radius), idx.ctypes.data, cnt.ctypes.data, threads)
+        return idx, cnt
+
+
+class Restated:
+    """The C restatement (oracle/rt_oracle.c)."""
+
+    def __init__(self, path: Path = RESTATE_SO):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle restate)")
+        L = ctypes.CDLL(str(path))
+        L.rto_bvh_build.argtypes = [P, U32, P, U32, P, ctypes.POINTER(P)]
+        L.rto_bvh_build.restype = I
+        L.rto_bvh_free.argtypes = [P]
+        L.rto_bvh_export.argtypes = [P, P, P, P]
+        L.rto_bvh_tie_rank.argtypes = [P, P]
+        L.rto_trace_ref_order.argtypes = [P, P, P, P, U64, I, P, P, I]
+        L.rto_triangle_intersects.argtypes = [P, U32, P, P, F, P, I]
+        L.rto_triangle_intersects.restype = I
+        L.rto_sphere_intersects.argtypes = [P, F, P, P, F, P]
+        L.rto_sphere_intersects.restype = I
+        L.rto_knn_brute.argtypes = [P, P, U64, P, P, U64, U32, F, P, P, P, I]
+        self.L = L
+
+    def bvh(self, verts, idx, transparent=None):
+        v = _np(verts, np.float32).reshape(-1, 3)
+        i = _np(idx, np.uint32).reshape(-1, 3)
+        tr = None if transparent is None else _np(transparent, np.uint8)
+        h = P()
+        if self.L.rto_bvh_build(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0],
+                                None if tr is None else tr.ctypes.data, ctypes.byref(h)) != 0:
+            raise ValueError("rto_bvh_build failed")
+        return RestatedBvh(self, h, i.shape[0])
+
+    def sphere_intersects(self, w2o, radius, o, d, tmax=np.inf, hit_offset=np.inf):
+        m = _np(w2o, np.float32).reshape(16)
+        o = _np(o, np.float32)
+        d = _np(d, np.float32)
+        h = np.array([hit_offset], np.float32)
+        r = self.L.rto_sphere_intersects(m.ctypes.data, float(radius), o.ctypes.data, d.ctypes.data, float(tmax),
+                                         h.ctypes.data)
+        return bool(r), float(h[0])
+
+    def knn(self, pos, shape, q, qshape, k, radius, threads=8):
+        p = _np(pos, np.float32).reshape(-1, 3)
+        s = _np(shape, np.int32)
+        q = _np(q, np.float32).reshape(-1, 3)
+        qs = None if qshape is None else _np(qshape, np.int32)
+        idx = np.zeros((q.shape[0], k), np.int32)
+        dist = np.zeros((q.shape[0], k), np.float32)
+        cnt = np.zeros(q.shape[0], np.uint32)
+        self.L.rto_knn_brute(p.ctypes.data, s.ctypes.data, p.shape[0], q.ctypes.data,
+                             None if qs is None else qs.ctypes.data, q.shape[0], k, float(radius), idx.ctypes.data,
+                             dist.ctypes.data, cnt.ctypes.data, threads)
+        return idx, dist, cnt
+
+
+class RestatedBvh:
+    def __init__(self, o: Restated, h, ntri):
+        self.o, self.h, self.ntri = o, h, ntri
+
+    def __del__(self):
+        try:
+            self.o.L.rto_bvh_free(self.h)
+        except Exception:
+            pass
+
+    def export(self):
+        boxes = np.zeros((2 * self.ntri - 1, 6), np.float32)
+        codes = np.zeros(self.ntri, np.uint32)
+        srt = np.zeros(self.ntri, np.uint32)
+        self.o.L.rto_bvh_export(self.h, boxes.ctypes.data, codes.ctypes.data, srt.ctypes.data)
+        return dict(boxes=boxes, codes=codes, sorted=srt)
+
+    def tie_rank(self):
+        r = np.zeros(self.ntri, np.uint32)
+        self.o.L.rto_bvh_tie_rank(self.h, r.ctypes.data)
+        return r
+
+    def intersect(self, o, d, tmax=None, shadow=False, threads=8):
+        o = _np(o, np.float32)
+        d = _np(d, np.float32)
+        tm = None if tmax is None else _np(tmax, np.float32)
+        out = np.zeros(o.shape[0], np.int32)
+        t = np.zeros(o.shape[0], np.float32)
+        self.o.L.rto_trace_ref_order(self.h, o.ctypes.data, d.ctypes.data, None if tm is None else tm.ctypes.data,
+                                     o.shape[0], int(shadow), out.ctypes.data, t.ctypes.data, threads)
+        return out, t
+
+    def triangle_intersects(self, tri, o, d, tmax=np.inf, hit_offset=np.inf, shadow=False):
+        o = _np(o, np.float32)
+        d = _np(d, np.float32)
+        h = np.array([hit_offset], np.float32)
+        r = self.o.L.rto_triangle_intersects(self.h, tri, o.ctypes.data, d.ctypes.data, float(tmax), h.ctypes.data,
+                                             int(shadow))
+        return bool(r), float(h[0])

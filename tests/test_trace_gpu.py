@@ -1,0 +1,210 @@
+"""Closest-hit parity of the CUDA path (through the C ABI) with the reference's own
+traversal: bit-exact triangle ids and hit distances."""
+import hashlib
+import importlib
+import json
+
+import numpy as np
+import pytest
+
+import cases
+from conftest import GOLDEN
+
+S = importlib.import_module("2023_render_engine_b200.scenes")
+N = importlib.import_module("2023_render_engine_b200._native")
+
+pytestmark = pytest.mark.gpu
+
+
+def _unpack(z, key):
+    return {k.split("__", 1)[1]: z[k] for k in z.files if k.startswith(key + "__")}
+
+
+def make_scene(core, ctx, v, f, transparent=None, spheres=()):
+    sc = core.Scene(ctx)
+    if f.shape[0]:
+        if transparent is None:
+            sc.add_mesh(v, f)
+        else:  # one mesh per triangle run with equal transparency, keeping global order
+            tr = np.asarray(transparent).astype(bool)
+            start = 0
+            while start < len(tr):
+                end = start
+                while end < len(tr) and tr[end] == tr[start]:
+                    end += 1
+                sc.add_mesh(v, f[start:end], transparent=bool(tr[start]))
+                start = end
+    for s in spheres:
+        sc.add_sphere(s["o2w"], s["w2o"], s["radius"], transparent=s.get("glass", False))
+    sc.commit()
+    return sc
+
+
+def trace_gpu(sc, o, d, tmax=None, flags=0):
+    import torch
+
+    rays = core_make_rays(o, d, tmax)
+    rd = torch.from_numpy(rays.view(np.float32).reshape(-1)).cuda()
+    hd = torch.empty(o.shape[0] * 4, dtype=torch.float32, device="cuda")
+    sc.trace_closest(rd, hd, o.shape[0], flags)
+    torch.cuda.synchronize()
+    h = hd.cpu().numpy().view(N.HIT_DTYPE)
+    return h["prim"].copy(), h["t"].copy(), h
+
+
+def core_make_rays(o, d, tmax=None):
+    core = importlib.import_module("2023_render_engine_b200.core")
+    return core.make_rays(o, d, tmax)
+
+
+@pytest.mark.parametrize("key", ["soup1000", "soup20000", "grids"])
+def test_closest_hit_matches_golden(core, gpu_ctx, key):
+    g = _unpack(np.load(GOLDEN / "trace_small.npz"), key)
+    sc = make_scene(core, gpu_ctx, g["v"], g["f"])
+    ids, t, _ = trace_gpu(sc, g["o"], g["d"])
+    assert np.array_equal(ids, g["ids"])
+    hit = ids >= 0
+    assert np.array_equal(t[hit], g["t"][hit])
+    assert np.all(np.isinf(t[~hit]))
+
+
+@pytest.mark.parametrize("nt,seed", [(2, 1), (3, 2), (4, 6), (17, 3), (513, 4), (5000, 5), (60000, 6)])
+def test_closest_hit_vs_restated(core, gpu_ctx, restated, nt, seed):
+    v, f = cases.soup(nt, seed, size=0.2)
+    o, d = S.random_rays(20000, seed=seed + 100, lo=-1.3, hi=1.3)
+    sc = make_scene(core, gpu_ctx, v, f)
+    ob = restated.bvh(v, f)
+    for shadow in (False, True):
+        ref, tref = ob.intersect(o, d, shadow=shadow)
+        ids, t, _ = trace_gpu(sc, o, d, flags=N.RT_TRACE_SHADOW if shadow else 0)
+        assert np.array_equal(ids, ref)
+        hit = ref >= 0
+        assert np.array_equal(t[hit], tref[hit])
+
+
+def test_closest_hit_edge_cases(core, gpu_ctx, restated):
+    """Exact ties on shared edges/vertices, axis-aligned rays, rays starting closer to a
+    surface than its error bound, transparency for shadow rays, finite tmax."""
+    v, f = cases.stacked_grids()
+    tr = np.zeros(f.shape[0], np.uint8)
+    tr[-2:] = 1
+    o, d = cases.edge_rays(9)
+    sc = make_scene(core, gpu_ctx, v, f, transparent=tr)
+    ob = restated.bvh(v, f, tr)
+    for shadow in (False, True):
+        ref, tref = ob.intersect(o, d, shadow=shadow)
+        ids, t, _ = trace_gpu(sc, o, d, flags=N.RT_TRACE_SHADOW if shadow else 0)
+        assert np.array_equal(ids, ref)
+        assert np.array_equal(t[ref >= 0], tref[ref >= 0])
+    tm = np.random.default_rng(2).uniform(0.1, 3.0, o.shape[0]).astype(np.float32)
+    ref, tref = ob.intersect(o, d, tmax=tm)
+    ids, t, _ = trace_gpu(sc, o, d, tmax=tm)
+    assert np.array_equal(ids, ref)
+    st = sc.trace_stats()
+    assert st["rays"] == o.shape[0]
+
+
+def test_fast_mode_agrees_on_generic_rays(core, gpu_ctx, restated):
+    v, f = cases.soup(20000, 12)
+    o, d = S.random_rays(50000, seed=3, lo=-1.2, hi=1.2)
+    sc = make_scene(core, gpu_ctx, v, f)
+    ref, _ = restated.bvh(v, f).intersect(o, d)
+    ids, _, _ = trace_gpu(sc, o, d, flags=N.RT_TRACE_FAST)
+    assert (ids == ref).mean() > 0.999
+
+
+def test_spheres_match_reference(core, gpu_ctx):
+    """Sphere::intersects arithmetic with the reference's own matrices (golden)."""
+    g = np.load(GOLDEN / "spheres_cornell.npz")
+    sph = [{"o2w": g[f"o2w{i}"], "w2o": g[f"w2o{i}"], "radius": float(g["radii"][i]), "glass": i == 1}
+           for i in range(len(g["radii"]))]
+    sc = make_scene(core, gpu_ctx, np.zeros((0, 3), np.float32), np.zeros((0, 3), np.uint32), spheres=sph)
+    ids, t, _ = trace_gpu(sc, g["o"], g["d"])
+    exp = np.where(g["ids"] >= 0, N.RT_PRIM_SHAPE | g["ids"], -1)
+    assert np.array_equal(ids, exp)
+    assert np.array_equal(t[ids >= 0], g["t"][g["ids"] >= 0])
+    ids, t, _ = trace_gpu(sc, g["o"], g["d"], flags=N.RT_TRACE_SHADOW)
+    exp = np.where(g["ids_shadow"] >= 0, N.RT_PRIM_SHAPE | g["ids_shadow"], -1)
+    assert np.array_equal(ids, exp)
+
+
+def test_cornell_triangles_and_spheres(core, gpu_ctx, restated):
+    """Scene::intersects order: the BVH triangle first, then each shape lowers the offset."""
+    g = np.load(GOLDEN / "spheres_cornell.npz")
+    v, f, _, sph = cases.cornell_soup()
+    spheres = [{"o2w": g[f"o2w{i}"], "w2o": g[f"w2o{i}"], "radius": float(g["radii"][i])} for i in range(2)]
+    sc = make_scene(core, gpu_ctx, v, f, spheres=spheres)
+    o, d = S.random_rays(20000, seed=44, lo=-0.99, hi=0.99)
+    tri, ttri = restated.bvh(v, f).intersect(o, d)
+    exp, texp = tri.copy(), np.where(tri >= 0, ttri, np.inf).astype(np.float32)
+    for r in range(o.shape[0]):
+        for i in range(2):
+            hit, tt = restated.sphere_intersects(g[f"w2o{i}"], g["radii"][i], o[r], d[r], hit_offset=texp[r])
+            if hit:
+                exp[r], texp[r] = N.RT_PRIM_SHAPE | i, tt
+    ids, t, _ = trace_gpu(sc, o, d)
+    assert np.array_equal(ids, exp)
+    assert np.array_equal(t[ids >= 0], texp[exp >= 0])
+
+
+def test_empty_and_degenerate_inputs(core, gpu_ctx):
+    import torch
+
+    sc = make_scene(core, gpu_ctx, np.zeros((0, 3), np.float32), np.zeros((0, 3), np.uint32))
+    o, d = S.random_rays(100, seed=1)
+    ids, t, _ = trace_gpu(sc, o, d)
+    assert np.all(ids == -1) and np.all(np.isinf(t))
+    # zero rays
+    rd = torch.empty(8, dtype=torch.float32, device="cuda")
+    hd = torch.empty(4, dtype=torch.float32, device="cuda")
+    sc.trace_closest(rd, hd, 0)
+    # a single triangle
+    v = np.array([[-1, -1, 0], [1, -1, 0], [0, 1, 0]], np.float32)
+    sc1 = make_scene(core, gpu_ctx, v, np.array([[0, 1, 2]], np.uint32))
+    o = np.array([[0, 0, 1], [5, 5, 1]], np.float32)
+    d = np.array([[0, 0, -1], [0, 0, -1]], np.float32)
+    ids, t, _ = trace_gpu(sc1, o, d)
+    assert ids.tolist() == [0, -1] and t[0] == 1.0
+
+
+def test_invalid_arguments_raise(core, gpu_ctx):
+    sc = core.Scene(gpu_ctx)
+    with pytest.raises(N.RtError):
+        sc.add_mesh(np.zeros((3, 3), np.float32), np.array([[0, 1, 5]], np.uint32))
+    import torch
+
+    rd = torch.empty(8, dtype=torch.float32, device="cuda")
+    hd = torch.empty(4, dtype=torch.float32, device="cuda")
+    with pytest.raises(N.RtError):  # trace before commit
+        sc.trace_closest(rd, hd, 1)
+
+
+def test_host_buffer_entry_point(core, gpu_ctx, restated):
+    v, f = cases.soup(3000, 8)
+    o, d = S.random_rays(10000, seed=9, lo=-1.2, hi=1.2)
+    sc = make_scene(core, gpu_ctx, v, f)
+    h = sc.trace_closest_host(core_make_rays(o, d))
+    ref, _ = restated.bvh(v, f).intersect(o, d)
+    assert np.array_equal(h["prim"], ref)
+
+
+def test_config1_full_ray_set_hash(core, gpu_ctx):
+    """All 2^24 rays of the BVH-stress ray set against the reference (1.31M-triangle
+    displaced icosphere in the Cornell box): the hash of every hit id and distance equals
+    the hash of the reference traversal's output."""
+    import torch
+
+    info = json.loads((GOLDEN / "config1_closest_hit.json").read_text())
+    sc_data = S.stress_scene()
+    v, f, _ = S.flatten(sc_data)
+    assert hashlib.sha256(v.tobytes()).hexdigest() == info["vertices_sha256"]
+    assert hashlib.sha256(f.tobytes()).hexdigest() == info["indices_sha256"]
+    o, d = S.random_rays(info["rays"], seed=info["ray_seed"])
+    assert hashlib.sha256(o.tobytes()).hexdigest() == info["origins_sha256"]
+    sc = make_scene(core, gpu_ctx, v, f)
+    ids, t, _ = trace_gpu(sc, o, d)
+    assert ids[info["sample_index"]].tolist() == info["sample_ids"]
+    assert hashlib.sha256(ids.astype(np.int32).tobytes()).hexdigest() == info["ids_sha256"]
+    tt = np.where(ids >= 0, t, -1.0).astype(np.float32)
+    assert hashlib.sha256(tt.tobytes()).hexdigest() == info["t_sha256"]
+    del torch
