@@ -65,8 +65,9 @@ void build_ref_tree(const float *tri9, uint32_t n, RefTreeHost &out)
     out.sorted.assign(n, 0);
     out.pos.assign(n, 0);
     out.rank.assign(n, 0);
-    out.boxes.assign(6 * (2 * (size_t)n - 1), 0.f);
+    out.boxes.clear();
     if (n == 0) return;
+    out.boxes.assign(6 * (2 * (size_t)n - 1), 0.f);
     float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     for (uint64_t i = 0; i < 9 * (uint64_t)n; i++) {
         int c = (int)(i % 3);
