@@ -11,7 +11,7 @@ namespace rtb {
 // errorBound(n) = (n*eps)/(1-n*eps), eps = FLT_EPSILON*0.5, evaluated in double and
 // returned as float (cuda_libraries/math.cu:117-120, types.h:23).
 constexpr double kMachEps = 5.9604644775390625e-08;  // 2^-24
-constexpr float error_bound(int n) { return (float)((n * kMachEps) / (1 - n * kMachEps)); }
+__host__ __device__ constexpr float error_bound(int n) { return (float)((n * kMachEps) / (1 - n * kMachEps)); }
 
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }

@@ -90,6 +90,9 @@ __device__ __forceinline__ void sort8(uint32_t k[8])
 }
 
 // Traverses the BVH8; returns false if the stack would overflow (result then unreliable).
+// The eight child boxes are tested in an unrolled block; the triangles of the hit leaves
+// are then tested in a rolled loop so the (long) exact triangle test exists once in the
+// instruction stream.
 __device__ __forceinline__ bool traverse_bvh8(const SceneView &v, const WatertightRay &w, float dx, float dy, float dz,
                                               bool shadow, bool anyhit, Best &best)
 {
@@ -99,17 +102,13 @@ __device__ __forceinline__ bool traverse_bvh8(const SceneView &v, const Watertig
     float st_t[kStack];
     int sp = 0;
     uint32_t cur = 0;
-    bool ok = true;
     uint32_t steps = 0;
     const uint32_t cap = v.nnodes + 1;
+#pragma unroll 1
     for (;;) {
-        if (++steps > cap) {
-            ok = false;
-            break;
-        }
+        if (++steps > cap) return false;
         const uint4 *np = reinterpret_cast<const uint4 *>(v.nodes + cur);
-        uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
-        const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+        const uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
         const float sx = __uint_as_float((n0.w & 0xFFu) << 23);
         const float sy = __uint_as_float(((n0.w >> 8) & 0xFFu) << 23);
         const float sz = __uint_as_float(((n0.w >> 16) & 0xFFu) << 23);
@@ -117,65 +116,67 @@ __device__ __forceinline__ bool traverse_bvh8(const SceneView &v, const Watertig
         const uint32_t child_base = n1.x, tri_base = n1.y;
         const uint32_t meta_lo = n1.z, meta_hi = n1.w;
         // per-axis affine map t = q * (s * inv) + (p * inv - o * inv)
-        const float ax = sx * ix, bx = fmaf(px, ix, oix);
-        const float ay = sy * iy, by = fmaf(py, iy, oiy);
-        const float az = sz * iz, bz = fmaf(pz, iz, oiz);
+        const float ax = sx * ix, bx = fmaf(__uint_as_float(n0.x), ix, oix);
+        const float ay = sy * iy, by = fmaf(__uint_as_float(n0.y), iy, oiy);
+        const float az = sz * iz, bz = fmaf(__uint_as_float(n0.z), iz, oiz);
         const float tlimit = fminf(best.t, w.tmax);
         uint32_t keys[8];
-        uint32_t hit_interior = 0;
+        uint32_t nint = 0, leafmask = 0;
 #pragma unroll
         for (int k = 0; k < 8; k++) {
+            const int b = k & 3;
+            const uint32_t meta = byte_of(k < 4 ? meta_lo : meta_hi, b);
+            const float qlx = (float)byte_of(k < 4 ? n2.x : n2.y, b);
+            const float qly = (float)byte_of(k < 4 ? n2.z : n2.w, b);
+            const float qlz = (float)byte_of(k < 4 ? n3.x : n3.y, b);
+            const float qhx = (float)byte_of(k < 4 ? n3.z : n3.w, b);
+            const float qhy = (float)byte_of(k < 4 ? n4.x : n4.y, b);
+            const float qhz = (float)byte_of(k < 4 ? n4.z : n4.w, b);
+            const float t1x = fmaf(qlx, ax, bx), t2x = fmaf(qhx, ax, bx);
+            const float t1y = fmaf(qly, ay, by), t2y = fmaf(qhy, ay, by);
+            const float t1z = fmaf(qlz, az, bz), t2z = fmaf(qhz, az, bz);
+            const float tn = fmaxf(fmaxf(fminf(t1x, t2x), fminf(t1y, t2y)), fmaxf(fminf(t1z, t2z), 0.0f));
+            const float tf = fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fminf(fmaxf(t1z, t2z), tlimit));
+            const bool hit = (meta != 0xFFu) && (tn <= tf);
+            const bool interior = (imask >> k) & 1u;
+            keys[k] = (hit && interior) ? ((__float_as_uint(tn) & ~7u) | (uint32_t)k) : 0xFFFFFFFFu;
+            nint += (hit && interior) ? 1u : 0u;
+            leafmask |= (hit && !interior) ? (1u << k) : 0u;
+        }
+        // leaves: one copy of the exact triangle test
+#pragma unroll 1
+        while (leafmask) {
+            const int k = __ffs(leafmask) - 1;
+            leafmask &= leafmask - 1;
             const uint32_t meta = byte_of(k < 4 ? meta_lo : meta_hi, k & 3);
-            const uint32_t wlo = k < 4 ? 0 : 1;
-            const float qlx = (float)byte_of(wlo ? n2.y : n2.x, k & 3);
-            const float qly = (float)byte_of(wlo ? n2.w : n2.z, k & 3);
-            const float qlz = (float)byte_of(wlo ? n3.y : n3.x, k & 3);
-            const float qhx = (float)byte_of(wlo ? n3.w : n3.z, k & 3);
-            const float qhy = (float)byte_of(wlo ? n4.y : n4.x, k & 3);
-            const float qhz = (float)byte_of(wlo ? n4.w : n4.z, k & 3);
-            float t1x = fmaf(qlx, ax, bx), t2x = fmaf(qhx, ax, bx);
-            float t1y = fmaf(qly, ay, by), t2y = fmaf(qhy, ay, by);
-            float t1z = fmaf(qlz, az, bz), t2z = fmaf(qhz, az, bz);
-            float tn = fmaxf(fmaxf(fminf(t1x, t2x), fminf(t1y, t2y)), fmaxf(fminf(t1z, t2z), 0.0f));
-            float tf = fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fminf(fmaxf(t1z, t2z), tlimit));
-            bool hit = (meta != 0xFFu) && (tn <= tf);
-            keys[k] = 0xFFFFFFFFu;
-            if (hit && ((imask >> k) & 1u)) {
-                keys[k] = (__float_as_uint(tn) & ~7u) | (uint32_t)k;
-                hit_interior++;
-            }
-            if (hit && !((imask >> k) & 1u)) {
-                const uint32_t cnt = (meta >> 5) + 1, off = meta & 31u;
-                for (uint32_t j = 0; j < cnt; j++) {
-                    test_triangle(w, v.tris, tri_base + off + j, shadow, best);
-                }
-                if (anyhit && best.prim >= 0) return true;
-            }
+            const uint32_t first = tri_base + (meta & 31u), cnt = (meta >> 5) + 1;
+#pragma unroll 1
+            for (uint32_t j = 0; j < cnt; j++) test_triangle(w, v.tris, first + j, shadow, best);
+            if (anyhit && best.prim >= 0) return true;
         }
         uint32_t next = 0xFFFFFFFFu;
-        if (hit_interior) {
+        const float tl = fminf(best.t, w.tmax);
+        if (nint) {
             sort8(keys);
-            const float tl = fminf(best.t, w.tmax);
-            // push far to near, keep the nearest as the next node
-            for (int j = (int)hit_interior - 1; j >= 1; j--) {
-                uint32_t slot = keys[j] & 7u;
-                float tn = __uint_as_float(keys[j] & ~7u);
-                if (tn > tl) continue;
-                uint32_t meta = byte_of(slot < 4 ? meta_lo : meta_hi, slot & 3);
-                if (sp >= kStack) {
-                    ok = false;
-                    break;
+            // push far to near (register-resident keys: unrolled with a predicate)
+#pragma unroll
+            for (int j = 7; j >= 1; j--) {
+                if (j < (int)nint) {
+                    const uint32_t slot = keys[j] & 7u;
+                    const float tn = __uint_as_float(keys[j] & ~7u);
+                    if (tn <= tl) {
+                        if (sp >= kStack) return false;
+                        st_node[sp] = child_base + byte_of(slot < 4 ? meta_lo : meta_hi, slot & 3);
+                        st_t[sp] = tn;
+                        sp++;
+                    }
                 }
-                st_node[sp] = child_base + meta;
-                st_t[sp] = tn;
-                sp++;
             }
-            if (!ok) break;
-            uint32_t slot = keys[0] & 7u;
+            const uint32_t slot = keys[0] & 7u;
             if (__uint_as_float(keys[0] & ~7u) <= tl) next = child_base + byte_of(slot < 4 ? meta_lo : meta_hi, slot & 3);
         }
         if (next == 0xFFFFFFFFu) {
-            const float tl = fminf(best.t, w.tmax);
+#pragma unroll 1
             while (sp > 0) {
                 sp--;
                 if (st_t[sp] <= tl) {
@@ -184,10 +185,9 @@ __device__ __forceinline__ bool traverse_bvh8(const SceneView &v, const Watertig
                 }
             }
         }
-        if (next == 0xFFFFFFFFu) break;
+        if (next == 0xFFFFFFFFu) return true;
         cur = next;
     }
-    return ok;
 }
 
 __device__ __forceinline__ void shade_spheres(const SceneView &v, float ox, float oy, float oz, float dx, float dy,

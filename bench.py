@@ -275,7 +275,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1 << 20)
     ap.add_argument("--ref-sample", type=int, default=1 << 18)
+    ap.add_argument("--rays-log2", type=int, default=24, help="smaller ray sets for profiler captures")
     args = ap.parse_args()
+    global NRAYS
+    NRAYS = 1 << args.rays_log2
     if args.impl == "reference":
         run_reference(args)
     else:
