@@ -39,6 +39,36 @@ class SceneStats(ctypes.Structure):
                 ("build_ms", ctypes.c_double)]
 
 
+class Material(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("color", ctypes.c_float * 3),
+                ("intensity", ctypes.c_float), ("eta", ctypes.c_float * 3), ("k", ctypes.c_float * 3),
+                ("roughness", ctypes.c_float * 2), ("ior", ctypes.c_float), ("pad", ctypes.c_float * 3)]
+
+
+class Camera(ctypes.Structure):
+    _fields_ = [("camera_to_world", ctypes.c_float * 16), ("raster_to_camera", ctypes.c_float * 16),
+                ("lens_radius", ctypes.c_float), ("focal_distance", ctypes.c_float),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
+
+
+class RenderOpts(ctypes.Structure):
+    _fields_ = [("spp", ctypes.c_uint32), ("sample_offset", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
+                ("rr_depth", ctypes.c_uint32), ("seed", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("max_paths", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("camera_rays", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64),
+                ("shadow_rays", ctypes.c_uint64), ("waves", ctypes.c_uint64), ("ms", ctypes.c_double)]
+
+
+RT_MAT_LAMBERTIAN, RT_MAT_TROWBRIDGE, RT_MAT_DIELECTRIC, RT_MAT_LIGHT, RT_MAT_MIRROR, RT_MAT_PLAIN = range(6)
+RT_MATF_TRANSPARENT = 0x1
+RT_RENDER_NEE_AREA = 0x1
+RT_RENDER_COMPAT = 0x2
+RT_RENDER_EXACT_TRACE = 0x4
+
+
 class TraceStats(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_uint64), ("exact_fallback_rays", ctypes.c_uint64)]
 
@@ -68,6 +98,10 @@ SIGNATURES = {
     "rt_trace_closest_host": [_P, _P, _U64, _P, _U32],
     "rt_trace_any": [_P, _P, _U64, _P, _U32],
     "rt_trace_stats_get": [_P, ctypes.POINTER(TraceStats)],
+    "rt_scene_set_materials": [_P, _P, _U32],
+    "rt_scene_set_triangle_materials": [_P, _U32, _U32, _P],
+    "rt_scene_add_point_light": [_P, _P, _P, _F32],
+    "rt_render": [_P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), _P, _P, _P, ctypes.POINTER(RenderStats)],
 }
 
 

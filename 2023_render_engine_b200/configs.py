@@ -1,0 +1,71 @@
+"""The benchmark configurations as ready-to-render scenes (geometry from scenes.py,
+materials and cameras per the configuration descriptions).
+
+* config0: Cornell box — walls 0.8 / red / green Lambertian, 0.5x0.5 ceiling light of
+  emission 15, Lambertian sphere (0.8) and glass sphere (IOR 1.5), pinhole camera at
+  (0,0,3.5) looking down -z with a 40 degree vertical field of view; 256x256, 16 spp,
+  max depth 8, Russian roulette after depth 3.
+* config1: BVH stress — the 1.31M-triangle displaced icosphere (GGX, F0 = 0.04 i.e.
+  eta = 1.5, k = 0, roughness uniform in [0.05, 0.5] per block of 64 triangles) in the
+  Cornell box; 1920x1080, 64 spp, max depth 12, NEE on the area light.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native as N
+from . import core, scenes
+
+CORNELL_MATERIALS = {
+    scenes.MAT_WHITE: dict(type_=N.RT_MAT_LAMBERTIAN, color=(0.8, 0.8, 0.8)),
+    scenes.MAT_RED: dict(type_=N.RT_MAT_LAMBERTIAN, color=(0.8, 0.1, 0.1)),
+    scenes.MAT_GREEN: dict(type_=N.RT_MAT_LAMBERTIAN, color=(0.1, 0.8, 0.1)),
+    scenes.MAT_LIGHT: dict(type_=N.RT_MAT_LIGHT, color=(1.0, 1.0, 1.0), intensity=15.0),
+    scenes.MAT_DIFFUSE_SPHERE: dict(type_=N.RT_MAT_LAMBERTIAN, color=(0.8, 0.8, 0.8)),
+    scenes.MAT_GLASS: dict(type_=N.RT_MAT_DIELECTRIC, color=(1.0, 1.0, 1.0), ior=1.5, transparent=True),
+    scenes.MAT_GGX: dict(type_=N.RT_MAT_TROWBRIDGE, color=(1.0, 1.0, 1.0), eta=(1.5, 1.5, 1.5), k=(0, 0, 0),
+                         roughness=(0.25, 0.25)),
+}
+
+
+def cornell_materials(extra=()):
+    mats = [core.material(**CORNELL_MATERIALS[i]) for i in range(len(CORNELL_MATERIALS))]
+    return mats + list(extra)
+
+
+def cornell_camera(width=256, height=256):
+    return core.look_at_camera((0, 0, 3.5), (0, 0, 0), (0, 1, 0), 40.0, width, height)
+
+
+def build_config0(ctx, width=256, height=256):
+    sc_data = scenes.cornell_box()
+    sc = core.Scene(ctx)
+    sc.set_materials(cornell_materials())
+    for i, (v, f, m) in enumerate(sc_data["meshes"]):
+        sc.add_mesh(v, f, material=m, shape_id=i)
+    for j, s in enumerate(sc_data["spheres"]):
+        o2w, w2o = scenes.sphere_matrices(s["center"], s["radius"])
+        sc.add_sphere(o2w, w2o, s["radius"], material=s["material"], shape_id=100 + j)
+    sc.commit()
+    return sc, cornell_camera(width, height), dict(spp=16, max_depth=8, rr_depth=3)
+
+
+def build_config1(ctx, width=1920, height=1080, subdiv=8):
+    sc_data = scenes.stress_scene(subdiv=subdiv)
+    rough = sc_data["roughness"]
+    nblocks = (rough.shape[0] + 63) // 64
+    block_r = rough[::64][:nblocks]
+    extra = [core.material(N.RT_MAT_TROWBRIDGE, color=(1, 1, 1), eta=(1.5, 1.5, 1.5), k=(0, 0, 0),
+                           roughness=(float(r), float(r))) for r in block_r]
+    base = len(CORNELL_MATERIALS)
+    sc = core.Scene(ctx)
+    sc.set_materials(cornell_materials(extra))
+    first = None
+    for i, (v, f, m) in enumerate(sc_data["meshes"]):
+        t0 = sc.add_mesh(v, f, material=m, shape_id=i)
+        if m == scenes.MAT_GGX:
+            first = t0
+            ids = base + (np.arange(f.shape[0]) // 64)
+            sc.set_triangle_materials(first, ids.astype(np.uint32))
+    sc.commit()
+    return sc, cornell_camera(width, height), dict(spp=64, max_depth=12, rr_depth=3)

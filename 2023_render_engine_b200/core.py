@@ -107,6 +107,40 @@ class Scene:
             n = rays_dev.numel() // 8
         N.check(N.lib().rt_trace_any(self.handle, rays_dev.data_ptr(), n, occluded_dev.data_ptr(), flags))
 
+    # ---- rendering ----
+    def set_materials(self, mats):
+        arr = (N.Material * len(mats))(*mats)
+        N.check(N.lib().rt_scene_set_materials(self.handle, ctypes.cast(arr, ctypes.c_void_p), len(mats)))
+
+    def set_triangle_materials(self, first: int, mat_ids):
+        m = np.ascontiguousarray(mat_ids, dtype=np.uint32)
+        N.check(N.lib().rt_scene_set_triangle_materials(self.handle, first, m.shape[0], m.ctypes.data))
+
+    def add_point_light(self, pos, rgb, intensity: float):
+        p = np.ascontiguousarray(pos, dtype=np.float32)
+        c = np.ascontiguousarray(rgb, dtype=np.float32)
+        N.check(N.lib().rt_scene_add_point_light(self.handle, p.ctypes.data, c.ctypes.data, float(intensity)))
+
+    def render(self, camera: "N.Camera", spp: int, max_depth: int, rr_depth: int = 3, seed: int = 0,
+               flags: int = 0, sample_offset: int = 0, film=None, fp64: bool = False, max_paths: int = 0):
+        """Adds spp samples per pixel into `film` (dict of torch tensors sum/count[/sum64]);
+        returns (film, stats)."""
+        import torch
+
+        w, h = camera.width, camera.height
+        if film is None:
+            film = {"sum": torch.zeros(h * w * 3, dtype=torch.float32, device="cuda"),
+                    "count": torch.zeros(h * w, dtype=torch.int32, device="cuda")}
+            if fp64:
+                film["sum64"] = torch.zeros(h * w * 3, dtype=torch.float64, device="cuda")
+        opts = N.RenderOpts(spp, sample_offset, max_depth, rr_depth, seed, flags, max_paths, 0)
+        st = N.RenderStats()
+        s64 = film.get("sum64")
+        N.check(N.lib().rt_render(self.handle, ctypes.byref(camera), ctypes.byref(opts), film["sum"].data_ptr(),
+                                  film["count"].data_ptr(), None if s64 is None else s64.data_ptr(),
+                                  ctypes.byref(st)))
+        return film, {f: getattr(st, f) for f, _ in N.RenderStats._fields_}
+
     def close(self):
         if self.handle:
             N.lib().rt_scene_destroy(self.handle)
@@ -127,3 +161,53 @@ def make_rays(o: np.ndarray, d: np.ndarray, tmax=None) -> np.ndarray:
     r["dx"], r["dy"], r["dz"] = d[:, 0], d[:, 1], d[:, 2]
     r["tmax"] = np.inf if tmax is None else tmax
     return r
+
+
+def material(type_, color=(0.8, 0.8, 0.8), intensity=0.0, eta=(1.5, 1.5, 1.5), k=(0.0, 0.0, 0.0),
+             roughness=(0.1, 0.1), ior=1.5, transparent=False) -> "N.Material":
+    m = N.Material()
+    m.type = type_
+    m.flags = N.RT_MATF_TRANSPARENT if transparent else 0
+    m.color[:] = [float(c) for c in color]
+    m.intensity = float(intensity)
+    m.eta[:] = [float(c) for c in eta]
+    m.k[:] = [float(c) for c in k]
+    m.roughness[:] = [float(c) for c in roughness]
+    m.ior = float(ior)
+    return m
+
+
+def look_at_camera(eye, target, up, vfov_deg: float, width: int, height: int, focal=0.8,
+                   lens_radius=0.0, focal_distance=1.0) -> "N.Camera":
+    """Pinhole camera in the reference's convention: camera space looks along +z, the image
+    plane at z = focal with half-height focal*tan(vfov/2) (an .obejota camera with
+    cts = (0,0,-focal), frameY = 2*focal*tan(vfov/2)); raster y grows downwards."""
+    eye = np.asarray(eye, np.float64)
+    f = np.asarray(target, np.float64) - eye
+    f /= np.linalg.norm(f)
+    r = np.cross(f, np.asarray(up, np.float64))
+    r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    c2w = np.eye(4)
+    c2w[:3, 0], c2w[:3, 1], c2w[:3, 2], c2w[:3, 3] = r, u, f, eye
+    half_h = focal * np.tan(np.radians(vfov_deg) / 2)
+    half_w = half_h * width / height
+    # raster (x, y) -> camera (x', y', focal): x' = (x/W - 0.5) * 2 half_w, y' = (0.5 - y/H) * 2 half_h
+    r2c = np.array([[2 * half_w / width, 0, 0, -half_w],
+                    [0, -2 * half_h / height, 0, half_h],
+                    [0, 0, 0, focal],
+                    [0, 0, 0, 1]], np.float64)
+    cam = N.Camera()
+    cam.camera_to_world[:] = [float(x) for x in c2w.reshape(-1)]
+    cam.raster_to_camera[:] = [float(x) for x in r2c.reshape(-1)]
+    cam.lens_radius = float(lens_radius)
+    cam.focal_distance = float(focal_distance)
+    cam.width, cam.height = int(width), int(height)
+    return cam
+
+
+def film_mean(film) -> np.ndarray:
+    """Per-pixel estimate sum / count as an (H*W, 3) float64 array."""
+    s = (film["sum64"] if "sum64" in film else film["sum"]).double().cpu().numpy().reshape(-1, 3)
+    c = film["count"].cpu().numpy().astype(np.float64)
+    return s / np.maximum(c, 1)[:, None]

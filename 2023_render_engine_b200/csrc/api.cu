@@ -181,8 +181,10 @@ int rt_scene_destroy(rt_scene *s)
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
     for (DevBuf *b : {&s->d_nodes, &s->d_tris, &s->d_leafpos, &s->d_ref_boxes, &s->d_ref_sorted, &s->d_ref_pos,
-                      &s->d_spheres, &s->scratch.queue, &s->scratch.counters, &s->h2d_rays, &s->d2h_hits})
+                      &s->d_spheres, &s->scratch.queue, &s->scratch.counters, &s->h2d_rays, &s->d2h_hits, &s->d_mats,
+                      &s->d_tri_mat, &s->d_tri_nidx, &s->d_normals, &s->d_emit_tri, &s->d_emit_cdf, &s->d_plights})
         b->release();
+    s->rscratch.release();
     delete s;
     return RT_OK;
 }
@@ -230,7 +232,7 @@ int rt_scene_add_sphere(rt_scene *s, const float o2w[16], const float w2o[16], f
     r.radius = radius;
     r.material = material;
     r.shape_id = shape_id;
-    r.flags = transparent ? 1u : 0u;
+    r.flags = transparent ? 3u : 0u;  // bit 1: requested at add time, bit 0: effective
     if (index) *index = (uint32_t)s->spheres.size();
     s->spheres.push_back(r);
     s->committed = false;
@@ -273,6 +275,9 @@ int rt_scene_commit(rt_scene *s)
         std::memset(bvh.nodes[0].meta, 0xFF, 8);
     }
     s->nnodes = bvh.nodes.size();
+    s->recs = recs;
+    s->leaf_tris = bvh.leaf_tris;
+    s->render_dirty = true;
     RTB_CHECK(s->d_nodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(Bvh8Node), st));
     RTB_CHECK(s->d_tris.upload(recs.data(), recs.size() * sizeof(TriRecord), st));
     RTB_CHECK(s->d_leafpos.upload(leafpos.data(), leafpos.size() * 4, st));
@@ -281,6 +286,7 @@ int rt_scene_commit(rt_scene *s)
     RTB_CHECK(s->d_ref_pos.upload(ref.pos.data(), ref.pos.size() * 4, st));
     RTB_CHECK(s->d_spheres.upload(s->spheres.data(), s->spheres.size() * sizeof(SphereRecord), st));
     RTB_CHECK(s->scratch.counters.reserve(64));
+    RTB_CHECK(refresh_transparency(s));
     RTB_CUDA(cudaStreamSynchronize(st));
     s->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     s->committed = true;

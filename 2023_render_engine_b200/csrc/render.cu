@@ -1,0 +1,851 @@
+// Wavefront path tracer (sm_100a): the reference's PathTracerIntegrator bounce loop
+// (integration/pathTracing.cu:284-414, PathTracerIntegrator.cu:26-210) as queues of
+// independent paths.
+//
+// One wave = one bounce of every path in flight:
+//   extend  - closest hit of the wave's rays (BVH8 traversal, trace.cu)
+//   shade   - per path: emission, next-event estimation (point lights as the reference,
+//             plus area lights with MIS when enabled), BSDF sampling, Russian roulette;
+//             continuing paths are appended to the next wave's queue, finished paths to
+//             the retire list, and a freed slot immediately starts the next camera sample
+//             (path regeneration)
+//   shadow  - any-hit test of the shadow rays; unoccluded contributions are added to the
+//             path they belong to
+//   retire  - finished paths add their radiance to the film (NaN/Inf samples dropped)
+// Path state moves with the queue (double-buffered SoA), so every stage reads and writes
+// its arrays with coalesced 16-byte accesses; queue appends are warp-aggregated.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "shading.cuh"
+#include "traverse.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace rtb {
+
+namespace {
+
+constexpr int kB = 128;
+
+// flags in st2.w
+constexpr uint32_t kDepthMask = 0xFFu;
+constexpr uint32_t kCameraRay = 0x100u;
+constexpr uint32_t kLastSpecular = 0x200u;
+
+constexpr uint32_t kRetireTarget = 0x80000000u;
+
+struct RenderView {
+    SceneView sv;
+    const rt_material *mats;
+    const uint32_t *tri_mat;
+    const int32_t *tri_nidx;  // 3 per triangle, -1 when the mesh has no normals
+    const float *normals;
+    const uint32_t *emit_tri;
+    const float *emit_cdf;
+    uint32_t nemit;
+    float emit_total;  // sum over emitters of area * luminance(Le)
+    const float4 *plights;  // 2 per light: position, radiant intensity rgb
+    uint32_t nplights;
+    uint32_t nmats;
+    rt_camera cam;
+    uint32_t spp, sample_offset, max_depth, rr_depth, seed, flags;
+    uint64_t total;  // width * height * spp
+};
+
+struct Buffers {
+    rt_ray *rays[2];
+    float4 *st0[2];  // beta.xyz, pdf of the last BSDF sample
+    float4 *st1[2];  // L.xyz, pixel index bits
+    uint4 *st2[2];   // rng state lo/hi, sample index, flags
+    rt_hit *hits;
+    rt_ray *srays;
+    float4 *scontrib;  // rgb, target index bits (kRetireTarget: retire list)
+    float4 *retire;    // L.xyz, pixel index bits
+    uint32_t cap, scap;
+    // counters (uint32): [0],[1] queue sizes of buffers 0/1, [2] shadow count, [3] retire count,
+    // [4] status; u64 at [8]: next sample, [10] extension rays, [12] shadow rays, [14] camera rays
+    uint32_t *cnt;
+};
+
+__device__ __forceinline__ unsigned long long *cnt64(uint32_t *c, int i)
+{
+    return reinterpret_cast<unsigned long long *>(c + i);
+}
+
+// Warp-aggregated queue append: one atomic per group of active lanes.
+__device__ __forceinline__ uint32_t append(uint32_t *counter)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+
+__device__ __forceinline__ V3 xform_point(const float *m, V3 p)
+{
+    float x = m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3];
+    float y = m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7];
+    float z = m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11];
+    float w = m[12] * p.x + m[13] * p.y + m[14] * p.z + m[15];
+    float iw = 1.0f / w;
+    return v3(x * iw, y * iw, z * iw);
+}
+__device__ __forceinline__ V3 xform_vec(const float *m, V3 v)
+{
+    return v3(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z,
+              m[8] * v.x + m[9] * v.y + m[10] * v.z);
+}
+
+// Camera sample g of this call -> primary path in slot q of buffer b.
+// Sampler::getCameraSample (Sampler.cu:165-180) + ProjectiveCamera::generateRay
+// (ProjectiveCamera.cu:71-104).
+__device__ void start_path(const RenderView &rv, const Buffers &bf, int b, uint32_t q, uint64_t g)
+{
+    const uint32_t W = rv.cam.width, H = rv.cam.height;
+    const uint32_t pix = (uint32_t)(g / rv.spp);
+    const uint32_t j = rv.sample_offset + (uint32_t)(g % rv.spp);
+    const uint32_t px = pix % W, py = pix / W;
+    Pcg r = pcg_init(pix, j, rv.seed);
+    float fx = fminf(fmaxf((float)px + pcg_float(r), 0.f), (float)W);
+    float fy = fminf(fmaxf((float)py + pcg_float(r), 0.f), (float)H);
+    float l1 = pcg_float(r), l2 = pcg_float(r);
+    V3 pc = xform_point(rv.cam.raster_to_camera, v3(fx, fy, 0.f));
+    V3 oc = v3(0, 0, 0), dc = normalize(pc);
+    if (rv.cam.lens_radius > 0) {
+        float lx, ly;
+        concentric_disk(l1, l2, lx, ly);
+        lx *= rv.cam.lens_radius;
+        ly *= rv.cam.lens_radius;
+        float ft = rv.cam.focal_distance / pc.z;
+        V3 pf = pc * ft;
+        oc = v3(lx, ly, 0);
+        dc = normalize(pf - oc);
+    }
+    V3 o = xform_point(rv.cam.camera_to_world, oc);
+    V3 d = normalize(xform_vec(rv.cam.camera_to_world, dc));
+    rt_ray ray;
+    ray.ox = o.x;
+    ray.oy = o.y;
+    ray.oz = o.z;
+    ray.tmax = INFINITY;
+    ray.dx = d.x;
+    ray.dy = d.y;
+    ray.dz = d.z;
+    ray.flags = 0;
+    reinterpret_cast<float4 *>(bf.rays[b])[2 * q] = make_float4(ray.ox, ray.oy, ray.oz, ray.tmax);
+    reinterpret_cast<float4 *>(bf.rays[b])[2 * q + 1] = make_float4(ray.dx, ray.dy, ray.dz, 0.f);
+    bf.st0[b][q] = make_float4(1.f, 1.f, 1.f, 0.f);
+    bf.st1[b][q] = make_float4(0.f, 0.f, 0.f, __uint_as_float(pix));
+    bf.st2[b][q] = make_uint4((uint32_t)r.state, (uint32_t)(r.state >> 32), j, kCameraRay);
+}
+
+// Takes the next camera sample (if any) and appends it to buffer b.
+__device__ __forceinline__ void regenerate(const RenderView &rv, const Buffers &bf, int b)
+{
+    unsigned long long g = atomicAdd(cnt64(bf.cnt, 8), 1ull);
+    if (g >= rv.total) return;
+    uint32_t q = append(bf.cnt + b);
+    start_path(rv, bf, b, q, g);
+    atomicAdd(cnt64(bf.cnt, 14), 1ull);
+}
+
+__global__ void __launch_bounds__(kB) k_start(RenderView rv, Buffers bf)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= bf.cap) return;
+    regenerate(rv, bf, 0);
+}
+
+struct Surface {
+    V3 p, n, perr;  // position, shading normal (faces the ray for triangles), error bound
+    uint32_t mat;
+    bool emissive_tri;
+    float area_cos;  // for MIS: |cos| at the emitter
+};
+
+// Triangle / sphere hit -> surface (Triangle::intersect, Triangle.cu:319-428;
+// Sphere::intersect, Sphere.cu:277-355).
+__device__ Surface surface_at(const RenderView &rv, const rt_hit &h, V3 o, V3 d, bool compat)
+{
+    Surface s;
+    if (h.prim & RT_PRIM_SHAPE) {
+        const SphereRecord &sr = rv.sv.spheres[h.prim & ~RT_PRIM_SHAPE];
+        V3 c = v3(sr.o2w[3], sr.o2w[7], sr.o2w[11]);
+        V3 p = o + d * h.t;
+        V3 n = normalize(p - c);
+        s.p = c + n * sr.radius;
+        s.n = n;  // outward: -cross(dpdu, dpdv) of the reference parametrisation (Sphere.cu:159-160)
+        const float eb5 = error_bound(5);
+        s.perr = (vabs(s.p - c) + vabs(c)) * eb5;
+        s.mat = sr.material;
+        s.emissive_tri = false;
+        s.area_cos = 0.f;
+        return s;
+    }
+    const TriRecord tr = rv.sv.tris[rv.sv.leafpos[h.prim]];
+    V3 p0 = v3(tr.v0.x, tr.v0.y, tr.v0.z), p1 = v3(tr.v1.x, tr.v1.y, tr.v1.z), p2 = v3(tr.v2.x, tr.v2.y, tr.v2.z);
+    float b1 = h.b1, b2 = h.b2, b0 = 1.f - b1 - b2;
+    s.p = p0 * b0 + p1 * b1 + p2 * b2;
+    V3 ng = normalize(cross(p0 - p2, p1 - p2));
+    if (dot(ng, d) > 0) ng = -ng;  // Triangle.cu:370-373
+    s.n = ng;
+    const float eb7 = error_bound(7);
+    s.perr = (vabs(p0 * b0) + vabs(p1 * b1) + vabs(p2 * b2)) * eb7;
+    if (rv.tri_nidx && rv.tri_nidx[3 * h.prim] >= 0) {
+        const int32_t *ni = rv.tri_nidx + 3 * h.prim;
+        V3 n0 = v3(rv.normals[3 * ni[0]], rv.normals[3 * ni[0] + 1], rv.normals[3 * ni[0] + 2]);
+        V3 n1 = v3(rv.normals[3 * ni[1]], rv.normals[3 * ni[1] + 1], rv.normals[3 * ni[1] + 2]);
+        V3 n2 = v3(rv.normals[3 * ni[2]], rv.normals[3 * ni[2] + 1], rv.normals[3 * ni[2] + 2]);
+        V3 ns = normalize(n0 * b0 + n1 * b1 + n2 * b2);
+        s.n = ns;
+        if (compat) s.p = s.p + ns * 0.15f;  // Triangle.cu:418
+    }
+    s.mat = rv.tri_mat[h.prim];
+    s.emissive_tri = true;
+    s.area_cos = fabsf(dot(ng, d));
+    return s;
+}
+
+struct Bsdf {
+    uint32_t type;
+    V3 color;
+    Ggx g;
+    V3 eta, k;
+    float ior;
+};
+
+__device__ __forceinline__ Bsdf load_bsdf(const rt_material &m)
+{
+    Bsdf b;
+    b.type = m.type;
+    b.color = v3(m.color[0], m.color[1], m.color[2]);
+    b.g.ax = sqrtf(m.roughness[0]);
+    b.g.ay = sqrtf(m.roughness[1]);
+    b.eta = v3(m.eta[0], m.eta[1], m.eta[2]);
+    b.k = v3(m.k[0], m.k[1], m.k[2]);
+    b.ior = m.ior;
+    return b;
+}
+
+__device__ __forceinline__ bool is_scattering(uint32_t type)
+{
+    return type == RT_MAT_LAMBERTIAN || type == RT_MAT_TROWBRIDGE || type == RT_MAT_PLAIN;
+}
+__device__ __forceinline__ bool is_specular(uint32_t type)
+{
+    return type == RT_MAT_TROWBRIDGE || type == RT_MAT_DIELECTRIC;  // Material::isSpecular overrides
+}
+
+// f * |cos wi| and pdf, shading space.
+__device__ __forceinline__ V3 bsdf_eval(const Bsdf &b, V3 wo, V3 wi, float &pdf)
+{
+    pdf = 0.f;
+    switch (b.type) {
+    case RT_MAT_LAMBERTIAN:  // LambertianBSDF.cu:32-47
+        pdf = (wo.z * wi.z > 0) ? fabsf(wi.z) * kInvPi : 0.f;
+        return b.color * (kInvPi * abs_cos(wi));
+    case RT_MAT_TROWBRIDGE:
+        pdf = ggx_pdf(b.g, wo, wi);
+        return ggx_eval(b.g, b.color, b.eta, b.k, wo, wi);
+    default:
+        return v3(0, 0, 0);
+    }
+}
+
+// Samples wi; returns f*|cos|/pdf (the reference's sampleDirection value).
+__device__ V3 bsdf_sample(const Bsdf &b, V3 wo, Pcg &r, bool compat, V3 &wi, float &pdf, bool &delta)
+{
+    delta = false;
+    pdf = 0.f;
+    switch (b.type) {
+    case RT_MAT_LAMBERTIAN: {  // LambertianBSDF.cu:56-75
+        float u1 = pcg_float(r), u2 = pcg_float(r);
+        wi = cosine_hemisphere(u1, u2);
+        pdf = wi.z * kInvPi;
+        return b.color;
+    }
+    case RT_MAT_TROWBRIDGE: {  // TrowbridgeBSDF.cu:207-246
+        float u1 = pcg_float(r), u2 = pcg_float(r);
+        V3 won = normalize(wo);
+        if (fmaxf(b.g.ax, b.g.ay) < 1e-3f) {
+            wi = v3(-won.x, -won.y, won.z);
+            delta = true;
+            float c = abs_cos(wi);
+            V3 F = v3(fresnel_conductor(c, b.eta.x, b.k.x), fresnel_conductor(c, b.eta.y, b.k.y),
+                      fresnel_conductor(c, b.eta.z, b.k.z));
+            return F * (1.0f / c);
+        }
+        V3 h = ggx_sample_h(b.g, won, u1, u2);
+        wi = h * (2 * dot(won, h)) - won;  // reflect (geometricMath.cu:197-200)
+        pdf = ggx_pdf_h(b.g, won, h) / (4 * abs_cos2(won, h));
+        V3 f = ggx_eval(b.g, b.color, b.eta, b.k, won, wi);
+        if (!(pdf > 0)) return v3(0, 0, 0);
+        return f * (1.0f / pdf);
+    }
+    case RT_MAT_DIELECTRIC: {
+        delta = true;
+        float u = pcg_float(r);
+        float c = wo.z / length(wo);
+        if (compat) {
+            // DielectricMaterial.cu:59-77: refraction with probability 0.7, no division
+            if (u < 0.7f) {  // SpecularRefractionBSDF.cu:31-63
+                float ni = 1.f, nt = b.ior;
+                if (c < 0) {
+                    float t = ni;
+                    ni = nt;
+                    nt = t;
+                }
+                float eta = ni / nt;
+                V3 n = (wo.z < 0.f) ? v3(0, 0, -1) : v3(0, 0, 1);
+                float co = dot(n, wo) / length(wo);
+                float s2o = fmaxf(0.f, 1.f - co * co);
+                float s2t = eta * eta * s2o;
+                if (s2t >= 1) return v3(0, 0, 0);
+                float ct = sqrtf(1 - s2t);
+                wi = (-wo) * eta + n * (eta * co - ct);
+                return b.color * (1 - fresnel_dielectric_ref(co, ni, nt));
+            }
+            wi = v3(-wo.x, -wo.y, wo.z);  // SpecularReflectionBSDF.cu:30-41
+            return b.color * fresnel_dielectric_ref(wi.z / length(wi), 1.f, b.ior);
+        }
+        float F = fresnel_dielectric(c, 1.f, b.ior);
+        if (u < F) {
+            wi = v3(-wo.x, -wo.y, wo.z);
+            return b.color;
+        }
+        float ni = 1.f, nt = b.ior;
+        V3 n = v3(0, 0, 1);
+        if (c < 0) {
+            ni = b.ior;
+            nt = 1.f;
+            n = v3(0, 0, -1);
+        }
+        float eta = ni / nt;
+        float co = dot(n, wo) / length(wo);
+        float s2t = eta * eta * fmaxf(0.f, 1.f - co * co);
+        float ct = sqrtf(fmaxf(0.f, 1 - s2t));
+        wi = (-wo) * eta + n * (eta * co - ct);
+        return b.color;
+    }
+    case RT_MAT_MIRROR:  // PerfectReflectionBSDF
+        delta = true;
+        wi = v3(-wo.x, -wo.y, wo.z);
+        return b.color;
+    default:  // Light (NullBSDF) and Plain: no scattering
+        wi = v3(0, 0, 0);
+        return v3(0, 0, 0);
+    }
+}
+
+__device__ __forceinline__ float emitter_pdf(const RenderView &rv, V3 Le, float dist2, float cosl)
+{
+    // p(select tri) / area = luminance(Le) / total; solid-angle conversion dist^2 / |cos|
+    if (!(cosl > 0) || rv.emit_total <= 0) return 0.f;
+    return luminance(Le) / rv.emit_total * dist2 / cosl;
+}
+
+// skip_transparent: the reference's checkShadow semantics (Scene::isVisible ->
+// Triangle::intersects(checkShadow), Triangle.cu:439-440): transparent materials cast no
+// shadow. Used for point lights in compat mode; area-light samples must be blocked by
+// glass so that their MIS pairing with BSDF-sampled emitter hits stays unbiased.
+__device__ __forceinline__ void push_shadow(const Buffers &bf, V3 o, V3 d, float tmax, V3 contrib, uint32_t target,
+                                            bool skip_transparent)
+{
+    uint32_t i = append(bf.cnt + 2);
+    if (i >= bf.scap) return;
+    reinterpret_cast<float4 *>(bf.srays)[2 * i] = make_float4(o.x, o.y, o.z, tmax);
+    reinterpret_cast<float4 *>(bf.srays)[2 * i + 1] =
+        make_float4(d.x, d.y, d.z, __uint_as_float(skip_transparent ? 1u : 0u));
+    bf.scontrib[i] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(target));
+}
+
+__global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur)
+{
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = min(bf.cnt[cur], bf.cap);
+    if (q >= n) return;
+    const int nxt = cur ^ 1;
+    const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
+    const bool nee_area = (rv.flags & RT_RENDER_NEE_AREA) != 0 && rv.nemit > 0;
+    float4 r0 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q];
+    float4 r1 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q + 1];
+    float4 s0 = bf.st0[cur][q], s1 = bf.st1[cur][q];
+    uint4 s2 = bf.st2[cur][q];
+    float4 hv = reinterpret_cast<const float4 *>(bf.hits)[q];
+    rt_hit h{hv.x, __float_as_int(hv.y), hv.z, hv.w};
+    V3 o = v3(r0.x, r0.y, r0.z), d = v3(r1.x, r1.y, r1.z);
+    V3 beta = v3(s0.x, s0.y, s0.z), L = v3(s1.x, s1.y, s1.z);
+    const float last_pdf = s0.w;
+    const uint32_t pix = __float_as_uint(s1.w);
+    uint32_t flags = s2.w;
+    const uint32_t depth = flags & kDepthMask;
+    Pcg rng;
+    rng.state = ((uint64_t)s2.y << 32) | s2.x;
+    rng.inc = ((((uint64_t)s2.z << 32) | rv.seed) << 1u) | 1u;
+
+    bool finished = h.prim < 0;  // missed: no environment light (Scene::getEnvironmentLight = 0)
+    uint32_t target = 0;
+    bool cont = false;
+    V3 next_o, next_d;
+    float next_pdf = 0.f;
+    uint32_t next_flags = 0;
+    if (!finished) {
+        Surface sf = surface_at(rv, h, o, d, compat);
+        const rt_material &m = rv.mats[min(sf.mat, rv.nmats - 1)];
+        Bsdf bs = load_bsdf(m);
+        V3 t, bvec;
+        onb(sf.n, t, bvec);
+        V3 wo_w = -d;
+        V3 wo = v3(dot(wo_w, t), dot(wo_w, bvec), dot(wo_w, sf.n));
+        const bool scattering = is_scattering(bs.type);
+        // where this path's radiance will live after this bounce: decided below, but shadow
+        // rays need the target now, so reserve it first.
+        // BSDF sample first (its outcome decides continue/retire), NEE uses beta before update.
+        V3 wi_l;
+        float pdf_b;
+        bool delta;
+        V3 beta_in = beta;
+        // emission of the hit surface (pathTracing.cu:49-50)
+        V3 Le = v3(0, 0, 0);
+        if (bs.type == RT_MAT_LIGHT) {
+            Le = bs.color * m.intensity;
+        } else if (bs.type == RT_MAT_PLAIN && (flags & kCameraRay)) {
+            Le = bs.color;  // PlainMaterial::getEmittedRadiance on camera rays
+        }
+        if (!is_black(Le)) {
+            float w = 1.f;
+            if (nee_area && bs.type == RT_MAT_LIGHT && depth > 0 && !(flags & kLastSpecular) && sf.emissive_tri) {
+                float pl = emitter_pdf(rv, Le, h.t * h.t, sf.area_cos);
+                w = (last_pdf * last_pdf) / (last_pdf * last_pdf + pl * pl);
+            }
+            L = L + beta_in * Le * w;
+        }
+        V3 f = bsdf_sample(bs, wo, rng, compat, wi_l, pdf_b, delta);
+        V3 wi_w = t * wi_l.x + bvec * wi_l.y + sf.n * wi_l.z;
+        beta = beta * f;
+        finished = is_black(f);
+        // Russian roulette (pathTracing.cu:91-102)
+        if (!finished && scattering && depth > rv.rr_depth) {
+            float qrr = fmaxf(0.05f, 1.f - luminance(beta));
+            if (pcg_float(rng) < qrr)
+                finished = true;
+            else
+                beta = beta * (1.f / (1.f - qrr));
+        }
+        if (!finished && depth + 1 >= rv.max_depth) finished = true;  // loop bound (pathTracing.cu:296)
+        // reserve the path's slot for the shadow contributions
+        if (!finished) {
+            uint32_t qn = append(bf.cnt + nxt);
+            target = qn;
+            cont = true;
+            next_o = spawn_origin(sf.p, sf.n, sf.perr, wi_w);
+            next_d = wi_w;
+            next_pdf = delta ? 0.f : pdf_b;
+            next_flags = (depth + 1) | (delta ? kLastSpecular : 0u) |
+                         (((flags & kCameraRay) && is_specular(bs.type)) ? kCameraRay : 0u);
+        } else {
+            target = kRetireTarget | append(bf.cnt + 3);
+        }
+        // next-event estimation with beta before this bounce (pathTracing.cu:173-205)
+        if (scattering) {
+            for (uint32_t li = 0; li < rv.nplights; li++) {  // Scene::estimateAllDirectLights, PointLight
+                float4 lp = rv.plights[2 * li], li4 = rv.plights[2 * li + 1];
+                V3 tol = v3(lp.x, lp.y, lp.z) - sf.p;
+                float dist2 = dot(tol, tol), dist = sqrtf(dist2);
+                V3 wl = tol * (1.0f / dist);
+                float ul1 = pcg_float(rng), ul2 = pcg_float(rng);
+                (void)ul1;
+                (void)ul2;
+                if (!(dot(wl, sf.n) > 0)) continue;  // isOrientedTo
+                V3 wls = v3(dot(wl, t), dot(wl, bvec), dot(wl, sf.n));
+                float pb;
+                V3 fl = bsdf_eval(bs, wo, wls, pb);
+                V3 Li = v3(li4.x, li4.y, li4.z) * (1.0f / dist2);
+                if (is_black(fl) || is_black(Li)) continue;
+                float w = compat ? 1.0f / (1.0f + pb * pb) : 1.0f;  // powerHeuristic(1,1,1,pdf), Scene.cu:331
+                V3 c = beta_in * fl * Li * w;
+                V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
+                push_shadow(bf, so, wl, dist, c, target, compat);
+                atomicAdd(cnt64(bf.cnt, 12), 1ull);
+            }
+            if (nee_area) {
+                float u0 = pcg_float(rng), u1 = pcg_float(rng), u2 = pcg_float(rng);
+                // pick an emitter by area * luminance
+                float x = u0 * rv.emit_total;
+                uint32_t lo = 0, hi = rv.nemit - 1;
+                while (lo < hi) {
+                    uint32_t mid = (lo + hi) >> 1;
+                    if (rv.emit_cdf[mid] <= x)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                uint32_t etri = rv.emit_tri[lo];
+                const TriRecord er = rv.sv.tris[rv.sv.leafpos[etri]];
+                V3 e0 = v3(er.v0.x, er.v0.y, er.v0.z), e1 = v3(er.v1.x, er.v1.y, er.v1.z),
+                   e2 = v3(er.v2.x, er.v2.y, er.v2.z);
+                float su = sqrtf(u1);
+                float c0 = 1 - su, c1 = u2 * su;
+                V3 xl = e0 * c0 + e1 * c1 + e2 * (1 - c0 - c1);
+                V3 nl = normalize(cross(e1 - e0, e2 - e0));
+                V3 tol = xl - sf.p;
+                float dist2 = dot(tol, tol), dist = sqrtf(dist2);
+                V3 wl = tol * (1.0f / dist);
+                float cosl = fabsf(dot(nl, wl));
+                const rt_material &em = rv.mats[min(rv.tri_mat[etri], rv.nmats - 1)];
+                V3 Lel = v3(em.color[0], em.color[1], em.color[2]) * em.intensity;
+                float pl = emitter_pdf(rv, Lel, dist2, cosl);
+                if (pl > 0 && dot(wl, sf.n) > 0) {
+                    V3 wls = v3(dot(wl, t), dot(wl, bvec), dot(wl, sf.n));
+                    float pb;
+                    V3 fl = bsdf_eval(bs, wo, wls, pb);
+                    if (!is_black(fl)) {
+                        float w = (pl * pl) / (pl * pl + pb * pb);
+                        V3 c = beta_in * fl * Lel * (w / pl);
+                        V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
+                        push_shadow(bf, so, wl, dist * (1.0f - 1e-4f), c, target, false);
+                        atomicAdd(cnt64(bf.cnt, 12), 1ull);
+                    }
+                }
+            }
+        }
+    } else {
+        target = kRetireTarget | append(bf.cnt + 3);
+    }
+    if (cont) {
+        const uint32_t qn = target;
+        reinterpret_cast<float4 *>(bf.rays[nxt])[2 * qn] = make_float4(next_o.x, next_o.y, next_o.z, INFINITY);
+        reinterpret_cast<float4 *>(bf.rays[nxt])[2 * qn + 1] = make_float4(next_d.x, next_d.y, next_d.z, 0.f);
+        bf.st0[nxt][qn] = make_float4(beta.x, beta.y, beta.z, next_pdf);
+        bf.st1[nxt][qn] = make_float4(L.x, L.y, L.z, __uint_as_float(pix));
+        bf.st2[nxt][qn] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), s2.z, next_flags);
+    } else {
+        bf.retire[target & ~kRetireTarget] = make_float4(L.x, L.y, L.z, __uint_as_float(pix));
+        regenerate(rv, bf, nxt);
+    }
+    atomicAdd(cnt64(bf.cnt, 10), 1ull);
+}
+
+__global__ void __launch_bounds__(kB) k_shadow(RenderView rv, Buffers bf, int nxt)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = min(bf.cnt[2], bf.scap);
+    if (i >= n) return;
+    float4 r0 = reinterpret_cast<const float4 *>(bf.srays)[2 * i];
+    float4 r1 = reinterpret_cast<const float4 *>(bf.srays)[2 * i + 1];
+    WatertightRay w = make_watertight(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w);
+    const bool skip_transparent = __float_as_uint(r1.w) & 1u;
+    Best best{INFINITY, -1, 0u, 0.f, 0.f, INFINITY};
+    bool occ = false;
+    if (rv.sv.ntri > 0) {
+        traverse_bvh8(rv.sv, w, r1.x, r1.y, r1.z, skip_transparent, true, best);
+        occ = best.prim >= 0 && best.t < r0.w;
+    }
+    if (!occ && rv.sv.nspheres) {
+        float t = r0.w;
+        int32_t prim = -1;
+        float b1 = 0, b2 = 0;
+        intersect_spheres(rv.sv, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w, skip_transparent, t, prim, b1, b2);
+        occ = prim >= 0 && t < r0.w;
+    }
+    if (occ) return;
+    float4 c = bf.scontrib[i];
+    uint32_t target = __float_as_uint(c.w);
+    float *dst = (target & kRetireTarget) ? reinterpret_cast<float *>(bf.retire + (target & ~kRetireTarget))
+                                           : reinterpret_cast<float *>(bf.st1[nxt] + target);
+    atomicAdd(dst + 0, c.x);
+    atomicAdd(dst + 1, c.y);
+    atomicAdd(dst + 2, c.z);
+}
+
+__global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t *count, double *sum64)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = min(bf.cnt[3], bf.cap);
+    if (i >= n) return;
+    float4 v = bf.retire[i];
+    if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) return;  // pathTracing.cu:473-486
+    uint32_t pix = __float_as_uint(v.w);
+    atomicAdd(sum + 3 * pix + 0, v.x);
+    atomicAdd(sum + 3 * pix + 1, v.y);
+    atomicAdd(sum + 3 * pix + 2, v.z);
+    atomicAdd(count + pix, 1u);
+    if (sum64) {
+        atomicAdd(sum64 + 3 * pix + 0, (double)v.x);
+        atomicAdd(sum64 + 3 * pix + 1, (double)v.y);
+        atomicAdd(sum64 + 3 * pix + 2, (double)v.z);
+    }
+}
+
+}  // namespace
+
+}  // namespace rtb
+
+using namespace rtb;
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" {
+
+int rt_scene_set_materials(rt_scene *s, const rt_material *table, uint32_t n)
+{
+    if (!s || (!table && n)) return fail(RT_ERR_INVALID, "rt_scene_set_materials: null argument");
+    for (uint32_t i = 0; i < n; i++)
+        if (table[i].type > RT_MAT_PLAIN) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_materials: unknown type");
+    s->materials.assign(table, table + n);
+    s->render_dirty = true;
+    return RT_OK;
+}
+
+int rt_scene_set_triangle_materials(rt_scene *s, uint32_t first, uint32_t n, const uint32_t *mats)
+{
+    if (!s || (!mats && n)) return fail(RT_ERR_INVALID, "rt_scene_set_triangle_materials: null argument");
+    if ((uint64_t)first + n > s->tri_material.size())
+        return fail(RT_ERR_INVALID, "rt_scene_set_triangle_materials: range out of bounds");
+    std::memcpy(s->tri_material.data() + first, mats, 4ull * n);
+    s->render_dirty = true;
+    return RT_OK;
+}
+
+int rt_scene_add_point_light(rt_scene *s, const float pos[3], const float rgb[3], float intensity)
+{
+    if (!s || !pos || !rgb) return fail(RT_ERR_INVALID, "rt_scene_add_point_light: null argument");
+    s->plights.push_back(make_float4(pos[0], pos[1], pos[2], 0.f));
+    s->plights.push_back(make_float4(rgb[0] * intensity, rgb[1] * intensity, rgb[2] * intensity, 0.f));
+    s->plight_rgbi.push_back({rgb[0], rgb[1], rgb[2], intensity});
+    s->render_dirty = true;
+    return RT_OK;
+}
+
+}  // extern "C"
+
+namespace rtb {
+
+// Uploads what the shading kernels need (materials, per-triangle data, emitters, lights).
+void RenderScratch::release()
+{
+    for (DevBuf *b : {&rays[0], &rays[1], &st0[0], &st0[1], &st1[0], &st1[1], &st2[0], &st2[1], &hits, &srays,
+                      &scontrib, &retire, &cnt})
+        b->release();
+    if (host_cnt) cudaFreeHost(host_cnt);
+    host_cnt = nullptr;
+}
+
+int refresh_transparency(rt_scene *s)
+{
+    cudaStream_t st = s->ctx->stream;
+    auto mat_transparent = [&](uint32_t m) {
+        return m < s->materials.size() && (s->materials[m].flags & RT_MATF_TRANSPARENT) != 0;
+    };
+    bool changed = false;
+    for (size_t r = 0; r < s->recs.size(); r++) {
+        uint32_t id = s->leaf_tris[r];
+        uint32_t f = (s->tri_transparent[id] || mat_transparent(s->tri_material[id])) ? 1u : 0u;
+        uint32_t old;
+        std::memcpy(&old, &s->recs[r].v2.w, 4);
+        if (old != f) {
+            std::memcpy(&s->recs[r].v2.w, &f, 4);
+            changed = true;
+        }
+    }
+    if (changed) RTB_CHECK(s->d_tris.upload(s->recs.data(), s->recs.size() * sizeof(TriRecord), st));
+    bool schanged = false;
+    for (auto &sp : s->spheres) {
+        uint32_t f = ((sp.flags & 2u) || mat_transparent(sp.material)) ? 1u : 0u;
+        uint32_t nf = (sp.flags & ~1u) | f;
+        if (nf != sp.flags) {
+            sp.flags = nf;
+            schanged = true;
+        }
+    }
+    if (schanged) RTB_CHECK(s->d_spheres.upload(s->spheres.data(), s->spheres.size() * sizeof(SphereRecord), st));
+    return RT_OK;
+}
+
+int upload_render_data(rt_scene *s)
+{
+    if (!s->render_dirty) return RT_OK;
+    cudaStream_t st = s->ctx->stream;
+    RTB_CHECK(refresh_transparency(s));
+    const uint32_t n = (uint32_t)(s->tri9.size() / 9);
+    if (s->materials.empty()) return fail(RT_ERR_STATE, "rt_render: no materials set");
+    for (uint32_t m : s->tri_material)
+        if (m >= s->materials.size()) return fail(RT_ERR_INVALID, "rt_render: triangle material id out of range");
+    for (const auto &sp : s->spheres)
+        if (sp.material >= s->materials.size()) return fail(RT_ERR_INVALID, "rt_render: sphere material out of range");
+    RTB_CHECK(s->d_mats.upload(s->materials.data(), s->materials.size() * sizeof(rt_material), st));
+    RTB_CHECK(s->d_tri_mat.upload(s->tri_material.data(), 4ull * n, st));
+    bool any_normals = false;
+    for (int32_t x : s->tri_normal_idx) any_normals |= x >= 0;
+    if (any_normals) {
+        RTB_CHECK(s->d_tri_nidx.upload(s->tri_normal_idx.data(), 4ull * s->tri_normal_idx.size(), st));
+        RTB_CHECK(s->d_normals.upload(s->normals.data(), 4ull * s->normals.size(), st));
+    }
+    s->has_normals = any_normals;
+    std::vector<uint32_t> etri;
+    std::vector<float> cdf;
+    double acc = 0;
+    for (uint32_t t = 0; t < n; t++) {
+        const rt_material &m = s->materials[s->tri_material[t]];
+        if (m.type != RT_MAT_LIGHT) continue;
+        const float *p = s->tri9.data() + 9ull * t;
+        double ax = p[3] - p[0], ay = p[4] - p[1], az = p[5] - p[2];
+        double bx = p[6] - p[0], by = p[7] - p[1], bz = p[8] - p[2];
+        double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+        double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+        double lum = 0.212671 * m.color[0] * m.intensity + 0.715160 * m.color[1] * m.intensity +
+                     0.072169 * m.color[2] * m.intensity;
+        if (!(area * lum > 0)) continue;
+        acc += area * lum;
+        etri.push_back(t);
+        cdf.push_back((float)acc);
+    }
+    s->emit_total = (float)acc;
+    s->nemit = (uint32_t)etri.size();
+    if (!etri.empty()) {
+        RTB_CHECK(s->d_emit_tri.upload(etri.data(), 4ull * etri.size(), st));
+        RTB_CHECK(s->d_emit_cdf.upload(cdf.data(), 4ull * cdf.size(), st));
+    }
+    if (!s->plights.empty()) RTB_CHECK(s->d_plights.upload(s->plights.data(), 16ull * s->plights.size(), st));
+    s->render_dirty = false;
+    return RT_OK;
+}
+
+}  // namespace rtb
+
+extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts *opts, float *sum_rgb,
+                         uint32_t *count, double *sum64, rt_render_stats *stats)
+{
+    if (!s || !cam || !opts || !sum_rgb || !count) return fail(RT_ERR_INVALID, "rt_render: null argument");
+    if (!s->committed) return fail(RT_ERR_STATE, "rt_render: scene not committed");
+    if (cam->width == 0 || cam->height == 0 || opts->spp == 0 || opts->max_depth == 0)
+        return fail(RT_ERR_INVALID, "rt_render: empty image, spp or depth");
+    if (opts->max_depth > 255) return fail(RT_ERR_INVALID, "rt_render: max_depth above 255");
+    RTB_CUDA(cudaSetDevice(s->ctx->device));
+    cudaStream_t st = s->ctx->stream;
+    RTB_CHECK(upload_render_data(s));
+    const uint64_t total = (uint64_t)cam->width * cam->height * opts->spp;
+    if ((uint64_t)cam->width * cam->height >= (1ull << 31)) return fail(RT_ERR_INVALID, "rt_render: image too large");
+    uint32_t cap = opts->max_paths ? opts->max_paths : (1u << 22);
+    cap = (uint32_t)std::min<uint64_t>(cap, std::max<uint64_t>(total, 1024));
+    cap = (cap + kB - 1) / kB * kB;
+    const uint32_t per_path_shadow = (uint32_t)(s->plights.size() / 2) + ((opts->flags & RT_RENDER_NEE_AREA) ? 1 : 0);
+    const uint32_t scap = std::max<uint32_t>(cap * std::max<uint32_t>(per_path_shadow, 1), kB);
+    RenderScratch &rs = s->rscratch;
+    RTB_CHECK(rs.rays[0].reserve(32ull * cap));
+    RTB_CHECK(rs.rays[1].reserve(32ull * cap));
+    for (int b = 0; b < 2; b++) {
+        RTB_CHECK(rs.st0[b].reserve(16ull * cap));
+        RTB_CHECK(rs.st1[b].reserve(16ull * cap));
+        RTB_CHECK(rs.st2[b].reserve(16ull * cap));
+    }
+    RTB_CHECK(rs.hits.reserve(16ull * cap));
+    RTB_CHECK(rs.srays.reserve(32ull * scap));
+    RTB_CHECK(rs.scontrib.reserve(16ull * scap));
+    RTB_CHECK(rs.retire.reserve(16ull * cap));
+    RTB_CHECK(rs.cnt.reserve(256));
+    RTB_CHECK(s->scratch.queue.reserve(4ull * cap));
+    RTB_CHECK(s->scratch.counters.reserve(64));
+    if (!rs.host_cnt) RTB_CUDA(cudaMallocHost(&rs.host_cnt, 256));
+
+    Buffers bf;
+    for (int b = 0; b < 2; b++) {
+        bf.rays[b] = rs.rays[b].as<rt_ray>();
+        bf.st0[b] = rs.st0[b].as<float4>();
+        bf.st1[b] = rs.st1[b].as<float4>();
+        bf.st2[b] = rs.st2[b].as<uint4>();
+    }
+    bf.hits = rs.hits.as<rt_hit>();
+    bf.srays = rs.srays.as<rt_ray>();
+    bf.scontrib = rs.scontrib.as<float4>();
+    bf.retire = rs.retire.as<float4>();
+    bf.cap = cap;
+    bf.scap = scap;
+    bf.cnt = rs.cnt.as<uint32_t>();
+
+    RenderView rv{};
+    rv.sv = s->view();
+    rv.mats = s->d_mats.as<rt_material>();
+    rv.nmats = (uint32_t)s->materials.size();
+    rv.tri_mat = s->d_tri_mat.as<uint32_t>();
+    rv.tri_nidx = s->has_normals ? s->d_tri_nidx.as<int32_t>() : nullptr;
+    rv.normals = s->has_normals ? s->d_normals.as<float>() : nullptr;
+    rv.emit_tri = s->d_emit_tri.as<uint32_t>();
+    rv.emit_cdf = s->d_emit_cdf.as<float>();
+    rv.nemit = s->nemit;
+    rv.emit_total = s->emit_total;
+    rv.plights = s->d_plights.as<float4>();
+    rv.nplights = (uint32_t)(s->plights.size() / 2);
+    rv.cam = *cam;
+    rv.spp = opts->spp;
+    rv.sample_offset = opts->sample_offset;
+    rv.max_depth = opts->max_depth;
+    rv.rr_depth = opts->rr_depth;
+    rv.seed = opts->seed;
+    rv.flags = opts->flags;
+    rv.total = total;
+
+    cudaEvent_t e0, e1;
+    RTB_CUDA(cudaEventCreate(&e0));
+    RTB_CUDA(cudaEventCreate(&e1));
+    RTB_CUDA(cudaEventRecord(e0, st));
+    RTB_CUDA(cudaMemsetAsync(bf.cnt, 0, 256, st));
+    const unsigned blocks = cap / kB;
+    k_start<<<blocks, kB, 0, st>>>(rv, bf);
+    RTB_CUDA(cudaGetLastError());
+    const uint32_t trace_flags = (opts->flags & RT_RENDER_EXACT_TRACE) ? 0u : RT_TRACE_FAST;
+    int cur = 0;
+    uint64_t waves = 0;
+    const uint64_t max_waves = (uint64_t)opts->max_depth * (total / std::max<uint32_t>(cap / 4, 1) + 8) + 64;
+    for (;;) {
+        const int nxt = cur ^ 1;
+        for (int k = 0; k < 4; k++) {
+            RTB_CHECK(launch_trace_closest_dev(rv.sv, bf.rays[cur], bf.cnt + cur, cap, bf.hits, trace_flags,
+                                               s->scratch.queue.as<uint32_t>(), s->scratch.counters.as<uint32_t>(),
+                                               st));
+            RTB_CUDA(cudaMemsetAsync(bf.cnt + ((cur ^ 1)), 0, 4, st));
+            RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 8, st));
+            k_shade<<<blocks, kB, 0, st>>>(rv, bf, cur);
+            RTB_CUDA(cudaGetLastError());
+            k_shadow<<<(scap + kB - 1) / kB, kB, 0, st>>>(rv, bf, cur ^ 1);
+            RTB_CUDA(cudaGetLastError());
+            k_retire<<<blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64);
+            RTB_CUDA(cudaGetLastError());
+            cur ^= 1;
+            waves++;
+        }
+        (void)nxt;
+        RTB_CUDA(cudaMemcpyAsync(rs.host_cnt, bf.cnt, 128, cudaMemcpyDeviceToHost, st));
+        RTB_CUDA(cudaStreamSynchronize(st));
+        const uint32_t *hc = static_cast<const uint32_t *>(rs.host_cnt);
+        uint64_t next_sample;
+        std::memcpy(&next_sample, hc + 8, 8);
+        if (hc[cur] == 0 && next_sample >= total) break;
+        if (waves > max_waves) return fail(RT_ERR_TIMEOUT, "rt_render: wave cap exceeded");
+    }
+    RTB_CUDA(cudaEventRecord(e1, st));
+    RTB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stats) {
+        const uint32_t *hc = static_cast<const uint32_t *>(rs.host_cnt);
+        uint64_t v;
+        std::memcpy(&v, hc + 10, 8);
+        stats->extension_rays = v;
+        std::memcpy(&v, hc + 12, 8);
+        stats->shadow_rays = v;
+        std::memcpy(&v, hc + 14, 8);
+        stats->camera_rays = v;
+        stats->waves = waves;
+        stats->ms = ms;
+    }
+    return RT_OK;
+}

@@ -131,9 +131,28 @@ struct TraceScratch {
 
 int launch_trace_closest(const SceneView &v, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags,
                          uint32_t *queue, uint32_t queue_cap, uint32_t *counters, cudaStream_t s);
+// Same with the ray count read on the device (queues built by other kernels); cap bounds it.
+int launch_trace_closest_dev(const SceneView &v, const rt_ray *rays, const uint32_t *n_dev, uint32_t cap, rt_hit *hits,
+                             uint32_t flags, uint32_t *queue, uint32_t *counters, cudaStream_t s);
 int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, uint8_t *occluded, uint32_t flags,
                      uint32_t *counters, cudaStream_t s);
 
+// Wavefront buffers of rt_render (grown on demand, kept between calls).
+struct RenderScratch {
+    DevBuf rays[2], st0[2], st1[2], st2[2], hits, srays, scontrib, retire, cnt;
+    void *host_cnt = nullptr;  // pinned
+    void release();
+};
+
+}  // namespace rtb
+
+struct rt_scene;
+namespace rtb {
+// Uploads materials, per-triangle data, emitters and lights when they changed.
+int upload_render_data(rt_scene *s);
+// Re-derives the shadow-ray transparency of triangle records / spheres from the
+// mesh flags and the material table; re-uploads what changed.
+int refresh_transparency(rt_scene *s);
 }  // namespace rtb
 
 // ------------------------------------------------------------- handles
@@ -163,6 +182,21 @@ struct rt_scene {
     rtb::TraceScratch scratch;
     uint64_t last_rays = 0, last_fallback = 0;
     rtb::DevBuf h2d_rays, d2h_hits;  // device staging for the host-buffer entry points
+    // rendering
+    std::vector<rt_material> materials;
+    std::vector<float4> plights;  // 2 per light: position, rgb * intensity
+    struct PL {
+        float r, g, b, i;
+    };
+    std::vector<PL> plight_rgbi;
+    std::vector<rtb::TriRecord> recs;  // host copy of the leaf-ordered triangle records
+    std::vector<uint32_t> leaf_tris;   // record index -> triangle id
+    bool render_dirty = true;
+    bool has_normals = false;
+    uint32_t nemit = 0;
+    float emit_total = 0.f;
+    rtb::DevBuf d_mats, d_tri_mat, d_tri_nidx, d_normals, d_emit_tri, d_emit_cdf, d_plights;
+    rtb::RenderScratch rscratch;
     rtb::SceneView view() const;
     uint64_t device_bytes() const;
 };

@@ -146,6 +146,89 @@ typedef struct rt_trace_stats {
 } rt_trace_stats;
 RT_API int rt_trace_stats_get(rt_scene *scene, rt_trace_stats *out);
 
+
+/* ------------------------------------------------------------- materials */
+
+/* Material kinds (materials/*.cu). */
+typedef enum rt_material_type {
+    RT_MAT_LAMBERTIAN = 0, /* LambertianMaterial / LambertianBRDF (LambertianBSDF.cu:10-77) */
+    RT_MAT_TROWBRIDGE = 1, /* TrowbridgeMaterial, GGX conductor (TrowbridgeBSDF.cu:12-253) */
+    RT_MAT_DIELECTRIC = 2, /* DielectricMaterial / GlassMaterial (DielectricMaterial.cu:12-83) */
+    RT_MAT_LIGHT = 3,      /* LightMaterial: emitter, no scattering (LightMaterial.cu:10-60) */
+    RT_MAT_MIRROR = 4,     /* perfect specular reflector (MirrorMaterial.cu) */
+    RT_MAT_PLAIN = 5       /* PlainMaterial: returns its colour on camera hits only */
+} rt_material_type;
+
+#define RT_MATF_TRANSPARENT 0x1u /* ignored by shadow rays (Material::isTransparent) */
+
+typedef struct rt_material {
+    uint32_t type;        /* rt_material_type */
+    uint32_t flags;       /* RT_MATF_* */
+    float color[3];       /* kd (Lambertian, Trowbridge), ks=kt (Dielectric), emission colour (Light) */
+    float intensity;      /* emission scale (Light): Le = color * intensity */
+    float eta[3], k[3];   /* conductor Fresnel (Trowbridge) */
+    float roughness[2];   /* Trowbridge roughness x/y; alpha = sqrt(roughness) */
+    float ior;            /* Dielectric index of refraction (Glass: 1.5) */
+    float pad[3];
+} rt_material;
+
+/* Replaces the Material* each Shape/Triangle points to (Triangle::setMaterial,
+ * Shape::setMaterial): a table indexed by the `material` ids given at add time. */
+RT_API int rt_scene_set_materials(rt_scene *scene, const rt_material *table, uint32_t n);
+
+/* Per-triangle material ids for triangles [first, first+n) (overrides the mesh id). */
+RT_API int rt_scene_set_triangle_materials(rt_scene *scene, uint32_t first, uint32_t n, const uint32_t *materials);
+
+/* PointLight(lightToWorld = translate(pos), color, intensity) (light/PointLight.cu:15-96). */
+RT_API int rt_scene_add_point_light(rt_scene *scene, const float pos[3], const float rgb[3], float intensity);
+
+/* ------------------------------------------------------------- rendering */
+
+/* ProjectiveCamera (camera/ProjectiveCamera.cu:10-104): raster -> camera is
+ * raster_to_camera (row-major 4x4, projective), camera -> world camera_to_world;
+ * lens_radius > 0 enables the thin lens with focal_distance. */
+typedef struct rt_camera {
+    float camera_to_world[16];
+    float raster_to_camera[16];
+    float lens_radius;
+    float focal_distance;
+    uint32_t width, height;
+} rt_camera;
+
+#define RT_RENDER_NEE_AREA 0x1u /* next-event estimation on emissive triangles, MIS with BSDF hits */
+#define RT_RENDER_COMPAT 0x2u   /* reference estimator quirks (delta-light MIS weight, 0.7/0.3 glass lobes
+                                   without pdf, reference Fresnel); off = physically consistent */
+#define RT_RENDER_EXACT_TRACE 0x4u /* reference-exact closest-hit ids for extension rays */
+
+typedef struct rt_render_opts {
+    uint32_t spp;            /* samples per pixel in this call */
+    uint32_t sample_offset;  /* index of the first sample (progressive rendering) */
+    uint32_t max_depth;      /* MAX_RAY_RECURSION_DEPTH (types.h:41) */
+    uint32_t rr_depth;       /* Russian roulette when depth > rr_depth (pathTracing.cu:91) */
+    uint32_t seed;           /* PCG stream base; per-pixel stream = pixel index */
+    uint32_t flags;          /* RT_RENDER_* */
+    uint32_t max_paths;      /* wavefront capacity (0: automatic) */
+    uint32_t reserved;
+} rt_render_opts;
+
+typedef struct rt_render_stats {
+    uint64_t camera_rays;
+    uint64_t extension_rays; /* closest-hit rays incl. camera rays */
+    uint64_t shadow_rays;
+    uint64_t waves;
+    double ms;               /* device time of the render call */
+} rt_render_stats;
+
+/* Path-traces spp samples per pixel and ADDS them to the caller's film (device
+ * buffers, width*height pixels): sum_rgb (3 floats per pixel), count (valid samples
+ * per pixel), optional sum_rgb64 (3 doubles per pixel, FP64 accumulation). The pixel
+ * estimate is sum/count: samples with NaN/Inf radiance are dropped, which equals the
+ * reference's replacement by the mean of the valid ones (pathTracing.cu:457-490).
+ * Replaces PathTracerIntegrator::render (integration/PathTracerIntegrator.cu:140-210)
+ * with its bounce loop computeSamples (pathTracing.cu:284-414). */
+RT_API int rt_render(rt_scene *scene, const rt_camera *camera, const rt_render_opts *opts, float *sum_rgb,
+                     uint32_t *count, double *sum_rgb64, rt_render_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -279,3 +279,45 @@ class RestatedBvh:
         r = self.o.L.rto_triangle_intersects(self.h, tri, o.ctypes.data, d.ctypes.data, float(tmax), h.ctypes.data,
                                              int(shadow))
         return bool(r), float(h[0])
+
+
+class PathTracerOracle:
+    """CPU restatement of the renderer's estimator (oracle/pt_oracle.c) over a scene
+    given as a triangle soup + spheres + materials + point lights."""
+
+    def __init__(self, restated: Restated, verts, idx, tri_mat, spheres, materials, plights=()):
+        import importlib
+
+        N = importlib.import_module("2023_render_engine_b200._native")
+        L = restated.L
+        L.pto_render.argtypes = [P, P, P, U32, P, U32, P, U32, P, U32, U32, U32, U32, U32, U32, U32, U32, P, P, I]
+        L.pto_render.restype = I
+        self.L = L
+        self.bvh = restated.bvh(verts, idx) if len(idx) else None
+        self.tri_mat = _np(tri_mat, np.uint32)
+        sph = np.zeros(len(spheres), dtype=np.dtype([("w2o", "<f4", 16), ("o2w", "<f4", 16), ("radius", "<f4"),
+                                                      ("material", "<u4")]))
+        for i, s in enumerate(spheres):
+            sph[i]["w2o"] = np.asarray(s["w2o"], np.float32).reshape(16)
+            sph[i]["o2w"] = np.asarray(s["o2w"], np.float32).reshape(16)
+            sph[i]["radius"] = s["radius"]
+            sph[i]["material"] = s["material"]
+        self.sph = sph
+        self.mats = (N.Material * len(materials))(*materials)
+        self.nmat = len(materials)
+        self.pl = _np(np.array([list(p) + list(np.asarray(c) * i) for p, c, i in plights], np.float32).reshape(-1),
+                      np.float32) if len(plights) else np.zeros(6, np.float32)
+        self.npl = len(plights)
+
+    def render(self, camera, spp, max_depth, rr_depth=3, seed=0, flags=0, sample_offset=0, threads=8,
+               pixels=None):
+        w, h = camera.width, camera.height
+        p0, p1 = (0, w * h) if pixels is None else pixels
+        s = np.zeros((w * h, 3), np.float64)
+        c = np.zeros(w * h, np.uint32)
+        self.L.pto_render(self.bvh.h if self.bvh is not None else None, self.tri_mat.ctypes.data,
+                          self.sph.ctypes.data if len(self.sph) else None, len(self.sph),
+                          ctypes.cast(self.mats, ctypes.c_void_p), self.nmat, self.pl.ctypes.data, self.npl,
+                          ctypes.addressof(camera), spp, sample_offset, max_depth, rr_depth, seed, flags, p0, p1,
+                          s.ctypes.data, c.ctypes.data, threads)
+        return s, c

@@ -6,6 +6,7 @@
  */
 #define _GNU_SOURCE
 #include "rt_oracle.h"
+#include "rt_oracle_internal.h"
 
 #include <float.h>
 #include <math.h>
@@ -206,7 +207,8 @@ static int box_intersects(const float *bx, const float *o, const float *inv, flo
 
 /* The geometric part of Triangle::intersects (Triangle.cu:442-593). Returns 0 when
  * the triangle is missed; otherwise the hit offset and its error bound deltaT. */
-static int tri_geom(const float *v, const float *o, const float *d, float tmax, float *tOut, float *dtOut)
+static int tri_geom_b(const float *v, const float *o, const float *d, float tmax, float *tOut, float *dtOut,
+                      float *b1Out, float *b2Out)
 {
     float lp0[3], lp1[3], lp2[3];
     for (int c = 0; c < 3; c++) {
@@ -271,7 +273,14 @@ static int tri_geom(const float *v, const float *o, const float *d, float tmax, 
     float deltaT = 3 * (error_bound(3) * maxE * maxZt + deltaE * maxZt + deltaZ * maxE) * fabsf(invDet);
     *tOut = t;
     *dtOut = deltaT;
+    if (b1Out) *b1Out = e1 * invDet;
+    if (b2Out) *b2Out = e2 * invDet;
     return 1;
+}
+
+static int tri_geom(const float *v, const float *o, const float *d, float tmax, float *tOut, float *dtOut)
+{
+    return tri_geom_b(v, o, d, tmax, tOut, dtOut, NULL, NULL);
 }
 
 /* Triangle::intersects with the reference's running-offset semantics
@@ -325,6 +334,27 @@ static int32_t trace_one(const rto_bvh *b, const float *o, const float *d, float
     *tOut = h;
     return hit;
 }
+
+void rto_trace_one_full(const rto_bvh *b, const float *o, const float *d, float tmax, int checkShadow,
+                        int32_t *id, float *t, float *b1, float *b2)
+{
+    float tt;
+    int32_t h = trace_one(b, o, d, tmax, checkShadow, &tt);
+    *id = h;
+    *t = tt;
+    *b1 = *b2 = 0.f;
+    if (h >= 0) {
+        float t2, dt;
+        tri_geom_b(b->tri + 9 * (size_t)h, o, d, tmax, &t2, &dt, b1, b2);
+    }
+}
+
+void rto_triangle_vertices(const rto_bvh *b, uint32_t tri, float *v9)
+{
+    memcpy(v9, b->tri + 9 * (size_t)tri, 9 * sizeof(float));
+}
+
+uint32_t rto_bvh_ntri(const rto_bvh *b) { return b->n; }
 
 /* -------------------------------------------------------------- threading */
 

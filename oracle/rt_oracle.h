@@ -47,6 +47,39 @@ void rto_knn_brute(const float *pos, const int32_t *shape, uint64_t n, const flo
                    const int32_t *qshape, uint64_t nq, uint32_t k, float radius,
                    int32_t *outIdx, float *outDist, uint32_t *outCount, int nthreads);
 
+/* ---- path tracing estimator (pt_oracle.c) ---- */
+
+typedef struct pto_material { /* same layout as rt_material in include/rt_b200.h */
+    uint32_t type, flags;
+    float color[3];
+    float intensity;
+    float eta[3], k[3];
+    float roughness[2];
+    float ior;
+    float pad[3];
+} pto_material;
+
+typedef struct pto_sphere {
+    float w2o[16];
+    float o2w[16];
+    float radius;
+    uint32_t material;
+} pto_sphere;
+
+typedef struct pto_camera { /* same layout as rt_camera */
+    float camera_to_world[16];
+    float raster_to_camera[16];
+    float lens_radius, focal_distance;
+    uint32_t width, height;
+} pto_camera;
+
+/* Renders pixels [pix_begin, pix_end) with spp samples each into sum (3 doubles per
+ * pixel, indexed by pixel) and count; flags: 1 = area-light NEE, 2 = reference quirks. */
+int pto_render(const rto_bvh *bvh, const uint32_t *tri_mat, const pto_sphere *sph, uint32_t nsph,
+               const pto_material *mats, uint32_t nmat, const float *plights, uint32_t npl, const pto_camera *cam,
+               uint32_t spp, uint32_t sample_offset, uint32_t max_depth, uint32_t rr_depth, uint32_t seed,
+               uint32_t flags, uint32_t pix_begin, uint32_t pix_end, double *sum, uint32_t *count, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif
