@@ -1,18 +1,23 @@
 """Benchmark: Mrays/s of the B200 rendering core on the BVH-stress configuration.
 
-Workload (one "step"): closest-hit tracing of the seeded 2^24-ray set of the BVH-stress
-scene (1,310,720-triangle displaced icosphere inside the Cornell box, 1,310,732
-triangles), reference-exact mode. Inputs: 512 MiB of rays (larger than the 126 MB L2).
+Workload (one "step"): a full path-traced render of the BVH-stress scene (1,310,720-triangle
+displaced icosphere with per-block GGX inside the Cornell box, 1,310,732 triangles) at
+1920x1080, 64 samples per pixel, max depth 12, Russian roulette after depth 3, NEE on the
+area light. Mrays/s = (closest-hit extension rays incl. camera rays + shadow rays) / render
+time. The film (sum + count buffers) is cleared at the start of every step.
+
+Secondary line items: closest-hit tracing of the seeded 2^24-ray BVH-stress ray set
+(reference-exact ids; 512 MiB of rays, larger than the 126 MB L2), which also gives the
+roofline of the dominant kernel (k_trace_closest).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torchrun: every rank traces its own seeded ray set (independent
-replicas, weak scaling, no collective on the data path); the time is the max over
-ranks, the value the rays of all ranks / that time.
+N > 1 runs under torchrun: every rank renders its own image (different seed; independent
+replicas, weak scaling, no collective on the data path); the time is the max over ranks.
 
 --impl reference times the reference renderer's own traversal (BVH::intersectRay,
 compiled from its sources into oracle/_ref) on this machine's host cores over a bounded
-sample of the same ray set; rank 0 alone runs it.
+sample of the BVH-stress ray set; rank 0 alone runs it.
 """
 from __future__ import annotations
 
@@ -32,8 +37,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "Mrays/s"
-WORKLOAD = "BVH-stress closest hit: 2^24 seeded rays (origins uniform in [-1,1]^3, directions uniform), " \
-           "1,310,732 triangles (displaced icosphere subdiv 8 + Cornell box), reference-exact ids"
+WORKLOAD = ("BVH-stress render: 1920x1080, 64 spp, max depth 12, RR after depth 3, NEE on the area light; "
+            "1,310,732 triangles (displaced icosphere subdiv 8, GGX F0=0.04 + Cornell box)")
+TRACE_WORKLOAD = "closest hit of 2^24 seeded rays (origins uniform in [-1,1]^3, directions uniform), reference-exact ids"
 NRAYS = 1 << 24
 ALG_BYTES_PER_RAY = 48  # 32 B ray in + 16 B hit out (queue level)
 
@@ -155,7 +161,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": val, "unit": "Mrays/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "rays_per_step": sample},
+        "config": {"workload": WORKLOAD, "rays_per_step": sample,
+                   "reference_path": "BVH::intersectRay over the BVH-stress ray set (the reference's render loop "
+                                     "needs its GPU BVH; its traversal alone is timed, shading excluded)"},
         "cpu_baseline": {"value": val, "unit": "Mrays/s", "cores": threads, "kind": "reference",
                          "sample": f"{sample} consecutive rays of the 2^24 set per step"},
         "e2e": {"value": val, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -177,81 +185,126 @@ def run_ours(args):
     core = importlib.import_module("2023_render_engine_b200.core")
     S = importlib.import_module("2023_render_engine_b200.scenes")
     N = importlib.import_module("2023_render_engine_b200._native")
+    cfgs = importlib.import_module("2023_render_engine_b200.configs")
     dev = torch.cuda.current_device()
     ctx = core.Context(dev)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
-    sc, v, f = build_scene(core, ctx, S)
-    o, d = S.random_rays(NRAYS, seed=7 + rank)
-    rays_np = core.make_rays(o, d)
-    rays_h = torch.from_numpy(rays_np.view(np.float32).reshape(-1)).pin_memory()
-    hits_h = torch.empty(NRAYS * 4, dtype=torch.float32).pin_memory()
-    rays_d = rays_h.cuda()
-    hits_d = torch.empty(NRAYS * 4, dtype=torch.float32, device="cuda")
-    torch.cuda.synchronize()
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
 
-    # ---- device-resident timing
-    for _ in range(args.warmup):
-        sc.trace_closest(rays_d, hits_d, NRAYS)
+    def max_over_ranks(vals):
+        if world == 1:
+            return vals
+        t = torch.tensor(vals, device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return [float(x) for x in t]
+
+    sc, cam, p = cfgs.build_config1(ctx, args.width, args.height)
+    v, f, _ = S.flatten(S.stress_scene())
+    W, H = cam.width, cam.height
+    film = {"sum": torch.zeros(H * W * 3, dtype=torch.float32, device="cuda"),
+            "count": torch.zeros(H * W, dtype=torch.int32, device="cuda")}
+    host_sum = torch.empty(H * W * 3, dtype=torch.float32).pin_memory()
+    host_cnt = torch.empty(H * W, dtype=torch.int32).pin_memory()
+    rflags = N.RT_RENDER_NEE_AREA
+
+    def render_step(seed):
+        film["sum"].zero_()
+        film["count"].zero_()
+        _, st = sc.render(cam, spp=args.spp, max_depth=p["max_depth"], rr_depth=p["rr_depth"], seed=seed,
+                          flags=rflags, film=film)
+        return st
+
+    # ---- render, film resident on the device
+    for w in range(args.warmup):
+        render_step(1000 + w + 97 * rank)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    rays = []
     with ClockSampler(dev) as clk:
         ev0.record(stream)
-        for _ in range(args.steps):
-            sc.trace_closest(rays_d, hits_d, NRAYS)
+        for k in range(args.steps):
+            st = render_step(k + 97 * rank)
+            rays.append(st["extension_rays"] + st["shadow_rays"])
         ev1.record(stream)
         torch.cuda.synchronize()
     barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
-    fallback = sc.trace_stats()["exact_fallback_rays"]
+    rays_step = float(np.mean(rays))
+    st_last = st
 
-    # ---- end to end: pinned host rays in, host hits out, through the public API
-    for _ in range(max(1, args.warmup // 2)):
-        N.check(N.lib().rt_trace_closest_host(sc.handle, rays_h.data_ptr(), NRAYS, hits_h.data_ptr(), 0))
+    # ---- end to end: the render call + the film read back into pinned host memory
     torch.cuda.synchronize()
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        N.check(N.lib().rt_trace_closest_host(sc.handle, rays_h.data_ptr(), NRAYS, hits_h.data_ptr(), 0))
+    for k in range(args.steps):
+        render_step(500 + k + 97 * rank)
+        host_sum.copy_(film["sum"], non_blocking=True)
+        host_cnt.copy_(film["count"], non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
     ms_e2e = e0.elapsed_time(e1) / args.steps
 
-    # ---- kernel-only duration of the dominant kernel (k_trace_closest) for the roofline:
-    # the exact-replay kernel and the counter memset are timed out by tracing in FAST mode
-    # would change the work, so time the full call and subtract nothing; report the call.
-    if world > 1:
-        t = torch.tensor([ms, ms_e2e], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
+    # ---- closest-hit trace of the 2^24-ray set (dominant kernel, roofline)
+    o, d = S.random_rays(NRAYS, seed=7 + rank)
+    rays_np = core.make_rays(o, d)
+    rays_d = torch.from_numpy(rays_np.view(np.float32).reshape(-1)).cuda()
+    hits_d = torch.empty(NRAYS * 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        sc.trace_closest(rays_d, hits_d, NRAYS)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        sc.trace_closest(rays_d, hits_d, NRAYS)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms_trace = t0.elapsed_time(t1) / args.steps
+    fallback = sc.trace_stats()["exact_fallback_rays"]
+
+    ms, ms_e2e, ms_trace = max_over_ranks([ms, ms_e2e, ms_trace])
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        rate = NRAYS * world / (ms / 1000) / 1e6
-        rate_e2e = NRAYS * world / (ms_e2e / 1000) / 1e6
-        achieved = NRAYS * ALG_BYTES_PER_RAY / (ms / 1000) / 1e9
+        rate = rays_step * world / (ms / 1000) / 1e6
+        rate_e2e = rays_step * world / (ms_e2e / 1000) / 1e6
+        trace_rate = NRAYS * world / (ms_trace / 1000) / 1e6
+        achieved = NRAYS * ALG_BYTES_PER_RAY / (ms_trace / 1000) / 1e9
+        samples = W * H * args.spp
         line = {
             "metric": METRIC, "value": rate, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and rays)",
-            "config": {"workload": WORKLOAD, "rays_per_step_per_gpu": NRAYS, "triangles": int(f.shape[0]),
-                       "l2": "inputs larger than L2 (512 MiB ray buffer per step)",
-                       "parallelism": f"replicas x{world}", "exact_fallback_rays": int(fallback)},
-            "e2e": {"value": rate_e2e, "unit": "Mrays/s", "h2d_bytes_per_step": NRAYS * 32,
-                    "d2h_bytes_per_step": NRAYS * 16},
-            "gpu_launches": 2 * args.steps,
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, camera and sample streams)",
+            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": args.spp,
+                       "max_depth": p["max_depth"], "triangles": int(f.shape[0]),
+                       "rays_per_step_per_gpu": rays_step,
+                       "extension_rays": int(st_last["extension_rays"]), "shadow_rays": int(st_last["shadow_rays"]),
+                       "camera_rays": int(st_last["camera_rays"]), "waves": int(st_last["waves"]),
+                       "samples_per_s": samples * world / (ms / 1000),
+                       "l2": "scene ~140 MB and path queues ~1 GB per step exceed the 126 MB L2",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": rate_e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 144 + 32,
+                    "d2h_bytes_per_step": W * H * 16,
+                    "note": "render call through the C ABI + film read back to pinned host memory; the inputs "
+                            "of a step are the camera and options structs"},
+            "trace": {"workload": TRACE_WORKLOAD, "value": trace_rate, "unit": "Mrays/s", "ms_per_step": ms_trace,
+                      "exact_fallback_rays": int(fallback)},
+            "gpu_launches": int(st_last["waves"]) * 5 + 1,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
-                         "note": f"48 B/ray queue-level bytes over the whole trace call; peak {peak_kind}"},
+                         "kernel": "k_trace_closest (2^24-ray closest-hit call, 48 B/ray queue-level bytes)",
+                         "note": f"peak {peak_kind}; traversal reads nodes/triangles from L2, see profiles/"},
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline:
@@ -259,8 +312,8 @@ def run_ours(args):
             ns = args.cpu_sample
             val, dt = cpu_reference_rate(v, f, o[:ns], d[:ns], threads)
             line["cpu_baseline"] = {"value": val, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-                                    "sample": f"first {ns} rays of the set, reference BVH::intersectRay, "
-                                              f"{dt:.1f} s"}
+                                    "sample": f"first {ns} rays of the BVH-stress ray set through the reference's "
+                                              f"BVH::intersectRay ({dt:.1f} s)"}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -269,13 +322,16 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1 << 20)
     ap.add_argument("--ref-sample", type=int, default=1 << 18)
     ap.add_argument("--rays-log2", type=int, default=24, help="smaller ray sets for profiler captures")
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--spp", type=int, default=64)
     args = ap.parse_args()
     global NRAYS
     NRAYS = 1 << args.rays_log2
