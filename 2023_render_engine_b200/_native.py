@@ -96,6 +96,7 @@ SIGNATURES = {
     "rt_scene_stats_get": [_P, ctypes.POINTER(SceneStats)],
     "rt_trace_closest": [_P, _P, _U64, _P, _U32],
     "rt_trace_closest_host": [_P, _P, _U64, _P, _U32],
+    "rt_trace_closest_noalloc": [_P, _P, _U64, _P, _U32],
     "rt_trace_any": [_P, _P, _U64, _P, _U32],
     "rt_trace_stats_get": [_P, ctypes.POINTER(TraceStats)],
     "rt_scene_set_materials": [_P, _P, _U32],

@@ -132,6 +132,18 @@ RT_API int rt_trace_closest(rt_scene *scene, const rt_ray *rays_dev, uint64_t n,
  * staging; the end-to-end form the reference's host-vector API corresponds to). */
 RT_API int rt_trace_closest_host(rt_scene *scene, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags);
 
+/* Closest hit exactly like rt_trace_closest, for callers that must not allocate device
+ * memory while they trace (a render thread that cannot afford the device synchronisation an
+ * allocation may cause, or a host whose own pool allocator owns all device memory). It has
+ * no counterpart in the reference. Its scratch (the reference-order replay queue and the
+ * counters) is a fixed device array inside this library, about 4 MiB, held on every GPU
+ * that loads the library until the process exits. At most 1048576 rays per call
+ * (RT_ERR_CAPACITY above that). The first call on a device looks up the array's device
+ * address (make that first call before any stream capture). All calls share the array:
+ * calls that overlap on the GPU (other threads or streams) race; serialise them. */
+RT_API int rt_trace_closest_noalloc(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, rt_hit *hits_dev,
+                                    uint32_t flags);
+
 /* Occlusion test: occluded[i] = 1 when a primitive is hit at t < rays[i].tmax.
  * Replaces the shadow-ray use of Scene::intersects in Scene::isVisible
  * (Scene.cu:238-276). Device pointers. */
