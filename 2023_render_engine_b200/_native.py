@@ -69,6 +69,15 @@ RT_RENDER_COMPAT = 0x2
 RT_RENDER_EXACT_TRACE = 0x4
 
 
+class PhotonTraceStats(ctypes.Structure):
+    _fields_ = [("emitted", ctypes.c_uint64), ("stored", ctypes.c_uint64), ("rays", ctypes.c_uint64),
+                ("ms", ctypes.c_double)]
+
+
+PHOTON_DTYPE = np.dtype([("pos", "<f4", 3), ("shape_id", "<i4"), ("dir", "<f4", 3), ("path", "<u4"),
+                         ("power", "<f4", 3), ("depth", "<u4"), ("normal", "<f4", 3), ("reserved", "<f4")])
+
+
 class TraceStats(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_uint64), ("exact_fallback_rays", ctypes.c_uint64)]
 
@@ -103,6 +112,13 @@ SIGNATURES = {
     "rt_scene_set_triangle_materials": [_P, _U32, _U32, _P],
     "rt_scene_add_point_light": [_P, _P, _P, _F32],
     "rt_render": [_P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), _P, _P, _P, ctypes.POINTER(RenderStats)],
+    "rt_photons_trace": [_P, _U64, _U32, _U32, _U32, _U32, ctypes.POINTER(_P), ctypes.POINTER(PhotonTraceStats)],
+    "rt_photon_map_from_points": [_P, _P, _P, _U64, ctypes.POINTER(_P)],
+    "rt_photon_map_build": [_P],
+    "rt_photon_map_count": [_P, ctypes.POINTER(_U64)],
+    "rt_photon_map_get": [_P, _U64, _U64, _P],
+    "rt_photon_map_destroy": [_P],
+    "rt_photon_knn": [_P, _P, _P, _U64, _U32, _F32, _P, _P, _P],
 }
 
 

@@ -141,6 +141,14 @@ class Scene:
                                   ctypes.byref(st)))
         return film, {f: getattr(st, f) for f, _ in N.RenderStats._fields_}
 
+    def trace_photons(self, n: int, max_depth: int = 30, rr_depth: int = 3, seed: int = 0, flags: int = 0):
+        """Scene::generatePhotons + computePhotons: returns (PhotonMap, stats)."""
+        h = ctypes.c_void_p()
+        st = N.PhotonTraceStats()
+        N.check(N.lib().rt_photons_trace(self.handle, n, max_depth, rr_depth, seed, flags, ctypes.byref(h),
+                                         ctypes.byref(st)))
+        return PhotonMap(h), {f: getattr(st, f) for f, _ in N.PhotonTraceStats._fields_}
+
     def close(self):
         if self.handle:
             N.lib().rt_scene_destroy(self.handle)
@@ -211,3 +219,58 @@ def film_mean(film) -> np.ndarray:
     s = (film["sum64"] if "sum64" in film else film["sum"]).double().cpu().numpy().reshape(-1, 3)
     c = film["count"].cpu().numpy().astype(np.float64)
     return s / np.maximum(c, 1)[:, None]
+
+
+class PhotonMap:
+    """Photon map handle: photons, kd-tree build, k-nearest gather (device buffers)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    @classmethod
+    def from_points(cls, ctx: Context, pos_dev, shape_dev=None):
+        h = ctypes.c_void_p()
+        n = pos_dev.numel() // 3
+        N.check(N.lib().rt_photon_map_from_points(ctx.handle, pos_dev.data_ptr(),
+                                                  None if shape_dev is None else shape_dev.data_ptr(), n,
+                                                  ctypes.byref(h)))
+        return cls(h)
+
+    def build(self):
+        N.check(N.lib().rt_photon_map_build(self.handle))
+        return self
+
+    def __len__(self):
+        n = ctypes.c_uint64()
+        N.check(N.lib().rt_photon_map_count(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def photons(self) -> np.ndarray:
+        n = len(self)
+        out = np.zeros(n, dtype=N.PHOTON_DTYPE)
+        if n:
+            N.check(N.lib().rt_photon_map_get(self.handle, 0, n, out.ctypes.data))
+        return out
+
+    def knn(self, queries_dev, k: int, radius: float, shape_dev=None, with_dist=True):
+        import torch
+
+        nq = queries_dev.numel() // 3
+        idx = torch.empty(nq * k, dtype=torch.int32, device="cuda")
+        dist = torch.empty(nq * k, dtype=torch.float32, device="cuda") if with_dist else None
+        cnt = torch.empty(nq, dtype=torch.int32, device="cuda")
+        N.check(N.lib().rt_photon_knn(self.handle, queries_dev.data_ptr(),
+                                      None if shape_dev is None else shape_dev.data_ptr(), nq, k, float(radius),
+                                      idx.data_ptr(), None if dist is None else dist.data_ptr(), cnt.data_ptr()))
+        return idx.view(nq, k), (None if dist is None else dist.view(nq, k)), cnt
+
+    def close(self):
+        if self.handle:
+            N.lib().rt_photon_map_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -182,7 +182,7 @@ int rt_scene_destroy(rt_scene *s)
     cudaStreamSynchronize(s->ctx->stream);
     for (DevBuf *b : {&s->d_nodes, &s->d_tris, &s->d_leafpos, &s->d_ref_boxes, &s->d_ref_sorted, &s->d_ref_pos,
                       &s->d_spheres, &s->scratch.queue, &s->scratch.counters, &s->h2d_rays, &s->d2h_hits, &s->d_mats,
-                      &s->d_tri_mat, &s->d_tri_nidx, &s->d_normals, &s->d_emit_tri, &s->d_emit_cdf, &s->d_plights})
+                      &s->d_tri_mat, &s->d_tri_shape, &s->d_tri_nidx, &s->d_normals, &s->d_emit_tri, &s->d_emit_cdf, &s->d_plights})
         b->release();
     s->rscratch.release();
     delete s;

@@ -30,10 +30,31 @@ int cuda_status(cudaError_t e, const char *what);
         if (rtb_s_ != RT_OK) return rtb_s_;      \
     } while (0)
 
-// Device buffer that remembers its size; grows on demand, never shrinks.
+// Device buffer that remembers its size; grows on demand, never shrinks. Move-only;
+// frees its memory when destroyed.
 struct DevBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : ptr(o.ptr), bytes(o.bytes)
+    {
+        o.ptr = nullptr;
+        o.bytes = 0;
+    }
+    DevBuf &operator=(DevBuf &&o) noexcept
+    {
+        if (this != &o) {
+            release();
+            ptr = o.ptr;
+            bytes = o.bytes;
+            o.ptr = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
     int reserve(size_t n);  // n bytes at least; contents are not preserved
     int upload(const void *src, size_t n, cudaStream_t s);
     void release();
@@ -195,7 +216,7 @@ struct rt_scene {
     bool has_normals = false;
     uint32_t nemit = 0;
     float emit_total = 0.f;
-    rtb::DevBuf d_mats, d_tri_mat, d_tri_nidx, d_normals, d_emit_tri, d_emit_cdf, d_plights;
+    rtb::DevBuf d_mats, d_tri_mat, d_tri_shape, d_tri_nidx, d_normals, d_emit_tri, d_emit_cdf, d_plights;
     rtb::RenderScratch rscratch;
     rtb::SceneView view() const;
     uint64_t device_bytes() const;

@@ -1,0 +1,253 @@
+// Surface reconstruction, materials and BSDF sampling shared by the path tracer
+// (render.cu) and the photon tracer (photon.cu).
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "shading.cuh"
+#include "traverse.cuh"
+
+namespace rtb {
+
+namespace cg = cooperative_groups;
+
+// Device view of everything shading needs.
+struct RenderView {
+    SceneView sv;
+    const rt_material *mats;
+    const uint32_t *tri_mat;
+    const int32_t *tri_shape;  // shape id per triangle (the reference's meshId)
+    const int32_t *tri_nidx;  // 3 per triangle, -1 when the mesh has no normals
+    const float *normals;
+    const uint32_t *emit_tri;
+    const float *emit_cdf;
+    uint32_t nemit;
+    float emit_total;  // sum over emitters of area * luminance(Le)
+    const float4 *plights;  // 2 per light: position, radiant intensity rgb
+    uint32_t nplights;
+    uint32_t nmats;
+    rt_camera cam;
+    uint32_t spp, sample_offset, max_depth, rr_depth, seed, flags;
+    uint64_t total;  // width * height * spp
+};
+
+// Warp-aggregated queue append: one atomic per group of active lanes.
+__device__ __forceinline__ uint32_t append(uint32_t *counter)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+
+__device__ __forceinline__ V3 xform_point(const float *m, V3 p)
+{
+    float x = m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3];
+    float y = m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7];
+    float z = m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11];
+    float w = m[12] * p.x + m[13] * p.y + m[14] * p.z + m[15];
+    float iw = 1.0f / w;
+    return v3(x * iw, y * iw, z * iw);
+}
+__device__ __forceinline__ V3 xform_vec(const float *m, V3 v)
+{
+    return v3(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z,
+              m[8] * v.x + m[9] * v.y + m[10] * v.z);
+}
+
+struct Surface {
+    V3 p, n, perr;  // position, shading normal (faces the ray for triangles), error bound
+    uint32_t mat;
+    int32_t shape;  // SurfaceInteraction::shapeId: mesh id for triangles, shape index for spheres
+    bool emissive_tri;
+    float area_cos;  // for MIS: |cos| at the emitter
+};
+
+// Triangle / sphere hit -> surface (Triangle::intersect, Triangle.cu:319-428;
+// Sphere::intersect, Sphere.cu:277-355).
+__device__ __forceinline__ Surface surface_at(const RenderView &rv, const rt_hit &h, V3 o, V3 d, bool compat)
+{
+    Surface s;
+    if (h.prim & RT_PRIM_SHAPE) {
+        const SphereRecord &sr = rv.sv.spheres[h.prim & ~RT_PRIM_SHAPE];
+        V3 c = v3(sr.o2w[3], sr.o2w[7], sr.o2w[11]);
+        V3 p = o + d * h.t;
+        V3 n = normalize(p - c);
+        s.p = c + n * sr.radius;
+        s.n = n;  // outward: -cross(dpdu, dpdv) of the reference parametrisation (Sphere.cu:159-160)
+        const float eb5 = error_bound(5);
+        s.perr = (vabs(s.p - c) + vabs(c)) * eb5;
+        s.mat = sr.material;
+        s.shape = sr.shape_id;
+        s.emissive_tri = false;
+        s.area_cos = 0.f;
+        return s;
+    }
+    const TriRecord tr = rv.sv.tris[rv.sv.leafpos[h.prim]];
+    V3 p0 = v3(tr.v0.x, tr.v0.y, tr.v0.z), p1 = v3(tr.v1.x, tr.v1.y, tr.v1.z), p2 = v3(tr.v2.x, tr.v2.y, tr.v2.z);
+    float b1 = h.b1, b2 = h.b2, b0 = 1.f - b1 - b2;
+    s.p = p0 * b0 + p1 * b1 + p2 * b2;
+    V3 ng = normalize(cross(p0 - p2, p1 - p2));
+    if (dot(ng, d) > 0) ng = -ng;  // Triangle.cu:370-373
+    s.n = ng;
+    const float eb7 = error_bound(7);
+    s.perr = (vabs(p0 * b0) + vabs(p1 * b1) + vabs(p2 * b2)) * eb7;
+    if (rv.tri_nidx && rv.tri_nidx[3 * h.prim] >= 0) {
+        const int32_t *ni = rv.tri_nidx + 3 * h.prim;
+        V3 n0 = v3(rv.normals[3 * ni[0]], rv.normals[3 * ni[0] + 1], rv.normals[3 * ni[0] + 2]);
+        V3 n1 = v3(rv.normals[3 * ni[1]], rv.normals[3 * ni[1] + 1], rv.normals[3 * ni[1] + 2]);
+        V3 n2 = v3(rv.normals[3 * ni[2]], rv.normals[3 * ni[2] + 1], rv.normals[3 * ni[2] + 2]);
+        V3 ns = normalize(n0 * b0 + n1 * b1 + n2 * b2);
+        s.n = ns;
+        if (compat) s.p = s.p + ns * 0.15f;  // Triangle.cu:418
+    }
+    s.mat = rv.tri_mat[h.prim];
+    s.shape = rv.tri_shape ? rv.tri_shape[h.prim] : 0;
+    s.emissive_tri = true;
+    s.area_cos = fabsf(dot(ng, d));
+    return s;
+}
+
+struct Bsdf {
+    uint32_t type;
+    V3 color;
+    Ggx g;
+    V3 eta, k;
+    float ior;
+};
+
+__device__ __forceinline__ Bsdf load_bsdf(const rt_material &m)
+{
+    Bsdf b;
+    b.type = m.type;
+    b.color = v3(m.color[0], m.color[1], m.color[2]);
+    b.g.ax = sqrtf(m.roughness[0]);
+    b.g.ay = sqrtf(m.roughness[1]);
+    b.eta = v3(m.eta[0], m.eta[1], m.eta[2]);
+    b.k = v3(m.k[0], m.k[1], m.k[2]);
+    b.ior = m.ior;
+    return b;
+}
+
+__device__ __forceinline__ bool is_scattering(uint32_t type)
+{
+    return type == RT_MAT_LAMBERTIAN || type == RT_MAT_TROWBRIDGE || type == RT_MAT_PLAIN;
+}
+__device__ __forceinline__ bool is_specular(uint32_t type)
+{
+    return type == RT_MAT_TROWBRIDGE || type == RT_MAT_DIELECTRIC;  // Material::isSpecular overrides
+}
+
+// f * |cos wi| and pdf, shading space.
+__device__ __forceinline__ V3 bsdf_eval(const Bsdf &b, V3 wo, V3 wi, float &pdf)
+{
+    pdf = 0.f;
+    switch (b.type) {
+    case RT_MAT_LAMBERTIAN:  // LambertianBSDF.cu:32-47
+        pdf = (wo.z * wi.z > 0) ? fabsf(wi.z) * kInvPi : 0.f;
+        return b.color * (kInvPi * abs_cos(wi));
+    case RT_MAT_TROWBRIDGE:
+        pdf = ggx_pdf(b.g, wo, wi);
+        return ggx_eval(b.g, b.color, b.eta, b.k, wo, wi);
+    default:
+        return v3(0, 0, 0);
+    }
+}
+
+// Samples wi; returns f*|cos|/pdf (the reference's sampleDirection value).
+__device__ __forceinline__ V3 bsdf_sample(const Bsdf &b, V3 wo, Pcg &r, bool compat, V3 &wi, float &pdf, bool &delta)
+{
+    delta = false;
+    pdf = 0.f;
+    switch (b.type) {
+    case RT_MAT_LAMBERTIAN: {  // LambertianBSDF.cu:56-75
+        float u1 = pcg_float(r), u2 = pcg_float(r);
+        wi = cosine_hemisphere(u1, u2);
+        pdf = wi.z * kInvPi;
+        return b.color;
+    }
+    case RT_MAT_TROWBRIDGE: {  // TrowbridgeBSDF.cu:207-246
+        float u1 = pcg_float(r), u2 = pcg_float(r);
+        V3 won = normalize(wo);
+        if (fmaxf(b.g.ax, b.g.ay) < 1e-3f) {
+            wi = v3(-won.x, -won.y, won.z);
+            delta = true;
+            float c = abs_cos(wi);
+            V3 F = v3(fresnel_conductor(c, b.eta.x, b.k.x), fresnel_conductor(c, b.eta.y, b.k.y),
+                      fresnel_conductor(c, b.eta.z, b.k.z));
+            return F * (1.0f / c);
+        }
+        V3 h = ggx_sample_h(b.g, won, u1, u2);
+        wi = h * (2 * dot(won, h)) - won;  // reflect (geometricMath.cu:197-200)
+        pdf = ggx_pdf_h(b.g, won, h) / (4 * abs_cos2(won, h));
+        V3 f = ggx_eval(b.g, b.color, b.eta, b.k, won, wi);
+        if (!(pdf > 0)) return v3(0, 0, 0);
+        return f * (1.0f / pdf);
+    }
+    case RT_MAT_DIELECTRIC: {
+        delta = true;
+        float u = pcg_float(r);
+        float c = wo.z / length(wo);
+        if (compat) {
+            // DielectricMaterial.cu:59-77: refraction with probability 0.7, no division
+            if (u < 0.7f) {  // SpecularRefractionBSDF.cu:31-63
+                float ni = 1.f, nt = b.ior;
+                if (c < 0) {
+                    float t = ni;
+                    ni = nt;
+                    nt = t;
+                }
+                float eta = ni / nt;
+                V3 n = (wo.z < 0.f) ? v3(0, 0, -1) : v3(0, 0, 1);
+                float co = dot(n, wo) / length(wo);
+                float s2o = fmaxf(0.f, 1.f - co * co);
+                float s2t = eta * eta * s2o;
+                if (s2t >= 1) return v3(0, 0, 0);
+                float ct = sqrtf(1 - s2t);
+                wi = (-wo) * eta + n * (eta * co - ct);
+                return b.color * (1 - fresnel_dielectric_ref(co, ni, nt));
+            }
+            wi = v3(-wo.x, -wo.y, wo.z);  // SpecularReflectionBSDF.cu:30-41
+            return b.color * fresnel_dielectric_ref(wi.z / length(wi), 1.f, b.ior);
+        }
+        float F = fresnel_dielectric(c, 1.f, b.ior);
+        if (u < F) {
+            wi = v3(-wo.x, -wo.y, wo.z);
+            return b.color;
+        }
+        float ni = 1.f, nt = b.ior;
+        V3 n = v3(0, 0, 1);
+        if (c < 0) {
+            ni = b.ior;
+            nt = 1.f;
+            n = v3(0, 0, -1);
+        }
+        float eta = ni / nt;
+        float co = dot(n, wo) / length(wo);
+        float s2t = eta * eta * fmaxf(0.f, 1.f - co * co);
+        float ct = sqrtf(fmaxf(0.f, 1 - s2t));
+        wi = (-wo) * eta + n * (eta * co - ct);
+        return b.color;
+    }
+    case RT_MAT_MIRROR:  // PerfectReflectionBSDF
+        delta = true;
+        wi = v3(-wo.x, -wo.y, wo.z);
+        return b.color;
+    default:  // Light (NullBSDF) and Plain: no scattering
+        wi = v3(0, 0, 0);
+        return v3(0, 0, 0);
+    }
+}
+
+__device__ __forceinline__ float emitter_pdf(const RenderView &rv, V3 Le, float dist2, float cosl)
+{
+    // p(select tri) / area = luminance(Le) / total; solid-angle conversion dist^2 / |cos|
+    if (!(cosl > 0) || rv.emit_total <= 0) return 0.f;
+    return luminance(Le) / rv.emit_total * dist2 / cosl;
+}
+
+
+// Host: device view of a scene for the shading kernels (uploads render data if needed).
+int make_render_view(rt_scene *s, RenderView &rv);
+
+}  // namespace rtb

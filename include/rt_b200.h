@@ -241,6 +241,64 @@ typedef struct rt_render_stats {
 RT_API int rt_render(rt_scene *scene, const rt_camera *camera, const rt_render_opts *opts, float *sum_rgb,
                      uint32_t *count, double *sum_rgb64, rt_render_stats *stats);
 
+/* --------------------------------------------------------------- photons */
+
+typedef struct rt_photon_map rt_photon_map;
+
+/* Photon record, 64 bytes (light/Photon.cu:9-47): where it landed, the direction it
+ * arrived along, its power, the shading normal, the shape id of the surface it landed on,
+ * and which emitted photon path / bounce produced it. */
+typedef struct rt_photon {
+    float pos[3];
+    int32_t shape_id;
+    float dir[3];
+    uint32_t path;   /* index of the emitted photon */
+    float power[3];
+    uint32_t depth;  /* bounce at which it was stored (0 = first hit) */
+    float normal[3];
+    float reserved;
+} rt_photon;
+
+typedef struct rt_photon_trace_stats {
+    uint64_t emitted;
+    uint64_t stored;
+    uint64_t rays;   /* closest-hit rays traced */
+    double ms;
+} rt_photon_trace_stats;
+
+/* Emits n photons from the scene's point lights — light chosen with probability
+ * proportional to its power, direction uniform on the sphere, power I*4pi / n_l / p_l
+ * (Scene::generatePhotons, Scene.cu:989-1018; PointLight::sampleLight, PointLight.cu:68-95)
+ * — and traces them up to max_depth bounces, storing a photon at every hit on a scattering
+ * material with power = carried light * path throughput before that hit's BSDF sample;
+ * the path continues by BSDF sampling with Russian roulette after rr_depth (computePhotons /
+ * samplePhotonIntersections, integration/photonDispersion.cu:26-172). Photons are ordered
+ * by (path, depth), independent of scheduling. flags: RT_RENDER_COMPAT as for rt_render. */
+RT_API int rt_photons_trace(rt_scene *scene, uint64_t n, uint32_t max_depth, uint32_t rr_depth, uint32_t seed,
+                            uint32_t flags, rt_photon_map **out, rt_photon_trace_stats *stats);
+
+/* A photon map over caller-given points (device pointers: 3 floats per point, optional
+ * shape ids) — the same structure rt_photons_trace builds. */
+RT_API int rt_photon_map_from_points(rt_context *ctx, const float *pos_dev, const int32_t *shape_dev, uint64_t n,
+                                     rt_photon_map **out);
+
+/* Builds the balanced kd-tree (median split on the largest extent, kdtree.h:78-108). */
+RT_API int rt_photon_map_build(rt_photon_map *map);
+
+RT_API int rt_photon_map_count(rt_photon_map *map, uint64_t *n);
+/* Copies photons [first, first+n) to host memory. */
+RT_API int rt_photon_map_get(rt_photon_map *map, uint64_t first, uint64_t n, rt_photon *out_host);
+RT_API int rt_photon_map_destroy(rt_photon_map *map);
+
+/* k nearest photons per query point within `radius` (distance < radius, same shape id
+ * unless the query's id is -1), as nn::KDTree::nearest_neighbors + Scene::search_nearest
+ * (kdtree.h:111-197, Scene.cu:704-722). Device pointers: queries 3 floats each,
+ * shape_ids (nullable = -1 for all), out_idx nq*k photon indices (-1 padded), out_dist
+ * nq*k distances (nullable), out_count nq. Results are ordered by distance. k <= 128. */
+RT_API int rt_photon_knn(rt_photon_map *map, const float *queries_dev, const int32_t *shape_ids_dev, uint64_t nq,
+                         uint32_t k, float radius, int32_t *out_idx_dev, float *out_dist_dev,
+                         uint32_t *out_count_dev);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,92 @@
+"""Photon map k-nearest gathering and photon tracing through the C ABI, against the
+reference's own kd-tree (nn::KDTree, compiled from its sources) and the C restatement."""
+import importlib
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+N = importlib.import_module("2023_render_engine_b200._native")
+S = importlib.import_module("2023_render_engine_b200.scenes")
+
+
+def _sets(idx, cnt):
+    return [set(idx[i, :cnt[i]].tolist()) for i in range(len(cnt))]
+
+
+def test_knn_matches_golden(core, gpu_ctx):
+    import torch
+
+    g = np.load(GOLDEN / "knn_small.npz")
+    pos = torch.from_numpy(g["pos"]).cuda()
+    shp = torch.from_numpy(g["shape"]).cuda()
+    m = core.PhotonMap.from_points(gpu_ctx, pos, shp).build()
+    idx, dist, cnt = m.knn(torch.from_numpy(g["q"]).cuda(), int(g["k"]), float(g["radius"]),
+                           torch.from_numpy(g["qshape"]).cuda())
+    idx, cnt = idx.cpu().numpy(), cnt.cpu().numpy()
+    assert np.array_equal(cnt, g["count"].astype(np.int32))
+    assert _sets(idx, cnt) == _sets(g["idx"], g["count"])
+    d = dist.cpu().numpy()
+    for i in range(len(cnt)):
+        assert np.all(np.diff(d[i, :cnt[i]]) >= 0)  # ascending
+
+
+@pytest.mark.parametrize("n,k,radius,with_shape", [(1, 1, 10.0, False), (7, 50, 10.0, False),
+                                                    (100000, 1, 100.0, False), (100000, 50, 0.1, True),
+                                                    (300000, 100, 100.0, True), (50000, 128, 0.3, True)])
+def test_knn_matches_reference_kdtree(core, gpu_ctx, refo, restated, n, k, radius, with_shape):
+    import torch
+    from oracle import bindings
+
+    rng = np.random.default_rng(n + k)
+    pos = rng.normal(0, 0.5, (n, 3)).astype(np.float32)
+    pos[: n // 10] = np.round(pos[: n // 10], 2)  # a slab of duplicated coordinates
+    shp = rng.integers(0, 3, n).astype(np.int32)
+    q = rng.normal(0, 0.5, (2000, 3)).astype(np.float32)
+    qs = rng.integers(-1, 3, 2000).astype(np.int32) if with_shape else None
+    m = core.PhotonMap.from_points(gpu_ctx, torch.from_numpy(pos).cuda(), torch.from_numpy(shp).cuda()).build()
+    gi, gd, gc = m.knn(torch.from_numpy(q).cuda(), k, radius, None if qs is None else torch.from_numpy(qs).cuda())
+    gi, gd, gc = gi.cpu().numpy(), gd.cpu().numpy(), gc.cpu().numpy()
+    kd = bindings.RefKdTree(refo, pos, shp)
+    ri, rc = kd.knn(q, k, radius, qs)
+    assert np.array_equal(gc, rc.astype(np.int32))
+    # the sorted distances equal the brute-force restatement's; the sets equal the
+    # reference's except for members tied at the k-th distance
+    bi, bd, bc = restated.knn(pos, shp, q, qs, k, radius)
+    for i in range(len(q)):
+        assert np.array_equal(gd[i, :gc[i]], bd[i, :bc[i]])
+        a, b = set(gi[i, :gc[i]].tolist()), set(ri[i, :rc[i]].tolist())
+        if a != b:
+            kth = bd[i, bc[i] - 1]
+            dd = np.sqrt(((pos[list(a ^ b)] - q[i]) ** 2).sum(1))
+            assert np.allclose(dd, kth, rtol=1e-6, atol=0)
+
+
+def test_photon_trace_and_gather_on_cornell(core, gpu_ctx):
+    import torch
+
+    cfg = importlib.import_module("2023_render_engine_b200.configs")
+    sc, cam, p = cfg.build_config0(gpu_ctx, 32, 32)
+    sc.add_point_light((0.0, 0.9, 0.0), (1.0, 1.0, 1.0), 5.0)
+    sc.commit()
+    pm, st = sc.trace_photons(200000, max_depth=30, seed=1)
+    ph = pm.photons()
+    assert st["emitted"] == 200000 and st["stored"] == len(ph) > 200000 * 0.5
+    keys = ph["path"].astype(np.uint64) << 8 | ph["depth"]
+    assert np.all(np.diff(keys.astype(np.int64)) > 0)  # (path, depth) order, no duplicates
+    assert np.isfinite(ph["power"]).all() and (ph["power"] >= 0).all()
+    # first-bounce photons of one light carry I * 4 pi / n (one light: p_l = 1)
+    first = ph[ph["depth"] == 0]
+    assert np.allclose(first["power"], 5.0 * 4 * np.pi / 200000, rtol=1e-5)
+    # photons lie on the scene's surfaces: inside the box
+    assert (np.abs(ph["pos"]) <= 1.0001).all()
+    pm2, _ = sc.trace_photons(200000, max_depth=30, seed=1)
+    assert np.array_equal(pm2.photons(), ph)  # deterministic
+    pm.build()
+    q = torch.from_numpy(ph["pos"][:1000].copy()).cuda()
+    idx, dist, cnt = pm.knn(q, 50, 100.0)
+    assert (cnt.cpu().numpy() == 50).all()
+    assert (idx.cpu().numpy()[:, 0] >= 0).all()
