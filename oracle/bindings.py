@@ -321,3 +321,24 @@ class PathTracerOracle:
                           ctypes.addressof(camera), spp, sample_offset, max_depth, rr_depth, seed, flags, p0, p1,
                           s.ctypes.data, c.ctypes.data, threads)
         return s, c
+
+    def trace_photons(self, tri_shape, sph_shape, plights, n, max_depth=30, rr_depth=3, seed=0, flags=0, cap=None):
+        """plights: list of (pos, rgb, intensity). Returns photons as a structured array."""
+        import importlib
+
+        N = importlib.import_module("2023_render_engine_b200._native")
+        L = self.L
+        L.pto_trace_photons.argtypes = [P, P, P, P, P, U32, P, U32, P, P, U32, U64, U32, U32, U32, U32, P, U64]
+        L.pto_trace_photons.restype = U64
+        pl = np.array([list(p) + list(np.asarray(c, np.float64) * i) for p, c, i in plights], np.float32)
+        rgbi = np.array([list(c) + [i] for p, c, i in plights], np.float32)
+        ts = _np(tri_shape, np.int32)
+        ss = _np(sph_shape, np.int32) if len(sph_shape) else np.zeros(1, np.int32)
+        cap = cap or 8 * n
+        out = np.zeros(cap, dtype=N.PHOTON_DTYPE)
+        got = L.pto_trace_photons(self.bvh.h if self.bvh is not None else None, self.tri_mat.ctypes.data,
+                                  ts.ctypes.data, self.sph.ctypes.data if len(self.sph) else None, ss.ctypes.data,
+                                  len(self.sph), ctypes.cast(self.mats, ctypes.c_void_p), self.nmat, pl.ctypes.data,
+                                  rgbi.ctypes.data, len(plights), n, max_depth, rr_depth, seed, flags,
+                                  out.ctypes.data, cap)
+        return out[:min(got, cap)]

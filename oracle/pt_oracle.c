@@ -715,3 +715,140 @@ int pto_render(const rto_bvh *bvh, const uint32_t *tri_mat, const pto_sphere *sp
     free(base.ecdf);
     return 0;
 }
+
+
+/* ------------------------------------------------------------------ photons */
+
+/* Photon tracing with the renderer's per-photon PCG streams (Scene::generatePhotons,
+ * Scene.cu:989-1018; PointLight::sampleLight, PointLight.cu:68-95; computePhotons /
+ * samplePhotonIntersections, photonDispersion.cu:26-172). Output photons in (path, depth)
+ * order, 16 floats each: pos[3], shape, dir[3], path, power[3], depth, normal[3], 0. */
+uint64_t pto_trace_photons(const rto_bvh *bvh, const uint32_t *tri_mat, const int32_t *tri_shape,
+                           const pto_sphere *sph, const int32_t *sph_shape, uint32_t nsph, const pto_material *mats,
+                           uint32_t nmat, const float *plights, const float *plight_rgbi, uint32_t npl, uint64_t n,
+                           uint32_t max_depth, uint32_t rr_depth, uint32_t seed, uint32_t flags, float *out,
+                           uint64_t cap)
+{
+    ctx_t c;
+    memset(&c, 0, sizeof(c));
+    c.bvh = bvh;
+    c.tri_mat = tri_mat;
+    c.sph = sph;
+    c.nsph = nsph;
+    c.mats = mats;
+    c.nmat = nmat;
+    const int compat = (flags & F_COMPAT) != 0;
+    float *power = (float *)malloc(sizeof(float) * npl);
+    float total = 0.f;
+    for (uint32_t l = 0; l < npl; l++) {
+        const float *q = plight_rgbi + 4 * l;
+        power[l] = (q[0] * q[3] * 4.0f * PI_F) + (q[1] * q[3] * 4.0f * PI_F) + (q[2] * q[3] * 4.0f * PI_F);
+        total += power[l];
+    }
+    uint32_t *sel = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    uint64_t *perl = (uint64_t *)calloc(npl, sizeof(uint64_t));
+    for (uint64_t i = 0; i < n; i++) {
+        pcg r = pcg_init((uint32_t)i, 0xFFFFFFFFu, seed ^ 0x9E3779B9u);
+        float u = pcg_f(&r);
+        uint32_t l = npl - 1;
+        for (uint32_t k = 0; k < npl; k++) {
+            u -= power[k] / total;
+            if (u <= 0) {
+                l = k;
+                break;
+            }
+        }
+        sel[i] = l;
+        perl[l]++;
+    }
+    uint64_t stored = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        pcg r = pcg_init((uint32_t)i, 0xFFFFFFFFu, seed ^ 0x9E3779B9u);
+        (void)pcg_f(&r);
+        uint32_t l = sel[i];
+        float u1 = pcg_f(&r), u2 = pcg_f(&r);
+        float phi = 2 * PI_F * u1, th = acosf(2 * u2 - 1);
+        v3 d = V(sinf(th) * cosf(phi), sinf(th) * sinf(phi), cosf(th));
+        const float *lp = plights + 6 * l;
+        float scale = (4 * PI_F) / (float)perl[l] / (power[l] / total);
+        v3 carry = V(lp[3] * scale, lp[4] * scale, lp[5] * scale);
+        v3 o = V(lp[0], lp[1], lp[2]);
+        v3 beta = V(1, 1, 1);
+        for (uint32_t depth = 0; depth < max_depth; depth++) {
+            float t, b1, b2;
+            int32_t prim = closest(&c, o, d, INFINITY, 0, &t, &b1, &b2);
+            if (prim < 0) break;
+            v3 P, nn, perr;
+            uint32_t mid;
+            int32_t shape;
+            if (prim & 0x40000000) {
+                uint32_t si = (uint32_t)(prim & ~0x40000000);
+                const pto_sphere *sp = &sph[si];
+                v3 ctr = V(sp->o2w[3], sp->o2w[7], sp->o2w[11]);
+                v3 p = add(o, mul(d, t));
+                nn = norm3(sub(p, ctr));
+                P = add(ctr, mul(nn, sp->radius));
+                perr = mul(add(vabs3(sub(P, ctr)), vabs3(ctr)), eb(5));
+                mid = sp->material;
+                shape = sph_shape[si];
+            } else {
+                float vv[9];
+                rto_triangle_vertices(bvh, (uint32_t)prim, vv);
+                v3 p0 = V(vv[0], vv[1], vv[2]), p1 = V(vv[3], vv[4], vv[5]), p2 = V(vv[6], vv[7], vv[8]);
+                float b0 = 1.f - b1 - b2;
+                P = add(add(mul(p0, b0), mul(p1, b1)), mul(p2, b2));
+                v3 ng = norm3(cross3(sub(p0, p2), sub(p1, p2)));
+                if (dot3(ng, d) > 0) ng = neg(ng);
+                nn = ng;
+                perr = mul(add(add(vabs3(mul(p0, b0)), vabs3(mul(p1, b1))), vabs3(mul(p2, b2))), eb(7));
+                mid = tri_mat[prim];
+                shape = tri_shape[prim];
+            }
+            if (mid >= nmat) mid = nmat - 1;
+            const pto_material *m = &mats[mid];
+            if (is_scat(m->type)) {
+                if (stored < cap) {
+                    float *ph = out + 16 * stored;
+                    v3 pw = vmul(carry, beta);
+                    uint32_t u32;
+                    ph[0] = P.x, ph[1] = P.y, ph[2] = P.z;
+                    memcpy(&ph[3], &shape, 4);
+                    ph[4] = d.x, ph[5] = d.y, ph[6] = d.z;
+                    u32 = (uint32_t)i;
+                    memcpy(&ph[7], &u32, 4);
+                    ph[8] = pw.x, ph[9] = pw.y, ph[10] = pw.z;
+                    memcpy(&ph[11], &depth, 4);
+                    ph[12] = nn.x, ph[13] = nn.y, ph[14] = nn.z, ph[15] = 0.f;
+                }
+                stored++;
+            }
+            v3 tt, bb;
+            onb(nn, &tt, &bb);
+            v3 wow = neg(d);
+            v3 wo = V(dot3(wow, tt), dot3(wow, bb), dot3(wow, nn));
+            v3 Le = (m->type == M_LIGHT) ? mul(mat_color(m), m->intensity) : V(0, 0, 0);
+            v3 wil;
+            float pdfb;
+            int delta;
+            v3 f = bsdf_sample(m, wo, &r, compat, &wil, &pdfb, &delta);
+            carry = add(carry, vmul(beta, Le));
+            beta = vmul(beta, f);
+            int finished = black(f);
+            if (!finished && is_scat(m->type) && depth > rr_depth) {
+                float q = fmaxf(0.05f, 1.f - lum(beta));
+                if (pcg_f(&r) < q)
+                    finished = 1;
+                else
+                    beta = mul(beta, 1.f / (1.f - q));
+            }
+            if (finished || depth + 1 >= max_depth) break;
+            v3 wiw = add(add(mul(tt, wil.x), mul(bb, wil.y)), mul(nn, wil.z));
+            o = spawn(P, nn, perr, wiw);
+            d = wiw;
+        }
+    }
+    free(power);
+    free(sel);
+    free(perl);
+    return stored;
+}

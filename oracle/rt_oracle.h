@@ -80,6 +80,15 @@ int pto_render(const rto_bvh *bvh, const uint32_t *tri_mat, const pto_sphere *sp
                uint32_t spp, uint32_t sample_offset, uint32_t max_depth, uint32_t rr_depth, uint32_t seed,
                uint32_t flags, uint32_t pix_begin, uint32_t pix_end, double *sum, uint32_t *count, int nthreads);
 
+/* Photon tracing restated (pt_oracle.c): returns the number of photons stored (written up
+ * to cap, 16 floats each in rt_photon layout) in (path, depth) order. plights: 6 floats per
+ * light (position, rgb*intensity); plight_rgbi: 4 floats per light (rgb, intensity). */
+uint64_t pto_trace_photons(const rto_bvh *bvh, const uint32_t *tri_mat, const int32_t *tri_shape,
+                           const pto_sphere *sph, const int32_t *sph_shape, uint32_t nsph, const pto_material *mats,
+                           uint32_t nmat, const float *plights, const float *plight_rgbi, uint32_t npl, uint64_t n,
+                           uint32_t max_depth, uint32_t rr_depth, uint32_t seed, uint32_t flags, float *out,
+                           uint64_t cap);
+
 #ifdef __cplusplus
 }
 #endif
