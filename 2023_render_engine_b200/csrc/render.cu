@@ -101,13 +101,16 @@ __device__ void start_path(const RenderView &rv, const Buffers &bf, int b, uint3
 }
 
 // Takes the next camera sample (if any) and appends it to buffer b.
+// Sample indices are handed out with one atomic per group of converged lanes.
 __device__ __forceinline__ void regenerate(const RenderView &rv, const Buffers &bf, int b)
 {
-    unsigned long long g = atomicAdd(cnt64(bf.cnt, 8), 1ull);
+    cg::coalesced_group grp = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (grp.thread_rank() == 0) base = atomicAdd(cnt64(bf.cnt, 8), (unsigned long long)grp.size());
+    const unsigned long long g = grp.shfl(base, 0) + grp.thread_rank();
     if (g >= rv.total) return;
     uint32_t q = append(bf.cnt + b);
     start_path(rv, bf, b, q, g);
-    atomicAdd(cnt64(bf.cnt, 14), 1ull);
 }
 
 __global__ void __launch_bounds__(kB) k_start(RenderView rv, Buffers bf)
@@ -136,6 +139,7 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
 {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = min(bf.cnt[cur], bf.cap);
+    if (q == 0) atomicAdd(cnt64(bf.cnt, 10), (unsigned long long)n);  // extension rays of this wave
     if (q >= n) return;
     const int nxt = cur ^ 1;
     const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
@@ -239,7 +243,6 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
                 V3 c = beta_in * fl * Li * w;
                 V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
                 push_shadow(bf, so, wl, dist, c, target, compat);
-                atomicAdd(cnt64(bf.cnt, 12), 1ull);
             }
             if (nee_area) {
                 float u0 = pcg_float(rng), u1 = pcg_float(rng), u2 = pcg_float(rng);
@@ -277,7 +280,6 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
                         V3 c = beta_in * fl * Lel * (w / pl);
                         V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
                         push_shadow(bf, so, wl, dist * (1.0f - 1e-4f), c, target, false);
-                        atomicAdd(cnt64(bf.cnt, 12), 1ull);
                     }
                 }
             }
@@ -296,13 +298,13 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
         bf.retire[target & ~kRetireTarget] = make_float4(L.x, L.y, L.z, __uint_as_float(pix));
         regenerate(rv, bf, nxt);
     }
-    atomicAdd(cnt64(bf.cnt, 10), 1ull);
 }
 
 __global__ void __launch_bounds__(kB) k_shadow(RenderView rv, Buffers bf, int nxt)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = min(bf.cnt[2], bf.scap);
+    if (i == 0) atomicAdd(cnt64(bf.cnt, 12), (unsigned long long)n);  // shadow rays of this wave
     if (i >= n) return;
     float4 r0 = reinterpret_cast<const float4 *>(bf.srays)[2 * i];
     float4 r1 = reinterpret_cast<const float4 *>(bf.srays)[2 * i + 1];
@@ -618,8 +620,8 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
         stats->extension_rays = v;
         std::memcpy(&v, hc + 12, 8);
         stats->shadow_rays = v;
-        std::memcpy(&v, hc + 14, 8);
-        stats->camera_rays = v;
+        std::memcpy(&v, hc + 8, 8);
+        stats->camera_rays = std::min<uint64_t>(v, total);
         stats->waves = waves;
         stats->ms = ms;
     }
