@@ -48,7 +48,8 @@ struct Buffers {
     float4 *retire;    // L.xyz, pixel index bits
     uint32_t cap, scap;
     // counters (uint32): [0],[1] queue sizes of buffers 0/1, [2] shadow count, [3] retire count,
-    // [4] status; u64 at [8]: next sample, [10] extension rays, [12] shadow rays, [14] camera rays
+    // [4] status, [5] shadow-kernel work counter; u64 at [8]: next sample, [10] extension rays,
+    // [12] shadow rays
     uint32_t *cnt;
 };
 
@@ -300,37 +301,39 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
     }
 }
 
+// Any-hit test of the wave's shadow rays (persistent warps, counter cnt[5]); an unoccluded
+// ray adds its contribution to the path it belongs to.
 __global__ void __launch_bounds__(kB) k_shadow(RenderView rv, Buffers bf, int nxt)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = min(bf.cnt[2], bf.scap);
-    if (i == 0) atomicAdd(cnt64(bf.cnt, 12), (unsigned long long)n);  // shadow rays of this wave
-    if (i >= n) return;
-    float4 r0 = reinterpret_cast<const float4 *>(bf.srays)[2 * i];
-    float4 r1 = reinterpret_cast<const float4 *>(bf.srays)[2 * i + 1];
-    WatertightRay w = make_watertight(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w);
-    const bool skip_transparent = __float_as_uint(r1.w) & 1u;
-    Best best{INFINITY, -1, 0u, 0.f, 0.f, INFINITY};
-    bool occ = false;
-    if (rv.sv.ntri > 0) {
-        traverse_bvh8(rv.sv, w, r1.x, r1.y, r1.z, skip_transparent, true, best);
-        occ = best.prim >= 0 && best.t < r0.w;
-    }
-    if (!occ && rv.sv.nspheres) {
-        float t = r0.w;
-        int32_t prim = -1;
-        float b1 = 0, b2 = 0;
-        intersect_spheres(rv.sv, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w, skip_transparent, t, prim, b1, b2);
-        occ = prim >= 0 && t < r0.w;
-    }
-    if (occ) return;
-    float4 c = bf.scontrib[i];
-    uint32_t target = __float_as_uint(c.w);
-    float *dst = (target & kRetireTarget) ? reinterpret_cast<float *>(bf.retire + (target & ~kRetireTarget))
-                                           : reinterpret_cast<float *>(bf.st1[nxt] + target);
-    atomicAdd(dst + 0, c.x);
-    atomicAdd(dst + 1, c.y);
-    atomicAdd(dst + 2, c.z);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(cnt64(bf.cnt, 12), (unsigned long long)n);  // stats
+    persistent_traverse(
+        rv.sv, n, bf.cnt + 5, true,
+        [&](uint32_t i, Trav &T) {
+            const float4 r0 = reinterpret_cast<const float4 *>(bf.srays)[2 * i];
+            const float4 r1 = reinterpret_cast<const float4 *>(bf.srays)[2 * i + 1];
+            trav_init(T, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w);
+            T.shadow = (__float_as_uint(r1.w) & 1u) != 0;
+        },
+        [&](uint32_t i, Trav &T) {
+            const float tmax = T.w.tmax;
+            bool occ = T.best.prim >= 0 && T.best.t < tmax;
+            if (!occ && rv.sv.nspheres) {
+                float t = tmax;
+                int32_t prim = -1;
+                float b1 = 0, b2 = 0;
+                intersect_spheres(rv.sv, T.w.ox, T.w.oy, T.w.oz, T.dx, T.dy, T.dz, tmax, T.shadow, t, prim, b1, b2);
+                occ = prim >= 0 && t < tmax;
+            }
+            if (occ) return;
+            const float4 c = bf.scontrib[i];
+            const uint32_t target = __float_as_uint(c.w);
+            float *dst = (target & kRetireTarget) ? reinterpret_cast<float *>(bf.retire + (target & ~kRetireTarget))
+                                                   : reinterpret_cast<float *>(bf.st1[nxt] + target);
+            atomicAdd(dst + 0, c.x);
+            atomicAdd(dst + 1, c.y);
+            atomicAdd(dst + 2, c.z);
+        });
 }
 
 __global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t *count, double *sum64)
@@ -575,6 +578,13 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
     RTB_CUDA(cudaEventRecord(e0, st));
     RTB_CUDA(cudaMemsetAsync(bf.cnt, 0, 256, st));
     const unsigned blocks = cap / kB;
+    static unsigned shadow_resident = 0;
+    if (!shadow_resident) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shadow, kB, 0);
+        shadow_resident = (unsigned)std::max(1, s->ctx->sm_count * std::max(per_sm, 1));
+    }
+    const unsigned shadow_blocks = std::min<unsigned>(shadow_resident, (scap + kB - 1) / kB);
     k_start<<<blocks, kB, 0, st>>>(rv, bf);
     RTB_CUDA(cudaGetLastError());
     const uint32_t trace_flags = (opts->flags & RT_RENDER_EXACT_TRACE) ? 0u : RT_TRACE_FAST;
@@ -588,10 +598,10 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
                                                s->scratch.queue.as<uint32_t>(), s->scratch.counters.as<uint32_t>(),
                                                st));
             RTB_CUDA(cudaMemsetAsync(bf.cnt + ((cur ^ 1)), 0, 4, st));
-            RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 8, st));
+            RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 16, st));
             k_shade<<<blocks, kB, 0, st>>>(rv, bf, cur);
             RTB_CUDA(cudaGetLastError());
-            k_shadow<<<(scap + kB - 1) / kB, kB, 0, st>>>(rv, bf, cur ^ 1);
+            k_shadow<<<shadow_blocks, kB, 0, st>>>(rv, bf, cur ^ 1);
             RTB_CUDA(cudaGetLastError());
             k_retire<<<blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64);
             RTB_CUDA(cudaGetLastError());

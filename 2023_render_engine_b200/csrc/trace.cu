@@ -17,6 +17,8 @@
 // does, for rays with tmax = inf and no zero direction component) and detects (b); the
 // remaining rays are queued for a replay of the reference traversal itself
 // (k_trace_exact).
+#include <algorithm>
+
 #include "traverse.cuh"
 
 namespace rtb {
@@ -25,37 +27,31 @@ namespace {
 
 constexpr int kBlock = 128;
 
-__global__ void __launch_bounds__(kBlock) k_trace_closest(SceneView v, const rt_ray *__restrict__ rays, uint64_t n,
-                                                          const uint32_t *__restrict__ n_dev, rt_hit *__restrict__ hits,
-                                                          uint32_t flags, uint32_t *__restrict__ queue,
-                                                          uint32_t queue_cap, uint32_t *__restrict__ counters)
+// Decides, for a finished ray, whether the kernel's answer provably equals the reference's
+// (see the file comment) and writes the hit, or queues the ray for k_trace_exact.
+__device__ __forceinline__ void closest_epilogue(const SceneView &v, uint64_t i, const Trav &T, uint32_t flags,
+                                                 rt_hit *__restrict__ hits, uint32_t *__restrict__ queue,
+                                                 uint32_t queue_cap, uint32_t *__restrict__ counters)
 {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n_dev) n = min((uint64_t)*n_dev, n);
-    if (i >= n) return;
-    float4 ra, rb;
-    load_ray(rays, i, ra, rb);
     const bool shadow = (flags & RT_TRACE_SHADOW) != 0;
-    WatertightRay w = make_watertight(ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w);
-    Best best{INFINITY, -1, 0u, 0.f, 0.f, INFINITY};
-    bool ok = true;
-    if (v.ntri > 0) ok = traverse_bvh8(v, w, rb.x, rb.y, rb.z, shadow, false, best);
+    const Best &best = T.best;
+    const float ox = T.w.ox, oy = T.w.oy, oz = T.w.oz, tmax = T.w.tmax;
     bool exact_needed = false, replay = false;
-    if (!ok) {
+    if (!T.ok) {
         exact_needed = replay = true;
         atomicCAS(counters + 1, 0u, (uint32_t)DEV_STACK_OVERFLOW);
     } else if (!(flags & RT_TRACE_FAST) && best.prim >= 0) {
         if (best.minblock < best.t) {
             exact_needed = replay = true;
-        } else if (!(ra.w == INFINITY) || rb.x == 0.f || rb.y == 0.f || rb.z == 0.f) {
+        } else if (!(tmax == INFINITY) || T.dx == 0.f || T.dy == 0.f || T.dz == 0.f) {
             exact_needed = true;  // ancestor walk in k_trace_exact
         } else {
             const float4 *p = reinterpret_cast<const float4 *>(v.tris + v.leafpos[best.prim]);
             float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
             float lx = fminf(fminf(a.x, b.x), c.x), ly = fminf(fminf(a.y, b.y), c.y), lz = fminf(fminf(a.z, b.z), c.z);
             float hx = fmaxf(fmaxf(a.x, b.x), c.x), hy = fmaxf(fmaxf(a.y, b.y), c.y), hz = fmaxf(fmaxf(a.z, b.z), c.z);
-            float ix = fdiv(1.0f, rb.x), iy = fdiv(1.0f, rb.y), iz = fdiv(1.0f, rb.z);
-            if (!ref_box_test(lx, ly, lz, hx, hy, hz, ra.x, ra.y, ra.z, ix, iy, iz, ra.w)) exact_needed = true;
+            float ix = fdiv(1.0f, T.dx), iy = fdiv(1.0f, T.dy), iz = fdiv(1.0f, T.dz);
+            if (!ref_box_test(lx, ly, lz, hx, hy, hz, ox, oy, oz, ix, iy, iz, tmax)) exact_needed = true;
         }
     }
     if (exact_needed) {
@@ -70,8 +66,27 @@ __global__ void __launch_bounds__(kBlock) k_trace_closest(SceneView v, const rt_
     float t = best.prim >= 0 ? best.t : INFINITY;
     int32_t prim = best.prim;
     float b1 = best.b1, b2 = best.b2;
-    intersect_spheres(v, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w, shadow, t, prim, b1, b2);
+    intersect_spheres(v, ox, oy, oz, T.dx, T.dy, T.dz, tmax, shadow, t, prim, b1, b2);
     reinterpret_cast<float4 *>(hits)[i] = make_float4(t, __int_as_float(prim), b1, b2);
+}
+
+// Persistent closest-hit kernel: warps fetch rays from counters[3] until all n are done.
+__global__ void __launch_bounds__(kBlock) k_trace_closest(SceneView v, const rt_ray *__restrict__ rays, uint64_t n,
+                                                          const uint32_t *__restrict__ n_dev, rt_hit *__restrict__ hits,
+                                                          uint32_t flags, uint32_t *__restrict__ queue,
+                                                          uint32_t queue_cap, uint32_t *__restrict__ counters)
+{
+    if (n_dev) n = min((uint64_t)*n_dev, n);
+    const bool shadow = (flags & RT_TRACE_SHADOW) != 0;
+    persistent_traverse(
+        v, (uint32_t)n, counters + 3, false,
+        [&](uint32_t i, Trav &T) {
+            float4 ra, rb;
+            load_ray(rays, i, ra, rb);
+            trav_init(T, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w);
+            T.shadow = shadow;
+        },
+        [&](uint32_t i, Trav &T) { closest_epilogue(v, i, T, flags, hits, queue, queue_cap, counters); });
 }
 
 __global__ void __launch_bounds__(kBlock) k_trace_exact(SceneView v, const rt_ray *__restrict__ rays,
@@ -147,12 +162,26 @@ __global__ void __launch_bounds__(kBlock) k_trace_any(SceneView v, const rt_ray 
 
 }  // namespace
 
+// Resident blocks of the persistent closest-hit kernel on this device (queried once).
+static unsigned persistent_blocks()
+{
+    static unsigned cached = 0;
+    if (!cached) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_closest, kBlock, 0);
+        cached = (unsigned)std::max(1, sms * std::max(per_sm, 1));
+    }
+    return cached;
+}
+
 int launch_trace_closest(const SceneView &v, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags,
                          uint32_t *queue, uint32_t queue_cap, uint32_t *counters, cudaStream_t s)
 {
     if (n == 0) return RT_OK;
     RTB_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), s));
-    const uint64_t blocks = (n + kBlock - 1) / kBlock;
+    const uint64_t blocks = std::min<uint64_t>((n + kBlock - 1) / kBlock, persistent_blocks());
     k_trace_closest<<<(unsigned)blocks, kBlock, 0, s>>>(v, rays, n, nullptr, hits, flags, queue, queue_cap, counters);
     RTB_CUDA(cudaGetLastError());
     // Always launched: stack-overflow rays are replayed even in RT_TRACE_FAST mode. It
@@ -167,7 +196,7 @@ int launch_trace_closest_dev(const SceneView &v, const rt_ray *rays, const uint3
 {
     if (cap == 0) return RT_OK;
     RTB_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), s));
-    const uint64_t blocks = ((uint64_t)cap + kBlock - 1) / kBlock;
+    const uint64_t blocks = std::min<uint64_t>(((uint64_t)cap + kBlock - 1) / kBlock, persistent_blocks());
     k_trace_closest<<<(unsigned)blocks, kBlock, 0, s>>>(v, rays, cap, n_dev, hits, flags, queue, cap, counters);
     RTB_CUDA(cudaGetLastError());
     k_trace_exact<<<148 * 4, kBlock, 0, s>>>(v, rays, hits, flags, queue, cap, counters);

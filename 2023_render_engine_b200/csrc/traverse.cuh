@@ -71,104 +71,188 @@ __device__ __forceinline__ void sort8(uint32_t k[8])
     cas(k[3], k[4]);
 }
 
-// Traverses the BVH8; returns false if the stack would overflow (result then unreliable).
-// The eight child boxes are tested in an unrolled block; the triangles of the hit leaves
-// are then tested in a rolled loop so the (long) exact triangle test exists once in the
-// instruction stream.
+// Per-ray traversal state of the BVH8 walk. The walk advances one node per trav_step so a
+// persistent warp can retire finished rays and start new ones lane by lane.
+struct Trav {
+    WatertightRay w;
+    float dx, dy, dz;
+    float ix, iy, iz, oix, oiy, oiz;
+    uint32_t cur;
+    int sp;
+    uint32_t steps;
+    bool ok;
+    bool shadow;  // checkShadow semantics: transparent primitives are skipped
+    Best best;
+    uint32_t st_node[kStack];
+    float st_t[kStack];
+};
+
+__device__ __forceinline__ void trav_init(Trav &T, float ox, float oy, float oz, float dx, float dy, float dz,
+                                          float tmax)
+{
+    T.w = make_watertight(ox, oy, oz, dx, dy, dz, tmax);
+    T.dx = dx;
+    T.dy = dy;
+    T.dz = dz;
+    T.ix = 1.0f / dx;
+    T.iy = 1.0f / dy;
+    T.iz = 1.0f / dz;
+    T.oix = -ox * T.ix;
+    T.oiy = -oy * T.iy;
+    T.oiz = -oz * T.iz;
+    T.cur = 0;
+    T.sp = 0;
+    T.steps = 0;
+    T.ok = true;
+    T.shadow = false;
+    T.best = Best{INFINITY, -1, 0u, 0.f, 0.f, INFINITY};
+}
+
+// Visits node T.cur: tests its eight quantized child boxes (unrolled), the triangles of the
+// hit leaves (rolled, so the long exact triangle test exists once in the instruction
+// stream), pushes the hit interior children far-to-near and selects the next node.
+// Returns true when the ray is done (T.ok = false if the stack or step cap was exceeded).
+__device__ __forceinline__ bool trav_step(const SceneView &v, Trav &T, bool anyhit)
+{
+    const bool shadow = T.shadow;
+    if (++T.steps > v.nnodes + 1) {
+        T.ok = false;
+        return true;
+    }
+    const uint4 *np = reinterpret_cast<const uint4 *>(v.nodes + T.cur);
+    const uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
+    const float sx = __uint_as_float((n0.w & 0xFFu) << 23);
+    const float sy = __uint_as_float(((n0.w >> 8) & 0xFFu) << 23);
+    const float sz = __uint_as_float(((n0.w >> 16) & 0xFFu) << 23);
+    const uint32_t imask = n0.w >> 24;
+    const uint32_t child_base = n1.x, tri_base = n1.y;
+    const uint32_t meta_lo = n1.z, meta_hi = n1.w;
+    // per-axis affine map t = q * (s * inv) + (p * inv - o * inv)
+    const float ax = sx * T.ix, bx = fmaf(__uint_as_float(n0.x), T.ix, T.oix);
+    const float ay = sy * T.iy, by = fmaf(__uint_as_float(n0.y), T.iy, T.oiy);
+    const float az = sz * T.iz, bz = fmaf(__uint_as_float(n0.z), T.iz, T.oiz);
+    const float tlimit = fminf(T.best.t, T.w.tmax);
+    uint32_t keys[8];
+    uint32_t nint = 0, leafmask = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int b = k & 3;
+        const uint32_t meta = byte_of(k < 4 ? meta_lo : meta_hi, b);
+        const float qlx = (float)byte_of(k < 4 ? n2.x : n2.y, b);
+        const float qly = (float)byte_of(k < 4 ? n2.z : n2.w, b);
+        const float qlz = (float)byte_of(k < 4 ? n3.x : n3.y, b);
+        const float qhx = (float)byte_of(k < 4 ? n3.z : n3.w, b);
+        const float qhy = (float)byte_of(k < 4 ? n4.x : n4.y, b);
+        const float qhz = (float)byte_of(k < 4 ? n4.z : n4.w, b);
+        const float t1x = fmaf(qlx, ax, bx), t2x = fmaf(qhx, ax, bx);
+        const float t1y = fmaf(qly, ay, by), t2y = fmaf(qhy, ay, by);
+        const float t1z = fmaf(qlz, az, bz), t2z = fmaf(qhz, az, bz);
+        const float tn = fmaxf(fmaxf(fminf(t1x, t2x), fminf(t1y, t2y)), fmaxf(fminf(t1z, t2z), 0.0f));
+        const float tf = fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fminf(fmaxf(t1z, t2z), tlimit));
+        const bool hit = (meta != 0xFFu) && (tn <= tf);
+        const bool interior = (imask >> k) & 1u;
+        keys[k] = (hit && interior) ? ((__float_as_uint(tn) & ~7u) | (uint32_t)k) : 0xFFFFFFFFu;
+        nint += (hit && interior) ? 1u : 0u;
+        leafmask |= (hit && !interior) ? (1u << k) : 0u;
+    }
+#pragma unroll 1
+    while (leafmask) {
+        const int k = __ffs(leafmask) - 1;
+        leafmask &= leafmask - 1;
+        const uint32_t meta = byte_of(k < 4 ? meta_lo : meta_hi, k & 3);
+        const uint32_t first = tri_base + (meta & 31u), cnt = (meta >> 5) + 1;
+#pragma unroll 1
+        for (uint32_t j = 0; j < cnt; j++) test_triangle(T.w, v.tris, first + j, shadow, T.best);
+        if (anyhit && T.best.prim >= 0) return true;
+    }
+    uint32_t next = 0xFFFFFFFFu;
+    const float tl = fminf(T.best.t, T.w.tmax);
+    if (nint) {
+        sort8(keys);
+#pragma unroll
+        for (int j = 7; j >= 1; j--) {
+            if (j < (int)nint) {
+                const uint32_t slot = keys[j] & 7u;
+                const float tn = __uint_as_float(keys[j] & ~7u);
+                if (tn <= tl) {
+                    if (T.sp >= kStack) {
+                        T.ok = false;
+                        return true;
+                    }
+                    T.st_node[T.sp] = child_base + byte_of(slot < 4 ? meta_lo : meta_hi, slot & 3);
+                    T.st_t[T.sp] = tn;
+                    T.sp++;
+                }
+            }
+        }
+        const uint32_t slot = keys[0] & 7u;
+        if (__uint_as_float(keys[0] & ~7u) <= tl) next = child_base + byte_of(slot < 4 ? meta_lo : meta_hi, slot & 3);
+    }
+    if (next == 0xFFFFFFFFu) {
+#pragma unroll 1
+        while (T.sp > 0) {
+            T.sp--;
+            if (T.st_t[T.sp] <= tl) {
+                next = T.st_node[T.sp];
+                break;
+            }
+        }
+    }
+    if (next == 0xFFFFFFFFu) return true;
+    T.cur = next;
+    return false;
+}
+
+// Whole traversal of one ray; returns false if the stack would overflow (result then
+// unreliable).
 __device__ __forceinline__ bool traverse_bvh8(const SceneView &v, const WatertightRay &w, float dx, float dy, float dz,
                                               bool shadow, bool anyhit, Best &best)
 {
-    const float ix = 1.0f / dx, iy = 1.0f / dy, iz = 1.0f / dz;
-    const float oix = -w.ox * ix, oiy = -w.oy * iy, oiz = -w.oz * iz;
-    uint32_t st_node[kStack];
-    float st_t[kStack];
-    int sp = 0;
-    uint32_t cur = 0;
-    uint32_t steps = 0;
-    const uint32_t cap = v.nnodes + 1;
-#pragma unroll 1
+    Trav T;
+    trav_init(T, w.ox, w.oy, w.oz, dx, dy, dz, w.tmax);
+    T.shadow = shadow;
+    T.best = best;
+    while (!trav_step(v, T, anyhit)) {
+    }
+    best = T.best;
+    return T.ok;
+}
+
+// Persistent-warp driver: every lane runs its own ray; a lane whose ray is done fetches the
+// next ray index from *work (one atomic per fetching warp) until n is exhausted.
+// init(i, T) prepares ray i (trav_init + T.shadow), finish(i, T) consumes the result.
+template <typename Init, typename Finish>
+__device__ __forceinline__ void persistent_traverse(const SceneView &v, uint32_t n, uint32_t *work, bool anyhit,
+                                                    Init init, Finish finish)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t ray = 0xFFFFFFFFu;
+    bool exhausted = false;
+    Trav T;
     for (;;) {
-        if (++steps > cap) return false;
-        const uint4 *np = reinterpret_cast<const uint4 *>(v.nodes + cur);
-        const uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
-        const float sx = __uint_as_float((n0.w & 0xFFu) << 23);
-        const float sy = __uint_as_float(((n0.w >> 8) & 0xFFu) << 23);
-        const float sz = __uint_as_float(((n0.w >> 16) & 0xFFu) << 23);
-        const uint32_t imask = n0.w >> 24;
-        const uint32_t child_base = n1.x, tri_base = n1.y;
-        const uint32_t meta_lo = n1.z, meta_hi = n1.w;
-        // per-axis affine map t = q * (s * inv) + (p * inv - o * inv)
-        const float ax = sx * ix, bx = fmaf(__uint_as_float(n0.x), ix, oix);
-        const float ay = sy * iy, by = fmaf(__uint_as_float(n0.y), iy, oiy);
-        const float az = sz * iz, bz = fmaf(__uint_as_float(n0.z), iz, oiz);
-        const float tlimit = fminf(best.t, w.tmax);
-        uint32_t keys[8];
-        uint32_t nint = 0, leafmask = 0;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int b = k & 3;
-            const uint32_t meta = byte_of(k < 4 ? meta_lo : meta_hi, b);
-            const float qlx = (float)byte_of(k < 4 ? n2.x : n2.y, b);
-            const float qly = (float)byte_of(k < 4 ? n2.z : n2.w, b);
-            const float qlz = (float)byte_of(k < 4 ? n3.x : n3.y, b);
-            const float qhx = (float)byte_of(k < 4 ? n3.z : n3.w, b);
-            const float qhy = (float)byte_of(k < 4 ? n4.x : n4.y, b);
-            const float qhz = (float)byte_of(k < 4 ? n4.z : n4.w, b);
-            const float t1x = fmaf(qlx, ax, bx), t2x = fmaf(qhx, ax, bx);
-            const float t1y = fmaf(qly, ay, by), t2y = fmaf(qhy, ay, by);
-            const float t1z = fmaf(qlz, az, bz), t2z = fmaf(qhz, az, bz);
-            const float tn = fmaxf(fmaxf(fminf(t1x, t2x), fminf(t1y, t2y)), fmaxf(fminf(t1z, t2z), 0.0f));
-            const float tf = fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fminf(fmaxf(t1z, t2z), tlimit));
-            const bool hit = (meta != 0xFFu) && (tn <= tf);
-            const bool interior = (imask >> k) & 1u;
-            keys[k] = (hit && interior) ? ((__float_as_uint(tn) & ~7u) | (uint32_t)k) : 0xFFFFFFFFu;
-            nint += (hit && interior) ? 1u : 0u;
-            leafmask |= (hit && !interior) ? (1u << k) : 0u;
-        }
-        // leaves: one copy of the exact triangle test
-#pragma unroll 1
-        while (leafmask) {
-            const int k = __ffs(leafmask) - 1;
-            leafmask &= leafmask - 1;
-            const uint32_t meta = byte_of(k < 4 ? meta_lo : meta_hi, k & 3);
-            const uint32_t first = tri_base + (meta & 31u), cnt = (meta >> 5) + 1;
-#pragma unroll 1
-            for (uint32_t j = 0; j < cnt; j++) test_triangle(w, v.tris, first + j, shadow, best);
-            if (anyhit && best.prim >= 0) return true;
-        }
-        uint32_t next = 0xFFFFFFFFu;
-        const float tl = fminf(best.t, w.tmax);
-        if (nint) {
-            sort8(keys);
-            // push far to near (register-resident keys: unrolled with a predicate)
-#pragma unroll
-            for (int j = 7; j >= 1; j--) {
-                if (j < (int)nint) {
-                    const uint32_t slot = keys[j] & 7u;
-                    const float tn = __uint_as_float(keys[j] & ~7u);
-                    if (tn <= tl) {
-                        if (sp >= kStack) return false;
-                        st_node[sp] = child_base + byte_of(slot < 4 ? meta_lo : meta_hi, slot & 3);
-                        st_t[sp] = tn;
-                        sp++;
-                    }
-                }
-            }
-            const uint32_t slot = keys[0] & 7u;
-            if (__uint_as_float(keys[0] & ~7u) <= tl) next = child_base + byte_of(slot < 4 ? meta_lo : meta_hi, slot & 3);
-        }
-        if (next == 0xFFFFFFFFu) {
-#pragma unroll 1
-            while (sp > 0) {
-                sp--;
-                if (st_t[sp] <= tl) {
-                    next = st_node[sp];
-                    break;
+        const bool idle = ray == 0xFFFFFFFFu;
+        const unsigned idle_mask = __ballot_sync(0xFFFFFFFFu, idle);
+        if (idle_mask && !exhausted) {
+            const unsigned leader = __ffs(idle_mask) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(work, (uint32_t)__popc(idle_mask));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (base >= n) exhausted = true;
+            if (idle) {
+                const uint32_t mine = base + __popc(idle_mask & ((1u << lane) - 1u));
+                if (mine < n) {
+                    ray = mine;
+                    init(ray, T);
                 }
             }
         }
-        if (next == 0xFFFFFFFFu) return true;
-        cur = next;
+        if (__all_sync(0xFFFFFFFFu, ray == 0xFFFFFFFFu)) break;
+        if (ray != 0xFFFFFFFFu) {
+            if (v.ntri == 0 || trav_step(v, T, anyhit)) {
+                finish(ray, T);
+                ray = 0xFFFFFFFFu;
+            }
+        }
     }
 }
 
