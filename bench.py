@@ -104,6 +104,22 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(vals, world, device="cuda"):
+    """Element-wise max of per-rank timings (every rank calls it in the same order)."""
+    if world == 1:
+        return [float(v) for v in vals]
+    import torch
+
+    t = torch.tensor(vals, device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Per-rank sample seed: every replica renders a statistically independent image."""
+    return base + 97 * rank
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -195,13 +211,6 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
-    def max_over_ranks(vals):
-        if world == 1:
-            return vals
-        t = torch.tensor(vals, device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return [float(x) for x in t]
-
     sc, cam, p = cfgs.build_config1(ctx, args.width, args.height)
     v, f, _ = S.flatten(S.stress_scene())
     W, H = cam.width, cam.height
@@ -220,7 +229,7 @@ def run_ours(args):
 
     # ---- render, film resident on the device
     for w in range(args.warmup):
-        render_step(1000 + w + 97 * rank)
+        render_step(rank_seed(1000 + w, rank))
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -230,7 +239,7 @@ def run_ours(args):
     with ClockSampler(dev) as clk:
         ev0.record(stream)
         for k in range(args.steps):
-            st = render_step(k + 97 * rank)
+            st = render_step(rank_seed(k, rank))
             rays.append(st["extension_rays"] + st["shadow_rays"])
         ev1.record(stream)
         torch.cuda.synchronize()
@@ -246,7 +255,7 @@ def run_ours(args):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for k in range(args.steps):
-        render_step(500 + k + 97 * rank)
+        render_step(rank_seed(500 + k, rank))
         host_sum.copy_(film["sum"], non_blocking=True)
         host_cnt.copy_(film["count"], non_blocking=True)
     e1.record(stream)
@@ -274,7 +283,7 @@ def run_ours(args):
     ms_trace = t0.elapsed_time(t1) / args.steps
     fallback = sc.trace_stats()["exact_fallback_rays"]
 
-    ms, ms_e2e, ms_trace = max_over_ranks([ms, ms_e2e, ms_trace])
+    ms, ms_e2e, ms_trace = max_over_ranks([ms, ms_e2e, ms_trace], world)
     if rank == 0:
         peak, peak_kind = measured_peaks()
         rate = rays_step * world / (ms / 1000) / 1e6
