@@ -342,3 +342,34 @@ class PathTracerOracle:
                                   rgbi.ctypes.data, len(plights), n, max_depth, rr_depth, seed, flags,
                                   out.ctypes.data, cap)
         return out[:min(got, cap)]
+
+
+class RefRender:
+    """The reference's own PathTracerIntegrator on a plane + point-light scene
+    (oracle/_ref/libref_render.so; image size, spp and depth fixed at its compile time)."""
+
+    def __init__(self, path=HERE / "_ref" / "libref_render.so"):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+        L = ctypes.CDLL(str(path))
+        L.refr_config.argtypes = [P, P, P, P]
+        L.refr_render.argtypes = [ctypes.c_char_p, I, P, P, P, P, P]
+        L.refr_render.restype = I
+        self.L = L
+        w, h, s, d = (ctypes.c_int() for _ in range(4))
+        L.refr_config(ctypes.byref(w), ctypes.byref(h), ctypes.byref(s), ctypes.byref(d))
+        self.width, self.height, self.spp, self.depth = w.value, h.value, s.value, d.value
+
+    def render(self, obejota_path, planes, kd):
+        """planes: (n, 12) Plane(corner, axisX, axisY, normal); kd: (n, 3). Returns
+        (mean image (h*w, 3), cameraToWorld 4x4, rasterToCamera 4x4)."""
+        pl = _np(planes, np.float32).reshape(-1, 12)
+        k = _np(kd, np.float32).reshape(-1, 3)
+        out = np.zeros((self.width * self.height, 3), np.float32)
+        c2w = np.zeros(16, np.float32)
+        r2c = np.zeros(16, np.float32)
+        rc = self.L.refr_render(str(obejota_path).encode(), pl.shape[0], pl.ctypes.data, k.ctypes.data,
+                                out.ctypes.data, c2w.ctypes.data, r2c.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("reference render failed")
+        return out, c2w.reshape(4, 4), r2c.reshape(4, 4)

@@ -1,0 +1,145 @@
+// Test infrastructure only: runs the reference renderer's OWN integrator
+// (PathTracerIntegrator::render, integration/PathTracerIntegrator.cu:140-210, with its bounce
+// loop computeSamples, pathTracing.cu:284-414) on a scene the reference can render without
+// its GPU BVH: Plane shapes (shapes/Plane.cu), Lambertian materials and the camera and point
+// lights read by its own .obejota loader (cuda_libraries/FileImporting.cu:466). The
+// reference's compile-time configuration (types.h:41-87) is set for the test image below.
+//
+// Used by the statistical image-parity test only; the product never links it.
+#include <thrust/device_vector.h>
+#include <thrust/host_vector.h>
+#include <thrust/sort.h>
+#include <thrust/transform.h>
+#include <thrust/sequence.h>
+#include <thrust/random.h>
+#include <thrust/functional.h>
+#include <iostream>
+#include <vector>
+#include <random>
+#include <string>
+#include <fstream>
+#include <thread>
+#include <atomic>
+#include <mutex>
+#include <cmath>
+#include <algorithm>
+#include <unordered_map>
+#include <sstream>
+#include <queue>
+#include <memory>
+#include <functional>
+#include <filesystem>
+#include <chrono>
+#include <bit>
+#include <array>
+#include <tuple>
+#include <utility>
+#include <cstdint>
+#include <curand_kernel.h>
+#include <math_constants.h>
+
+// See ref_harness.cu: the reference's global template swap is renamed.
+#define swap ref_swap_
+#include "cuda_libraries/types.h"
+
+// Test image configuration (the reference fixes these at compile time in types.h).
+#undef resolutionX
+#undef resolutionY
+#undef SAMPLES_PER_PIXEL
+#undef MAX_RAY_RECURSION_DEPTH
+#undef CHECK_SUBSURFACE_SCATTERING
+#undef RENDER_MODE
+#define resolutionX 48
+#define resolutionY 48
+#define SAMPLES_PER_PIXEL 32
+#define MAX_RAY_RECURSION_DEPTH 8
+#define CHECK_SUBSURFACE_SCATTERING false
+#define RENDER_MODE PATH_TRACING
+
+// include order of the reference's own mains (cornellBoxGuion.cu:1-22)
+#include "shapes/Sphere.cu"
+#include "shapes/Plane.cu"
+#include "shapes/Triangle.cu"
+#include "integration/Scene.cu"
+#include "integration/PathTracerIntegrator.cu"
+#include "integration/photonDispersion.cu"
+#include "camera/ProjectiveCamera.cu"
+#include "sampling/Sampler.cu"
+#include "light/PointLight.cu"
+#include "materials/LambertianMaterial.cu"
+#include "materials/LightMaterial.cu"
+#include "materials/GlassMaterial.cu"
+#include "materials/MirrorMaterial.cu"
+#include "materials/SSMaterial.cu"
+#include "materials/PlasticUnrealMaterial.cu"
+#include "textures/Texture.cu"
+#include "textures/SphericalTexture.cu"
+#include "cuda_libraries/FileImporting.cu"
+#undef swap
+
+#define REFR_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+struct FilmPeek : public Film {
+    using Film::pixelLight;
+};
+struct CameraPeek : public ProjectiveCamera {
+    using ProjectiveCamera::rasterToCamera;
+};
+}  // namespace
+
+REFR_API int refr_config(int *w, int *h, int *spp, int *depth)
+{
+    *w = resolutionX;
+    *h = resolutionY;
+    *spp = SAMPLES_PER_PIXEL;
+    *depth = MAX_RAY_RECURSION_DEPTH;
+    return 0;
+}
+
+// planes: per plane 12 floats (bottom-left corner, axisX, axisY, normal) as
+// Plane(Point3f, Vector3f, Vector3f, Vector3f) (Plane.cu:26-50); kd: 3 floats per plane.
+// out_mean: per-pixel mean radiance (Film sum / spp), row-major, 3 floats per pixel.
+// out_c2w / out_r2c: the camera's cameraToWorld and rasterToCamera matrices (row-major).
+REFR_API int refr_render(const char *obejota, int nplanes, const float *planes, const float *kd, float *out_mean,
+                         float *out_c2w, float *out_r2c)
+{
+    std::vector<Plane *> pl;
+    std::vector<LambertianMaterial *> mats;
+    std::vector<Shape *> shapes;
+    for (int i = 0; i < nplanes; i++) {
+        const float *p = planes + 12 * i;
+        Plane *s = new Plane(Point3f(p[0], p[1], p[2]), Vector3f(p[3], p[4], p[5]), Vector3f(p[6], p[7], p[8]),
+                             Vector3f(p[9], p[10], p[11]));
+        LambertianMaterial *m = new LambertianMaterial(Spectrum(kd[3 * i], kd[3 * i + 1], kd[3 * i + 2]));
+        s->setMaterial(m);
+        pl.push_back(s);
+        mats.push_back(m);
+        shapes.push_back(s);
+    }
+    std::vector<Light *> lights;
+    Camera *camera = nullptr;
+    loadObejota(obejota, lights, shapes, camera);
+    if (!camera) return 1;
+    std::shared_ptr<std::vector<TriangleMesh>> meshes = std::make_shared<std::vector<TriangleMesh>>();
+    std::vector<std::vector<Triangle>> triangles;
+    Scene scene;
+    scene.build(shapes, lights, triangles, meshes);
+    PathTracerIntegrator integrator(camera);
+    integrator.render(&scene);
+    FilmPeek *film = static_cast<FilmPeek *>(camera->getFilm());
+    for (int i = 0; i < resolutionX * resolutionY; i++) {
+        out_mean[3 * i + 0] = (float)(film->pixelLight[i].getR() / SAMPLES_PER_PIXEL);
+        out_mean[3 * i + 1] = (float)(film->pixelLight[i].getG() / SAMPLES_PER_PIXEL);
+        out_mean[3 * i + 2] = (float)(film->pixelLight[i].getB() / SAMPLES_PER_PIXEL);
+    }
+    CameraPeek *pc = static_cast<CameraPeek *>(static_cast<ProjectiveCamera *>(camera));
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) {
+            out_c2w[4 * r + c] = camera->cameraToWorld.getMatrix()[r][c];
+            out_r2c[4 * r + c] = pc->rasterToCamera.getMatrix()[r][c];
+        }
+    for (auto *s : pl) delete s;
+    for (auto *m : mats) delete m;
+    return 0;
+}
