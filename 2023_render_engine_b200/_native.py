@@ -67,6 +67,7 @@ RT_MATF_TRANSPARENT = 0x1
 RT_RENDER_NEE_AREA = 0x1
 RT_RENDER_COMPAT = 0x2
 RT_RENDER_EXACT_TRACE = 0x4
+RT_RENDER_PHOTON_MAP = 0x8
 
 
 class PhotonTraceStats(ctypes.Structure):
@@ -119,6 +120,8 @@ SIGNATURES = {
     "rt_photon_map_get": [_P, _U64, _U64, _P],
     "rt_photon_map_destroy": [_P],
     "rt_photon_knn": [_P, _P, _P, _U64, _U32, _F32, _P, _P, _P],
+    "rt_photon_density": [_P, ctypes.POINTER(Material), _P, _P, _P, _P, _U64, _U32, _F32, _P],
+    "rt_render_set_photon_map": [_P, _P, _U32, _F32],
 }
 
 

@@ -141,6 +141,12 @@ class Scene:
                                   ctypes.byref(st)))
         return film, {f: getattr(st, f) for f, _ in N.RenderStats._fields_}
 
+    def set_photon_map(self, pmap, k: int = 100, radius: float = 100.0):
+        """Photon map for RT_RENDER_PHOTON_MAP renders (MAX_NEIGHBOURS, PHOTON_SEARCH_RADIUS)."""
+        N.check(N.lib().rt_render_set_photon_map(self.handle, None if pmap is None else pmap.handle, k,
+                                                 float(radius)))
+        self._pmap = pmap
+
     def trace_photons(self, n: int, max_depth: int = 30, rr_depth: int = 3, seed: int = 0, flags: int = 0):
         """Scene::generatePhotons + computePhotons: returns (PhotonMap, stats)."""
         h = ctypes.c_void_p()
@@ -263,6 +269,19 @@ class PhotonMap:
                                       None if shape_dev is None else shape_dev.data_ptr(), nq, k, float(radius),
                                       idx.data_ptr(), None if dist is None else dist.data_ptr(), cnt.data_ptr()))
         return idx.view(nq, k), (None if dist is None else dist.view(nq, k)), cnt
+
+    def density(self, material: "N.Material", points_dev, normals_dev, wo_dev, k: int, radius: float,
+                shape_dev=None):
+        """Scene::combinePhotonContributions at each point; returns (nq, 3) CUDA tensor."""
+        import torch
+
+        nq = points_dev.numel() // 3
+        out = torch.empty(nq * 3, dtype=torch.float32, device="cuda")
+        N.check(N.lib().rt_photon_density(self.handle, ctypes.byref(material), points_dev.data_ptr(),
+                                          normals_dev.data_ptr(), wo_dev.data_ptr(),
+                                          None if shape_dev is None else shape_dev.data_ptr(), nq, k, float(radius),
+                                          out.data_ptr()))
+        return out.view(nq, 3)
 
     def close(self):
         if self.handle:

@@ -20,22 +20,12 @@
 #include <thread>
 #include <vector>
 
-#include "surface.cuh"
-
-struct rt_photon_map {
-    rt_context *ctx = nullptr;
-    uint64_t n = 0;
-    rtb::DevBuf photons;  // rt_photon[n], (path, depth) order
-    rtb::DevBuf node_pos;  // float4 per tree slot: xyz, split axis (uint bits)
-    rtb::DevBuf node_aux;  // int2 per tree slot: shape id, photon index
-    bool built = false;
-};
+#include "photon_query.cuh"
 
 namespace rtb {
 namespace {
 
 constexpr int kPB = 128;
-constexpr uint32_t kMaxK = 128;
 
 struct PhotonBuffers {
     rt_ray *rays[2];
@@ -198,15 +188,6 @@ __global__ void k_iota(uint32_t *v, uint64_t n)
 
 // ------------------------------------------------------------------- kNN
 
-// Euclidean norm as the reference evaluates it: s = 0; s += r*r per axis; sqrt
-// (kdtree.h:175-176, difference kdtree.h:67-76).
-__device__ __forceinline__ float ref_dist(float qx, float qy, float qz, float4 p)
-{
-    float dx = __fsub_rn(qx, p.x), dy = __fsub_rn(qy, p.y), dz = __fsub_rn(qz, p.z);
-    float s = __fadd_rn(__fadd_rn(__fadd_rn(0.f, __fmul_rn(dx, dx)), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-    return __fsqrt_rn(s);
-}
-
 __global__ void __launch_bounds__(128) k_knn(const float4 *__restrict__ node_pos, const int2 *__restrict__ node_aux,
                                              uint32_t n, const float *__restrict__ queries,
                                              const int32_t *__restrict__ qshape, uint64_t nq, uint32_t k,
@@ -215,116 +196,36 @@ __global__ void __launch_bounds__(128) k_knn(const float4 *__restrict__ node_pos
 {
     const uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= nq) return;
-    const float qx = queries[3 * qi], qy = queries[3 * qi + 1], qz = queries[3 * qi + 2];
-    const int32_t sid = qshape ? qshape[qi] : -1;
-    float hd[kMaxK];
-    int32_t hi[kMaxK];
-    uint32_t cnt = 0;
-    float rcur = radius;  // current bound: radius, then the k-th best distance once k are held
-    // stack of subranges [l, r) with the distance to their splitting plane
-    uint32_t sl[64], sr[64];
-    float sd[64];
-    int sp = 0;
-    sl[0] = 0;
-    sr[0] = n;
-    sd[0] = 0.f;
-    sp = 1;
-    while (sp > 0) {
-        sp--;
-        const uint32_t l = sl[sp], r = sr[sp];
-        if (!(sd[sp] < rcur) || r <= l) continue;
-        const uint32_t m = (l + r) >> 1;
-        const float4 p = __ldg(node_pos + m);
-        const int2 aux = __ldg(node_aux + m);
-        const float dist = ref_dist(qx, qy, qz, p);
-        if (dist < rcur && (sid == -1 || aux.x == sid)) {
-            if (cnt < k) {  // sift up into the max-heap
-                uint32_t c = cnt++;
-                while (c > 0) {
-                    uint32_t par = (c - 1) >> 1;
-                    if (!(hd[par] < dist)) break;
-                    hd[c] = hd[par];
-                    hi[c] = hi[par];
-                    c = par;
-                }
-                hd[c] = dist;
-                hi[c] = aux.y;
-                if (cnt == k) rcur = hd[0];
-            } else {  // replace the farthest, sift down
-                uint32_t c = 0;
-                for (;;) {
-                    uint32_t a = 2 * c + 1, b = a + 1, big = c;
-                    float bd = dist;
-                    if (a < k && hd[a] > bd) {
-                        big = a;
-                        bd = hd[a];
-                    }
-                    if (b < k && hd[b] > bd) {
-                        big = b;
-                        bd = hd[b];
-                    }
-                    if (big == c) break;
-                    hd[c] = hd[big];
-                    hi[c] = hi[big];
-                    c = big;
-                }
-                hd[c] = dist;
-                hi[c] = aux.y;
-                rcur = hd[0];
-            }
-        }
-        if (r - l > 1) {
-            const uint32_t axis = __float_as_uint(p.w);
-            const float qa = axis == 0 ? qx : (axis == 1 ? qy : qz);
-            const float pa = axis == 0 ? p.x : (axis == 1 ? p.y : p.z);
-            const float diff = __fsub_rn(qa, pa);
-            const float pd = __fsqrt_rn(__fmul_rn(diff, diff));  // norm(p - pplane) (kdtree.h:138-148)
-            uint32_t nl, nr, fl, fr;
-            if (qa < pa) {
-                nl = l, nr = m, fl = m + 1, fr = r;
-            } else {
-                nl = m + 1, nr = r, fl = l, fr = m;
-            }
-            if (sp + 2 <= 64) {
-                sl[sp] = fl, sr[sp] = fr, sd[sp] = pd, sp++;  // far side, tested again when popped
-                sl[sp] = nl, sr[sp] = nr, sd[sp] = 0.f, sp++;
-            }
-        }
-    }
-    // heap -> ascending distance (heap sort in place)
-    for (uint32_t end = cnt; end > 1; end--) {
-        float td = hd[0];
-        int32_t ti = hi[0];
-        float ld = hd[end - 1];
-        int32_t li = hi[end - 1];
-        uint32_t c = 0;
-        const uint32_t m = end - 1;
-        for (;;) {
-            uint32_t a = 2 * c + 1, b = a + 1, big = c;
-            float bd = ld;
-            if (a < m && hd[a] > bd) {
-                big = a;
-                bd = hd[a];
-            }
-            if (b < m && hd[b] > bd) {
-                big = b;
-                bd = hd[b];
-            }
-            if (big == c) break;
-            hd[c] = hd[big];
-            hi[c] = hi[big];
-            c = big;
-        }
-        hd[c] = ld;
-        hi[c] = li;
-        hd[end - 1] = td;
-        hi[end - 1] = ti;
-    }
+    float hd[kKnnMaxK];
+    int32_t hi[kKnnMaxK];
+    const uint32_t cnt = knn_query(node_pos, node_aux, n, queries[3 * qi], queries[3 * qi + 1], queries[3 * qi + 2],
+                                   qshape ? qshape[qi] : -1, k, radius, hd, hi);
+    heap_to_sorted(hd, hi, cnt);
     for (uint32_t j = 0; j < k; j++) {
         out_idx[qi * k + j] = j < cnt ? hi[j] : -1;
         if (out_dist) out_dist[qi * k + j] = j < cnt ? hd[j] : INFINITY;
     }
     out_count[qi] = cnt;
+}
+
+// Scene::combinePhotonContributions (Scene.cu:607-635) per query: the k nearest photons on
+// the same shape within radius, sum of power * lightScattered(-photon direction), divided by
+// pi * (largest neighbour distance)^2.
+__global__ void __launch_bounds__(128) k_density(const float4 *__restrict__ node_pos, const int2 *__restrict__ node_aux,
+                                                 const rt_photon *__restrict__ photons, uint32_t n, rt_material mat,
+                                                 const float *__restrict__ pts, const float *__restrict__ nrm,
+                                                 const float *__restrict__ wo, const int32_t *__restrict__ shape,
+                                                 uint64_t nq, uint32_t k, float radius, float *__restrict__ out)
+{
+    const uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= nq) return;
+    V3 p = v3(pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]);
+    V3 nn = normalize(v3(nrm[3 * qi], nrm[3 * qi + 1], nrm[3 * qi + 2]));
+    V3 w = v3(wo[3 * qi], wo[3 * qi + 1], wo[3 * qi + 2]);
+    V3 c = photon_density(node_pos, node_aux, photons, n, load_bsdf(mat), p, nn, w, shape ? shape[qi] : -1, k, radius);
+    out[3 * qi] = c.x;
+    out[3 * qi + 1] = c.y;
+    out[3 * qi + 2] = c.z;
 }
 
 // ---------------------------------------------------- host kd-tree build
@@ -482,13 +383,31 @@ int rt_photon_knn(rt_photon_map *m, const float *q, const int32_t *qs, uint64_t 
 {
     if (!m || (nq && (!q || !out_idx || !out_count))) return fail(RT_ERR_INVALID, "rt_photon_knn: null argument");
     if (!m->built) return fail(RT_ERR_STATE, "rt_photon_knn: map not built (rt_photon_map_build)");
-    if (k == 0 || k > kMaxK) return fail(RT_ERR_INVALID, "rt_photon_knn: k must be in [1, 128]");
+    if (k == 0 || k > kKnnMaxK) return fail(RT_ERR_INVALID, "rt_photon_knn: k must be in [1, 128]");
     if (nq == 0) return RT_OK;
     RTB_CUDA(cudaSetDevice(m->ctx->device));
     const uint64_t blocks = (nq + 127) / 128;
     k_knn<<<(unsigned)blocks, 128, 0, m->ctx->stream>>>(m->node_pos.as<float4>(), m->node_aux.as<int2>(),
                                                         (uint32_t)m->n, q, qs, nq, k, radius, out_idx, out_dist,
                                                         out_count);
+    RTB_CUDA(cudaGetLastError());
+    RTB_CUDA(cudaStreamSynchronize(m->ctx->stream));
+    return RT_OK;
+}
+
+int rt_photon_density(rt_photon_map *m, const rt_material *mat, const float *pts, const float *nrm, const float *wo,
+                      const int32_t *shape, uint64_t nq, uint32_t k, float radius, float *out_rgb)
+{
+    if (!m || !mat || (nq && (!pts || !nrm || !wo || !out_rgb)))
+        return fail(RT_ERR_INVALID, "rt_photon_density: null argument");
+    if (!m->built) return fail(RT_ERR_STATE, "rt_photon_density: map not built (rt_photon_map_build)");
+    if (k == 0 || k > kKnnMaxK) return fail(RT_ERR_INVALID, "rt_photon_density: k must be in [1, 128]");
+    if (nq == 0) return RT_OK;
+    RTB_CUDA(cudaSetDevice(m->ctx->device));
+    const uint64_t blocks = (nq + 127) / 128;
+    k_density<<<(unsigned)blocks, 128, 0, m->ctx->stream>>>(m->node_pos.as<float4>(), m->node_aux.as<int2>(),
+                                                            m->photons.as<rt_photon>(), (uint32_t)m->n, *mat, pts,
+                                                            nrm, wo, shape, nq, k, radius, out_rgb);
     RTB_CUDA(cudaGetLastError());
     RTB_CUDA(cudaStreamSynchronize(m->ctx->stream));
     return RT_OK;

@@ -22,7 +22,7 @@
 #include <cstring>
 #include <vector>
 
-#include "surface.cuh"
+#include "photon_query.cuh"
 
 namespace rtb {
 
@@ -46,10 +46,11 @@ struct Buffers {
     rt_ray *srays;
     float4 *scontrib;  // rgb, target index bits (kRetireTarget: retire list)
     float4 *retire;    // L.xyz, pixel index bits
+    float4 *gather;    // photon-map gather requests, 4 float4 each: p+shape, n+material, wo+target, beta
     uint32_t cap, scap;
     // counters (uint32): [0],[1] queue sizes of buffers 0/1, [2] shadow count, [3] retire count,
-    // [4] status, [5] shadow-kernel work counter; u64 at [8]: next sample, [10] extension rays,
-    // [12] shadow rays
+    // [4] status, [5] shadow-kernel work counter, [6] gather requests; u64 at [8]: next sample,
+    // [10] extension rays, [12] shadow rays
     uint32_t *cnt;
 };
 
@@ -136,6 +137,14 @@ __device__ __forceinline__ void push_shadow(const Buffers &bf, V3 o, V3 d, float
     bf.scontrib[i] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(target));
 }
 
+struct PhotonView {
+    const float4 *node_pos;
+    const int2 *node_aux;
+    const rt_photon *photons;
+    uint32_t n, k;
+    float radius;
+};
+
 __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur)
 {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -145,6 +154,7 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
     const int nxt = cur ^ 1;
     const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
     const bool nee_area = (rv.flags & RT_RENDER_NEE_AREA) != 0 && rv.nemit > 0;
+    const bool photon_mode = (rv.flags & RT_RENDER_PHOTON_MAP) != 0;
     float4 r0 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q];
     float4 r1 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q + 1];
     float4 s0 = bf.st0[cur][q], s1 = bf.st1[cur][q];
@@ -202,6 +212,22 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
         V3 wi_w = t * wi_l.x + bvec * wi_l.y + sf.n * wi_l.z;
         beta = beta * f;
         finished = is_black(f);
+        if (photon_mode && scattering) {
+            // RENDER_MODE PHOTON_MAPPING: the density estimate at this hit ends the path
+            // (Scene::getPhotonContributions, Scene.cu:822-840; finishStep, pathTracing.cu:85-89)
+            finished = true;
+            const uint32_t rt = kRetireTarget | append(bf.cnt + 3);
+            const uint32_t gi = append(bf.cnt + 6);
+            if (gi < bf.cap) {
+                bf.gather[4 * gi + 0] = make_float4(sf.p.x, sf.p.y, sf.p.z, __int_as_float(sf.shape));
+                bf.gather[4 * gi + 1] = make_float4(sf.n.x, sf.n.y, sf.n.z, __uint_as_float(sf.mat));
+                bf.gather[4 * gi + 2] = make_float4(wo_w.x, wo_w.y, wo_w.z, __uint_as_float(rt));
+                bf.gather[4 * gi + 3] = make_float4(beta_in.x, beta_in.y, beta_in.z, 0.f);
+            }
+            bf.retire[rt & ~kRetireTarget] = make_float4(L.x, L.y, L.z, __uint_as_float(pix));
+            regenerate(rv, bf, nxt);
+            return;
+        }
         // Russian roulette (pathTracing.cu:91-102)
         if (!finished && scattering && depth > rv.rr_depth) {
             float qrr = fmaxf(0.05f, 1.f - luminance(beta));
@@ -336,6 +362,26 @@ __global__ void __launch_bounds__(kB) k_shadow(RenderView rv, Buffers bf, int nx
         });
 }
 
+// Photon-map gathers queued by k_shade: the density estimate times the path throughput is
+// added to the finished path's radiance.
+__global__ void __launch_bounds__(kB) k_gather(RenderView rv, Buffers bf, PhotonView pv)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = min(bf.cnt[6], bf.cap);
+    if (i >= n) return;
+    const float4 a = bf.gather[4 * i], b = bf.gather[4 * i + 1], c = bf.gather[4 * i + 2], d = bf.gather[4 * i + 3];
+    const rt_material &m = rv.mats[min(__float_as_uint(b.w), rv.nmats - 1)];
+    V3 e = photon_density(pv.node_pos, pv.node_aux, pv.photons, pv.n, load_bsdf(m), v3(a.x, a.y, a.z),
+                          v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), __float_as_int(a.w), pv.k, pv.radius,
+                          (rv.flags & RT_RENDER_COMPAT) != 0);
+    V3 contrib = v3(d.x, d.y, d.z) * e;
+    const uint32_t target = __float_as_uint(c.w);
+    float *dst = reinterpret_cast<float *>(bf.retire + (target & ~kRetireTarget));
+    atomicAdd(dst + 0, contrib.x);
+    atomicAdd(dst + 1, contrib.y);
+    atomicAdd(dst + 2, contrib.z);
+}
+
 __global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t *count, double *sum64)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -385,6 +431,16 @@ int rt_scene_set_triangle_materials(rt_scene *s, uint32_t first, uint32_t n, con
     return RT_OK;
 }
 
+int rt_render_set_photon_map(rt_scene *s, rt_photon_map *m, uint32_t k, float radius)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_render_set_photon_map: null scene");
+    if (m && (k == 0 || k > kKnnMaxK)) return fail(RT_ERR_INVALID, "rt_render_set_photon_map: k must be in [1, 128]");
+    s->pmap = m;
+    s->pm_k = k;
+    s->pm_radius = radius;
+    return RT_OK;
+}
+
 int rt_scene_add_point_light(rt_scene *s, const float pos[3], const float rgb[3], float intensity)
 {
     if (!s || !pos || !rgb) return fail(RT_ERR_INVALID, "rt_scene_add_point_light: null argument");
@@ -403,7 +459,7 @@ namespace rtb {
 void RenderScratch::release()
 {
     for (DevBuf *b : {&rays[0], &rays[1], &st0[0], &st0[1], &st1[0], &st1[1], &st2[0], &st2[1], &hits, &srays,
-                      &scontrib, &retire, &cnt})
+                      &scontrib, &retire, &cnt, &gather})
         b->release();
     if (host_cnt) cudaFreeHost(host_cnt);
     host_cnt = nullptr;
@@ -541,6 +597,12 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
     RTB_CHECK(rs.srays.reserve(32ull * scap));
     RTB_CHECK(rs.scontrib.reserve(16ull * scap));
     RTB_CHECK(rs.retire.reserve(16ull * cap));
+    const bool photon_mode = (opts->flags & RT_RENDER_PHOTON_MAP) != 0;
+    if (photon_mode) {
+        if (!s->pmap || !s->pmap->built)
+            return fail(RT_ERR_STATE, "rt_render: RT_RENDER_PHOTON_MAP needs a built photon map (rt_render_set_photon_map)");
+        RTB_CHECK(rs.gather.reserve(64ull * cap));
+    }
     RTB_CHECK(rs.cnt.reserve(256));
     RTB_CHECK(s->scratch.queue.reserve(4ull * cap));
     RTB_CHECK(s->scratch.counters.reserve(64));
@@ -557,6 +619,16 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
     bf.srays = rs.srays.as<rt_ray>();
     bf.scontrib = rs.scontrib.as<float4>();
     bf.retire = rs.retire.as<float4>();
+    bf.gather = rs.gather.as<float4>();
+    PhotonView pv{};
+    if (photon_mode) {
+        pv.node_pos = s->pmap->node_pos.as<float4>();
+        pv.node_aux = s->pmap->node_aux.as<int2>();
+        pv.photons = s->pmap->photons.as<rt_photon>();
+        pv.n = (uint32_t)s->pmap->n;
+        pv.k = std::min<uint32_t>(std::max<uint32_t>(s->pm_k, 1u), kKnnMaxK);
+        pv.radius = s->pm_radius;
+    }
     bf.cap = cap;
     bf.scap = scap;
     bf.cnt = rs.cnt.as<uint32_t>();
@@ -598,11 +670,15 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
                                                s->scratch.queue.as<uint32_t>(), s->scratch.counters.as<uint32_t>(),
                                                st));
             RTB_CUDA(cudaMemsetAsync(bf.cnt + ((cur ^ 1)), 0, 4, st));
-            RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 16, st));
+            RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 20, st));
             k_shade<<<blocks, kB, 0, st>>>(rv, bf, cur);
             RTB_CUDA(cudaGetLastError());
             k_shadow<<<shadow_blocks, kB, 0, st>>>(rv, bf, cur ^ 1);
             RTB_CUDA(cudaGetLastError());
+            if (photon_mode) {
+                k_gather<<<blocks, kB, 0, st>>>(rv, bf, pv);
+                RTB_CUDA(cudaGetLastError());
+            }
             k_retire<<<blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64);
             RTB_CUDA(cudaGetLastError());
             cur ^= 1;

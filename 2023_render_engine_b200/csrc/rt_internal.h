@@ -160,7 +160,7 @@ int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, uint8_t
 
 // Wavefront buffers of rt_render (grown on demand, kept between calls).
 struct RenderScratch {
-    DevBuf rays[2], st0[2], st1[2], st2[2], hits, srays, scontrib, retire, cnt;
+    DevBuf rays[2], st0[2], st1[2], st2[2], hits, srays, scontrib, retire, cnt, gather;
     void *host_cnt = nullptr;  // pinned
     void release();
 };
@@ -183,6 +183,15 @@ struct rt_context {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int sm_count = 0;
+};
+
+struct rt_photon_map {
+    rt_context *ctx = nullptr;
+    uint64_t n = 0;
+    rtb::DevBuf photons;   // rt_photon[n], (path, depth) order
+    rtb::DevBuf node_pos;  // float4 per tree slot: xyz, split axis (uint bits)
+    rtb::DevBuf node_aux;  // int2 per tree slot: shape id, photon index
+    bool built = false;
 };
 
 struct rt_scene {
@@ -216,6 +225,9 @@ struct rt_scene {
     bool has_normals = false;
     uint32_t nemit = 0;
     float emit_total = 0.f;
+    rt_photon_map *pmap = nullptr;  // RT_RENDER_PHOTON_MAP gather source
+    uint32_t pm_k = 100;
+    float pm_radius = 100.f;
     rtb::DevBuf d_mats, d_tri_mat, d_tri_shape, d_tri_nidx, d_normals, d_emit_tri, d_emit_cdf, d_plights;
     rtb::RenderScratch rscratch;
     rtb::SceneView view() const;

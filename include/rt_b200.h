@@ -211,6 +211,9 @@ typedef struct rt_camera {
 #define RT_RENDER_COMPAT 0x2u   /* reference estimator quirks (delta-light MIS weight, 0.7/0.3 glass lobes
                                    without pdf, reference Fresnel); off = physically consistent */
 #define RT_RENDER_EXACT_TRACE 0x4u /* reference-exact closest-hit ids for extension rays */
+#define RT_RENDER_PHOTON_MAP 0x8u  /* photon-mapping mode (RENDER_MODE PHOTON_MAPPING): at the first
+                                      scattering hit the photon density estimate replaces the rest
+                                      of the path; needs rt_render_set_photon_map */
 
 typedef struct rt_render_opts {
     uint32_t spp;            /* samples per pixel in this call */
@@ -289,6 +292,19 @@ RT_API int rt_photon_map_count(rt_photon_map *map, uint64_t *n);
 /* Copies photons [first, first+n) to host memory. */
 RT_API int rt_photon_map_get(rt_photon_map *map, uint64_t first, uint64_t n, rt_photon *out_host);
 RT_API int rt_photon_map_destroy(rt_photon_map *map);
+
+/* Scene::combinePhotonContributions (Scene.cu:607-635) at nq surface points (device
+ * buffers, 3 floats each: position, shading normal, outgoing direction toward the viewer;
+ * shape ids nullable): sum over the k nearest photons on the same shape within radius of
+ * power * f(wo, -photon direction)|cos| for material `mat`, divided by pi * (largest
+ * neighbour distance)^2. out_rgb: 3 floats per point. */
+RT_API int rt_photon_density(rt_photon_map *map, const rt_material *mat, const float *points_dev,
+                             const float *normals_dev, const float *wo_dev, const int32_t *shape_ids_dev, uint64_t nq,
+                             uint32_t k, float radius, float *out_rgb_dev);
+
+/* Photon map used by rt_render in RT_RENDER_PHOTON_MAP mode, with the gather size and radius
+ * (the reference's MAX_NEIGHBOURS and PHOTON_SEARCH_RADIUS, types.h:57-60). NULL detaches. */
+RT_API int rt_render_set_photon_map(rt_scene *scene, rt_photon_map *map, uint32_t k, float radius);
 
 /* k nearest photons per query point within `radius` (distance < radius, same shape id
  * unless the query's id is -1), as nn::KDTree::nearest_neighbors + Scene::search_nearest
