@@ -69,3 +69,24 @@ def build_config1(ctx, width=1920, height=1080, subdiv=8):
             sc.set_triangle_materials(first, ids.astype(np.uint32))
     sc.commit()
     return sc, cornell_camera(width, height), dict(spp=64, max_depth=12, rr_depth=3)
+
+
+def build_config2(ctx, width=1280, height=720, seed=3, target_triangles=200_000):
+    """Config 2: the guiding room (mostly indirect light through a gap in a wall)."""
+    meshes, mats = scenes.guiding_room(seed=seed, target_triangles=target_triangles)
+    table = []
+    for m in mats:
+        if m["kind"] == "lambert":
+            table.append(core.material(N.RT_MAT_LAMBERTIAN, color=m["albedo"]))
+        elif m["kind"] == "ggx":
+            table.append(core.material(N.RT_MAT_TROWBRIDGE, color=(1, 1, 1), eta=(1.5, 1.5, 1.5), k=(0, 0, 0),
+                                       roughness=(m["roughness"], m["roughness"])))
+        else:
+            table.append(core.material(N.RT_MAT_LIGHT, color=m["emission"], intensity=1.0))
+    sc = core.Scene(ctx)
+    sc.set_materials(table)
+    for i, (v, f, mi) in enumerate(meshes):
+        sc.add_mesh(v, f, material=mi, shape_id=i)
+    sc.commit()
+    cam = core.look_at_camera((-1.6, 1.6, -1.8), (0.5, 0.8, 0.8), (0, 1, 0), 60.0, width, height)
+    return sc, cam, dict(spp=64, max_depth=16, rr_depth=3)

@@ -157,3 +157,70 @@ def flatten(scene):
         mats.append(np.full(f.shape[0], m, np.uint32))
         base += v.shape[0]
     return np.concatenate(vs), np.concatenate(fs), np.concatenate(mats)
+
+
+def subdivided_box(lo, hi, n):
+    """Axis-aligned box [lo, hi] with each face split into an n x n grid (12 n^2 triangles),
+    outward-facing winding."""
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    vs, fs = [], []
+    g = np.linspace(0.0, 1.0, n + 1)
+    U, V = np.meshgrid(g, g, indexing="ij")
+    idx = np.arange((n + 1) * (n + 1)).reshape(n + 1, n + 1)
+    a, b, c, d = idx[:-1, :-1].ravel(), idx[1:, :-1].ravel(), idx[1:, 1:].ravel(), idx[:-1, 1:].ravel()
+    quad = np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)])
+    base = 0
+    for axis in range(3):
+        u_ax, v_ax = (axis + 1) % 3, (axis + 2) % 3
+        for side, val in ((0, lo[axis]), (1, hi[axis])):
+            P = np.zeros((U.size, 3))
+            P[:, axis] = val
+            P[:, u_ax] = lo[u_ax] + U.ravel() * (hi[u_ax] - lo[u_ax])
+            P[:, v_ax] = lo[v_ax] + V.ravel() * (hi[v_ax] - lo[v_ax])
+            f = quad if side == 1 else quad[:, ::-1]
+            vs.append(P)
+            fs.append(f + base)
+            base += P.shape[0]
+    return np.concatenate(vs).astype(np.float32), np.concatenate(fs).astype(np.uint32)
+
+
+def guiding_room(seed=3, target_triangles=200_000):
+    """Config 2 geometry: a closed room [-2,2]x[0,2.5]x[-2,2] split by a wall at z = 1 with a
+    0.2-wide vertical gap; a 0.3x0.3 emitter (Le = 20) behind the wall; seeded random boxes
+    (each 12 n^2 triangles with n chosen so a box has 20..2000 triangles, sizes log-uniform in
+    [0.05, 1]) on the floor until about `target_triangles` triangles. Per-box material:
+    Lambertian albedo U[0.2, 0.9], or (30%) GGX roughness U[0.1, 0.4].
+    Returns meshes [(v, f, material_key)] and a material list (dicts for configs.py)."""
+    rng = np.random.default_rng(seed)
+    meshes, mats = [], []
+
+    def add(v, f, m):
+        mats.append(m)
+        meshes.append((v, f, len(mats) - 1))
+
+    wall = dict(kind="lambert", albedo=(0.7, 0.7, 0.7))
+    room = subdivided_box((-2, 0, -2), (2, 2.5, 2), 2)
+    add(room[0], room[1][:, ::-1].copy(), wall)  # inward-facing
+    # dividing wall at z = 1 (0.1 thick) with a gap 0.2 wide at x in [0.4, 0.6]
+    add(*subdivided_box((-2, 0, 0.95), (0.4, 2.5, 1.05), 2), wall)
+    add(*subdivided_box((0.6, 0, 0.95), (2, 2.5, 1.05), 2), wall)
+    # the emitter behind the wall, facing -z towards the wall
+    lv = np.array([[0.35, 1.0, 1.8], [0.65, 1.0, 1.8], [0.65, 1.3, 1.8], [0.35, 1.3, 1.8]], np.float32)
+    add(lv, np.array([[0, 2, 1], [0, 3, 2]], np.uint32), dict(kind="light", emission=(20.0, 20.0, 20.0)))
+    ntri = sum(f.shape[0] for _, f, _ in meshes)
+    while ntri < target_triangles:
+        size = np.exp(rng.uniform(np.log(0.05), np.log(1.0), 3))
+        x, z = rng.uniform(-1.9, 1.9 - size[0]), rng.uniform(-1.9, 0.9 - size[2])
+        lo = np.array([x, 0.0, z])
+        hi = lo + size
+        n = int(rng.integers(1, 13))  # 12 n^2 in [12 .. 1728]
+        n = max(n, 2)                 # at least 48 triangles
+        v, f = subdivided_box(lo, hi, n)
+        if rng.uniform() < 0.3:
+            m = dict(kind="ggx", roughness=float(rng.uniform(0.1, 0.4)))
+        else:
+            m = dict(kind="lambert", albedo=tuple(float(a) for a in rng.uniform(0.2, 0.9, 3)))
+        add(v, f, m)
+        ntri += f.shape[0]
+    return meshes, mats
