@@ -68,6 +68,7 @@ RT_RENDER_NEE_AREA = 0x1
 RT_RENDER_COMPAT = 0x2
 RT_RENDER_EXACT_TRACE = 0x4
 RT_RENDER_PHOTON_MAP = 0x8
+RT_RENDER_GUIDE = 0x10
 
 
 class PhotonTraceStats(ctypes.Structure):
@@ -77,6 +78,16 @@ class PhotonTraceStats(ctypes.Structure):
 
 PHOTON_DTYPE = np.dtype([("pos", "<f4", 3), ("shape_id", "<i4"), ("dir", "<f4", 3), ("path", "<u4"),
                          ("power", "<f4", 3), ("depth", "<u4"), ("normal", "<f4", 3), ("reserved", "<f4")])
+
+
+class GuideOpts(ctypes.Structure):
+    _fields_ = [("bbox_min", ctypes.c_float * 3), ("bbox_max", ctypes.c_float * 3), ("learning_rate", ctypes.c_float),
+                ("seed", ctypes.c_uint32), ("record_capacity", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+GUIDE_INPUTS = 144
+GUIDE_OUTPUTS = 48
+GUIDE_LOBES = 8
 
 
 class TraceStats(ctypes.Structure):
@@ -122,6 +133,20 @@ SIGNATURES = {
     "rt_photon_knn": [_P, _P, _P, _U64, _U32, _F32, _P, _P, _P],
     "rt_photon_density": [_P, ctypes.POINTER(Material), _P, _P, _P, _P, _U64, _U32, _F32, _P],
     "rt_render_set_photon_map": [_P, _P, _U32, _F32],
+    "rt_guide_create": [_P, ctypes.POINTER(GuideOpts), ctypes.POINTER(_P)],
+    "rt_guide_destroy": [_P],
+    "rt_guide_param_count": [_P, ctypes.POINTER(_U64)],
+    "rt_guide_params_get": [_P, _P, _U64],
+    "rt_guide_params_set": [_P, _P, _U64],
+    "rt_guide_steps": [_P, ctypes.POINTER(_U64)],
+    "rt_guide_eval": [_P, _P, _U64, _P],
+    "rt_guide_pdf": [_P, _P, _P, _P, _U64, _P],
+    "rt_guide_sample": [_P, _P, _P, _U64, _P, _P],
+    "rt_guide_train_step": [_P, _P, _P, _P, _P, _U64, _INT, _P, ctypes.POINTER(_F32)],
+    "rt_render_set_guide": [_P, _P, _INT],
+    "rt_guide_record_count": [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)],
+    "rt_guide_train_records": [_P, _U32, _U32, _U32, ctypes.POINTER(_F32)],
+    "rt_guide_records_get": [_P, _U64, _U64, _P],
 }
 
 

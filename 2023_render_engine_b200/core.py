@@ -147,6 +147,11 @@ class Scene:
                                                  float(radius)))
         self._pmap = pmap
 
+    def set_guide(self, guide, train: bool = False):
+        """Learned proposal for RT_RENDER_GUIDE renders; train=True records training samples."""
+        N.check(N.lib().rt_render_set_guide(self.handle, None if guide is None else guide.handle, int(train)))
+        self._guide = guide
+
     def trace_photons(self, n: int, max_depth: int = 30, rr_depth: int = 3, seed: int = 0, flags: int = 0):
         """Scene::generatePhotons + computePhotons: returns (PhotonMap, stats)."""
         h = ctypes.c_void_p()
@@ -286,6 +291,122 @@ class PhotonMap:
     def close(self):
         if self.handle:
             N.lib().rt_photon_map_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def rmse(film_a, film_b) -> float:
+    """computeRMSE (camera/Film.cu:611-632): sqrt(sum over pixels of |mean_a - mean_b|^2 / pixels),
+    |.|^2 the squared norm of the RGB difference. Accepts films or (H*W, 3) arrays."""
+    a = film_mean(film_a) if isinstance(film_a, dict) else np.asarray(film_a, dtype=np.float64).reshape(-1, 3)
+    b = film_mean(film_b) if isinstance(film_b, dict) else np.asarray(film_b, dtype=np.float64).reshape(-1, 3)
+    if a.shape != b.shape:
+        return -1.0
+    return float(np.sqrt(np.sum((a - b) ** 2) / a.shape[0]))
+
+
+class Guide:
+    """Learned path guide (vMF-mixture MLP): evaluation, training, parameters (device buffers)."""
+
+    def __init__(self, ctx: Context, bbox_min, bbox_max, learning_rate: float = 1e-2, seed: int = 0,
+                 record_capacity: int = 0):
+        o = N.GuideOpts()
+        for a in range(3):
+            o.bbox_min[a] = float(bbox_min[a])
+            o.bbox_max[a] = float(bbox_max[a])
+        o.learning_rate = learning_rate
+        o.seed = seed
+        o.record_capacity = record_capacity
+        h = ctypes.c_void_p()
+        N.check(N.lib().rt_guide_create(ctx.handle, ctypes.byref(o), ctypes.byref(h)))
+        self.handle = h
+        self.opts = o
+
+    @property
+    def param_count(self) -> int:
+        n = ctypes.c_uint64()
+        N.check(N.lib().rt_guide_param_count(self.handle, ctypes.byref(n)))
+        return n.value
+
+    @property
+    def steps(self) -> int:
+        n = ctypes.c_uint64()
+        N.check(N.lib().rt_guide_steps(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.param_count, dtype=np.float32)
+        N.check(N.lib().rt_guide_params_get(self.handle, out.ctypes.data, out.size))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        N.check(N.lib().rt_guide_params_set(self.handle, p.ctypes.data, p.size))
+
+    def eval(self, queries_dev):
+        import torch
+
+        B = queries_dev.numel() // 9
+        out = torch.empty(B * N.GUIDE_OUTPUTS, dtype=torch.float32, device=queries_dev.device)
+        N.check(N.lib().rt_guide_eval(self.handle, queries_dev.data_ptr(), B, out.data_ptr()))
+        return out.view(B, N.GUIDE_OUTPUTS)
+
+    def pdf(self, queries_dev, dirs_dev, bsdf_pdf_dev):
+        import torch
+
+        B = queries_dev.numel() // 9
+        out = torch.empty(B, dtype=torch.float32, device=queries_dev.device)
+        N.check(N.lib().rt_guide_pdf(self.handle, queries_dev.data_ptr(), dirs_dev.data_ptr(),
+                                     bsdf_pdf_dev.data_ptr(), B, out.data_ptr()))
+        return out
+
+    def sample(self, queries_dev, u3_dev):
+        import torch
+
+        B = queries_dev.numel() // 9
+        dirs = torch.empty(B * 3, dtype=torch.float32, device=queries_dev.device)
+        pdf = torch.empty(B, dtype=torch.float32, device=queries_dev.device)
+        N.check(N.lib().rt_guide_sample(self.handle, queries_dev.data_ptr(), u3_dev.data_ptr(), B, dirs.data_ptr(),
+                                        pdf.data_ptr()))
+        return dirs.view(B, 3), pdf
+
+    def train_step(self, queries_dev, dirs_dev, bsdf_pdf_dev, weights_dev, apply: bool = True,
+                   want_grad: bool = False):
+        """One step; returns (loss, gradient or None)."""
+        B = weights_dev.numel()
+        grad = np.zeros(self.param_count, dtype=np.float32) if want_grad else None
+        loss = ctypes.c_float()
+        N.check(N.lib().rt_guide_train_step(self.handle, queries_dev.data_ptr(), dirs_dev.data_ptr(),
+                                            bsdf_pdf_dev.data_ptr(), weights_dev.data_ptr(), B, int(apply),
+                                            None if grad is None else grad.ctypes.data, ctypes.byref(loss)))
+        return loss.value, grad
+
+    def record_count(self):
+        r, nz = ctypes.c_uint64(), ctypes.c_uint64()
+        N.check(N.lib().rt_guide_record_count(self.handle, ctypes.byref(r), ctypes.byref(nz)))
+        return r.value, nz.value
+
+    def records(self) -> np.ndarray:
+        """Training records of the last recording render, (n, 20) float32 (see rt_guide_records_get)."""
+        n, _ = self.record_count()
+        out = np.zeros((n, 20), dtype=np.float32)
+        if n:
+            N.check(N.lib().rt_guide_records_get(self.handle, 0, n, out.ctypes.data))
+        return out
+
+    def train_records(self, steps: int, batch: int = 1 << 18, seed: int = 0) -> float:
+        loss = ctypes.c_float()
+        N.check(N.lib().rt_guide_train_records(self.handle, steps, batch, seed, ctypes.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if self.handle:
+            N.lib().rt_guide_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -1,0 +1,731 @@
+// Path-guide network: training on the tensor cores and the rt_guide_* entry points.
+//
+// One training step on B samples (rows padded to a multiple of 16):
+//   k_guide_wmean     mean of the sample weights (normalises the loss)
+//   k_guide_train_fb  per 16-row warp tile: encode, forward (activations kept in shared
+//                     memory), loss gradient per row, backward through the 5 layers; writes
+//                     every layer's input and output gradient transposed (feature-major) so
+//                     the weight gradient is a plain tensor-core contraction over rows
+//   k_guide_wgrad     dW_l = X_l^T G_l and db_l = sum G_l per chunk of rows (FP32 partials)
+//   k_guide_reduce    sum of the chunk partials in a fixed order (deterministic gradient)
+//   k_guide_adam      Adam on the FP32 master weights; refreshes the FP16 image
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "guide.cuh"
+#include "rt_internal.h"
+
+namespace rtb {
+
+namespace {
+
+constexpr int kTrainWarps = 8;  // 16 rows per warp
+constexpr int kTrainX0 = 0, kTrainH = 16 * 152 * 2, kTrainD = kTrainH + 4 * 16 * 72 * 2, kTrainO = kTrainD + 16 * 56 * 2;
+constexpr int kTrainWarpBytes = kTrainO + 16 * 49 * 4;
+constexpr int kTrainSmem = kGuideImgBytes + kTrainWarps * kTrainWarpBytes;
+static_assert(kTrainSmem <= 227 * 1024, "training kernel shared memory");
+constexpr uint32_t kWgradChunk = 2048;  // rows per weight-gradient block
+constexpr float kAdamB1 = 0.9f, kAdamB2 = 0.99f, kAdamEps = 1e-8f;
+
+__device__ __forceinline__ uint32_t pack_h2(__half a, __half b)
+{
+    __half2 h = __halves2half2(a, b);
+    return *reinterpret_cast<uint32_t *>(&h);
+}
+
+// 16 rows x W features (stride S halves) -> feature-major planes dst[f * Bpad + row0 + r]
+template <int W, int S>
+__device__ __forceinline__ void store_t(const __half *buf, __half *dst, uint64_t Bpad, uint64_t row0, int lane)
+{
+#pragma unroll
+    for (int c = 2 * lane; c < W; c += 64) {
+        uint32_t lo[8], hi[8];
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+            const __half2 v0 = *reinterpret_cast<const __half2 *>(buf + (2 * p) * S + c);
+            const __half2 v1 = *reinterpret_cast<const __half2 *>(buf + (2 * p + 1) * S + c);
+            lo[p] = pack_h2(__low2half(v0), __low2half(v1));
+            hi[p] = pack_h2(__high2half(v0), __high2half(v1));
+        }
+        uint4 *d0 = reinterpret_cast<uint4 *>(dst + (uint64_t)c * Bpad + row0);
+        uint4 *d1 = reinterpret_cast<uint4 *>(dst + (uint64_t)(c + 1) * Bpad + row0);
+        d0[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        d0[1] = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+        d1[0] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        d1[1] = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+    }
+}
+
+// G_{l-1} = acc * [H > 0], written over H (same positions, so no lane reads another's)
+template <int N, int S>
+__device__ __forceinline__ void mask_store(const float (&acc)[1][N / 8][4], __half *H, int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < N / 8; nt++) {
+        const int n = nt * 8 + 2 * t;
+        __half2 *p0 = reinterpret_cast<__half2 *>(H + g * S + n);
+        __half2 *p1 = reinterpret_cast<__half2 *>(H + (g + 8) * S + n);
+        const float2 h0 = __half22float2(*p0), h1 = __half22float2(*p1);
+        *p0 = __floats2half2_rn(h0.x > 0.f ? acc[0][nt][0] : 0.f, h0.y > 0.f ? acc[0][nt][1] : 0.f);
+        *p1 = __floats2half2_rn(h1.x > 0.f ? acc[0][nt][2] : 0.f, h1.y > 0.f ? acc[0][nt][3] : 0.f);
+    }
+}
+
+struct TrainArgs {
+    const float *q, *dir, *pdf, *w;
+    uint64_t B, Bpad;
+    __half *xt, *gt;
+    float *scal;  // [0] weight mean (in), [1] loss sum (accumulated)
+    GuideBox box;
+};
+
+__global__ void __launch_bounds__(kTrainWarps * 32, 1) k_guide_train_fb(const uint4 *img, TrainArgs A)
+{
+    extern __shared__ uint4 train_smem[];
+    for (int i = threadIdx.x; i < kGuideImgBytes / 16; i += blockDim.x) train_smem[i] = img[i];
+    __syncthreads();
+    unsigned char *sm = reinterpret_cast<unsigned char *>(train_smem);
+    const __half *W = reinterpret_cast<const __half *>(sm);
+    const float *bias = reinterpret_cast<const float *>(sm + kGuideImgBias);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *wb = sm + kGuideImgBytes + warp * kTrainWarpBytes;
+    __half *X0 = reinterpret_cast<__half *>(wb + kTrainX0);
+    __half *H1 = reinterpret_cast<__half *>(wb + kTrainH);
+    __half *H2 = H1 + 16 * 72, *H3 = H2 + 16 * 72, *H4 = H3 + 16 * 72;
+    __half *D = reinterpret_cast<__half *>(wb + kTrainD);
+    float *O = reinterpret_cast<float *>(wb + kTrainO);
+    const float wmean = A.scal[0];
+    const float winv = wmean > 0.f ? 1.f / wmean : 0.f;
+    const uint64_t Bp = A.Bpad;
+    float lsum = 0.f;
+    for (uint64_t tile = (uint64_t)blockIdx.x * kTrainWarps + warp; tile * 16 < Bp;
+         tile += (uint64_t)gridDim.x * kTrainWarps) {
+        const uint64_t row0 = tile * 16;
+        {
+            const uint64_t r = row0 + (lane & 15);
+            float q[9];
+#pragma unroll
+            for (int i = 0; i < 9; i++) q[i] = r < A.B ? A.q[9 * r + i] : 0.f;
+            guide_encode(lane >> 4, q, A.box, reinterpret_cast<__half2 *>(X0 + (lane & 15) * 152));
+        }
+        __syncwarp();
+        store_t<kGuideIn, 152>(X0, A.xt + (uint64_t)guide_xoff(0) * Bp, Bp, row0, lane);
+        {
+            float acc[1][8][4];
+            guide_gemm<1, kGuideIn, 64, 152, 152>(acc, X0, W + guide_iw(0), lane);
+            guide_store_hidden<1, 64, 72>(acc, bias + guide_ib(0), H1, lane);
+            __syncwarp();
+            store_t<64, 72>(H1, A.xt + (uint64_t)guide_xoff(1) * Bp, Bp, row0, lane);
+            guide_gemm<1, 64, 64, 72, 72>(acc, H1, W + guide_iw(1), lane);
+            guide_store_hidden<1, 64, 72>(acc, bias + guide_ib(1), H2, lane);
+            __syncwarp();
+            store_t<64, 72>(H2, A.xt + (uint64_t)guide_xoff(2) * Bp, Bp, row0, lane);
+            guide_gemm<1, 64, 64, 72, 72>(acc, H2, W + guide_iw(2), lane);
+            guide_store_hidden<1, 64, 72>(acc, bias + guide_ib(2), H3, lane);
+            __syncwarp();
+            store_t<64, 72>(H3, A.xt + (uint64_t)guide_xoff(3) * Bp, Bp, row0, lane);
+            guide_gemm<1, 64, 64, 72, 72>(acc, H3, W + guide_iw(3), lane);
+            guide_store_hidden<1, 64, 72>(acc, bias + guide_ib(3), H4, lane);
+            __syncwarp();
+            store_t<64, 72>(H4, A.xt + (uint64_t)guide_xoff(4) * Bp, Bp, row0, lane);
+        }
+        {
+            float acc[1][6][4];
+            guide_gemm<1, 64, kGuideOut, 72, 72>(acc, H4, W + guide_iw(4), lane);
+            guide_store_out<1, kGuideOut, 49>(acc, bias + guide_ib(4), O, lane);
+        }
+        __syncwarp();
+        if (lane < 16) {
+            const uint64_t r = row0 + lane;
+            float dout[kGuideOut];
+            if (r < A.B) {
+                const float wt = fminf(A.w[r] * winv, kGuideWeightClip);
+                const V3 wi = v3(A.dir[3 * r], A.dir[3 * r + 1], A.dir[3 * r + 2]);
+                lsum += guide_loss_grad(O + lane * 49, wi, A.pdf[r], wt, dout);
+            } else {
+#pragma unroll
+                for (int i = 0; i < kGuideOut; i++) dout[i] = 0.f;
+            }
+            __half2 *drow = reinterpret_cast<__half2 *>(D + lane * 56);
+#pragma unroll
+            for (int i = 0; i < kGuideOut / 2; i++)
+                drow[i] = __floats2half2_rn(dout[2 * i] * (1.f / kGuideGradScale), dout[2 * i + 1] * (1.f / kGuideGradScale));
+        }
+        __syncwarp();
+        store_t<kGuideOut, 56>(D, A.gt + (uint64_t)guide_goff(4) * Bp, Bp, row0, lane);
+        {
+            float acc[1][8][4];
+            guide_gemm_bt<1, kGuideOut, 64, 56, 72>(acc, D, W + guide_iw(4), lane);
+            mask_store<64, 72>(acc, H4, lane);  // G3
+            __syncwarp();
+            store_t<64, 72>(H4, A.gt + (uint64_t)guide_goff(3) * Bp, Bp, row0, lane);
+            guide_gemm_bt<1, 64, 64, 72, 72>(acc, H4, W + guide_iw(3), lane);
+            mask_store<64, 72>(acc, H3, lane);  // G2
+            __syncwarp();
+            store_t<64, 72>(H3, A.gt + (uint64_t)guide_goff(2) * Bp, Bp, row0, lane);
+            guide_gemm_bt<1, 64, 64, 72, 72>(acc, H3, W + guide_iw(2), lane);
+            mask_store<64, 72>(acc, H2, lane);  // G1
+            __syncwarp();
+            store_t<64, 72>(H2, A.gt + (uint64_t)guide_goff(1) * Bp, Bp, row0, lane);
+            guide_gemm_bt<1, 64, 64, 72, 72>(acc, H2, W + guide_iw(1), lane);
+            mask_store<64, 72>(acc, H1, lane);  // G0
+            __syncwarp();
+            store_t<64, 72>(H1, A.gt + (uint64_t)guide_goff(0) * Bp, Bp, row0, lane);
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    if (lane == 0 && lsum != 0.f) atomicAdd(A.scal + 1, lsum);
+}
+
+// dW (16 input features x NT*8 outputs) over rows [r0, r1): A = X^T plane rows, B = G^T plane rows
+template <int NT>
+__device__ __forceinline__ void wgrad_tile(const __half *X, const __half *G, uint64_t Bp, int mt, uint64_t r0,
+                                           uint64_t r1, float *dW, int out, int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+    float acc[NT][4];
+#pragma unroll
+    for (int n = 0; n < NT; n++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc[n][i] = 0.f;
+    const uint32_t *xa = reinterpret_cast<const uint32_t *>(X + (uint64_t)(mt * 16 + g) * Bp);
+    const uint32_t *xb = reinterpret_cast<const uint32_t *>(X + (uint64_t)(mt * 16 + g + 8) * Bp);
+    const uint32_t *gb[NT];
+#pragma unroll
+    for (int n = 0; n < NT; n++) gb[n] = reinterpret_cast<const uint32_t *>(G + (uint64_t)(n * 8 + g) * Bp);
+    for (uint64_t r = r0; r < r1; r += 16) {
+        const uint64_t i0 = (r >> 1) + t;
+        const uint32_t a[4] = {__ldg(xa + i0), __ldg(xb + i0), __ldg(xa + i0 + 4), __ldg(xb + i0 + 4)};
+#pragma unroll
+        for (int n = 0; n < NT; n++) mma16816(acc[n], a, __ldg(gb[n] + i0), __ldg(gb[n] + i0 + 4));
+    }
+    const int m = mt * 16 + g;
+#pragma unroll
+    for (int n = 0; n < NT; n++) {
+        const int c = n * 8 + 2 * t;
+        dW[m * out + c] = acc[n][0];
+        dW[m * out + c + 1] = acc[n][1];
+        dW[(m + 8) * out + c] = acc[n][2];
+        dW[(m + 8) * out + c + 1] = acc[n][3];
+    }
+}
+
+__global__ void __launch_bounds__(128) k_guide_wgrad(const __half *xt, const __half *gt, uint64_t Bp, float *partial)
+{
+    const uint32_t c = blockIdx.x;
+    const int l = blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t r0 = (uint64_t)c * kWgradChunk, r1 = std::min<uint64_t>(r0 + kWgradChunk, Bp);
+    float *part = partial + (uint64_t)c * kGuideParamCount;
+    if (l < kGuideLayers) {
+        const __half *X = xt + (uint64_t)guide_xoff(l) * Bp;
+        const __half *G = gt + (uint64_t)guide_goff(l) * Bp;
+        const int mtiles = guide_in(l) / 16;
+        for (int mt = warp; mt < mtiles; mt += 4) {
+            if (l == kGuideLayers - 1)
+                wgrad_tile<6>(X, G, Bp, mt, r0, r1, part + guide_pw(l), kGuideOut, lane);
+            else
+                wgrad_tile<8>(X, G, Bp, mt, r0, r1, part + guide_pw(l), kGuideHidden, lane);
+        }
+    } else {
+        for (int f = warp; f < kGuideGFeatures; f += 4) {
+            const __half2 *g2 = reinterpret_cast<const __half2 *>(gt + (uint64_t)f * Bp + r0);
+            float s = 0.f;
+            for (uint64_t i = lane; i < (r1 - r0) / 2; i += 32) {
+                const float2 v = __half22float2(g2[i]);
+                s += v.x + v.y;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) {
+                const int ll = f < 4 * kGuideHidden ? f / kGuideHidden : 4;
+                part[guide_pb(ll) + (f - guide_goff(ll))] = s;
+            }
+        }
+    }
+}
+
+// deterministic weight mean (one block)
+__global__ void __launch_bounds__(1024) k_guide_wmean(const float *w, uint64_t B, float *scal)
+{
+    __shared__ double red[32];
+    double s = 0.0;
+    for (uint64_t i = threadIdx.x; i < B; i += blockDim.x) s += (double)w[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) {
+            scal[0] = B ? (float)(s / (double)B) : 0.f;
+            scal[1] = 0.f;
+            reinterpret_cast<uint32_t *>(scal)[2] = 0u;
+        }
+    }
+}
+
+__global__ void k_guide_reduce(const float *partial, uint32_t nchunks, float scale, float *grad, float *scal)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (uint32_t)kGuideParamCount) return;
+    float g = 0.f;
+    for (uint32_t c = 0; c < nchunks; c++) g += partial[(uint64_t)c * kGuideParamCount + p];
+    g *= scale;
+    grad[p] = g;
+    if (!isfinite(g)) atomicOr(reinterpret_cast<uint32_t *>(scal) + 2, 1u);
+}
+
+struct AdamArgs {
+    float lr, bc1, bc2;
+};
+
+__device__ __forceinline__ void image_write(int p, float w, __half *img_w, float *img_b)
+{
+    int l = 0;
+    while (l < kGuideLayers - 1 && p >= guide_pw(l + 1)) l++;
+    if (p < guide_pb(l)) {
+        const int i = p - guide_pw(l), out = guide_out(l);
+        img_w[guide_iw(l) + (i % out) * guide_stride(l) + i / out] = __float2half_rn(w);
+    } else {
+        img_b[guide_ib(l) + (p - guide_pb(l))] = w;
+    }
+}
+
+__global__ void k_guide_adam(const float *grad, const float *scal, float *master, float *m, float *v, __half *img_w,
+                             float *img_b, AdamArgs a)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kGuideParamCount) return;
+    if (reinterpret_cast<const uint32_t *>(scal)[2]) return;  // a non-finite gradient: skip the step
+    const float g = grad[p];
+    const float mm = kAdamB1 * m[p] + (1.f - kAdamB1) * g;
+    const float vv = kAdamB2 * v[p] + (1.f - kAdamB2) * g * g;
+    m[p] = mm;
+    v[p] = vv;
+    const float w = master[p] - a.lr * (mm / a.bc1) / (sqrtf(vv / a.bc2) + kAdamEps);
+    master[p] = w;
+    image_write(p, w, img_w, img_b);
+}
+
+// ------------------------------------------------------------------ batched evaluation
+
+struct QuerySrc {
+    const float *q;
+    __device__ bool operator()(uint32_t row, float *o) const
+    {
+#pragma unroll
+        for (int i = 0; i < 9; i++) o[i] = q[9ull * row + i];
+        return true;
+    }
+};
+
+struct RawSink {
+    float *out;
+    __device__ void operator()(uint32_t row, bool, const float *o) const
+    {
+        for (int i = 0; i < kGuideOut; i++) out[(uint64_t)row * kGuideOut + i] = o[i];
+    }
+};
+
+struct PdfSink {
+    const float *dir, *pdfb;
+    float *out;
+    __device__ void operator()(uint32_t row, bool, const float *o) const
+    {
+        GuideParams P;
+        guide_decode(o, P);
+        const V3 w = v3(dir[3ull * row], dir[3ull * row + 1], dir[3ull * row + 2]);
+        out[row] = P.alpha * guide_pdf(P, w) + (1.f - P.alpha) * pdfb[row];
+    }
+};
+
+struct SampleSink {
+    const float *u;
+    float *dirs, *pdf;
+    __device__ void operator()(uint32_t row, bool, const float *o) const
+    {
+        GuideParams P;
+        guide_decode(o, P);
+        const V3 w = guide_sample(P, u[3ull * row], u[3ull * row + 1], u[3ull * row + 2]);
+        dirs[3ull * row] = w.x;
+        dirs[3ull * row + 1] = w.y;
+        dirs[3ull * row + 2] = w.z;
+        pdf[row] = guide_pdf(P, w);
+    }
+};
+
+template <class Sink>
+__global__ void __launch_bounds__(kInferWarps * 32) k_guide_eval(const uint4 *img, GuideBox box, uint32_t n,
+                                                                  QuerySrc src, Sink sink)
+{
+    guide_infer_rows(img, box, n, src, sink);
+}
+
+// ------------------------------------------------------------------ training samples
+
+// PCG hash (Jarzynski and Olano, "Hash Functions for GPU Rendering", 2020)
+__device__ __forceinline__ uint32_t pcg_hash(uint32_t x)
+{
+    const uint32_t s = x * 747796405u + 2891336453u;
+    const uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+
+__device__ __forceinline__ float record_weight(const GuideRecord &r)
+{
+    float s = 0.f;
+    if (r.d.y > 0.f) s += r.e.x / r.d.y;
+    if (r.d.z > 0.f) s += r.e.y / r.d.z;
+    if (r.d.w > 0.f) s += r.e.z / r.d.w;
+    return s * (1.f / 3.f);
+}
+
+__global__ void k_guide_gather(const GuideRecord *recs, const uint32_t *nz, uint32_t nnz, uint32_t B, uint32_t seed,
+                               float *q, float *dir, float *pdf, float *w)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B) return;
+    const uint32_t h = pcg_hash(i ^ pcg_hash(seed));
+    const uint32_t j = (uint32_t)(((uint64_t)h * nnz) >> 32);
+    const GuideRecord r = recs[nz[j]];
+    const float v[9] = {r.a.x, r.a.y, r.a.z, r.a.w, r.b.x, r.b.y, r.b.z, r.b.w, r.c.x};
+#pragma unroll
+    for (int k = 0; k < 9; k++) q[9ull * i + k] = v[k];
+    dir[3ull * i] = r.c.y;
+    dir[3ull * i + 1] = r.c.z;
+    dir[3ull * i + 2] = r.c.w;
+    pdf[i] = r.d.x;
+    w[i] = record_weight(r);
+}
+
+}  // namespace
+
+GuideBox guide_box(const rt_guide *g)
+{
+    GuideBox b;
+    const float *lo = g->opts.bbox_min, *hi = g->opts.bbox_max;
+    b.lo = make_float3(lo[0], lo[1], lo[2]);
+    b.inv_ext = make_float3(1.f / (hi[0] - lo[0]), 1.f / (hi[1] - lo[1]), 1.f / (hi[2] - lo[2]));
+    return b;
+}
+
+static void build_image(const float *master, std::vector<uint8_t> &img)
+{
+    img.assign(kGuideImgBytes, 0);
+    __half *h = reinterpret_cast<__half *>(img.data());
+    float *b = reinterpret_cast<float *>(img.data() + kGuideImgBias);
+    for (int l = 0; l < kGuideLayers; l++) {
+        const int in = guide_in(l), out = guide_out(l);
+        for (int k = 0; k < in; k++)
+            for (int n = 0; n < out; n++)
+                h[guide_iw(l) + n * guide_stride(l) + k] = __float2half_rn(master[guide_pw(l) + k * out + n]);
+        for (int n = 0; n < out; n++) b[guide_ib(l) + n] = master[guide_pb(l) + n];
+    }
+}
+
+static int guide_upload_params(rt_guide *g, const float *host)
+{
+    cudaStream_t st = g->ctx->stream;
+    std::vector<uint8_t> img;
+    build_image(host, img);
+    RTB_CHECK(g->master.upload(host, 4ull * kGuideParamCount, st));
+    RTB_CHECK(g->img.upload(img.data(), img.size(), st));
+    RTB_CHECK(g->adam_m.reserve(4ull * kGuideParamCount));
+    RTB_CHECK(g->adam_v.reserve(4ull * kGuideParamCount));
+    RTB_CUDA(cudaMemsetAsync(g->adam_m.ptr, 0, 4ull * kGuideParamCount, st));
+    RTB_CUDA(cudaMemsetAsync(g->adam_v.ptr, 0, 4ull * kGuideParamCount, st));
+    RTB_CUDA(cudaStreamSynchronize(st));  // `img` is pageable host memory
+    g->step = 0;
+    return RT_OK;
+}
+
+// One training step on device arrays (B rows). loss_out / grad_host may be null.
+int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf, const float *w, uint64_t B, int apply,
+                float *grad_host, float *loss_out)
+{
+    cudaStream_t st = g->ctx->stream;
+    if (B == 0) {
+        if (loss_out) *loss_out = 0.f;
+        if (grad_host) std::memset(grad_host, 0, 4ull * kGuideParamCount);
+        return RT_OK;
+    }
+    const uint64_t Bp = (B + 15) / 16 * 16;
+    const uint32_t nchunks = (uint32_t)((Bp + kWgradChunk - 1) / kWgradChunk);
+    RTB_CHECK(g->xt.reserve(2ull * kGuideXFeatures * Bp));
+    RTB_CHECK(g->gt.reserve(2ull * kGuideGFeatures * Bp));
+    RTB_CHECK(g->partial.reserve(4ull * kGuideParamCount * nchunks));
+    RTB_CHECK(g->grad.reserve(4ull * kGuideParamCount));
+    RTB_CHECK(g->scal.reserve(64));
+    if (!g->host_scal) RTB_CUDA(cudaMallocHost(&g->host_scal, 64));
+    float *scal = g->scal.as<float>();
+    k_guide_wmean<<<1, 1024, 0, st>>>(w, B, scal);
+    RTB_CUDA(cudaGetLastError());
+    static bool attr = false;
+    if (!attr) {
+        RTB_CUDA(cudaFuncSetAttribute(k_guide_train_fb, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem));
+        attr = true;
+    }
+    TrainArgs a{q, dir, pdf, w, B, Bp, g->xt.as<__half>(), g->gt.as<__half>(), scal, guide_box(g)};
+    const uint64_t tiles = Bp / 16;
+    const unsigned grid =
+        (unsigned)std::min<uint64_t>((tiles + kTrainWarps - 1) / kTrainWarps, (uint64_t)std::max(g->ctx->sm_count, 1));
+    k_guide_train_fb<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(g->img.as<uint4>(), a);
+    RTB_CUDA(cudaGetLastError());
+    k_guide_wgrad<<<dim3(nchunks, kGuideLayers + 1), 128, 0, st>>>(g->xt.as<__half>(), g->gt.as<__half>(), Bp,
+                                                                   g->partial.as<float>());
+    RTB_CUDA(cudaGetLastError());
+    const unsigned pblocks = (kGuideParamCount + 255) / 256;
+    k_guide_reduce<<<pblocks, 256, 0, st>>>(g->partial.as<float>(), nchunks, kGuideGradScale / (float)B,
+                                            g->grad.as<float>(), scal);
+    RTB_CUDA(cudaGetLastError());
+    if (apply) {
+        g->step++;
+        AdamArgs ad;
+        ad.lr = g->opts.learning_rate;
+        ad.bc1 = 1.f - (float)std::pow((double)kAdamB1, (double)g->step);
+        ad.bc2 = 1.f - (float)std::pow((double)kAdamB2, (double)g->step);
+        k_guide_adam<<<pblocks, 256, 0, st>>>(g->grad.as<float>(), scal, g->master.as<float>(), g->adam_m.as<float>(),
+                                              g->adam_v.as<float>(), g->img.as<__half>(),
+                                              reinterpret_cast<float *>(g->img.as<uint8_t>() + kGuideImgBias), ad);
+        RTB_CUDA(cudaGetLastError());
+    }
+    if (loss_out || grad_host) {
+        RTB_CUDA(cudaMemcpyAsync(g->host_scal, scal, 16, cudaMemcpyDeviceToHost, st));
+        if (grad_host)
+            RTB_CUDA(cudaMemcpyAsync(grad_host, g->grad.ptr, 4ull * kGuideParamCount, cudaMemcpyDeviceToHost, st));
+        RTB_CUDA(cudaStreamSynchronize(st));
+        if (loss_out) *loss_out = static_cast<const float *>(g->host_scal)[1] / (float)B;
+    }
+    return RT_OK;
+}
+
+}  // namespace rtb
+
+using namespace rtb;
+
+extern "C" {
+
+int rt_guide_create(rt_context *ctx, const rt_guide_opts *opts, rt_guide **out)
+{
+    if (!ctx || !opts || !out) return fail(RT_ERR_INVALID, "rt_guide_create: null argument");
+    for (int a = 0; a < 3; a++)
+        if (!(opts->bbox_max[a] > opts->bbox_min[a]))
+            return fail(RT_ERR_INVALID, "rt_guide_create: empty bounding box");
+    if (!(opts->learning_rate > 0)) return fail(RT_ERR_INVALID, "rt_guide_create: learning rate must be positive");
+    if (opts->record_capacity > kRecNone - 1)
+        return fail(RT_ERR_INVALID, "rt_guide_create: record capacity above 4,194,302");
+    RTB_CUDA(cudaSetDevice(ctx->device));
+    rt_guide *g = new rt_guide();
+    g->ctx = ctx;
+    g->opts = *opts;
+    g->rec_cap = opts->record_capacity ? opts->record_capacity : kRecNone - 1;
+    // He-uniform hidden layers, Glorot-uniform output layer, zero biases (seeded PCG32)
+    std::vector<float> p(kGuideParamCount, 0.f);
+    uint64_t state = 0x853c49e6748fea9bull ^ ((uint64_t)opts->seed << 1);
+    auto next = [&]() {
+        const uint64_t old = state;
+        state = old * 6364136223846793005ull + 1442695040888963407ull;
+        const uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u), rot = (uint32_t)(old >> 59u);
+        const uint32_t r = (xs >> rot) | (xs << ((32u - rot) & 31u));
+        return (float)(r >> 8) * (1.0f / 16777216.0f);
+    };
+    for (int l = 0; l < kGuideLayers; l++) {
+        const int in = guide_in(l), o = guide_out(l);
+        const float a = l == kGuideLayers - 1 ? std::sqrt(6.f / (float)(in + o)) : std::sqrt(6.f / (float)in);
+        for (int i = 0; i < in * o; i++) p[guide_pw(l) + i] = (2.f * next() - 1.f) * a;
+    }
+    int s = guide_upload_params(g, p.data());
+    if (s != RT_OK) {
+        delete g;
+        return s;
+    }
+    *out = g;
+    return RT_OK;
+}
+
+int rt_guide_destroy(rt_guide *g)
+{
+    if (!g) return RT_OK;
+    cudaSetDevice(g->ctx->device);
+    cudaStreamSynchronize(g->ctx->stream);
+    if (g->host_scal) cudaFreeHost(g->host_scal);
+    delete g;
+    return RT_OK;
+}
+
+int rt_guide_param_count(rt_guide *g, uint64_t *n)
+{
+    if (!g || !n) return fail(RT_ERR_INVALID, "rt_guide_param_count: null argument");
+    *n = kGuideParamCount;
+    return RT_OK;
+}
+
+int rt_guide_params_get(rt_guide *g, float *host, uint64_t n)
+{
+    if (!g || !host) return fail(RT_ERR_INVALID, "rt_guide_params_get: null argument");
+    if (n != (uint64_t)kGuideParamCount) return fail(RT_ERR_INVALID, "rt_guide_params_get: wrong parameter count");
+    RTB_CUDA(cudaSetDevice(g->ctx->device));
+    RTB_CUDA(cudaMemcpyAsync(host, g->master.ptr, 4ull * n, cudaMemcpyDeviceToHost, g->ctx->stream));
+    RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    return RT_OK;
+}
+
+int rt_guide_params_set(rt_guide *g, const float *host, uint64_t n)
+{
+    if (!g || !host) return fail(RT_ERR_INVALID, "rt_guide_params_set: null argument");
+    if (n != (uint64_t)kGuideParamCount) return fail(RT_ERR_INVALID, "rt_guide_params_set: wrong parameter count");
+    for (uint64_t i = 0; i < n; i++)
+        if (!std::isfinite(host[i])) return fail(RT_ERR_INVALID, "rt_guide_params_set: non-finite parameter");
+    RTB_CUDA(cudaSetDevice(g->ctx->device));
+    return guide_upload_params(g, host);
+}
+
+int rt_guide_steps(rt_guide *g, uint64_t *steps)
+{
+    if (!g || !steps) return fail(RT_ERR_INVALID, "rt_guide_steps: null argument");
+    *steps = g->step;
+    return RT_OK;
+}
+
+static int guide_eval_common(rt_guide *g, uint64_t B, const char *who)
+{
+    if (!g) return fail(RT_ERR_INVALID, std::string(who) + ": null guide");
+    if (B >= (1ull << 31)) return fail(RT_ERR_INVALID, std::string(who) + ": batch too large");
+    RTB_CUDA(cudaSetDevice(g->ctx->device));
+    static bool attr = false;
+    if (!attr) {
+        RTB_CUDA(cudaFuncSetAttribute(k_guide_eval<RawSink>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
+        RTB_CUDA(cudaFuncSetAttribute(k_guide_eval<PdfSink>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
+        RTB_CUDA(
+            cudaFuncSetAttribute(k_guide_eval<SampleSink>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
+        attr = true;
+    }
+    return RT_OK;
+}
+
+static unsigned infer_grid(rt_guide *g, uint64_t B)
+{
+    const uint64_t tiles = (B + 31) / 32;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((tiles + kInferWarps - 1) / kInferWarps,
+                                                              2ull * std::max(g->ctx->sm_count, 1)));
+}
+
+int rt_guide_eval(rt_guide *g, const float *queries, uint64_t B, float *out)
+{
+    RTB_CHECK(guide_eval_common(g, B, "rt_guide_eval"));
+    if (B == 0) return RT_OK;
+    if (!queries || !out) return fail(RT_ERR_INVALID, "rt_guide_eval: null buffer");
+    k_guide_eval<RawSink><<<infer_grid(g, B), kInferWarps * 32, kInferSmem, g->ctx->stream>>>(
+        g->img.as<uint4>(), guide_box(g), (uint32_t)B, QuerySrc{queries}, RawSink{out});
+    RTB_CUDA(cudaGetLastError());
+    RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    return RT_OK;
+}
+
+int rt_guide_pdf(rt_guide *g, const float *queries, const float *dirs, const float *bsdf_pdf, uint64_t B, float *out)
+{
+    RTB_CHECK(guide_eval_common(g, B, "rt_guide_pdf"));
+    if (B == 0) return RT_OK;
+    if (!queries || !dirs || !bsdf_pdf || !out) return fail(RT_ERR_INVALID, "rt_guide_pdf: null buffer");
+    k_guide_eval<PdfSink><<<infer_grid(g, B), kInferWarps * 32, kInferSmem, g->ctx->stream>>>(
+        g->img.as<uint4>(), guide_box(g), (uint32_t)B, QuerySrc{queries}, PdfSink{dirs, bsdf_pdf, out});
+    RTB_CUDA(cudaGetLastError());
+    RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    return RT_OK;
+}
+
+int rt_guide_sample(rt_guide *g, const float *queries, const float *u3, uint64_t B, float *out_dirs, float *out_pdf)
+{
+    RTB_CHECK(guide_eval_common(g, B, "rt_guide_sample"));
+    if (B == 0) return RT_OK;
+    if (!queries || !u3 || !out_dirs || !out_pdf) return fail(RT_ERR_INVALID, "rt_guide_sample: null buffer");
+    k_guide_eval<SampleSink><<<infer_grid(g, B), kInferWarps * 32, kInferSmem, g->ctx->stream>>>(
+        g->img.as<uint4>(), guide_box(g), (uint32_t)B, QuerySrc{queries}, SampleSink{u3, out_dirs, out_pdf});
+    RTB_CUDA(cudaGetLastError());
+    RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    return RT_OK;
+}
+
+int rt_guide_train_step(rt_guide *g, const float *queries, const float *dirs, const float *bsdf_pdf,
+                        const float *weights, uint64_t B, int apply, float *grad_host, float *loss_out)
+{
+    if (!g) return fail(RT_ERR_INVALID, "rt_guide_train_step: null guide");
+    if (B && (!queries || !dirs || !bsdf_pdf || !weights))
+        return fail(RT_ERR_INVALID, "rt_guide_train_step: null buffer");
+    if (B >= (1ull << 31)) return fail(RT_ERR_INVALID, "rt_guide_train_step: batch too large");
+    RTB_CUDA(cudaSetDevice(g->ctx->device));
+    return guide_train(g, queries, dirs, bsdf_pdf, weights, B, apply, grad_host, loss_out);
+}
+
+int rt_render_set_guide(rt_scene *s, rt_guide *g, int train)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_render_set_guide: null scene");
+    if (g && g->ctx->device != s->ctx->device) return fail(RT_ERR_INVALID, "rt_render_set_guide: device mismatch");
+    s->guide = g;
+    s->guide_train = g ? (train != 0) : 0;
+    return RT_OK;
+}
+
+int rt_guide_record_count(rt_guide *g, uint64_t *records, uint64_t *nonzero)
+{
+    if (!g) return fail(RT_ERR_INVALID, "rt_guide_record_count: null guide");
+    uint32_t c[2] = {0, 0};
+    if (g->rcnt.ptr) {
+        RTB_CUDA(cudaSetDevice(g->ctx->device));
+        RTB_CUDA(cudaMemcpyAsync(c, g->rcnt.ptr, 8, cudaMemcpyDeviceToHost, g->ctx->stream));
+        RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    }
+    if (records) *records = std::min(c[0], g->rec_cap);
+    if (nonzero) *nonzero = std::min(c[1], g->rec_cap);
+    return RT_OK;
+}
+
+int rt_guide_records_get(rt_guide *g, uint64_t first, uint64_t n, float *host)
+{
+    if (!g || (!host && n)) return fail(RT_ERR_INVALID, "rt_guide_records_get: null argument");
+    uint64_t have = 0;
+    RTB_CHECK(rt_guide_record_count(g, &have, nullptr));
+    if (first + n > have) return fail(RT_ERR_INVALID, "rt_guide_records_get: range beyond the recorded samples");
+    if (n == 0) return RT_OK;
+    RTB_CUDA(cudaMemcpyAsync(host, g->recs.as<GuideRecord>() + first, sizeof(GuideRecord) * n, cudaMemcpyDeviceToHost,
+                             g->ctx->stream));
+    RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    return RT_OK;
+}
+
+int rt_guide_train_records(rt_guide *g, uint32_t steps, uint32_t batch, uint32_t seed, float *loss_out)
+{
+    if (!g) return fail(RT_ERR_INVALID, "rt_guide_train_records: null guide");
+    if (batch == 0 || batch >= (1u << 30)) return fail(RT_ERR_INVALID, "rt_guide_train_records: bad batch size");
+    uint64_t nnz = 0;
+    RTB_CHECK(rt_guide_record_count(g, nullptr, &nnz));
+    if (loss_out) *loss_out = 0.f;
+    if (nnz == 0 || steps == 0) return RT_OK;
+    cudaStream_t st = g->ctx->stream;
+    RTB_CHECK(g->tq.reserve(36ull * batch));
+    RTB_CHECK(g->tdir.reserve(12ull * batch));
+    RTB_CHECK(g->tpdf.reserve(4ull * batch));
+    RTB_CHECK(g->tw.reserve(4ull * batch));
+    for (uint32_t k = 0; k < steps; k++) {
+        k_guide_gather<<<(batch + 255) / 256, 256, 0, st>>>(
+            g->recs.as<GuideRecord>(), g->nz.as<uint32_t>(), (uint32_t)nnz, batch,
+            seed * 0x9E3779B9u + (uint32_t)g->step * 0x85EBCA6Bu + k, g->tq.as<float>(), g->tdir.as<float>(),
+            g->tpdf.as<float>(), g->tw.as<float>());
+        RTB_CUDA(cudaGetLastError());
+        RTB_CHECK(guide_train(g, g->tq.as<float>(), g->tdir.as<float>(), g->tpdf.as<float>(), g->tw.as<float>(), batch,
+                              1, nullptr, (k + 1 == steps) ? loss_out : nullptr));
+    }
+    return RT_OK;
+}
+
+}  // extern "C"

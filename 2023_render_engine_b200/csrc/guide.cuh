@@ -1,0 +1,447 @@
+// Learned path guide: device-side pieces shared by the training kernels (guide.cu) and the
+// path tracer (render.cu). The reference renderer has no counterpart; this is the estimator's
+// importance-sampling proposal, combined with BSDF sampling by one-sample MIS.
+//
+// Network: 144 encoded inputs -> 4 hidden layers of 64 (ReLU) -> 48 outputs, FP16 weights and
+// activations on the tensor cores (mma.sync m16n8k16, FP32 accumulation), FP32 master weights.
+// Input encoding of a shading point (position p, shading normal n, outgoing direction wo):
+//   [0, 72)    p normalised to the guide's box, per axis 12 frequency bands: sin, cos(2^k pi u)
+//   [72, 104)  theta(wo) / pi, one-blob over 32 bins (Gaussian, sigma = 1/32)
+//   [104, 136) phi(wo) / 2pi + 1/2, one-blob over 32 bins
+//   [136, 139) n;  [139, 144) zero
+// Outputs per lobe j (8 von Mises-Fisher lobes): o[4j] -> theta = pi sigmoid, o[4j+1] -> phi =
+// 2 pi sigmoid, o[4j+2] -> kappa = exp(clamp(., -4, 8)), o[4j+3] -> softmax weight logit;
+// o[32] -> alpha = 0.95 sigmoid, the probability of sampling the guide. o[33..47] unused.
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include "shading.cuh"
+
+namespace rtb {
+
+constexpr int kGuideIn = 144, kGuideHidden = 64, kGuideOut = 48, kGuideLayers = 5, kGuideLobes = 8;
+constexpr int kGuideParamCount = 24880;  // 144*64+64 + 3*(64*64+64) + 64*48+48
+constexpr float kGuideAlphaMax = 0.95f;
+constexpr float kGuideLogKappaMin = -4.f, kGuideLogKappaMax = 8.f;
+constexpr float kGuideWeightClip = 32.f;   // training weight / batch mean is clipped here
+constexpr float kGuideGradClamp = 8192.f;  // per-output gradient clamp
+constexpr float kGuideGradScale = 8.f;     // output gradients are stored as fp16(g / scale)
+
+// path-state record link: bits [10, 32) of the flags word
+constexpr uint32_t kRecNone = 0x3FFFFFu;
+constexpr int kRecShift = 10;
+
+__host__ __device__ constexpr int guide_in(int l) { return l == 0 ? kGuideIn : kGuideHidden; }
+__host__ __device__ constexpr int guide_out(int l) { return l == kGuideLayers - 1 ? kGuideOut : kGuideHidden; }
+// FP32 master parameters: for each layer W_l (in x out, row-major), then b_l
+__host__ __device__ constexpr int guide_pw(int l)
+{
+    return l == 0 ? 0 : guide_pw(l - 1) + guide_in(l - 1) * guide_out(l - 1) + guide_out(l - 1);
+}
+__host__ __device__ constexpr int guide_pb(int l) { return guide_pw(l) + guide_in(l) * guide_out(l); }
+static_assert(guide_pb(4) + 48 == kGuideParamCount, "parameter count");
+
+// FP16 weight image (the shared-memory copy, loaded with 16-byte copies): W_l transposed,
+// out_l rows of stride guide_stride(l) halves (padding keeps ldmatrix conflict-free), then
+// the FP32 biases (64 per hidden layer, 48 for the output layer).
+__host__ __device__ constexpr int guide_stride(int l) { return l == 0 ? 152 : 72; }
+__host__ __device__ constexpr int guide_iw(int l)
+{
+    return l == 0 ? 0 : guide_iw(l - 1) + guide_out(l - 1) * guide_stride(l - 1);
+}
+constexpr int kGuideImgHalves = 64 * 152 + 3 * 64 * 72 + 48 * 72;
+static_assert(guide_iw(4) + 48 * 72 == kGuideImgHalves, "image layout");
+constexpr int kGuideImgBias = kGuideImgHalves * 2;  // byte offset of the biases
+__host__ __device__ constexpr int guide_ib(int l) { return l * 64; }  // float index of b_l
+constexpr int kGuideImgBytes = kGuideImgBias + 4 * (4 * 64 + 48);
+static_assert(kGuideImgBias % 16 == 0 && kGuideImgBytes % 16 == 0, "image alignment");
+
+// transposed activations / gradients for the weight-gradient kernel: feature-major planes
+__host__ __device__ constexpr int guide_xoff(int l) { return l == 0 ? 0 : kGuideIn + (l - 1) * kGuideHidden; }
+__host__ __device__ constexpr int guide_goff(int l) { return l * kGuideHidden; }
+constexpr int kGuideXFeatures = kGuideIn + 4 * kGuideHidden;   // 400
+constexpr int kGuideGFeatures = 4 * kGuideHidden + kGuideOut;  // 304
+
+// Per queue slot: the decoded mixture at the path's current hit (written by the inference
+// kernel, read by shading). alpha = 0 marks a hit that is not guided.
+struct GuideParams {
+    float4 lobe[kGuideLobes];  // mean direction xyz (world), concentration
+    float lam[kGuideLobes];    // lobe weights, sum 1
+    float lamn[kGuideLobes];   // lam * vMF normalisation
+    float alpha;
+    float pad[3];
+};
+static_assert(sizeof(GuideParams) == 208, "GuideParams layout");
+
+// One training sample: a guided vertex of a traced path.
+struct GuideRecord {
+    float4 a;  // position xyz, normal x
+    float4 b;  // normal yz, wo xy
+    float4 c;  // wo z, sampled direction wi xyz
+    float4 d;  // BSDF sampling pdf of wi, path throughput before the vertex rgb
+    float4 e;  // radiance arriving after the vertex rgb (its suffix sum once the path retired),
+               // previous record of the path (uint bits, kRecNone: none)
+};
+static_assert(sizeof(GuideRecord) == 80, "GuideRecord layout");
+
+struct GuideBox {
+    float3 lo, inv_ext;
+};
+}  // namespace rtb
+struct rt_guide;
+namespace rtb {
+GuideBox guide_box(const rt_guide *g);  // position encoding domain of a guide
+
+// ------------------------------------------------------------------ tensor-core helpers
+
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void *p)
+{
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const void *p)
+{
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+// acc[MT x 16 rows][N] = A[MT*16 rows][K] (stride SA) * W, W^T stored [N][SW] (forward layers)
+template <int MT, int K, int N, int SA, int SW>
+__device__ __forceinline__ void guide_gemm(float (&acc)[MT][N / 8][4], const __half *A, const __half *Wt, int lane)
+{
+#pragma unroll
+    for (int m = 0; m < MT; m++)
+#pragma unroll
+        for (int n = 0; n < N / 8; n++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) acc[m][n][i] = 0.f;
+#pragma unroll
+    for (int ks = 0; ks < K / 16; ks++) {
+        uint32_t a[MT][4];
+#pragma unroll
+        for (int m = 0; m < MT; m++)
+            ldsm_x4(a[m], A + (m * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * SA + ks * 16 + (lane >> 4) * 8);
+#pragma unroll
+        for (int np = 0; np < N / 16; np++) {
+            uint32_t b[4];
+            ldsm_x4(b, Wt + (np * 16 + (lane & 7) + (lane >> 4) * 8) * SW + ks * 16 + ((lane >> 3) & 1) * 8);
+#pragma unroll
+            for (int m = 0; m < MT; m++) {
+                mma16816(acc[m][2 * np], a[m], b[0], b[1]);
+                mma16816(acc[m][2 * np + 1], a[m], b[2], b[3]);
+            }
+        }
+    }
+}
+
+// acc[MT x 16 rows][N] = G[rows][K] (stride SA) * W_l^T, with W_l^T stored [K][SW]
+// (backward: K = the layer's outputs, N = its inputs)
+template <int MT, int K, int N, int SA, int SW>
+__device__ __forceinline__ void guide_gemm_bt(float (&acc)[MT][N / 8][4], const __half *A, const __half *Wt, int lane)
+{
+#pragma unroll
+    for (int m = 0; m < MT; m++)
+#pragma unroll
+        for (int n = 0; n < N / 8; n++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) acc[m][n][i] = 0.f;
+#pragma unroll
+    for (int ks = 0; ks < K / 16; ks++) {
+        uint32_t a[MT][4];
+#pragma unroll
+        for (int m = 0; m < MT; m++)
+            ldsm_x4(a[m], A + (m * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * SA + ks * 16 + (lane >> 4) * 8);
+#pragma unroll
+        for (int np = 0; np < N / 16; np++) {
+            uint32_t b[4];
+            ldsm_x4_t(b, Wt + (ks * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * SW + np * 16 + (lane >> 4) * 8);
+#pragma unroll
+            for (int m = 0; m < MT; m++) {
+                mma16816(acc[m][2 * np], a[m], b[0], b[1]);
+                mma16816(acc[m][2 * np + 1], a[m], b[2], b[3]);
+            }
+        }
+    }
+}
+
+// bias + ReLU, FP16 store (stride SO halves)
+template <int MT, int N, int SO>
+__device__ __forceinline__ void guide_store_hidden(const float (&acc)[MT][N / 8][4], const float *bias, __half *out,
+                                                   int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int m = 0; m < MT; m++)
+#pragma unroll
+        for (int nt = 0; nt < N / 8; nt++) {
+            const int n = nt * 8 + 2 * t, r = m * 16 + g;
+            const float b0 = bias[n], b1 = bias[n + 1];
+            *reinterpret_cast<__half2 *>(out + r * SO + n) =
+                __floats2half2_rn(fmaxf(acc[m][nt][0] + b0, 0.f), fmaxf(acc[m][nt][1] + b1, 0.f));
+            *reinterpret_cast<__half2 *>(out + (r + 8) * SO + n) =
+                __floats2half2_rn(fmaxf(acc[m][nt][2] + b0, 0.f), fmaxf(acc[m][nt][3] + b1, 0.f));
+        }
+}
+
+// bias, FP32 store (stride SO floats)
+template <int MT, int N, int SO>
+__device__ __forceinline__ void guide_store_out(const float (&acc)[MT][N / 8][4], const float *bias, float *out,
+                                                int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int m = 0; m < MT; m++)
+#pragma unroll
+        for (int nt = 0; nt < N / 8; nt++) {
+            const int n = nt * 8 + 2 * t, r = m * 16 + g;
+            out[r * SO + n] = acc[m][nt][0] + bias[n];
+            out[r * SO + n + 1] = acc[m][nt][1] + bias[n + 1];
+            out[(r + 8) * SO + n] = acc[m][nt][2] + bias[n];
+            out[(r + 8) * SO + n + 1] = acc[m][nt][3] + bias[n + 1];
+        }
+}
+
+// ------------------------------------------------------------------ encoding
+
+__device__ __forceinline__ float guide_blob(float x, int i)
+{
+    const float d = x * 32.f - ((float)i + 0.5f);
+    return expf(-0.5f * d * d);
+}
+
+// part 0: position bands (half2 0..35); part 1: direction blobs, normal, zero pad (36..71)
+__device__ __forceinline__ void guide_encode(int part, const float *q, const GuideBox &bx, __half2 *row)
+{
+    if (part == 0) {
+        const float u[3] = {fminf(fmaxf((q[0] - bx.lo.x) * bx.inv_ext.x, 0.f), 1.f),
+                            fminf(fmaxf((q[1] - bx.lo.y) * bx.inv_ext.y, 0.f), 1.f),
+                            fminf(fmaxf((q[2] - bx.lo.z) * bx.inv_ext.z, 0.f), 1.f)};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            float x = u[a];
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                float s, c;
+                sincospif(x, &s, &c);
+                row[a * 12 + k] = __floats2half2_rn(s, c);
+                x *= 2.f;
+            }
+        }
+    } else {
+        const float th = acosf(fminf(fmaxf(q[8], -1.f), 1.f)) * (1.f / 3.14159265358979f);
+        const float ph = atan2f(q[7], q[6]) * (1.f / 6.28318530717959f) + 0.5f;
+#pragma unroll
+        for (int i = 0; i < 16; i++) row[36 + i] = __floats2half2_rn(guide_blob(th, 2 * i), guide_blob(th, 2 * i + 1));
+#pragma unroll
+        for (int i = 0; i < 16; i++) row[52 + i] = __floats2half2_rn(guide_blob(ph, 2 * i), guide_blob(ph, 2 * i + 1));
+        row[68] = __floats2half2_rn(q[3], q[4]);
+        row[69] = __floats2half2_rn(q[5], 0.f);
+        row[70] = __floats2half2_rn(0.f, 0.f);
+        row[71] = __floats2half2_rn(0.f, 0.f);
+    }
+}
+
+// ------------------------------------------------------------------ vMF mixture
+
+__device__ __forceinline__ float guide_sigmoid(float x) { return 1.f / (1.f + expf(-x)); }
+
+// kappa / (2 pi (1 - exp(-2 kappa))): the vMF density is norm * exp(kappa (mu.w - 1))
+__device__ __forceinline__ float vmf_norm(float k) { return k / (6.28318530717959f * (-expm1f(-2.f * k))); }
+
+__device__ __forceinline__ void guide_decode(const float *o, GuideParams &P)
+{
+    float lmax = o[3];
+#pragma unroll
+    for (int j = 1; j < kGuideLobes; j++) lmax = fmaxf(lmax, o[4 * j + 3]);
+    float e[kGuideLobes], se = 0.f;
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) {
+        e[j] = expf(o[4 * j + 3] - lmax);
+        se += e[j];
+    }
+    const float inv = 1.f / se;
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) {
+        const float th = 3.14159265358979f * guide_sigmoid(o[4 * j]);
+        const float ph = 6.28318530717959f * guide_sigmoid(o[4 * j + 1]);
+        const float k = expf(fminf(fmaxf(o[4 * j + 2], kGuideLogKappaMin), kGuideLogKappaMax));
+        float st, ct, sp, cp;
+        sincosf(th, &st, &ct);
+        sincosf(ph, &sp, &cp);
+        P.lobe[j] = make_float4(st * cp, st * sp, ct, k);
+        P.lam[j] = e[j] * inv;
+        P.lamn[j] = P.lam[j] * vmf_norm(k);
+    }
+    P.alpha = kGuideAlphaMax * guide_sigmoid(o[32]);
+}
+
+// mixture density of the vMF lobes at world direction w (unit)
+__device__ __forceinline__ float guide_pdf(const GuideParams &P, V3 w)
+{
+    float s = 0.f;
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) {
+        const float4 l = P.lobe[j];
+        s += P.lamn[j] * expf(l.w * (l.x * w.x + l.y * w.y + l.z * w.z - 1.f));
+    }
+    return s;
+}
+
+// vMF mixture sample: lobe by u0, direction by the inversion of Jakob (2012), "Numerically
+// stable sampling of the von Mises Fisher distribution on S2".
+__device__ __forceinline__ V3 guide_sample(const GuideParams &P, float u0, float u1, float u2)
+{
+    int j = 0;
+    float c = P.lam[0];
+    while (j < kGuideLobes - 1 && u0 >= c) c += P.lam[++j];
+    const float4 l = P.lobe[j];
+    const float xi = 1.f - u1;  // (0, 1]
+    float w = 1.f + logf(xi + (1.f - xi) * expf(-2.f * l.w)) / l.w;
+    w = fminf(fmaxf(w, -1.f), 1.f);
+    const float s = sqrtf(fmaxf(0.f, 1.f - w * w));
+    float sp, cp;
+    sincospif(2.f * u2, &sp, &cp);
+    V3 mu = v3(l.x, l.y, l.z), t, b;
+    onb(mu, t, b);
+    return normalize(t * (s * cp) + b * (s * sp) + mu * w);
+}
+
+// Training loss of one sample and its gradient with respect to the raw outputs:
+//   loss = -wt * log(alpha * vmf_mixture(wi) + (1 - alpha) * pdf_bsdf)
+// dout[0..47] receives d loss / d o (clamped to +-kGuideGradClamp; 0 for the unused outputs).
+__device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, float pdfb, float wt, float *dout)
+{
+    float lmax = o[3];
+#pragma unroll
+    for (int j = 1; j < kGuideLobes; j++) lmax = fmaxf(lmax, o[4 * j + 3]);
+    float lam[kGuideLobes], se = 0.f;
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) {
+        lam[j] = expf(o[4 * j + 3] - lmax);
+        se += lam[j];
+    }
+    float s[kGuideLobes], V = 0.f;
+    float kap[kGuideLobes], cj[kGuideLobes];
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) {
+        lam[j] /= se;
+        const float th = 3.14159265358979f * guide_sigmoid(o[4 * j]);
+        const float ph = 6.28318530717959f * guide_sigmoid(o[4 * j + 1]);
+        kap[j] = expf(fminf(fmaxf(o[4 * j + 2], kGuideLogKappaMin), kGuideLogKappaMax));
+        float st, ct, sp, cp;
+        sincosf(th, &st, &ct);
+        sincosf(ph, &sp, &cp);
+        cj[j] = st * cp * wi.x + st * sp * wi.y + ct * wi.z;
+        s[j] = lam[j] * vmf_norm(kap[j]) * expf(kap[j] * (cj[j] - 1.f));
+        V += s[j];
+    }
+    const float sa = guide_sigmoid(o[32]);
+    const float alpha = kGuideAlphaMax * sa;
+    const float q = fmaxf(alpha * V + (1.f - alpha) * pdfb, 1e-8f);
+    const float iq = 1.f / q;
+    const float gscale = -wt;  // d loss / d log q
+    auto clampg = [](float g) { return fminf(fmaxf(g, -kGuideGradClamp), kGuideGradClamp); };
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) {
+        const float th = 3.14159265358979f * guide_sigmoid(o[4 * j]);
+        const float ph = 6.28318530717959f * guide_sigmoid(o[4 * j + 1]);
+        const float sth = guide_sigmoid(o[4 * j]), sph = guide_sigmoid(o[4 * j + 1]);
+        float st, ct, sp, cp;
+        sincosf(th, &st, &ct);
+        sincosf(ph, &sp, &cp);
+        const float r = alpha * s[j] * iq;  // d log q / d log s_j
+        const float k = kap[j];
+        // d log q / d mu = r * kappa * wi, through mu(theta, phi)
+        const float dth = r * k * (ct * cp * wi.x + ct * sp * wi.y - st * wi.z) * 3.14159265358979f * sth * (1.f - sth);
+        const float dph = r * k * (-st * sp * wi.x + st * cp * wi.y) * 6.28318530717959f * sph * (1.f - sph);
+        const bool kin = o[4 * j + 2] > kGuideLogKappaMin && o[4 * j + 2] < kGuideLogKappaMax;
+        const float dk = kin ? r * (1.f - 2.f * k / expm1f(2.f * k) + k * (cj[j] - 1.f)) : 0.f;
+        const float dl = alpha * iq * (s[j] - lam[j] * V);
+        dout[4 * j + 0] = clampg(gscale * dth);
+        dout[4 * j + 1] = clampg(gscale * dph);
+        dout[4 * j + 2] = clampg(gscale * dk);
+        dout[4 * j + 3] = clampg(gscale * dl);
+    }
+    dout[32] = clampg(gscale * (V - pdfb) * iq * kGuideAlphaMax * sa * (1.f - sa));
+#pragma unroll
+    for (int i = 33; i < kGuideOut; i++) dout[i] = 0.f;
+    return -wt * logf(q);
+}
+
+// ------------------------------------------------------------------ batched inference
+
+constexpr int kInferWarps = 4;  // 32 rows per warp
+constexpr int kInferWarpBytes = 32 * 152 * 2;
+constexpr int kInferSmem = kGuideImgBytes + kInferWarps * kInferWarpBytes;
+
+// Forward pass over rows [0, n): src(row, q) fills the 9-float query and says whether the row
+// is guided; sink(row, valid, out) receives the 48 raw outputs (biases added). Persistent
+// warps, 32 rows per warp; the weight image is staged in shared memory once per block.
+// Launch with kInferWarps * 32 threads and kInferSmem bytes of dynamic shared memory.
+template <class Src, class Sink>
+__device__ __forceinline__ void guide_infer_rows(const uint4 *img, const GuideBox &box, uint32_t n, Src &src,
+                                                 Sink &sink)
+{
+    extern __shared__ uint4 guide_smem[];
+    for (int i = threadIdx.x; i < kGuideImgBytes / 16; i += blockDim.x) guide_smem[i] = img[i];
+    __syncthreads();
+    unsigned char *sm = reinterpret_cast<unsigned char *>(guide_smem);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __half *A = reinterpret_cast<__half *>(sm + kGuideImgBytes + warp * kInferWarpBytes);
+    float *O = reinterpret_cast<float *>(A);
+    const __half *W = reinterpret_cast<const __half *>(sm);
+    const float *bias = reinterpret_cast<const float *>(sm + kGuideImgBias);
+    const uint32_t stride = gridDim.x * kInferWarps;
+    for (uint32_t tile = blockIdx.x * kInferWarps + warp; tile * 32u < n; tile += stride) {
+        const uint32_t row = tile * 32u + lane;
+        float q[9];
+        bool valid = row < n && src(row, q);
+        if (!valid)
+#pragma unroll
+            for (int i = 0; i < 9; i++) q[i] = 0.f;
+        __half2 *arow = reinterpret_cast<__half2 *>(A + lane * 152);
+        guide_encode(0, q, box, arow);
+        guide_encode(1, q, box, arow);
+        __syncwarp();
+        {
+            float acc[2][8][4];
+            guide_gemm<2, kGuideIn, 64, 152, 152>(acc, A, W + guide_iw(0), lane);
+            __syncwarp();
+            guide_store_hidden<2, 64, 72>(acc, bias + guide_ib(0), A, lane);
+            __syncwarp();
+#pragma unroll 1
+            for (int l = 1; l < 4; l++) {
+                guide_gemm<2, 64, 64, 72, 72>(acc, A, W + guide_iw(l), lane);
+                __syncwarp();
+                guide_store_hidden<2, 64, 72>(acc, bias + guide_ib(l), A, lane);
+                __syncwarp();
+            }
+        }
+        {
+            float acc[2][6][4];
+            guide_gemm<2, 64, kGuideOut, 72, 72>(acc, A, W + guide_iw(4), lane);
+            __syncwarp();
+            guide_store_out<2, kGuideOut, 49>(acc, bias + guide_ib(4), O, lane);
+        }
+        __syncwarp();
+        if (row < n) sink(row, valid, O + lane * 49);
+        __syncwarp();
+    }
+}
+
+}  // namespace rtb

@@ -14,6 +14,13 @@
 //   retire  - finished paths add their radiance to the film (NaN/Inf samples dropped)
 // Path state moves with the queue (double-buffered SoA), so every stage reads and writes
 // its arrays with coalesced 16-byte accesses; queue appends are warp-aggregated.
+//
+// Guided mode (RT_RENDER_GUIDE) adds an inference kernel between extend and shade: the
+// guide network maps each hit to a vMF mixture, and shade samples it or the BSDF (one-sample
+// MIS, density alpha * guide + (1 - alpha) * bsdf). With training on, every guided vertex
+// appends a record; radiance found later on the path (emission hits, unoccluded shadow rays)
+// is added to the path's newest record, and retire turns those into suffix sums, i.e. the
+// radiance each vertex's sampled direction carried back.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -22,6 +29,7 @@
 #include <cstring>
 #include <vector>
 
+#include "guide.cuh"
 #include "photon_query.cuh"
 
 namespace rtb {
@@ -36,6 +44,7 @@ constexpr uint32_t kCameraRay = 0x100u;
 constexpr uint32_t kLastSpecular = 0x200u;
 
 constexpr uint32_t kRetireTarget = 0x80000000u;
+constexpr uint32_t kRecBits = kRecNone << kRecShift;  // newest guide record of the path
 
 struct Buffers {
     rt_ray *rays[2];
@@ -53,6 +62,32 @@ struct Buffers {
     // [10] extension rays, [12] shadow rays
     uint32_t *cnt;
 };
+
+struct GuideView {
+    const GuideParams *params;  // per queue slot; null while the guide is untrained
+    GuideRecord *recs;
+    uint32_t *rcnt;        // [0] records, [1] nonzero-weight records
+    uint32_t *nz;          // records with nonzero weight
+    uint32_t *retire_rec;  // newest record of each retiring path
+    uint32_t rec_cap;
+    int enabled, train;
+};
+
+// vertices that sample with the guide: diffuse and rough-conductor BSDFs, seen from the side
+// their BSDF sampler covers
+__device__ __forceinline__ bool guide_vertex(const Bsdf &b, float wo_z)
+{
+    return wo_z > 0.f &&
+           (b.type == RT_MAT_LAMBERTIAN || (b.type == RT_MAT_TROWBRIDGE && fmaxf(b.g.ax, b.g.ay) >= 1e-3f));
+}
+
+// density of bsdf_sample's direction at wi (shading space), for the guide vertices
+__device__ __forceinline__ float bsdf_sampling_pdf(const Bsdf &b, V3 wo, V3 wi)
+{
+    if (b.type == RT_MAT_LAMBERTIAN) return wi.z > 0.f ? wi.z * kInvPi : 0.f;
+    if (b.type == RT_MAT_TROWBRIDGE) return ggx_pdf(b.g, normalize(wo), wi);
+    return 0.f;
+}
 
 __device__ __forceinline__ unsigned long long *cnt64(uint32_t *c, int i)
 {
@@ -99,7 +134,7 @@ __device__ void start_path(const RenderView &rv, const Buffers &bf, int b, uint3
     reinterpret_cast<float4 *>(bf.rays[b])[2 * q + 1] = make_float4(ray.dx, ray.dy, ray.dz, 0.f);
     bf.st0[b][q] = make_float4(1.f, 1.f, 1.f, 0.f);
     bf.st1[b][q] = make_float4(0.f, 0.f, 0.f, __uint_as_float(pix));
-    bf.st2[b][q] = make_uint4((uint32_t)r.state, (uint32_t)(r.state >> 32), j, kCameraRay);
+    bf.st2[b][q] = make_uint4((uint32_t)r.state, (uint32_t)(r.state >> 32), j, kCameraRay | kRecBits);
 }
 
 // Takes the next camera sample (if any) and appends it to buffer b.
@@ -126,14 +161,15 @@ __global__ void __launch_bounds__(kB) k_start(RenderView rv, Buffers bf)
 // Triangle::intersects(checkShadow), Triangle.cu:439-440): transparent materials cast no
 // shadow. Used for point lights in compat mode; area-light samples must be blocked by
 // glass so that their MIS pairing with BSDF-sampled emitter hits stays unbiased.
+// rec: the guide record the contribution also belongs to (kRecNone: none).
 __device__ __forceinline__ void push_shadow(const Buffers &bf, V3 o, V3 d, float tmax, V3 contrib, uint32_t target,
-                                            bool skip_transparent)
+                                            bool skip_transparent, uint32_t rec = kRecNone)
 {
     uint32_t i = append(bf.cnt + 2);
     if (i >= bf.scap) return;
     reinterpret_cast<float4 *>(bf.srays)[2 * i] = make_float4(o.x, o.y, o.z, tmax);
     reinterpret_cast<float4 *>(bf.srays)[2 * i + 1] =
-        make_float4(d.x, d.y, d.z, __uint_as_float(skip_transparent ? 1u : 0u));
+        make_float4(d.x, d.y, d.z, __uint_as_float((rec << 1) | (skip_transparent ? 1u : 0u)));
     bf.scontrib[i] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(target));
 }
 
@@ -145,7 +181,7 @@ struct PhotonView {
     float radius;
 };
 
-__global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur)
+__global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur, GuideView gv)
 {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = min(bf.cnt[cur], bf.cap);
@@ -167,6 +203,7 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
     const uint32_t pix = __float_as_uint(s1.w);
     uint32_t flags = s2.w;
     const uint32_t depth = flags & kDepthMask;
+    uint32_t rec = (flags >> kRecShift) & kRecNone;  // newest guide record of this path
     Pcg rng;
     rng.state = ((uint64_t)s2.y << 32) | s2.x;
     rng.inc = ((((uint64_t)s2.z << 32) | rv.seed) << 1u) | 1u;
@@ -207,9 +244,57 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
                 w = (last_pdf * last_pdf) / (last_pdf * last_pdf + pl * pl);
             }
             L = L + beta_in * Le * w;
+            if (gv.train && rec != kRecNone) {
+                float4 &e = gv.recs[rec].e;
+                e.x += beta_in.x * Le.x * w;
+                e.y += beta_in.y * Le.y * w;
+                e.z += beta_in.z * Le.z * w;
+            }
         }
-        V3 f = bsdf_sample(bs, wo, rng, compat, wi_l, pdf_b, delta);
-        V3 wi_w = t * wi_l.x + bvec * wi_l.y + sf.n * wi_l.z;
+        const bool guided = gv.enabled && guide_vertex(bs, wo.z);
+        const uint32_t rec_in = rec;  // this vertex's NEE belongs to the previous record
+        float alpha = 0.f;
+        const GuideParams *gp = nullptr;
+        if (guided && gv.params) {
+            gp = gv.params + q;
+            alpha = gp->alpha;
+        }
+        V3 f, wi_w;
+        if (guided) {
+            // one-sample MIS between the guide's vMF mixture and the BSDF
+            const float usel = pcg_float(rng);
+            if (usel < alpha) {
+                const float u1 = pcg_float(rng), u2 = pcg_float(rng);
+                wi_w = guide_sample(*gp, usel / alpha, u1, u2);
+                wi_l = v3(dot(wi_w, t), dot(wi_w, bvec), dot(wi_w, sf.n));
+            } else {
+                (void)bsdf_sample(bs, wo, rng, compat, wi_l, pdf_b, delta);
+                wi_w = t * wi_l.x + bvec * wi_l.y + sf.n * wi_l.z;
+            }
+            float pe;
+            V3 fc = bsdf_eval(bs, wo, wi_l, pe);
+            pdf_b = bsdf_sampling_pdf(bs, wo, wi_l);
+            const float pmix = (alpha > 0.f ? alpha * guide_pdf(*gp, wi_w) : 0.f) + (1.f - alpha) * pdf_b;
+            f = (pdf_b > 0.f && pmix > 0.f) ? fc * (1.f / pmix) : v3(0, 0, 0);
+            delta = false;
+            if (gv.train && !is_black(f)) {
+                const uint32_t ri = append(gv.rcnt);
+                if (ri < gv.rec_cap) {
+                    GuideRecord r;
+                    r.a = make_float4(sf.p.x, sf.p.y, sf.p.z, sf.n.x);
+                    r.b = make_float4(sf.n.y, sf.n.z, wo_w.x, wo_w.y);
+                    r.c = make_float4(wo_w.z, wi_w.x, wi_w.y, wi_w.z);
+                    r.d = make_float4(pdf_b, beta_in.x, beta_in.y, beta_in.z);
+                    r.e = make_float4(0.f, 0.f, 0.f, __uint_as_float(rec));
+                    gv.recs[ri] = r;
+                    rec = ri;
+                }
+            }
+            pdf_b = pmix;  // the density MIS pairs with area-light sampling
+        } else {
+            f = bsdf_sample(bs, wo, rng, compat, wi_l, pdf_b, delta);
+            wi_w = t * wi_l.x + bvec * wi_l.y + sf.n * wi_l.z;
+        }
         beta = beta * f;
         finished = is_black(f);
         if (photon_mode && scattering) {
@@ -246,7 +331,7 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
             next_d = wi_w;
             next_pdf = delta ? 0.f : pdf_b;
             next_flags = (depth + 1) | (delta ? kLastSpecular : 0u) |
-                         (((flags & kCameraRay) && is_specular(bs.type)) ? kCameraRay : 0u);
+                         (((flags & kCameraRay) && is_specular(bs.type)) ? kCameraRay : 0u) | (rec << kRecShift);
         } else {
             target = kRetireTarget | append(bf.cnt + 3);
         }
@@ -269,7 +354,7 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
                 float w = compat ? 1.0f / (1.0f + pb * pb) : 1.0f;  // powerHeuristic(1,1,1,pdf), Scene.cu:331
                 V3 c = beta_in * fl * Li * w;
                 V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
-                push_shadow(bf, so, wl, dist, c, target, compat);
+                push_shadow(bf, so, wl, dist, c, target, compat, rec_in);
             }
             if (nee_area) {
                 float u0 = pcg_float(rng), u1 = pcg_float(rng), u2 = pcg_float(rng);
@@ -302,11 +387,14 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
                     V3 wls = v3(dot(wl, t), dot(wl, bvec), dot(wl, sf.n));
                     float pb;
                     V3 fl = bsdf_eval(bs, wo, wls, pb);
+                    if (guided)
+                        pb = (alpha > 0.f ? alpha * guide_pdf(*gp, wl) : 0.f) +
+                             (1.f - alpha) * bsdf_sampling_pdf(bs, wo, wls);
                     if (!is_black(fl)) {
                         float w = (pl * pl) / (pl * pl + pb * pb);
                         V3 c = beta_in * fl * Lel * (w / pl);
                         V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
-                        push_shadow(bf, so, wl, dist * (1.0f - 1e-4f), c, target, false);
+                        push_shadow(bf, so, wl, dist * (1.0f - 1e-4f), c, target, false, rec_in);
                     }
                 }
             }
@@ -323,13 +411,14 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
         bf.st2[nxt][qn] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), s2.z, next_flags);
     } else {
         bf.retire[target & ~kRetireTarget] = make_float4(L.x, L.y, L.z, __uint_as_float(pix));
+        if (gv.train) gv.retire_rec[target & ~kRetireTarget] = rec;
         regenerate(rv, bf, nxt);
     }
 }
 
 // Any-hit test of the wave's shadow rays (persistent warps, counter cnt[5]); an unoccluded
 // ray adds its contribution to the path it belongs to.
-__global__ void __launch_bounds__(kB) k_shadow(RenderView rv, Buffers bf, int nxt)
+__global__ void __launch_bounds__(kB) k_shadow(RenderView rv, Buffers bf, int nxt, GuideView gv)
 {
     const uint32_t n = min(bf.cnt[2], bf.scap);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(cnt64(bf.cnt, 12), (unsigned long long)n);  // stats
@@ -359,6 +448,16 @@ __global__ void __launch_bounds__(kB) k_shadow(RenderView rv, Buffers bf, int nx
             atomicAdd(dst + 0, c.x);
             atomicAdd(dst + 1, c.y);
             atomicAdd(dst + 2, c.z);
+            if (gv.train) {
+                const uint32_t rec = (__float_as_uint(reinterpret_cast<const float4 *>(bf.srays)[2 * i + 1].w) >> 1) &
+                                     kRecNone;
+                if (rec != kRecNone) {
+                    float4 *e = &gv.recs[rec].e;
+                    atomicAdd(&e->x, c.x);
+                    atomicAdd(&e->y, c.y);
+                    atomicAdd(&e->z, c.z);
+                }
+            }
         });
 }
 
@@ -382,11 +481,40 @@ __global__ void __launch_bounds__(kB) k_gather(RenderView rv, Buffers bf, Photon
     atomicAdd(dst + 2, contrib.z);
 }
 
-__global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t *count, double *sum64)
+__device__ __forceinline__ float record_weight(const GuideRecord &r)
+{
+    float s = 0.f;
+    if (r.d.y > 0.f) s += r.e.x / r.d.y;
+    if (r.d.z > 0.f) s += r.e.y / r.d.z;
+    if (r.d.w > 0.f) s += r.e.z / r.d.w;
+    return s * (1.f / 3.f);
+}
+
+__global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t *count, double *sum64, GuideView gv)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = min(bf.cnt[3], bf.cap);
     if (i >= n) return;
+    if (gv.train) {
+        // the path is complete: each of its records gets the radiance of everything after it
+        uint32_t r = gv.retire_rec[i];
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        for (int guard = 0; r != kRecNone && r < gv.rec_cap && guard < 256; guard++) {
+            GuideRecord &R = gv.recs[r];
+            ax += R.e.x;
+            ay += R.e.y;
+            az += R.e.z;
+            R.e.x = ax;
+            R.e.y = ay;
+            R.e.z = az;
+            const float w = record_weight(R);
+            if (w > 0.f && isfinite(w)) {
+                const uint32_t k = append(gv.rcnt + 1);
+                if (k < gv.rec_cap) gv.nz[k] = r;
+            }
+            r = __float_as_uint(R.e.w);
+        }
+    }
     float4 v = bf.retire[i];
     if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) return;  // pathTracing.cu:473-486
     uint32_t pix = __float_as_uint(v.w);
@@ -399,6 +527,46 @@ __global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t 
         atomicAdd(sum64 + 3 * pix + 1, (double)v.y);
         atomicAdd(sum64 + 3 * pix + 2, (double)v.z);
     }
+}
+
+// Guide network at the wave's hits (queue slots of buffer `cur`); writes the decoded mixture
+// per slot, alpha = 0 where the vertex is not guided.
+__global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(RenderView rv, Buffers bf, int cur, const uint4 *img,
+                                                                   GuideBox box, GuideParams *params)
+{
+    const uint32_t n = min(bf.cnt[cur], bf.cap);
+    const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
+    auto src = [&](uint32_t q, float *out) -> bool {
+        const float4 hv = reinterpret_cast<const float4 *>(bf.hits)[q];
+        const rt_hit h{hv.x, __float_as_int(hv.y), hv.z, hv.w};
+        if (h.prim < 0) return false;
+        const float4 r0 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q];
+        const float4 r1 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q + 1];
+        const V3 d = v3(r1.x, r1.y, r1.z);
+        const Surface sf = surface_at(rv, h, v3(r0.x, r0.y, r0.z), d, compat);
+        const Bsdf bs = load_bsdf(rv.mats[min(sf.mat, rv.nmats - 1)]);
+        if (!guide_vertex(bs, -dot(d, sf.n))) return false;
+        out[0] = sf.p.x;
+        out[1] = sf.p.y;
+        out[2] = sf.p.z;
+        out[3] = sf.n.x;
+        out[4] = sf.n.y;
+        out[5] = sf.n.z;
+        out[6] = -d.x;
+        out[7] = -d.y;
+        out[8] = -d.z;
+        return true;
+    };
+    auto sink = [&](uint32_t q, bool valid, const float *o) {
+        if (!valid) {
+            params[q].alpha = 0.f;
+            return;
+        }
+        GuideParams P;
+        guide_decode(o, P);
+        params[q] = P;
+    };
+    guide_infer_rows(img, box, n, src, sink);
 }
 
 }  // namespace
@@ -603,6 +771,31 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
             return fail(RT_ERR_STATE, "rt_render: RT_RENDER_PHOTON_MAP needs a built photon map (rt_render_set_photon_map)");
         RTB_CHECK(rs.gather.reserve(64ull * cap));
     }
+    const bool guided = (opts->flags & RT_RENDER_GUIDE) != 0;
+    GuideView gv{};
+    rt_guide *guide = s->guide;
+    if (guided) {
+        if (!guide) return fail(RT_ERR_STATE, "rt_render: RT_RENDER_GUIDE needs a guide (rt_render_set_guide)");
+        if (photon_mode) return fail(RT_ERR_UNSUPPORTED, "rt_render: RT_RENDER_GUIDE with RT_RENDER_PHOTON_MAP");
+        gv.enabled = 1;
+        gv.train = s->guide_train;
+        if (guide->step > 0) {
+            RTB_CHECK(guide->params.reserve(sizeof(GuideParams) * (uint64_t)cap));
+            gv.params = guide->params.as<GuideParams>();
+        }
+        if (gv.train) {
+            RTB_CHECK(guide->recs.reserve(sizeof(GuideRecord) * (uint64_t)guide->rec_cap));
+            RTB_CHECK(guide->nz.reserve(4ull * guide->rec_cap));
+            RTB_CHECK(guide->retire_rec.reserve(4ull * cap));
+            RTB_CHECK(guide->rcnt.reserve(16));
+            RTB_CUDA(cudaMemsetAsync(guide->rcnt.ptr, 0, 16, st));
+            gv.recs = guide->recs.as<GuideRecord>();
+            gv.nz = guide->nz.as<uint32_t>();
+            gv.retire_rec = guide->retire_rec.as<uint32_t>();
+            gv.rcnt = guide->rcnt.as<uint32_t>();
+            gv.rec_cap = guide->rec_cap;
+        }
+    }
     RTB_CHECK(rs.cnt.reserve(256));
     RTB_CHECK(s->scratch.queue.reserve(4ull * cap));
     RTB_CHECK(s->scratch.counters.reserve(64));
@@ -657,6 +850,13 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
         shadow_resident = (unsigned)std::max(1, s->ctx->sm_count * std::max(per_sm, 1));
     }
     const unsigned shadow_blocks = std::min<unsigned>(shadow_resident, (scap + kB - 1) / kB);
+    static bool infer_attr = false;
+    if (gv.params && !infer_attr) {
+        RTB_CUDA(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
+        infer_attr = true;
+    }
+    const unsigned infer_blocks = (unsigned)std::max(1, 2 * s->ctx->sm_count);
+    const GuideBox gbox = guided ? guide_box(guide) : GuideBox{};
     k_start<<<blocks, kB, 0, st>>>(rv, bf);
     RTB_CUDA(cudaGetLastError());
     const uint32_t trace_flags = (opts->flags & RT_RENDER_EXACT_TRACE) ? 0u : RT_TRACE_FAST;
@@ -669,17 +869,22 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
             RTB_CHECK(launch_trace_closest_dev(rv.sv, bf.rays[cur], bf.cnt + cur, cap, bf.hits, trace_flags,
                                                s->scratch.queue.as<uint32_t>(), s->scratch.counters.as<uint32_t>(),
                                                st));
+            if (gv.params) {
+                k_guide_infer<<<infer_blocks, kInferWarps * 32, kInferSmem, st>>>(
+                    rv, bf, cur, guide->img.as<uint4>(), gbox, guide->params.as<GuideParams>());
+                RTB_CUDA(cudaGetLastError());
+            }
             RTB_CUDA(cudaMemsetAsync(bf.cnt + ((cur ^ 1)), 0, 4, st));
             RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 20, st));
-            k_shade<<<blocks, kB, 0, st>>>(rv, bf, cur);
+            k_shade<<<blocks, kB, 0, st>>>(rv, bf, cur, gv);
             RTB_CUDA(cudaGetLastError());
-            k_shadow<<<shadow_blocks, kB, 0, st>>>(rv, bf, cur ^ 1);
+            k_shadow<<<shadow_blocks, kB, 0, st>>>(rv, bf, cur ^ 1, gv);
             RTB_CUDA(cudaGetLastError());
             if (photon_mode) {
                 k_gather<<<blocks, kB, 0, st>>>(rv, bf, pv);
                 RTB_CUDA(cudaGetLastError());
             }
-            k_retire<<<blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64);
+            k_retire<<<blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64, gv);
             RTB_CUDA(cudaGetLastError());
             cur ^= 1;
             waves++;

@@ -194,6 +194,24 @@ struct rt_photon_map {
     bool built = false;
 };
 
+struct rt_guide {
+    rt_context *ctx = nullptr;
+    rt_guide_opts opts{};
+    uint64_t step = 0;  // Adam steps taken
+    // parameters: FP32 master, Adam moments, last gradient, FP16 shared-memory image
+    rtb::DevBuf master, adam_m, adam_v, grad, img;
+    // training scratch: transposed activations / gradients, per-chunk weight-gradient
+    // partials, scalars ([0] weight mean, [1] loss sum, [2] non-finite flag)
+    rtb::DevBuf xt, gt, partial, scal;
+    rtb::DevBuf tq, tdir, tpdf, tw;  // batch drawn from the records
+    // path-tracer side: decoded mixture per queue slot, training records, the list of records
+    // with nonzero weight, the open record of each retiring path, counters ([0] records,
+    // [1] nonzero)
+    rtb::DevBuf params, recs, nz, retire_rec, rcnt;
+    uint32_t rec_cap = 0;
+    void *host_scal = nullptr;  // pinned
+};
+
 struct rt_scene {
     rt_context *ctx = nullptr;
     // host copies of what was added
@@ -226,6 +244,8 @@ struct rt_scene {
     uint32_t nemit = 0;
     float emit_total = 0.f;
     rt_photon_map *pmap = nullptr;  // RT_RENDER_PHOTON_MAP gather source
+    rt_guide *guide = nullptr;      // RT_RENDER_GUIDE proposal
+    int guide_train = 0;            // record training samples while rendering
     uint32_t pm_k = 100;
     float pm_radius = 100.f;
     rtb::DevBuf d_mats, d_tri_mat, d_tri_shape, d_tri_nidx, d_normals, d_emit_tri, d_emit_cdf, d_plights;

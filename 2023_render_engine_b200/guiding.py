@@ -1,0 +1,59 @@
+"""Progressive guided rendering: online training of the path guide on the tracer's own samples.
+
+Each pass renders `spp` samples per pixel into the same film (distinct sample indices, so the
+passes are independent); during the first `train_passes` passes the tracer records every guided
+vertex and the guide takes Adam steps on those records after the pass. Sampling uses the guide
+from the first pass after its first step (before that the guided vertices sample the BSDF).
+"""
+from __future__ import annotations
+
+import time
+
+from . import _native as N
+
+
+def pass_schedule(total_spp: int, first: int = 1, growth: float = 2.0, cap: int = 64):
+    """Pass sizes: first, first*growth, ... capped at `cap`, summing to total_spp."""
+    out, done, s = [], 0, first
+    while done < total_spp:
+        k = min(int(s), cap, total_spp - done)
+        out.append(k)
+        done += k
+        s = s * growth
+    return out
+
+
+def render_progressive(scene, camera, guide, passes, max_depth: int, rr_depth: int = 3, seed: int = 0,
+                       flags: int = 0, train_passes: int = 0, steps_per_pass: int = 4, batch: int = 1 << 18,
+                       film=None, fp64: bool = False, on_pass=None, sync=None):
+    """Renders len(passes) passes (passes[i] spp each); guided when `guide` is not None.
+
+    on_pass(i, spp_done, film, seconds) is called after each pass (its own time is not
+    counted); `sync` is a callable that waits for the device (torch.cuda.synchronize).
+    Returns (film, seconds spent rendering and training)."""
+    total_s = 0.0
+    done = 0
+    for i, spp in enumerate(passes):
+        if sync:
+            sync()
+        t0 = time.perf_counter()
+        f = flags
+        if guide is not None:
+            train = i < train_passes
+            scene.set_guide(guide, train=train)
+            f |= N.RT_RENDER_GUIDE
+        film, _ = scene.render(camera, spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed, flags=f,
+                               sample_offset=done, film=film, fp64=fp64)
+        if guide is not None and i < train_passes:
+            _, nnz = guide.record_count()
+            if nnz:
+                guide.train_records(steps_per_pass, batch, seed=seed * 7919 + i)
+        if sync:
+            sync()
+        total_s += time.perf_counter() - t0
+        done += spp
+        if on_pass is not None:
+            on_pass(i, done, film, total_s)
+    if guide is not None:
+        scene.set_guide(guide, train=False)
+    return film, total_s

@@ -315,6 +315,72 @@ RT_API int rt_photon_knn(rt_photon_map *map, const float *queries_dev, const int
                          uint32_t k, float radius, int32_t *out_idx_dev, float *out_dist_dev,
                          uint32_t *out_count_dev);
 
+/* ------------------------------------------------------------ path guide */
+
+/* Learned path-guiding proposal (new in this build; the reference has no counterpart).
+ * A small MLP maps an encoded shading point — position (12 frequency bands per axis inside
+ * the guide's box), outgoing direction (one-blob, 32 theta + 32 phi bins), shading normal:
+ * 139 inputs padded to 144 — through 4 hidden layers of 64 (ReLU) to 48 outputs: 8 von
+ * Mises-Fisher lobes (mean direction, log concentration, weight logit) and the probability
+ * alpha of sampling the guide rather than the BSDF. FP16 weights and activations on the
+ * tensor cores, FP32 accumulation, FP32 master weights with Adam (beta 0.9 / 0.99). */
+typedef struct rt_guide rt_guide;
+
+typedef struct rt_guide_opts {
+    float bbox_min[3], bbox_max[3]; /* position encoding domain (the scene bounds) */
+    float learning_rate;            /* Adam step size; 1e-2 in the guiding configuration */
+    uint32_t seed;                  /* weight initialisation */
+    uint32_t record_capacity;       /* training records kept per render (0: 4,194,302, the maximum) */
+    uint32_t reserved;
+} rt_guide_opts;
+
+#define RT_GUIDE_INPUTS 144
+#define RT_GUIDE_OUTPUTS 48
+#define RT_GUIDE_LOBES 8
+#define RT_RENDER_GUIDE 0x10u /* rt_render_opts.flags: sample with the scene's guide (one-sample MIS) */
+
+RT_API int rt_guide_create(rt_context *ctx, const rt_guide_opts *opts, rt_guide **out);
+RT_API int rt_guide_destroy(rt_guide *g);
+/* Parameter count and the FP32 master copy, in this order: for each layer l = 0..4,
+ * W_l (inputs x outputs, row-major) then b_l. Setting them resets the Adam moments. */
+RT_API int rt_guide_param_count(rt_guide *g, uint64_t *n);
+RT_API int rt_guide_params_get(rt_guide *g, float *host, uint64_t n);
+RT_API int rt_guide_params_set(rt_guide *g, const float *host, uint64_t n);
+RT_API int rt_guide_steps(rt_guide *g, uint64_t *steps); /* Adam steps taken */
+
+/* Raw network outputs for B shading points (device buffers): queries are 9 floats each
+ * (position, shading normal, outgoing direction), out is B*48 floats. */
+RT_API int rt_guide_eval(rt_guide *g, const float *queries_dev, uint64_t B, float *out_dev);
+/* One-sample MIS density alpha * vmf_mixture(dir) + (1 - alpha) * bsdf_pdf at B (query, dir) pairs. */
+RT_API int rt_guide_pdf(rt_guide *g, const float *queries_dev, const float *dirs_dev, const float *bsdf_pdf_dev,
+                        uint64_t B, float *out_pdf_dev);
+/* Direction samples of the vMF mixture alone from 3 uniforms per query; out_pdf: its density there. */
+RT_API int rt_guide_sample(rt_guide *g, const float *queries_dev, const float *u3_dev, uint64_t B, float *out_dirs_dev,
+                           float *out_pdf_dev);
+
+/* One training step on B samples:
+ *   loss = mean_i( -wt_i * log(alpha * vmf_mixture(dir_i) + (1 - alpha) * bsdf_pdf_i) ),
+ *   wt_i = min(w_i / mean(w), 32), w_i = the sample's incident radiance times f * cos / pdf.
+ * apply = 0 computes the gradient only; apply = 1 also takes an Adam step. grad_host (nullable)
+ * receives the gradient (parameter order as rt_guide_params_get), loss_out (nullable) the loss. */
+RT_API int rt_guide_train_step(rt_guide *g, const float *queries_dev, const float *dirs_dev,
+                               const float *bsdf_pdf_dev, const float *weights_dev, uint64_t B, int apply,
+                               float *grad_host, float *loss_out);
+
+/* Online training on the tracer's own samples. rt_render_set_guide(scene, g, train) makes
+ * rt_render with RT_RENDER_GUIDE sample with g; with train != 0 each such call also records
+ * every guided vertex (query, sampled direction, BSDF pdf, the radiance the path later
+ * carried back through it). rt_guide_train_records then takes `steps` Adam steps on batches
+ * of `batch` records drawn (seeded, with replacement) from those with nonzero weight. */
+RT_API int rt_render_set_guide(rt_scene *s, rt_guide *g, int train);
+RT_API int rt_guide_record_count(rt_guide *g, uint64_t *records, uint64_t *nonzero);
+/* Copies records [first, first + n) to host, 20 floats each: position, shading normal, outgoing
+ * direction, sampled direction, BSDF pdf of it, throughput before the vertex (rgb), radiance the
+ * path carried back through the sampled direction (rgb), previous record of the path (uint32
+ * bits; 0x3FFFFF: none). */
+RT_API int rt_guide_records_get(rt_guide *g, uint64_t first, uint64_t n, float *host);
+RT_API int rt_guide_train_records(rt_guide *g, uint32_t steps, uint32_t batch, uint32_t seed, float *loss_out);
+
 #ifdef __cplusplus
 }
 #endif
