@@ -490,6 +490,7 @@ int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf,
     RTB_CUDA(cudaGetLastError());
     if (apply) {
         g->step++;
+        g->trained = true;
         AdamArgs ad;
         ad.lr = g->opts.learning_rate;
         ad.bc1 = 1.f - (float)std::pow((double)kAdamB1, (double)g->step);
@@ -587,7 +588,9 @@ int rt_guide_params_set(rt_guide *g, const float *host, uint64_t n)
     for (uint64_t i = 0; i < n; i++)
         if (!std::isfinite(host[i])) return fail(RT_ERR_INVALID, "rt_guide_params_set: non-finite parameter");
     RTB_CUDA(cudaSetDevice(g->ctx->device));
-    return guide_upload_params(g, host);
+    RTB_CHECK(guide_upload_params(g, host));
+    g->trained = true;
+    return RT_OK;
 }
 
 int rt_guide_steps(rt_guide *g, uint64_t *steps)

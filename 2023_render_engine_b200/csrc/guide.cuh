@@ -10,8 +10,8 @@
 //   [104, 136) phi(wo) / 2pi + 1/2, one-blob over 32 bins
 //   [136, 139) n;  [139, 144) zero
 // Outputs per lobe j (8 von Mises-Fisher lobes): o[4j] -> theta = pi sigmoid, o[4j+1] -> phi =
-// 2 pi sigmoid, o[4j+2] -> kappa = exp(clamp(., -4, 8)), o[4j+3] -> softmax weight logit;
-// o[32] -> alpha = 0.95 sigmoid, the probability of sampling the guide. o[33..47] unused.
+// 2 pi sigmoid, o[4j+2] -> kappa = exp(-4 + 12 sigmoid), o[4j+3] -> softmax weight logit;
+// o[32] -> alpha = 0.05 + 0.9 sigmoid, the probability of sampling the guide. o[33..47] unused.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -22,8 +22,8 @@ namespace rtb {
 
 constexpr int kGuideIn = 144, kGuideHidden = 64, kGuideOut = 48, kGuideLayers = 5, kGuideLobes = 8;
 constexpr int kGuideParamCount = 24880;  // 144*64+64 + 3*(64*64+64) + 64*48+48
-constexpr float kGuideAlphaMax = 0.95f;
-constexpr float kGuideLogKappaMin = -4.f, kGuideLogKappaMax = 8.f;
+constexpr float kGuideAlphaMin = 0.05f, kGuideAlphaSpan = 0.9f;  // alpha in [0.05, 0.95]
+constexpr float kGuideLogKappaMin = -4.f, kGuideLogKappaSpan = 12.f;  // log kappa in (-4, 8)
 constexpr float kGuideWeightClip = 32.f;   // training weight / batch mean is clipped here
 constexpr float kGuideGradClamp = 8192.f;  // per-output gradient clamp
 constexpr float kGuideGradScale = 8.f;     // output gradients are stored as fp16(g / scale)
@@ -279,7 +279,7 @@ __device__ __forceinline__ void guide_decode(const float *o, GuideParams &P)
     for (int j = 0; j < kGuideLobes; j++) {
         const float th = 3.14159265358979f * guide_sigmoid(o[4 * j]);
         const float ph = 6.28318530717959f * guide_sigmoid(o[4 * j + 1]);
-        const float k = expf(fminf(fmaxf(o[4 * j + 2], kGuideLogKappaMin), kGuideLogKappaMax));
+        const float k = expf(kGuideLogKappaMin + kGuideLogKappaSpan * guide_sigmoid(o[4 * j + 2]));
         float st, ct, sp, cp;
         sincosf(th, &st, &ct);
         sincosf(ph, &sp, &cp);
@@ -287,7 +287,7 @@ __device__ __forceinline__ void guide_decode(const float *o, GuideParams &P)
         P.lam[j] = e[j] * inv;
         P.lamn[j] = P.lam[j] * vmf_norm(k);
     }
-    P.alpha = kGuideAlphaMax * guide_sigmoid(o[32]);
+    P.alpha = kGuideAlphaMin + kGuideAlphaSpan * guide_sigmoid(o[32]);
 }
 
 // mixture density of the vMF lobes at world direction w (unit)
@@ -321,66 +321,71 @@ __device__ __forceinline__ V3 guide_sample(const GuideParams &P, float u0, float
     return normalize(t * (s * cp) + b * (s * sp) + mu * w);
 }
 
-// Training loss of one sample and its gradient with respect to the raw outputs:
-//   loss = -wt * log(alpha * vmf_mixture(wi) + (1 - alpha) * pdf_bsdf)
-// dout[0..47] receives d loss / d o (clamped to +-kGuideGradClamp; 0 for the unused outputs).
+// Training loss of one sample and its gradient with respect to the raw outputs. The lobes are
+// fitted to the sampled integrand on their own, and the selection probability on the mixture
+// with the lobes held fixed, so a guide that starts out worse than the BSDF still learns:
+//   loss = -wt * (log V(wi) + log(alpha * V(wi) + (1 - alpha) * pdf_bsdf)),  V = vMF mixture,
+// with V treated as a constant inside the second term (it only trains alpha). log V is a
+// log-sum-exp over the lobes, so samples far from every lobe keep a gradient.
+// dout[0..47] receives the gradient (clamped to +-kGuideGradClamp; 0 for the unused outputs).
 __device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, float pdfb, float wt, float *dout)
 {
     float lmax = o[3];
 #pragma unroll
     for (int j = 1; j < kGuideLobes; j++) lmax = fmaxf(lmax, o[4 * j + 3]);
-    float lam[kGuideLobes], se = 0.f;
+    float se = 0.f;
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) se += expf(o[4 * j + 3] - lmax);
+    const float lse_l = lmax + logf(se);
+    float ls[kGuideLobes], kap[kGuideLobes], cj[kGuideLobes];
+    float lsmax = -INFINITY;
 #pragma unroll
     for (int j = 0; j < kGuideLobes; j++) {
-        lam[j] = expf(o[4 * j + 3] - lmax);
-        se += lam[j];
-    }
-    float s[kGuideLobes], V = 0.f;
-    float kap[kGuideLobes], cj[kGuideLobes];
-#pragma unroll
-    for (int j = 0; j < kGuideLobes; j++) {
-        lam[j] /= se;
         const float th = 3.14159265358979f * guide_sigmoid(o[4 * j]);
         const float ph = 6.28318530717959f * guide_sigmoid(o[4 * j + 1]);
-        kap[j] = expf(fminf(fmaxf(o[4 * j + 2], kGuideLogKappaMin), kGuideLogKappaMax));
+        const float lk = kGuideLogKappaMin + kGuideLogKappaSpan * guide_sigmoid(o[4 * j + 2]);
+        kap[j] = expf(lk);
         float st, ct, sp, cp;
         sincosf(th, &st, &ct);
         sincosf(ph, &sp, &cp);
         cj[j] = st * cp * wi.x + st * sp * wi.y + ct * wi.z;
-        s[j] = lam[j] * vmf_norm(kap[j]) * expf(kap[j] * (cj[j] - 1.f));
-        V += s[j];
+        // log(lam_j * norm_j * exp(kappa_j (c_j - 1)))
+        ls[j] = (o[4 * j + 3] - lse_l) + lk - 1.83787706640935f - logf(-expm1f(-2.f * kap[j])) +
+                kap[j] * (cj[j] - 1.f);
+        lsmax = fmaxf(lsmax, ls[j]);
     }
+    float sv = 0.f;
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) sv += expf(ls[j] - lsmax);
+    const float logV = lsmax + logf(sv);
+    const float V = expf(logV);
     const float sa = guide_sigmoid(o[32]);
-    const float alpha = kGuideAlphaMax * sa;
-    const float q = fmaxf(alpha * V + (1.f - alpha) * pdfb, 1e-8f);
-    const float iq = 1.f / q;
-    const float gscale = -wt;  // d loss / d log q
+    const float alpha = kGuideAlphaMin + kGuideAlphaSpan * sa;
+    const float q = fmaxf(alpha * V + (1.f - alpha) * pdfb, 1e-30f);
     auto clampg = [](float g) { return fminf(fmaxf(g, -kGuideGradClamp), kGuideGradClamp); };
 #pragma unroll
     for (int j = 0; j < kGuideLobes; j++) {
-        const float th = 3.14159265358979f * guide_sigmoid(o[4 * j]);
-        const float ph = 6.28318530717959f * guide_sigmoid(o[4 * j + 1]);
         const float sth = guide_sigmoid(o[4 * j]), sph = guide_sigmoid(o[4 * j + 1]);
+        const float th = 3.14159265358979f * sth, ph = 6.28318530717959f * sph;
         float st, ct, sp, cp;
         sincosf(th, &st, &ct);
         sincosf(ph, &sp, &cp);
-        const float r = alpha * s[j] * iq;  // d log q / d log s_j
+        const float r = expf(ls[j] - logV);  // share of lobe j in V(wi)
         const float k = kap[j];
-        // d log q / d mu = r * kappa * wi, through mu(theta, phi)
+        const float lam = expf(o[4 * j + 3] - lse_l);
         const float dth = r * k * (ct * cp * wi.x + ct * sp * wi.y - st * wi.z) * 3.14159265358979f * sth * (1.f - sth);
         const float dph = r * k * (-st * sp * wi.x + st * cp * wi.y) * 6.28318530717959f * sph * (1.f - sph);
-        const bool kin = o[4 * j + 2] > kGuideLogKappaMin && o[4 * j + 2] < kGuideLogKappaMax;
-        const float dk = kin ? r * (1.f - 2.f * k / expm1f(2.f * k) + k * (cj[j] - 1.f)) : 0.f;
-        const float dl = alpha * iq * (s[j] - lam[j] * V);
-        dout[4 * j + 0] = clampg(gscale * dth);
-        dout[4 * j + 1] = clampg(gscale * dph);
-        dout[4 * j + 2] = clampg(gscale * dk);
-        dout[4 * j + 3] = clampg(gscale * dl);
+        const float sk = guide_sigmoid(o[4 * j + 2]);
+        const float dk = r * (1.f - 2.f * k / expm1f(2.f * k) + k * (cj[j] - 1.f)) * kGuideLogKappaSpan * sk * (1.f - sk);
+        dout[4 * j + 0] = clampg(-wt * dth);
+        dout[4 * j + 1] = clampg(-wt * dph);
+        dout[4 * j + 2] = clampg(-wt * dk);
+        dout[4 * j + 3] = clampg(-wt * (r - lam));
     }
-    dout[32] = clampg(gscale * (V - pdfb) * iq * kGuideAlphaMax * sa * (1.f - sa));
+    dout[32] = clampg(-wt * (V - pdfb) / q * kGuideAlphaSpan * sa * (1.f - sa));
 #pragma unroll
     for (int i = 33; i < kGuideOut; i++) dout[i] = 0.f;
-    return -wt * logf(q);
+    return -wt * (logV + logf(q));
 }
 
 // ------------------------------------------------------------------ batched inference

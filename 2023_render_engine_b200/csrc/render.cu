@@ -64,7 +64,7 @@ struct Buffers {
 };
 
 struct GuideView {
-    const GuideParams *params;  // per queue slot; null while the guide is untrained
+    const GuideParams *params;  // per queue slot; null while the guide is untrained (BSDF sampling)
     GuideRecord *recs;
     uint32_t *rcnt;        // [0] records, [1] nonzero-weight records
     uint32_t *nz;          // records with nonzero weight
@@ -779,7 +779,7 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
         if (photon_mode) return fail(RT_ERR_UNSUPPORTED, "rt_render: RT_RENDER_GUIDE with RT_RENDER_PHOTON_MAP");
         gv.enabled = 1;
         gv.train = s->guide_train;
-        if (guide->step > 0) {
+        if (guide->trained) {
             RTB_CHECK(guide->params.reserve(sizeof(GuideParams) * (uint64_t)cap));
             gv.params = guide->params.as<GuideParams>();
         }

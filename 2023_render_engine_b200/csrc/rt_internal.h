@@ -197,7 +197,8 @@ struct rt_photon_map {
 struct rt_guide {
     rt_context *ctx = nullptr;
     rt_guide_opts opts{};
-    uint64_t step = 0;  // Adam steps taken
+    uint64_t step = 0;     // Adam steps taken
+    bool trained = false;  // parameters came from training or the caller: rendering samples the guide
     // parameters: FP32 master, Adam moments, last gradient, FP16 shared-memory image
     rtb::DevBuf master, adam_m, adam_v, grad, img;
     // training scratch: transposed activations / gradients, per-chunk weight-gradient

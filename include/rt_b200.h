@@ -322,7 +322,7 @@ RT_API int rt_photon_knn(rt_photon_map *map, const float *queries_dev, const int
  * the guide's box), outgoing direction (one-blob, 32 theta + 32 phi bins), shading normal:
  * 139 inputs padded to 144 — through 4 hidden layers of 64 (ReLU) to 48 outputs: 8 von
  * Mises-Fisher lobes (mean direction, log concentration, weight logit) and the probability
- * alpha of sampling the guide rather than the BSDF. FP16 weights and activations on the
+ * alpha (in [0.05, 0.95]) of sampling the guide rather than the BSDF. FP16 weights and activations on the
  * tensor cores, FP32 accumulation, FP32 master weights with Adam (beta 0.9 / 0.99). */
 typedef struct rt_guide rt_guide;
 
@@ -359,7 +359,8 @@ RT_API int rt_guide_sample(rt_guide *g, const float *queries_dev, const float *u
                            float *out_pdf_dev);
 
 /* One training step on B samples:
- *   loss = mean_i( -wt_i * log(alpha * vmf_mixture(dir_i) + (1 - alpha) * bsdf_pdf_i) ),
+ *   loss = mean_i( -wt_i * (log V(dir_i) + log(alpha * V(dir_i) + (1 - alpha) * bsdf_pdf_i)) ),
+ *   V = the vMF mixture, held constant inside the second term (which trains alpha only),
  *   wt_i = min(w_i / mean(w), 32), w_i = the sample's incident radiance times f * cos / pdf.
  * apply = 0 computes the gradient only; apply = 1 also takes an Adam step. grad_host (nullable)
  * receives the gradient (parameter order as rt_guide_params_get), loss_out (nullable) the loss. */

@@ -9,8 +9,10 @@ the specification the GPU kernels are checked against (guide.cuh, guide.cu):
   and hidden activations are rounded to IEEE half where the GPU stores them, everything else
   is float64 (the GPU accumulates in float32, so results agree to accumulation order).
 * decode() / mixture_pdf(): 8 von Mises-Fisher lobes plus the guide selection probability.
-* loss_grad_out() / loss_and_grad(): the training loss  mean(-wt * log q)  and its analytic
-  gradient, with the GPU's clamps and FP16 gradient storage (scale 8).
+* loss_grad_out() / loss_and_grad(): the training loss
+  mean(-wt * (log V + log(alpha V + (1 - alpha) pdf_bsdf))), V the vMF mixture held constant
+  inside the second term, and its analytic gradient, with the GPU's clamps and FP16 gradient
+  storage (scale 8).
 * adam(): beta1 0.9, beta2 0.99, eps 1e-8, bias-corrected.
 * sample(): vMF mixture sampling by the inversion of Jakob (2012).
 
@@ -22,8 +24,8 @@ from __future__ import annotations
 import numpy as np
 
 N_IN, N_HID, N_OUT, N_LAYERS, N_LOBES = 144, 64, 48, 5, 8
-ALPHA_MAX = 0.95
-LOGK_MIN, LOGK_MAX = -4.0, 8.0
+ALPHA_MIN, ALPHA_SPAN = 0.05, 0.9
+LOGK_MIN, LOGK_SPAN = -4.0, 12.0
 WEIGHT_CLIP = 32.0
 GRAD_CLAMP = 8192.0
 GRAD_SCALE = 8.0
@@ -117,12 +119,12 @@ def decode(out):
     L = o[:, :32].reshape(-1, N_LOBES, 4)
     th = np.pi * _sig(L[..., 0])
     ph = 2 * np.pi * _sig(L[..., 1])
-    k = np.exp(np.clip(L[..., 2], LOGK_MIN, LOGK_MAX))
+    k = np.exp(LOGK_MIN + LOGK_SPAN * _sig(L[..., 2]))
     lg = L[..., 3] - L[..., 3].max(axis=1, keepdims=True)
     lam = np.exp(lg)
     lam /= lam.sum(axis=1, keepdims=True)
     mu = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], axis=-1)
-    alpha = ALPHA_MAX * _sig(o[:, 32])
+    alpha = ALPHA_MIN + ALPHA_SPAN * _sig(o[:, 32])
     return {"mu": mu, "kappa": k, "lam": lam, "alpha": alpha}
 
 
@@ -140,41 +142,62 @@ def mixture_pdf(out, w, pdfb):
     return d["alpha"] * guide_pdf(d, w) + (1 - d["alpha"]) * np.asarray(pdfb, dtype=np.float64)
 
 
-def loss_grad_out(out, wi, pdfb, wt, clamp=True):
-    """Per-row loss -wt log q and d loss / d out (B, 48)."""
-    o = np.asarray(out, dtype=np.float64)
-    wi = np.asarray(wi, dtype=np.float64)
+def _lobe_terms(o, wi):
     B = o.shape[0]
     L = o[:, :32].reshape(B, N_LOBES, 4)
     sth, sph = _sig(L[..., 0]), _sig(L[..., 1])
     th, ph = np.pi * sth, 2 * np.pi * sph
     r = L[..., 2]
-    k = np.exp(np.clip(r, LOGK_MIN, LOGK_MAX))
-    lg = L[..., 3] - L[..., 3].max(axis=1, keepdims=True)
-    lam = np.exp(lg)
-    lam /= lam.sum(axis=1, keepdims=True)
+    lk = LOGK_MIN + LOGK_SPAN * _sig(r)
+    k = np.exp(lk)
+    lg = L[..., 3]
+    lse_l = lg.max(1, keepdims=True) + np.log(np.exp(lg - lg.max(1, keepdims=True)).sum(1, keepdims=True))
     st, ct, sp, cp = np.sin(th), np.cos(th), np.sin(ph), np.cos(ph)
     c = st * cp * wi[:, 0:1] + st * sp * wi[:, 1:2] + ct * wi[:, 2:3]
-    s = lam * vmf_norm(k) * np.exp(k * (c - 1))
-    V = s.sum(1)
+    ls = (lg - lse_l) + lk - np.log(2 * np.pi) - np.log(-np.expm1(-2 * k)) + k * (c - 1)
+    m = ls.max(1, keepdims=True)
+    logV = (m + np.log(np.exp(ls - m).sum(1, keepdims=True)))[:, 0]
+    return dict(sth=sth, sph=sph, st=st, ct=ct, sp=sp, cp=cp, r=r, k=k, c=c, ls=ls, logV=logV,
+                lam=np.exp(lg - lse_l))
+
+
+def loss_value(out, wi, pdfb, wt, V_fixed=None):
+    """Per-row loss -wt (log V + log(alpha V' + (1 - alpha) pdf_bsdf)), V' = V_fixed if given
+    (the second term trains alpha only, so its V is a constant)."""
+    o = np.asarray(out, dtype=np.float64)
+    t = _lobe_terms(o, np.asarray(wi, dtype=np.float64))
+    V = np.exp(t["logV"]) if V_fixed is None else V_fixed
+    alpha = ALPHA_MIN + ALPHA_SPAN * _sig(o[:, 32])
+    q = np.maximum(alpha * V + (1 - alpha) * pdfb, 1e-30)
+    return -wt * (t["logV"] + np.log(q))
+
+
+def loss_grad_out(out, wi, pdfb, wt, clamp=True):
+    """Per-row loss and d loss / d out (B, 48), V constant inside the alpha term."""
+    o = np.asarray(out, dtype=np.float64)
+    wi = np.asarray(wi, dtype=np.float64)
+    B = o.shape[0]
+    t = _lobe_terms(o, wi)
+    V = np.exp(t["logV"])
     sa = _sig(o[:, 32])
-    alpha = ALPHA_MAX * sa
-    q = np.maximum(alpha * V + (1 - alpha) * pdfb, 1e-8)
-    loss = -wt * np.log(q)
-    rr = alpha[:, None] * s / q[:, None]
-    dth = rr * k * (ct * cp * wi[:, 0:1] + ct * sp * wi[:, 1:2] - st * wi[:, 2:3]) * np.pi * sth * (1 - sth)
-    dph = rr * k * (-st * sp * wi[:, 0:1] + st * cp * wi[:, 1:2]) * 2 * np.pi * sph * (1 - sph)
-    kin = (r > LOGK_MIN) & (r < LOGK_MAX)
+    alpha = ALPHA_MIN + ALPHA_SPAN * sa
+    q = np.maximum(alpha * V + (1 - alpha) * pdfb, 1e-30)
+    loss = -wt * (t["logV"] + np.log(q))
+    rr = np.exp(t["ls"] - t["logV"][:, None])
+    k, c, st, ct, sp, cp = t["k"], t["c"], t["st"], t["ct"], t["sp"], t["cp"]
+    dth = rr * k * (ct * cp * wi[:, 0:1] + ct * sp * wi[:, 1:2] - st * wi[:, 2:3]) * np.pi * t["sth"] * (1 - t["sth"])
+    dph = rr * k * (-st * sp * wi[:, 0:1] + st * cp * wi[:, 1:2]) * 2 * np.pi * t["sph"] * (1 - t["sph"])
     with np.errstate(over="ignore", invalid="ignore"):
         frac = np.where(2 * k > 700, 0.0, 2 * k / np.expm1(np.minimum(2 * k, 700)))
-    dk = np.where(kin, rr * (1 - frac + k * (c - 1)), 0.0)
-    dl = alpha[:, None] / q[:, None] * (s - lam * V[:, None])
+    sk = _sig(t["r"])
+    dk = rr * (1 - frac + k * (c - 1)) * LOGK_SPAN * sk * (1 - sk)
+    dl = rr - t["lam"]
     g = np.zeros((B, N_OUT))
     g[:, 0:32:4] = -wt[:, None] * dth
     g[:, 1:32:4] = -wt[:, None] * dph
     g[:, 2:32:4] = -wt[:, None] * dk
     g[:, 3:32:4] = -wt[:, None] * dl
-    g[:, 32] = -wt * (V - pdfb) / q * ALPHA_MAX * sa * (1 - sa)
+    g[:, 32] = -wt * (V - pdfb) / q * ALPHA_SPAN * sa * (1 - sa)
     if clamp:
         g = np.clip(g, -GRAD_CLAMP, GRAD_CLAMP)
     return loss, g
@@ -185,6 +208,17 @@ def train_weights(w):
     mean = np.float32(w.astype(np.float64).mean()) if w.size else np.float32(0)
     inv = np.float32(1.0) / mean if mean > 0 else np.float32(0)
     return np.minimum(w * inv, np.float32(WEIGHT_CLIP)).astype(np.float64)
+
+
+def loss_fixed(params, q, dirs, pdfb, w, bmin, bmax, params_V):
+    """float64 mean loss with the alpha term's V taken from `params_V` (finite-difference
+    checks of loss_and_grad at params == params_V)."""
+    X = encode(q, bmin, bmax)
+    _, out = forward(params, X, fp16=False)
+    _, outV = forward(params_V, X, fp16=False)
+    V = np.exp(_lobe_terms(outV, np.asarray(dirs, dtype=np.float64))["logV"])
+    wt = train_weights(w)
+    return float(loss_value(out, dirs, np.asarray(pdfb, dtype=np.float64), wt, V_fixed=V).mean())
 
 
 def loss_and_grad(params, q, dirs, pdfb, w, bmin, bmax, fp16=True):

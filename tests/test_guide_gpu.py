@@ -65,27 +65,45 @@ def test_pdf_matches_oracle(guide):
     assert np.allclose(pdf, ref, rtol=2e-2, atol=1e-4)
 
 
-def test_sample_matches_oracle_and_density(guide):
-    import torch
+def fib_sphere(m):
+    i = np.arange(m) + 0.5
+    z = 1 - 2 * i / m
+    r = np.sqrt(1 - z * z)
+    ph = np.pi * (1 + 5 ** 0.5) * i
+    return np.stack([r * np.cos(ph), r * np.sin(ph), z], 1)
 
+
+def cube_face(d):
+    a = np.argmax(np.abs(d), 1)
+    return a * 2 + (d[np.arange(len(d)), a] > 0)
+
+
+def test_sample_matches_oracle_and_density(guide):
     rng = np.random.default_rng(2)
-    q, _, _, _ = batch(rng, 8)
-    reps = 1 << 15
+    nq, reps = 6, 1 << 15
+    q, _, _, _ = batch(rng, nq)
     qq = np.repeat(q, reps, axis=0)
     u = rng.uniform(size=(qq.shape[0], 3)).astype(np.float32)
     dirs, pdf = guide.sample(cuda(qq), cuda(u))
-    dirs, pdf = dirs.cpu().numpy(), pdf.cpu().numpy()
+    dirs, pdf = dirs.cpu().numpy().astype(np.float64), pdf.cpu().numpy()
     assert np.allclose(np.linalg.norm(dirs, axis=1), 1, atol=1e-4)
-    # the same uniforms through the oracle give the same directions (lobe picks may differ
-    # only where u0 sits on a lobe boundary after FP16 rounding of the network)
-    _, out = G.forward(guide.params(), G.encode(q, BMIN, BMAX))
+    out = guide.eval(cuda(q)).cpu().numpy()
+    # the same uniforms through the oracle give the same directions (a lobe pick may differ
+    # where u0 falls on a lobe boundary)
     ref = G.sample(np.repeat(out, reps, axis=0), u)
-    close = np.linalg.norm(dirs - ref, axis=1) < 2e-2
-    assert close.mean() > 0.99
-    # E[1 / p(w)] = 4 pi for samples of a density p with full support
-    est = (1.0 / pdf.astype(np.float64)).reshape(8, reps).mean(1)
-    assert np.all(np.abs(est / (4 * np.pi) - 1) < 0.05), est / (4 * np.pi)
-    del torch
+    assert (np.linalg.norm(dirs - ref, axis=1) < 2e-2).mean() > 0.99
+    # the returned density is the mixture's at the sample
+    dec = G.decode(np.repeat(out, reps, axis=0))
+    assert np.allclose(pdf, G.guide_pdf(dec, dirs), rtol=2e-3, atol=1e-6)
+    # and the samples follow it: per cube face, sample frequency vs quadrature of the density
+    fib = fib_sphere(1 << 21)
+    ff = cube_face(fib)
+    for b in range(nq):
+        hist = np.bincount(cube_face(dirs[b * reps:(b + 1) * reps]), minlength=6) / reps
+        d1 = {k: v[b:b + 1].repeat(len(fib), 0) for k, v in G.decode(out).items()}
+        p = G.guide_pdf(d1, fib)
+        expect = np.array([(p * (ff == k)).mean() * 4 * np.pi for k in range(6)])
+        assert np.allclose(hist, expect, atol=0.015), (b, hist, expect)
 
 
 def test_gradient_matches_oracle(guide):
@@ -116,7 +134,9 @@ def test_adam_step_matches_oracle(guide):
     # the FP16 image follows the master weights: outputs match the oracle on the new weights
     out = guide.eval(cuda(q[:512])).cpu().numpy()
     _, r = G.forward(p1, G.encode(q[:512], BMIN, BMAX))
+    _, r0 = G.forward(p0, G.encode(q[:512], BMIN, BMAX))
     assert np.allclose(out, r, atol=3e-2, rtol=3e-2)
+    assert np.abs(out - r).mean() < 0.2 * np.abs(out - r0).mean()
 
 
 def test_set_params_roundtrip_resets_adam(guide):
