@@ -1,7 +1,7 @@
 // Path-guide network: training on the tensor cores and the rt_guide_* entry points.
 //
 // One training step on B samples (rows padded to a multiple of 16):
-//   k_guide_wmean     mean of the sample weights (normalises the loss)
+//   k_guide_wsum      partial sums of the sample weights (their mean normalises the loss)
 //   k_guide_train_fb  per 16-row warp tile: encode, forward (activations kept in shared
 //                     memory), loss gradient per row, backward through the 5 layers; writes
 //                     every layer's input and output gradient transposed (feature-major) so
@@ -28,7 +28,9 @@ constexpr int kTrainX0 = 0, kTrainH = 16 * 152 * 2, kTrainD = kTrainH + 4 * 16 *
 constexpr int kTrainWarpBytes = kTrainO + 16 * 49 * 4;
 constexpr int kTrainSmem = kGuideImgBytes + kTrainWarps * kTrainWarpBytes;
 static_assert(kTrainSmem <= 227 * 1024, "training kernel shared memory");
-constexpr uint32_t kWgradChunk = 2048;  // rows per weight-gradient block
+constexpr uint32_t kWgradChunk = 1024;  // rows per weight-gradient block
+constexpr int kWgradItems = 28;         // 25 input-feature tiles + 3 bias groups
+constexpr int kWsumBlocks = 128;
 constexpr float kAdamB1 = 0.9f, kAdamB2 = 0.99f, kAdamEps = 1e-8f;
 
 __device__ __forceinline__ uint32_t pack_h2(__half a, __half b)
@@ -80,14 +82,23 @@ struct TrainArgs {
     const float *q, *dir, *pdf, *w;
     uint64_t B, Bpad;
     __half *xt, *gt;
-    float *scal;  // [0] weight mean (in), [1] loss sum (accumulated)
+    float *scal;          // [1] loss sum (accumulated)
+    const double *wpart;  // kWsumBlocks partial sums of the weights
     GuideBox box;
 };
 
 __global__ void __launch_bounds__(kTrainWarps * 32, 1) k_guide_train_fb(const uint4 *img, TrainArgs A)
 {
     extern __shared__ uint4 train_smem[];
+    __shared__ double wsum;
     for (int i = threadIdx.x; i < kGuideImgBytes / 16; i += blockDim.x) train_smem[i] = img[i];
+    if (threadIdx.x < 32) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < kWsumBlocks; i += 32) s += A.wpart[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) wsum = s;
+    }
     __syncthreads();
     unsigned char *sm = reinterpret_cast<unsigned char *>(train_smem);
     const __half *W = reinterpret_cast<const __half *>(sm);
@@ -99,7 +110,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32, 1) k_guide_train_fb(const ui
     __half *H2 = H1 + 16 * 72, *H3 = H2 + 16 * 72, *H4 = H3 + 16 * 72;
     __half *D = reinterpret_cast<__half *>(wb + kTrainD);
     float *O = reinterpret_cast<float *>(wb + kTrainO);
-    const float wmean = A.scal[0];
+    const float wmean = A.B ? (float)(wsum / (double)A.B) : 0.f;
     const float winv = wmean > 0.f ? 1.f / wmean : 0.f;
     const uint64_t Bp = A.Bpad;
     float lsum = 0.f;
@@ -184,7 +195,10 @@ __global__ void __launch_bounds__(kTrainWarps * 32, 1) k_guide_train_fb(const ui
     if (lane == 0 && lsum != 0.f) atomicAdd(A.scal + 1, lsum);
 }
 
-// dW (16 input features x NT*8 outputs) over rows [r0, r1): A = X^T plane rows, B = G^T plane rows
+// dW (16 input features x NT*8 outputs) over rows [r0, r1), r0 and r1 multiples of 32.
+// The reduction runs over rows, so their order inside a 32-row block is free: logical k-slots
+// {2t, 2t+1, 2t+8, 2t+9} of the two m16n8k16 steps map to rows 8t .. 8t+7, which lets every
+// lane fetch its A and B fragments with one 16-byte load per feature plane.
 template <int NT>
 __device__ __forceinline__ void wgrad_tile(const __half *X, const __half *G, uint64_t Bp, int mt, uint64_t r0,
                                            uint64_t r1, float *dW, int out, int lane)
@@ -195,16 +209,22 @@ __device__ __forceinline__ void wgrad_tile(const __half *X, const __half *G, uin
     for (int n = 0; n < NT; n++)
 #pragma unroll
         for (int i = 0; i < 4; i++) acc[n][i] = 0.f;
-    const uint32_t *xa = reinterpret_cast<const uint32_t *>(X + (uint64_t)(mt * 16 + g) * Bp);
-    const uint32_t *xb = reinterpret_cast<const uint32_t *>(X + (uint64_t)(mt * 16 + g + 8) * Bp);
-    const uint32_t *gb[NT];
+    const uint4 *xa = reinterpret_cast<const uint4 *>(X + (uint64_t)(mt * 16 + g) * Bp);
+    const uint4 *xb = reinterpret_cast<const uint4 *>(X + (uint64_t)(mt * 16 + g + 8) * Bp);
+    const uint4 *gb[NT];
 #pragma unroll
-    for (int n = 0; n < NT; n++) gb[n] = reinterpret_cast<const uint32_t *>(G + (uint64_t)(n * 8 + g) * Bp);
-    for (uint64_t r = r0; r < r1; r += 16) {
-        const uint64_t i0 = (r >> 1) + t;
-        const uint32_t a[4] = {__ldg(xa + i0), __ldg(xb + i0), __ldg(xa + i0 + 4), __ldg(xb + i0 + 4)};
+    for (int n = 0; n < NT; n++) gb[n] = reinterpret_cast<const uint4 *>(G + (uint64_t)(n * 8 + g) * Bp);
+#pragma unroll 2
+    for (uint64_t r = r0; r < r1; r += 32) {
+        const uint64_t i = (r >> 3) + t;
+        const uint4 a = __ldg(xa + i), b = __ldg(xb + i);
+        const uint32_t a0[4] = {a.x, b.x, a.y, b.y}, a1[4] = {a.z, b.z, a.w, b.w};
 #pragma unroll
-        for (int n = 0; n < NT; n++) mma16816(acc[n], a, __ldg(gb[n] + i0), __ldg(gb[n] + i0 + 4));
+        for (int n = 0; n < NT; n++) {
+            const uint4 v = __ldg(gb[n] + i);
+            mma16816(acc[n], a0, v.x, v.y);
+            mma16816(acc[n], a1, v.z, v.w);
+        }
     }
     const int m = mt * 16 + g;
 #pragma unroll
@@ -217,57 +237,68 @@ __device__ __forceinline__ void wgrad_tile(const __half *X, const __half *G, uin
     }
 }
 
+// One warp per work item and chunk of rows: items 0..24 are the layers' 16-feature input
+// tiles (9 for layer 0, 4 for each other layer), items 25..27 the bias sums (a third of the
+// 304 output features each). Grid: (chunks, 7) blocks of 4 warps.
 __global__ void __launch_bounds__(128) k_guide_wgrad(const __half *xt, const __half *gt, uint64_t Bp, float *partial)
 {
     const uint32_t c = blockIdx.x;
-    const int l = blockIdx.y;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint64_t r0 = (uint64_t)c * kWgradChunk, r1 = std::min<uint64_t>(r0 + kWgradChunk, Bp);
+    const int item = blockIdx.y * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (item >= kWgradItems) return;
+    const uint64_t r0 = (uint64_t)c * kWgradChunk;
+    const uint64_t r1 = r0 + kWgradChunk < Bp ? r0 + kWgradChunk : Bp;
     float *part = partial + (uint64_t)c * kGuideParamCount;
-    if (l < kGuideLayers) {
+    if (item < 25) {
+        const int l = item < 9 ? 0 : 1 + (item - 9) / 4;
+        const int mt = item < 9 ? item : (item - 9) % 4;
         const __half *X = xt + (uint64_t)guide_xoff(l) * Bp;
         const __half *G = gt + (uint64_t)guide_goff(l) * Bp;
-        const int mtiles = guide_in(l) / 16;
-        for (int mt = warp; mt < mtiles; mt += 4) {
-            if (l == kGuideLayers - 1)
-                wgrad_tile<6>(X, G, Bp, mt, r0, r1, part + guide_pw(l), kGuideOut, lane);
-            else
-                wgrad_tile<8>(X, G, Bp, mt, r0, r1, part + guide_pw(l), kGuideHidden, lane);
-        }
-    } else {
-        for (int f = warp; f < kGuideGFeatures; f += 4) {
-            const __half2 *g2 = reinterpret_cast<const __half2 *>(gt + (uint64_t)f * Bp + r0);
-            float s = 0.f;
-            for (uint64_t i = lane; i < (r1 - r0) / 2; i += 32) {
-                const float2 v = __half22float2(g2[i]);
-                s += v.x + v.y;
-            }
+        if (l == kGuideLayers - 1)
+            wgrad_tile<6>(X, G, Bp, mt, r0, r1, part + guide_pw(l), kGuideOut, lane);
+        else
+            wgrad_tile<8>(X, G, Bp, mt, r0, r1, part + guide_pw(l), kGuideHidden, lane);
+        return;
+    }
+    constexpr int kPer = (kGuideGFeatures + 2) / 3;
+    const int f0 = (item - 25) * kPer, f1 = f0 + kPer < kGuideGFeatures ? f0 + kPer : kGuideGFeatures;
+    for (int f = f0; f < f1; f++) {
+        const uint4 *g4 = reinterpret_cast<const uint4 *>(gt + (uint64_t)f * Bp + r0);
+        float s = 0.f;
+        for (uint64_t i = lane; i < (r1 - r0) / 8; i += 32) {
+            const uint4 v = __ldg(g4 + i);
+            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) {
-                const int ll = f < 4 * kGuideHidden ? f / kGuideHidden : 4;
-                part[guide_pb(ll) + (f - guide_goff(ll))] = s;
+            for (int k = 0; k < 4; k++) {
+                const float2 h = __half22float2(*reinterpret_cast<const __half2 *>(&w[k]));
+                s += h.x + h.y;
             }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            const int ll = f < 4 * kGuideHidden ? f / kGuideHidden : 4;
+            part[guide_pb(ll) + (f - guide_goff(ll))] = s;
         }
     }
 }
 
-// deterministic weight mean (one block)
-__global__ void __launch_bounds__(1024) k_guide_wmean(const float *w, uint64_t B, float *scal)
+// partial sums of the sample weights (double, fixed order); block 0 also clears the loss
+// sum and the non-finite flag of this step
+__global__ void __launch_bounds__(256) k_guide_wsum(const float *w, uint64_t B, double *part, float *scal)
 {
-    __shared__ double red[32];
+    __shared__ double red[8];
     double s = 0.0;
-    for (uint64_t i = threadIdx.x; i < B; i += blockDim.x) s += (double)w[i];
+    for (uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x; i < B; i += (uint64_t)kWsumBlocks * 256)
+        s += (double)w[i];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        s = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (threadIdx.x == 0) {
-            scal[0] = B ? (float)(s / (double)B) : 0.f;
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < 8; i++) t += red[i];
+        part[blockIdx.x] = t;
+        if (blockIdx.x == 0) {
             scal[1] = 0.f;
             reinterpret_cast<uint32_t *>(scal)[2] = 0u;
         }
@@ -459,29 +490,30 @@ int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf,
         if (grad_host) std::memset(grad_host, 0, 4ull * kGuideParamCount);
         return RT_OK;
     }
-    const uint64_t Bp = (B + 15) / 16 * 16;
+    const uint64_t Bp = (B + 31) / 32 * 32;
     const uint32_t nchunks = (uint32_t)((Bp + kWgradChunk - 1) / kWgradChunk);
     RTB_CHECK(g->xt.reserve(2ull * kGuideXFeatures * Bp));
     RTB_CHECK(g->gt.reserve(2ull * kGuideGFeatures * Bp));
     RTB_CHECK(g->partial.reserve(4ull * kGuideParamCount * nchunks));
     RTB_CHECK(g->grad.reserve(4ull * kGuideParamCount));
-    RTB_CHECK(g->scal.reserve(64));
+    RTB_CHECK(g->scal.reserve(64 + 8 * kWsumBlocks));
     if (!g->host_scal) RTB_CUDA(cudaMallocHost(&g->host_scal, 64));
     float *scal = g->scal.as<float>();
-    k_guide_wmean<<<1, 1024, 0, st>>>(w, B, scal);
+    double *wpart = reinterpret_cast<double *>(g->scal.as<uint8_t>() + 64);
+    k_guide_wsum<<<kWsumBlocks, 256, 0, st>>>(w, B, wpart, scal);
     RTB_CUDA(cudaGetLastError());
     static bool attr = false;
     if (!attr) {
         RTB_CUDA(cudaFuncSetAttribute(k_guide_train_fb, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem));
         attr = true;
     }
-    TrainArgs a{q, dir, pdf, w, B, Bp, g->xt.as<__half>(), g->gt.as<__half>(), scal, guide_box(g)};
+    TrainArgs a{q, dir, pdf, w, B, Bp, g->xt.as<__half>(), g->gt.as<__half>(), scal, wpart, guide_box(g)};
     const uint64_t tiles = Bp / 16;
     const unsigned grid =
         (unsigned)std::min<uint64_t>((tiles + kTrainWarps - 1) / kTrainWarps, (uint64_t)std::max(g->ctx->sm_count, 1));
     k_guide_train_fb<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(g->img.as<uint4>(), a);
     RTB_CUDA(cudaGetLastError());
-    k_guide_wgrad<<<dim3(nchunks, kGuideLayers + 1), 128, 0, st>>>(g->xt.as<__half>(), g->gt.as<__half>(), Bp,
+    k_guide_wgrad<<<dim3(nchunks, (kWgradItems + 3) / 4), 128, 0, st>>>(g->xt.as<__half>(), g->gt.as<__half>(), Bp,
                                                                    g->partial.as<float>());
     RTB_CUDA(cudaGetLastError());
     const unsigned pblocks = (kGuideParamCount + 255) / 256;

@@ -5,7 +5,9 @@
 // Network: 144 encoded inputs -> 4 hidden layers of 64 (ReLU) -> 48 outputs, FP16 weights and
 // activations on the tensor cores (mma.sync m16n8k16, FP32 accumulation), FP32 master weights.
 // Input encoding of a shading point (position p, shading normal n, outgoing direction wo):
-//   [0, 72)    p normalised to the guide's box, per axis 12 frequency bands: sin, cos(2^k pi u)
+//   [0, 72)    p normalised to the guide's box (u in [0, 1]), per axis 12 frequency bands:
+//              sin, cos(2^(k/2) pi u), k = 0..11 (half-octave steps: the finest band resolves
+//              about 1/90 of the box, the scale of the lighting detail, not of the geometry)
 //   [72, 104)  theta(wo) / pi, one-blob over 32 bins (Gaussian, sigma = 1/32)
 //   [104, 136) phi(wo) / 2pi + 1/2, one-blob over 32 bins
 //   [136, 139) n;  [139, 144) zero
@@ -24,7 +26,7 @@ constexpr int kGuideIn = 144, kGuideHidden = 64, kGuideOut = 48, kGuideLayers = 
 constexpr int kGuideParamCount = 24880;  // 144*64+64 + 3*(64*64+64) + 64*48+48
 constexpr float kGuideAlphaMin = 0.05f, kGuideAlphaSpan = 0.9f;  // alpha in [0.05, 0.95]
 constexpr float kGuideLogKappaMin = -4.f, kGuideLogKappaSpan = 12.f;  // log kappa in (-4, 8)
-constexpr float kGuideWeightClip = 32.f;   // training weight / batch mean is clipped here
+constexpr float kGuideWeightClip = 32.f;    // training weight / batch mean is clipped here
 constexpr float kGuideGradClamp = 8192.f;  // per-output gradient clamp
 constexpr float kGuideGradScale = 8.f;     // output gradients are stored as fp16(g / scale)
 
@@ -231,17 +233,16 @@ __device__ __forceinline__ void guide_encode(int part, const float *q, const Gui
         const float u[3] = {fminf(fmaxf((q[0] - bx.lo.x) * bx.inv_ext.x, 0.f), 1.f),
                             fminf(fmaxf((q[1] - bx.lo.y) * bx.inv_ext.y, 0.f), 1.f),
                             fminf(fmaxf((q[2] - bx.lo.z) * bx.inv_ext.z, 0.f), 1.f)};
+        const float scale[12] = {1.f, 1.41421356f, 2.f, 2.82842712f, 4.f, 5.65685425f,
+                                 8.f, 11.3137085f, 16.f, 22.6274170f, 32.f, 45.2548340f};
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-            float x = u[a];
+        for (int a = 0; a < 3; a++)
 #pragma unroll
             for (int k = 0; k < 12; k++) {
                 float s, c;
-                sincospif(x, &s, &c);
+                sincospif(u[a] * scale[k], &s, &c);
                 row[a * 12 + k] = __floats2half2_rn(s, c);
-                x *= 2.f;
             }
-        }
     } else {
         const float th = acosf(fminf(fmaxf(q[8], -1.f), 1.f)) * (1.f / 3.14159265358979f);
         const float ph = atan2f(q[7], q[6]) * (1.f / 6.28318530717959f) + 0.5f;
@@ -322,11 +323,13 @@ __device__ __forceinline__ V3 guide_sample(const GuideParams &P, float u0, float
 }
 
 // Training loss of one sample and its gradient with respect to the raw outputs. The lobes are
-// fitted to the sampled integrand on their own, and the selection probability on the mixture
-// with the lobes held fixed, so a guide that starts out worse than the BSDF still learns:
-//   loss = -wt * (log V(wi) + log(alpha * V(wi) + (1 - alpha) * pdf_bsdf)),  V = vMF mixture,
-// with V treated as a constant inside the second term (it only trains alpha). log V is a
-// log-sum-exp over the lobes, so samples far from every lobe keep a gradient.
+// fitted to the sampled integrand on their own (KL divergence), and the selection probability
+// alpha minimises the estimator's second moment with the lobes held fixed, so a guide that
+// starts out worse than the BSDF still learns and alpha follows what the guide is worth:
+//   loss = -wt * log V(wi) + wt^2 * qc / q,   q = alpha * Vc + (1 - alpha) * pdf_bsdf,
+// V the vMF mixture; Vc and qc are V and q held constant (the second term trains alpha only;
+// its value is wt^2). log V is a log-sum-exp over the lobes, so samples far from every lobe
+// keep a gradient.
 // dout[0..47] receives the gradient (clamped to +-kGuideGradClamp; 0 for the unused outputs).
 __device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, float pdfb, float wt, float *dout)
 {
@@ -382,10 +385,10 @@ __device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, float pd
         dout[4 * j + 2] = clampg(-wt * dk);
         dout[4 * j + 3] = clampg(-wt * (r - lam));
     }
-    dout[32] = clampg(-wt * (V - pdfb) / q * kGuideAlphaSpan * sa * (1.f - sa));
+    dout[32] = clampg(-wt * wt * (V - pdfb) / q * kGuideAlphaSpan * sa * (1.f - sa));
 #pragma unroll
     for (int i = 33; i < kGuideOut; i++) dout[i] = 0.f;
-    return -wt * (logV + logf(q));
+    return -wt * logV + wt * wt;
 }
 
 // ------------------------------------------------------------------ batched inference

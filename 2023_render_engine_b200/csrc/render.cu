@@ -244,7 +244,9 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
                 w = (last_pdf * last_pdf) / (last_pdf * last_pdf + pl * pl);
             }
             L = L + beta_in * Le * w;
-            if (gv.train && rec != kRecNone) {
+            // the guide is not trained on emitters that next-event estimation samples: with
+            // area NEE on, the direct light is NEE's job and the guide learns the rest
+            if (gv.train && rec != kRecNone && !(nee_area && bs.type == RT_MAT_LIGHT && sf.emissive_tri)) {
                 float4 &e = gv.recs[rec].e;
                 e.x += beta_in.x * Le.x * w;
                 e.y += beta_in.y * Le.y * w;
@@ -313,9 +315,11 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
             regenerate(rv, bf, nxt);
             return;
         }
-        // Russian roulette (pathTracing.cu:91-102)
+        // Russian roulette (pathTracing.cu:91-102) on the reference's brightness (luminance) in
+        // compat mode; on the largest component otherwise, so that no channel of a surviving
+        // path's throughput grows past 1 (luminance lets a saturated red path grow 4.7x)
         if (!finished && scattering && depth > rv.rr_depth) {
-            float qrr = fmaxf(0.05f, 1.f - luminance(beta));
+            float qrr = fmaxf(0.05f, 1.f - (compat ? luminance(beta) : fmaxf(beta.x, fmaxf(beta.y, beta.z))));
             if (pcg_float(rng) < qrr)
                 finished = true;
             else

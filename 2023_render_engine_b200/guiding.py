@@ -57,3 +57,50 @@ def render_progressive(scene, camera, guide, passes, max_depth: int, rr_depth: i
     if guide is not None:
         scene.set_guide(guide, train=False)
     return film, total_s
+
+
+def film_rmse(film, ref_mean) -> float:
+    """computeRMSE (camera/Film.cu:611-632) of a device film against a device (H*W, 3) float64
+    mean image: sqrt(sum over pixels of the squared RGB difference / pixels)."""
+    s = (film["sum64"] if "sum64" in film else film["sum"]).double().view(-1, 3)
+    c = film["count"].double().clamp_min(1).view(-1, 1)
+    d = s / c - ref_mean
+    return float((d * d).sum().sqrt().item() / (ref_mean.shape[0] ** 0.5))
+
+
+def time_to_rmse(scene, camera, ref_mean, target: float, guide=None, pass_spp: int = 4, max_spp: int = 4096,
+                 max_depth: int = 16, rr_depth: int = 3, seed: int = 0, flags: int = 0, train_passes: int = 0,
+                 steps_per_pass: int = 32, batch: int = 1 << 16):
+    """Renders progressively until the RMSE against `ref_mean` reaches `target`.
+
+    Plain (guide None): passes of `pass_spp`. Guided: first `train_passes` passes of 1 spp, each
+    followed by `steps_per_pass` training steps on its records, then passes of `pass_spp` with
+    the trained guide. The clock (device-synchronised) covers rendering and training, not the
+    RMSE checks. Returns dict(seconds, spp, rmse, reached, curve)."""
+    import torch
+
+    passes = [1] * train_passes if guide is not None else []
+    while sum(passes) < max_spp:
+        passes.append(pass_spp)
+    curve = []
+    state = {"done": False}
+
+    class _Stop(Exception):
+        pass
+
+    def on_pass(i, spp, film, seconds):
+        e = film_rmse(film, ref_mean)
+        curve.append((spp, seconds, e))
+        if e <= target:
+            raise _Stop()
+
+    try:
+        render_progressive(scene, camera, guide, passes, max_depth=max_depth, rr_depth=rr_depth, seed=seed,
+                           flags=flags, train_passes=train_passes, steps_per_pass=steps_per_pass, batch=batch,
+                           on_pass=on_pass, sync=torch.cuda.synchronize)
+    except _Stop:
+        state["done"] = True
+        if guide is not None:
+            scene.set_guide(guide, train=False)
+    spp, seconds, e = curve[-1]
+    return {"seconds": seconds, "spp": spp, "rmse": e, "reached": state["done"], "curve": curve}

@@ -187,6 +187,49 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def measure_guiding(args, core, N, cfgs, ctx, torch):
+    """Time to RMSE <= args.guide_target on the guiding room (1280x720, max depth 16, area NEE):
+    plain BSDF sampling vs the online-trained guide, against a converged FP64 render."""
+    GD = importlib.import_module("2023_render_engine_b200.guiding")
+    sc, cam, p = cfgs.build_config2(ctx, args.guide_width, args.guide_height)
+    flags = N.RT_RENDER_NEE_AREA
+    t0 = time.perf_counter()
+    ref = None
+    per = 256
+    for k in range((args.guide_ref_spp + per - 1) // per):
+        ref, _ = sc.render(cam, spp=per, max_depth=p["max_depth"], rr_depth=p["rr_depth"], seed=424242, flags=flags,
+                           fp64=True, film=ref, sample_offset=per * k)
+    torch.cuda.synchronize()
+    ref_s = time.perf_counter() - t0
+    ref_mean = (ref["sum64"].view(-1, 3) / ref["count"].double().clamp_min(1).view(-1, 1))
+    # warm the kernels and allocations of both paths once (not timed)
+    T = cfgs.GUIDE_TRAINING
+    g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=11)
+    GD.render_progressive(sc, cam, g, [1, 1], max_depth=p["max_depth"], seed=7, flags=flags, train_passes=1,
+                          steps_per_pass=1, batch=args.guide_batch)
+    g.close()
+    plain = GD.time_to_rmse(sc, cam, ref_mean, args.guide_target, None, pass_spp=4, max_depth=p["max_depth"],
+                            rr_depth=p["rr_depth"], seed=1, flags=flags)
+    g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=2)
+    guided = GD.time_to_rmse(sc, cam, ref_mean, args.guide_target, g, pass_spp=4, max_depth=p["max_depth"],
+                             rr_depth=p["rr_depth"], seed=2, flags=flags, train_passes=args.guide_train_passes,
+                             steps_per_pass=args.guide_steps, batch=args.guide_batch)
+    steps = g.steps
+    g.close()
+    return {
+        "metric": f"time to RMSE<={args.guide_target} vs FP64 oracle (computeRMSE), guided vs plain",
+        "workload": f"guiding room {args.guide_width}x{args.guide_height}, 200k triangles, max depth 16, "
+                    f"area NEE with MIS",
+        "oracle": {"spp": args.guide_ref_spp, "seconds": ref_s, "estimator": "plain BSDF sampling, FP64 film"},
+        "plain": {k: plain[k] for k in ("seconds", "spp", "rmse", "reached")},
+        "guided": {k: guided[k] for k in ("seconds", "spp", "rmse", "reached")},
+        "speedup": (plain["seconds"] / guided["seconds"]) if guided["reached"] and plain["reached"] else None,
+        "training": {"passes": args.guide_train_passes, "steps": steps, "batch": args.guide_batch,
+                     "learning_rate": T["learning_rate"]},
+        "curves": {"plain": plain["curve"][::4], "guided": guided["curve"][::4]},
+    }
+
+
 def run_ours(args):
     import torch
 
@@ -283,6 +326,12 @@ def run_ours(args):
     ms_trace = t0.elapsed_time(t1) / args.steps
     fallback = sc.trace_stats()["exact_fallback_rays"]
 
+    # ---- learned guiding: time to RMSE <= target against the FP64 converged render, guided vs
+    # plain, on the guiding room (one process only: it is a sequence of dependent passes)
+    guiding = None
+    if world == 1 and args.guide_ref_spp > 0:
+        guiding = measure_guiding(args, core, N, cfgs, ctx, torch)
+
     ms, ms_e2e, ms_trace = max_over_ranks([ms, ms_e2e, ms_trace], world)
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -315,6 +364,7 @@ def run_ours(args):
                          "kernel": "k_trace_closest (2^24-ray closest-hit call, 48 B/ray queue-level bytes)",
                          "note": f"peak {peak_kind}; traversal reads nodes/triangles from L2, see profiles/"},
             "clocks": clk.summary(),
+            "guiding": guiding,
         }
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
@@ -341,6 +391,13 @@ def main():
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--guide-ref-spp", type=int, default=4096, help="0 skips the guiding measurement")
+    ap.add_argument("--guide-target", type=float, default=0.01)
+    ap.add_argument("--guide-width", type=int, default=1280)
+    ap.add_argument("--guide-height", type=int, default=720)
+    ap.add_argument("--guide-train-passes", type=int, default=24)
+    ap.add_argument("--guide-steps", type=int, default=32)
+    ap.add_argument("--guide-batch", type=int, default=1 << 16)
     args = ap.parse_args()
     global NRAYS
     NRAYS = 1 << args.rays_log2

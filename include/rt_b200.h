@@ -318,8 +318,8 @@ RT_API int rt_photon_knn(rt_photon_map *map, const float *queries_dev, const int
 /* ------------------------------------------------------------ path guide */
 
 /* Learned path-guiding proposal (new in this build; the reference has no counterpart).
- * A small MLP maps an encoded shading point — position (12 frequency bands per axis inside
- * the guide's box), outgoing direction (one-blob, 32 theta + 32 phi bins), shading normal:
+ * A small MLP maps an encoded shading point — position (12 frequency bands 2^(k/2) per axis
+ * inside the guide's box), outgoing direction (one-blob, 32 theta + 32 phi bins), shading normal:
  * 139 inputs padded to 144 — through 4 hidden layers of 64 (ReLU) to 48 outputs: 8 von
  * Mises-Fisher lobes (mean direction, log concentration, weight logit) and the probability
  * alpha (in [0.05, 0.95]) of sampling the guide rather than the BSDF. FP16 weights and activations on the
@@ -359,8 +359,9 @@ RT_API int rt_guide_sample(rt_guide *g, const float *queries_dev, const float *u
                            float *out_pdf_dev);
 
 /* One training step on B samples:
- *   loss = mean_i( -wt_i * (log V(dir_i) + log(alpha * V(dir_i) + (1 - alpha) * bsdf_pdf_i)) ),
- *   V = the vMF mixture, held constant inside the second term (which trains alpha only),
+ *   loss = mean_i( -wt_i * log V(dir_i) + wt_i^2 * qc_i / q_i ),
+ *   V = the vMF mixture (its KL term fits the lobes), q = alpha * V + (1 - alpha) * bsdf_pdf and
+ *   qc = q held constant with V (the estimator's second moment, which trains alpha only),
  *   wt_i = min(w_i / mean(w), 32), w_i = the sample's incident radiance times f * cos / pdf.
  * apply = 0 computes the gradient only; apply = 1 also takes an Adam step. grad_host (nullable)
  * receives the gradient (parameter order as rt_guide_params_get), loss_out (nullable) the loss. */

@@ -3,16 +3,16 @@
 The reference renderer has no learned guide, so nothing here restates reference code: it is
 the specification the GPU kernels are checked against (guide.cuh, guide.cu):
 
-* encode(): 144 inputs per shading point — 12 frequency bands per position axis, one-blob
+* encode(): 144 inputs per shading point — 12 frequency bands 2^(k/2) per position axis, one-blob
   encodings of the outgoing direction's spherical angles (32 bins each), the shading normal.
 * forward(): 144 -> 64 -> 64 -> 64 -> 64 -> 48 with ReLU; with fp16=True the weights, inputs
   and hidden activations are rounded to IEEE half where the GPU stores them, everything else
   is float64 (the GPU accumulates in float32, so results agree to accumulation order).
 * decode() / mixture_pdf(): 8 von Mises-Fisher lobes plus the guide selection probability.
-* loss_grad_out() / loss_and_grad(): the training loss
-  mean(-wt * (log V + log(alpha V + (1 - alpha) pdf_bsdf))), V the vMF mixture held constant
-  inside the second term, and its analytic gradient, with the GPU's clamps and FP16 gradient
-  storage (scale 8).
+* loss_grad_out() / loss_and_grad(): the training loss mean(-wt log V + wt^2 qc / q) — the
+  lobes' KL term and the estimator's second moment in alpha (q = alpha V + (1 - alpha)
+  pdf_bsdf, V and qc held constant there) — and its analytic gradient, with the GPU's clamps
+  and FP16 gradient storage (scale 8).
 * adam(): beta1 0.9, beta2 0.99, eps 1e-8, bias-corrected.
 * sample(): vMF mixture sampling by the inversion of Jakob (2012).
 
@@ -85,7 +85,7 @@ def encode(q, bmin, bmax):
     u = u.astype(np.float64)
     for a in range(3):
         for k in range(12):
-            x = u[:, a] * 2.0 ** k
+            x = (u[:, a].astype(np.float32) * np.float32(2.0 ** (k / 2))).astype(np.float64)
             e[:, a * 24 + 2 * k] = np.sin(np.pi * x)
             e[:, a * 24 + 2 * k + 1] = np.cos(np.pi * x)
     th = np.arccos(np.clip(q[:, 8], -1, 1)) / np.pi
@@ -161,15 +161,16 @@ def _lobe_terms(o, wi):
                 lam=np.exp(lg - lse_l))
 
 
-def loss_value(out, wi, pdfb, wt, V_fixed=None):
-    """Per-row loss -wt (log V + log(alpha V' + (1 - alpha) pdf_bsdf)), V' = V_fixed if given
-    (the second term trains alpha only, so its V is a constant)."""
+def loss_value(out, wi, pdfb, wt, V_fixed=None, q_fixed=None):
+    """Per-row loss -wt log V + wt^2 qc / q, q = alpha Vc + (1 - alpha) pdf_bsdf, with Vc, qc
+    the given constants (defaults: V and q at `out`); the second term trains alpha only."""
     o = np.asarray(out, dtype=np.float64)
     t = _lobe_terms(o, np.asarray(wi, dtype=np.float64))
     V = np.exp(t["logV"]) if V_fixed is None else V_fixed
     alpha = ALPHA_MIN + ALPHA_SPAN * _sig(o[:, 32])
     q = np.maximum(alpha * V + (1 - alpha) * pdfb, 1e-30)
-    return -wt * (t["logV"] + np.log(q))
+    qc = q if q_fixed is None else q_fixed
+    return -wt * t["logV"] + wt * wt * qc / q
 
 
 def loss_grad_out(out, wi, pdfb, wt, clamp=True):
@@ -182,7 +183,7 @@ def loss_grad_out(out, wi, pdfb, wt, clamp=True):
     sa = _sig(o[:, 32])
     alpha = ALPHA_MIN + ALPHA_SPAN * sa
     q = np.maximum(alpha * V + (1 - alpha) * pdfb, 1e-30)
-    loss = -wt * (t["logV"] + np.log(q))
+    loss = -wt * t["logV"] + wt * wt
     rr = np.exp(t["ls"] - t["logV"][:, None])
     k, c, st, ct, sp, cp = t["k"], t["c"], t["st"], t["ct"], t["sp"], t["cp"]
     dth = rr * k * (ct * cp * wi[:, 0:1] + ct * sp * wi[:, 1:2] - st * wi[:, 2:3]) * np.pi * t["sth"] * (1 - t["sth"])
@@ -197,7 +198,7 @@ def loss_grad_out(out, wi, pdfb, wt, clamp=True):
     g[:, 1:32:4] = -wt[:, None] * dph
     g[:, 2:32:4] = -wt[:, None] * dk
     g[:, 3:32:4] = -wt[:, None] * dl
-    g[:, 32] = -wt * (V - pdfb) / q * ALPHA_SPAN * sa * (1 - sa)
+    g[:, 32] = -wt * wt * (V - pdfb) / q * ALPHA_SPAN * sa * (1 - sa)
     if clamp:
         g = np.clip(g, -GRAD_CLAMP, GRAD_CLAMP)
     return loss, g
@@ -217,8 +218,11 @@ def loss_fixed(params, q, dirs, pdfb, w, bmin, bmax, params_V):
     _, out = forward(params, X, fp16=False)
     _, outV = forward(params_V, X, fp16=False)
     V = np.exp(_lobe_terms(outV, np.asarray(dirs, dtype=np.float64))["logV"])
+    pdfb = np.asarray(pdfb, dtype=np.float64)
+    aV = ALPHA_MIN + ALPHA_SPAN * _sig(outV[:, 32])
+    qc = np.maximum(aV * V + (1 - aV) * pdfb, 1e-30)
     wt = train_weights(w)
-    return float(loss_value(out, dirs, np.asarray(pdfb, dtype=np.float64), wt, V_fixed=V).mean())
+    return float(loss_value(out, dirs, pdfb, wt, V_fixed=V, q_fixed=qc).mean())
 
 
 def loss_and_grad(params, q, dirs, pdfb, w, bmin, bmax, fp16=True):

@@ -559,7 +559,9 @@ static v3 trace_sample(const ctx_t *c, uint32_t pix, uint32_t j)
         beta = vmul(beta, f);
         int finished = black(f);
         if (!finished && scat && depth > c->rr_depth) {
-            float q = fmaxf(0.05f, 1.f - lum(beta));
+            /* the reference's brightness (luminance) in compat mode; the largest component
+             * otherwise, so no channel's throughput grows past 1 by surviving */
+            float q = fmaxf(0.05f, 1.f - (compat ? lum(beta) : fmaxf(beta.x, fmaxf(beta.y, beta.z))));
             if (pcg_f(&r) < q)
                 finished = 1;
             else

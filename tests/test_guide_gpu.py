@@ -251,17 +251,20 @@ def test_trained_guide_lowers_error(core, gpu_ctx):
     estimator's error against a converged render is lower than BSDF sampling's at equal spp."""
     import torch
 
-    sc, cam, cfg = C.build_config2(gpu_ctx, 128, 72, target_triangles=20000)
+    sc, cam, cfg = C.build_config2(gpu_ctx, 256, 144)
     flags = N.RT_RENDER_NEE_AREA
-    ref, _ = sc.render(cam, spp=1024, max_depth=16, seed=9, flags=flags, fp64=True)
-    g = core.Guide(gpu_ctx, [-2.01, -0.01, -2.01], [2.01, 2.51, 2.01], seed=2)
-    GD.render_progressive(sc, cam, g, [4] * 8, max_depth=16, seed=300, flags=flags, train_passes=8,
-                          steps_per_pass=8, batch=1 << 15)
+    ref = None
+    for k in range(4):
+        ref, _ = sc.render(cam, spp=512, max_depth=16, seed=9, flags=flags, fp64=True, film=ref, sample_offset=512 * k)
+    T = C.GUIDE_TRAINING
+    g = core.Guide(gpu_ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=2)
+    GD.render_progressive(sc, cam, g, [1] * 24, max_depth=16, seed=300, flags=flags, train_passes=24,
+                          steps_per_pass=32, batch=1 << 16)
     errs_g, errs_p = [], []
-    for k in range(3):
+    for k in range(4):
         sc.set_guide(g, train=False)
-        fg, _ = sc.render(cam, spp=32, max_depth=16, seed=500 + k, flags=flags | N.RT_RENDER_GUIDE)
-        fp, _ = sc.render(cam, spp=32, max_depth=16, seed=600 + k, flags=flags)
+        fg, _ = sc.render(cam, spp=64, max_depth=16, seed=500 + k, flags=flags | N.RT_RENDER_GUIDE)
+        fp, _ = sc.render(cam, spp=64, max_depth=16, seed=600 + k, flags=flags)
         errs_g.append(core.rmse(fg, ref))
         errs_p.append(core.rmse(fp, ref))
     assert np.mean(errs_g) < 0.9 * np.mean(errs_p), (errs_g, errs_p)

@@ -101,12 +101,15 @@ def test_output_gradient_finite_differences():
     wt = w / w.mean()
     _, g = G.loss_grad_out(out, wi, pdfb, wt, clamp=False)
     V0 = np.exp(G._lobe_terms(out, wi)["logV"])
+    a0 = G.ALPHA_MIN + G.ALPHA_SPAN / (1 + np.exp(-out[:, 32]))
+    q0 = a0 * V0 + (1 - a0) * pdfb
     h = 1e-6
     for j in list(range(33)):
         o1, o2 = out.copy(), out.copy()
         o1[:, j] += h
         o2[:, j] -= h
-        fd = (G.loss_value(o1, wi, pdfb, wt, V_fixed=V0) - G.loss_value(o2, wi, pdfb, wt, V_fixed=V0)) / (2 * h)
+        fd = (G.loss_value(o1, wi, pdfb, wt, V_fixed=V0, q_fixed=q0) -
+              G.loss_value(o2, wi, pdfb, wt, V_fixed=V0, q_fixed=q0)) / (2 * h)
         assert np.allclose(g[:, j], fd, rtol=1e-5, atol=1e-7), j
     assert np.all(g[:, 33:] == 0)
 
