@@ -82,7 +82,7 @@ PHOTON_DTYPE = np.dtype([("pos", "<f4", 3), ("shape_id", "<i4"), ("dir", "<f4", 
 
 class GuideOpts(ctypes.Structure):
     _fields_ = [("bbox_min", ctypes.c_float * 3), ("bbox_max", ctypes.c_float * 3), ("learning_rate", ctypes.c_float),
-                ("seed", ctypes.c_uint32), ("record_capacity", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("seed", ctypes.c_uint32), ("record_capacity", ctypes.c_uint32), ("max_depth", ctypes.c_uint32)]
 
 
 GUIDE_INPUTS = 144
@@ -139,6 +139,7 @@ SIGNATURES = {
     "rt_guide_params_get": [_P, _P, _U64],
     "rt_guide_params_set": [_P, _P, _U64],
     "rt_guide_steps": [_P, ctypes.POINTER(_U64)],
+    "rt_guide_reset": [_P],
     "rt_guide_eval": [_P, _P, _U64, _P],
     "rt_guide_pdf": [_P, _P, _P, _P, _U64, _P],
     "rt_guide_sample": [_P, _P, _P, _U64, _P, _P],

@@ -314,7 +314,7 @@ class Guide:
     """Learned path guide (vMF-mixture MLP): evaluation, training, parameters (device buffers)."""
 
     def __init__(self, ctx: Context, bbox_min, bbox_max, learning_rate: float = 1e-2, seed: int = 0,
-                 record_capacity: int = 0):
+                 record_capacity: int = 0, max_depth: int = 0):
         o = N.GuideOpts()
         for a in range(3):
             o.bbox_min[a] = float(bbox_min[a])
@@ -322,6 +322,7 @@ class Guide:
         o.learning_rate = learning_rate
         o.seed = seed
         o.record_capacity = record_capacity
+        o.max_depth = max_depth
         h = ctypes.c_void_p()
         N.check(N.lib().rt_guide_create(ctx.handle, ctypes.byref(o), ctypes.byref(h)))
         self.handle = h
@@ -338,6 +339,10 @@ class Guide:
         n = ctypes.c_uint64()
         N.check(N.lib().rt_guide_steps(self.handle, ctypes.byref(n)))
         return n.value
+
+    def reset(self):
+        """Seeded initial weights again, Adam state cleared, untrained (device buffers kept)."""
+        N.check(N.lib().rt_guide_reset(self.handle))
 
     def params(self) -> np.ndarray:
         out = np.zeros(self.param_count, dtype=np.float32)

@@ -546,6 +546,8 @@ int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf,
 
 using namespace rtb;
 
+static int guide_init_params(rt_guide *g);
+
 extern "C" {
 
 int rt_guide_create(rt_context *ctx, const rt_guide_opts *opts, rt_guide **out)
@@ -562,9 +564,29 @@ int rt_guide_create(rt_context *ctx, const rt_guide_opts *opts, rt_guide **out)
     g->ctx = ctx;
     g->opts = *opts;
     g->rec_cap = opts->record_capacity ? opts->record_capacity : kRecNone - 1;
-    // He-uniform hidden layers, Glorot-uniform output layer, zero biases (seeded PCG32)
+    int s = guide_init_params(g);
+    if (s != RT_OK) {
+        delete g;
+        return s;
+    }
+    *out = g;
+    return RT_OK;
+}
+
+int rt_guide_reset(rt_guide *g)
+{
+    if (!g) return fail(RT_ERR_INVALID, "rt_guide_reset: null guide");
+    RTB_CUDA(cudaSetDevice(g->ctx->device));
+    return guide_init_params(g);
+}
+
+}  // extern "C"
+
+// He-uniform hidden layers, Glorot-uniform output layer, zero biases (seeded PCG32)
+static int guide_init_params(rt_guide *g)
+{
     std::vector<float> p(kGuideParamCount, 0.f);
-    uint64_t state = 0x853c49e6748fea9bull ^ ((uint64_t)opts->seed << 1);
+    uint64_t state = 0x853c49e6748fea9bull ^ ((uint64_t)g->opts.seed << 1);
     auto next = [&]() {
         const uint64_t old = state;
         state = old * 6364136223846793005ull + 1442695040888963407ull;
@@ -577,14 +599,12 @@ int rt_guide_create(rt_context *ctx, const rt_guide_opts *opts, rt_guide **out)
         const float a = l == kGuideLayers - 1 ? std::sqrt(6.f / (float)(in + o)) : std::sqrt(6.f / (float)in);
         for (int i = 0; i < in * o; i++) p[guide_pw(l) + i] = (2.f * next() - 1.f) * a;
     }
-    int s = guide_upload_params(g, p.data());
-    if (s != RT_OK) {
-        delete g;
-        return s;
-    }
-    *out = g;
+    RTB_CHECK(guide_upload_params(g, p.data()));
+    g->trained = false;
     return RT_OK;
 }
+
+extern "C" {
 
 int rt_guide_destroy(rt_guide *g)
 {

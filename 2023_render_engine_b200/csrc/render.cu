@@ -70,6 +70,7 @@ struct GuideView {
     uint32_t *nz;          // records with nonzero weight
     uint32_t *retire_rec;  // newest record of each retiring path
     uint32_t rec_cap;
+    uint32_t max_depth;  // vertices at this path depth or deeper sample the BSDF only
     int enabled, train;
 };
 
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
                 e.z += beta_in.z * Le.z * w;
             }
         }
-        const bool guided = gv.enabled && guide_vertex(bs, wo.z);
+        const bool guided = gv.enabled && depth < gv.max_depth && guide_vertex(bs, wo.z);
         const uint32_t rec_in = rec;  // this vertex's NEE belongs to the previous record
         float alpha = 0.f;
         const GuideParams *gp = nullptr;
@@ -536,14 +537,14 @@ __global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t 
 // Guide network at the wave's hits (queue slots of buffer `cur`); writes the decoded mixture
 // per slot, alpha = 0 where the vertex is not guided.
 __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(RenderView rv, Buffers bf, int cur, const uint4 *img,
-                                                                   GuideBox box, GuideParams *params)
+                                                                   GuideBox box, GuideParams *params, uint32_t max_depth)
 {
     const uint32_t n = min(bf.cnt[cur], bf.cap);
     const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
     auto src = [&](uint32_t q, float *out) -> bool {
         const float4 hv = reinterpret_cast<const float4 *>(bf.hits)[q];
         const rt_hit h{hv.x, __float_as_int(hv.y), hv.z, hv.w};
-        if (h.prim < 0) return false;
+        if (h.prim < 0 || (bf.st2[cur][q].w & kDepthMask) >= max_depth) return false;
         const float4 r0 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q];
         const float4 r1 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q + 1];
         const V3 d = v3(r1.x, r1.y, r1.z);
@@ -783,6 +784,7 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
         if (photon_mode) return fail(RT_ERR_UNSUPPORTED, "rt_render: RT_RENDER_GUIDE with RT_RENDER_PHOTON_MAP");
         gv.enabled = 1;
         gv.train = s->guide_train;
+        gv.max_depth = guide->opts.max_depth ? guide->opts.max_depth : 0xFFFFFFFFu;
         if (guide->trained) {
             RTB_CHECK(guide->params.reserve(sizeof(GuideParams) * (uint64_t)cap));
             gv.params = guide->params.as<GuideParams>();
@@ -875,7 +877,7 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
                                                st));
             if (gv.params) {
                 k_guide_infer<<<infer_blocks, kInferWarps * 32, kInferSmem, st>>>(
-                    rv, bf, cur, guide->img.as<uint4>(), gbox, guide->params.as<GuideParams>());
+                    rv, bf, cur, guide->img.as<uint4>(), gbox, guide->params.as<GuideParams>(), gv.max_depth);
                 RTB_CUDA(cudaGetLastError());
             }
             RTB_CUDA(cudaMemsetAsync(bf.cnt + ((cur ^ 1)), 0, 4, st));

@@ -202,15 +202,15 @@ def measure_guiding(args, core, N, cfgs, ctx, torch):
     torch.cuda.synchronize()
     ref_s = time.perf_counter() - t0
     ref_mean = (ref["sum64"].view(-1, 3) / ref["count"].double().clamp_min(1).view(-1, 1))
-    # warm the kernels and allocations of both paths once (not timed)
+    # warm the kernels and the guide's device buffers once (not timed), then reset the guide
     T = cfgs.GUIDE_TRAINING
-    g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=11)
+    g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=2,
+                   max_depth=T["max_depth"])
     GD.render_progressive(sc, cam, g, [1, 1], max_depth=p["max_depth"], seed=7, flags=flags, train_passes=1,
                           steps_per_pass=1, batch=args.guide_batch)
-    g.close()
+    g.reset()
     plain = GD.time_to_rmse(sc, cam, ref_mean, args.guide_target, None, pass_spp=4, max_depth=p["max_depth"],
                             rr_depth=p["rr_depth"], seed=1, flags=flags)
-    g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=2)
     guided = GD.time_to_rmse(sc, cam, ref_mean, args.guide_target, g, pass_spp=4, max_depth=p["max_depth"],
                              rr_depth=p["rr_depth"], seed=2, flags=flags, train_passes=args.guide_train_passes,
                              steps_per_pass=args.guide_steps, batch=args.guide_batch)
@@ -225,7 +225,7 @@ def measure_guiding(args, core, N, cfgs, ctx, torch):
         "guided": {k: guided[k] for k in ("seconds", "spp", "rmse", "reached")},
         "speedup": (plain["seconds"] / guided["seconds"]) if guided["reached"] and plain["reached"] else None,
         "training": {"passes": args.guide_train_passes, "steps": steps, "batch": args.guide_batch,
-                     "learning_rate": T["learning_rate"]},
+                     "learning_rate": T["learning_rate"], "guided_depths": T["max_depth"]},
         "curves": {"plain": plain["curve"][::4], "guided": guided["curve"][::4]},
     }
 
@@ -395,8 +395,8 @@ def main():
     ap.add_argument("--guide-target", type=float, default=0.01)
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)
-    ap.add_argument("--guide-train-passes", type=int, default=24)
-    ap.add_argument("--guide-steps", type=int, default=32)
+    ap.add_argument("--guide-train-passes", type=int, default=4)
+    ap.add_argument("--guide-steps", type=int, default=64)
     ap.add_argument("--guide-batch", type=int, default=1 << 16)
     args = ap.parse_args()
     global NRAYS

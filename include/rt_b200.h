@@ -331,7 +331,7 @@ typedef struct rt_guide_opts {
     float learning_rate;            /* Adam step size; 1e-2 in the guiding configuration */
     uint32_t seed;                  /* weight initialisation */
     uint32_t record_capacity;       /* training records kept per render (0: 4,194,302, the maximum) */
-    uint32_t reserved;
+    uint32_t max_depth;             /* vertices at path depth >= max_depth sample the BSDF only (0: no limit) */
 } rt_guide_opts;
 
 #define RT_GUIDE_INPUTS 144
@@ -347,6 +347,9 @@ RT_API int rt_guide_param_count(rt_guide *g, uint64_t *n);
 RT_API int rt_guide_params_get(rt_guide *g, float *host, uint64_t n);
 RT_API int rt_guide_params_set(rt_guide *g, const float *host, uint64_t n);
 RT_API int rt_guide_steps(rt_guide *g, uint64_t *steps); /* Adam steps taken */
+/* Back to the freshly created state (seeded weights, zero Adam moments, untrained: renders
+ * sample the BSDF until the next training step); device buffers are kept. */
+RT_API int rt_guide_reset(rt_guide *g);
 
 /* Raw network outputs for B shading points (device buffers): queries are 9 floats each
  * (position, shading normal, outgoing direction), out is B*48 floats. */
