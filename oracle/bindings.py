@@ -373,3 +373,32 @@ class RefRender:
         if rc != 0:
             raise RuntimeError("reference render failed")
         return out, c2w.reshape(4, 4), r2c.reshape(4, 4)
+
+
+class RefCompat:
+    """The reference's own scene objects (Plane shapes, Lambertian materials, its .obejota
+    camera and point lights) rendered by this repository's core through
+    include/rt_b200_compat.hpp (oracle/_ref/libref_compat.so)."""
+
+    def __init__(self, path=HERE / "_ref" / "libref_compat.so"):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+        L = ctypes.CDLL(str(path))
+        L.refc_config.argtypes = [P, P, P, P]
+        L.refc_render.argtypes = [ctypes.c_char_p, I, P, P, ctypes.c_uint32, P]
+        L.refc_render.restype = I
+        L.refc_error.restype = ctypes.c_char_p
+        self.L = L
+        w, h, s, d = (ctypes.c_int() for _ in range(4))
+        L.refc_config(ctypes.byref(w), ctypes.byref(h), ctypes.byref(s), ctypes.byref(d))
+        self.width, self.height, self.spp, self.depth = w.value, h.value, s.value, d.value
+
+    def render(self, obejota_path, planes, kd, seed):
+        pl = _np(planes, np.float32).reshape(-1, 12)
+        k = _np(kd, np.float32).reshape(-1, 3)
+        out = np.zeros((self.width * self.height, 3), np.float32)
+        rc = self.L.refc_render(str(obejota_path).encode(), pl.shape[0], pl.ctypes.data, k.ctypes.data, seed,
+                                out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("compat render failed: " + self.L.refc_error().decode())
+        return out

@@ -1,0 +1,144 @@
+// Test infrastructure only: the reference's own scene objects — Plane shapes, Lambertian
+// materials, and the camera, film and point lights read by its .obejota loader
+// (cuda_libraries/FileImporting.cu:466) — rendered by this repository's GPU core through
+// include/rt_b200_compat.hpp, the drop-in for Scene::build and PathTracerIntegrator::render
+// (integration/Scene.cu:56-95, integration/PathTracerIntegrator.cu:140-210). The scene setup
+// mirrors ref_render_harness.cu, which renders the same objects with the reference's own
+// integrator; the image-parity test compares the two.
+#include <thrust/device_vector.h>
+#include <thrust/host_vector.h>
+#include <thrust/sort.h>
+#include <thrust/transform.h>
+#include <thrust/sequence.h>
+#include <thrust/random.h>
+#include <thrust/functional.h>
+#include <iostream>
+#include <vector>
+#include <random>
+#include <string>
+#include <fstream>
+#include <thread>
+#include <atomic>
+#include <mutex>
+#include <cmath>
+#include <algorithm>
+#include <unordered_map>
+#include <sstream>
+#include <queue>
+#include <memory>
+#include <functional>
+#include <filesystem>
+#include <chrono>
+#include <bit>
+#include <array>
+#include <tuple>
+#include <utility>
+#include <cstdint>
+#include <curand_kernel.h>
+#include <math_constants.h>
+
+// See ref_harness.cu: the reference's global template swap is renamed.
+#define swap ref_swap_
+#include "cuda_libraries/types.h"
+
+#undef resolutionX
+#undef resolutionY
+#undef SAMPLES_PER_PIXEL
+#undef MAX_RAY_RECURSION_DEPTH
+#undef CHECK_SUBSURFACE_SCATTERING
+#undef RENDER_MODE
+#define resolutionX 48
+#define resolutionY 48
+#define SAMPLES_PER_PIXEL 32
+#define MAX_RAY_RECURSION_DEPTH 8
+#define CHECK_SUBSURFACE_SCATTERING false
+#define RENDER_MODE PATH_TRACING
+
+#include "shapes/Sphere.cu"
+#include "shapes/Plane.cu"
+#include "shapes/Triangle.cu"
+#include "integration/Scene.cu"
+#include "integration/PathTracerIntegrator.cu"
+#include "integration/photonDispersion.cu"
+#include "camera/ProjectiveCamera.cu"
+#include "sampling/Sampler.cu"
+#include "light/PointLight.cu"
+#include "materials/LambertianMaterial.cu"
+#include "materials/LightMaterial.cu"
+#include "materials/GlassMaterial.cu"
+#include "materials/MirrorMaterial.cu"
+#include "materials/SSMaterial.cu"
+#include "materials/PlasticUnrealMaterial.cu"
+#include "materials/PlainMaterial.cu"
+#include "textures/Texture.cu"
+#include "textures/SphericalTexture.cu"
+#include "cuda_libraries/FileImporting.cu"
+#undef swap
+
+#include "../include/rt_b200_compat.hpp"
+
+#define REFC_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+struct FilmPeek : public Film {
+    using Film::pixelLight;
+};
+thread_local std::string g_error;
+}  // namespace
+
+REFC_API int refc_config(int *w, int *h, int *spp, int *depth)
+{
+    *w = resolutionX;
+    *h = resolutionY;
+    *spp = SAMPLES_PER_PIXEL;
+    *depth = MAX_RAY_RECURSION_DEPTH;
+    return 0;
+}
+
+REFC_API const char *refc_error() { return g_error.c_str(); }
+
+// planes: 12 floats each, Plane(corner, axisX, axisY, normal); kd: 3 floats each. out_mean:
+// the film's per-pixel sum / spp after rtb::PathTracerIntegrator::render. Returns 0, or 1
+// with refc_error() set.
+REFC_API int refc_render(const char *obejota, int nplanes, const float *planes, const float *kd, uint32_t seed,
+                         float *out_mean)
+{
+    std::vector<Plane *> pl;
+    std::vector<LambertianMaterial *> mats;
+    std::vector<Shape *> shapes;
+    int rc = 0;
+    try {
+        for (int i = 0; i < nplanes; i++) {
+            const float *p = planes + 12 * i;
+            Plane *s = new Plane(Point3f(p[0], p[1], p[2]), Vector3f(p[3], p[4], p[5]), Vector3f(p[6], p[7], p[8]),
+                                 Vector3f(p[9], p[10], p[11]));
+            LambertianMaterial *m = new LambertianMaterial(Spectrum(kd[3 * i], kd[3 * i + 1], kd[3 * i + 2]));
+            s->setMaterial(m);
+            pl.push_back(s);
+            mats.push_back(m);
+            shapes.push_back(s);
+        }
+        std::vector<Light *> lights;
+        Camera *camera = nullptr;
+        loadObejota(obejota, lights, shapes, camera);
+        if (!camera) throw std::runtime_error("no camera in the scene file");
+        std::shared_ptr<std::vector<TriangleMesh>> meshes = std::make_shared<std::vector<TriangleMesh>>();
+        std::vector<std::vector<Triangle>> triangles;
+        rtb::Scene scene(0);
+        scene.build(shapes, lights, triangles, meshes);  // was: Scene::build
+        rtb::PathTracerIntegrator integrator(camera, RT_RENDER_COMPAT, seed);
+        integrator.render(&scene);                        // was: PathTracerIntegrator::render
+        FilmPeek *film = static_cast<FilmPeek *>(camera->getFilm());
+        for (int i = 0; i < resolutionX * resolutionY; i++) {
+            out_mean[3 * i + 0] = (float)(film->pixelLight[i].getR() / SAMPLES_PER_PIXEL);
+            out_mean[3 * i + 1] = (float)(film->pixelLight[i].getG() / SAMPLES_PER_PIXEL);
+            out_mean[3 * i + 2] = (float)(film->pixelLight[i].getB() / SAMPLES_PER_PIXEL);
+        }
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        rc = 1;
+    }
+    for (auto *s : pl) delete s;
+    for (auto *m : mats) delete m;
+    return rc;
+}

@@ -91,3 +91,30 @@ def test_statistical_parity_with_reference_integrator(core, gpu_ctx, tmp_path):
     assert abs(zs.mean()) < 0.25
     rel = abs(M.mean() - R.mean()) / R.mean()
     assert rel < 0.01
+
+
+def test_compat_layer_is_a_drop_in_for_the_reference_integrator(tmp_path):
+    """The same reference objects (its Plane, LambertianMaterial, loadObejota camera, film and
+    point light) through include/rt_b200_compat.hpp — rtb::Scene::build and
+    rtb::PathTracerIntegrator::render in place of the reference's — give the reference
+    integrator's image (per-tile z-test as above), written into the reference's own Film."""
+    from oracle import bindings
+
+    try:
+        ref = bindings.RefRender()
+        comp = bindings.RefCompat()
+    except FileNotFoundError as e:
+        pytest.skip(str(e))
+    path = tmp_path / "box.obejota"
+    path.write_text(OBEJOTA)
+    runs = 8
+    R = np.stack([tiles(ref.render(path, PLANES, KD)[0], ref.width, ref.height) for _ in range(runs)])
+    M = np.stack([tiles(comp.render(path, PLANES, KD, 700 + r), comp.width, comp.height) for r in range(runs)])
+    assert (comp.width, comp.height, comp.spp, comp.depth) == (ref.width, ref.height, ref.spp, ref.depth)
+    se = np.sqrt(R.var(axis=0, ddof=1) / runs + M.var(axis=0, ddof=1) / runs)
+    z = (M.mean(0) - R.mean(0)) / np.maximum(se, 1e-12)
+    zs = z[se > 0]
+    assert np.abs(zs).mean() < 1.2
+    assert (np.abs(zs) > 4).mean() < 0.01
+    assert abs(zs.mean()) < 0.25
+    assert abs(M.mean() - R.mean()) / R.mean() < 0.01
