@@ -158,7 +158,7 @@ class Scene:
         st = N.PhotonTraceStats()
         N.check(N.lib().rt_photons_trace(self.handle, n, max_depth, rr_depth, seed, flags, ctypes.byref(h),
                                          ctypes.byref(st)))
-        return PhotonMap(h), {f: getattr(st, f) for f, _ in N.PhotonTraceStats._fields_}
+        return PhotonMap(h, owner=self), {f: getattr(st, f) for f, _ in N.PhotonTraceStats._fields_}
 
     def close(self):
         if self.handle:
@@ -235,8 +235,9 @@ def film_mean(film) -> np.ndarray:
 class PhotonMap:
     """Photon map handle: photons, kd-tree build, k-nearest gather (device buffers)."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, owner=None):
         self.handle = handle
+        self.owner = owner  # keeps the context (or the scene holding it) alive
 
     @classmethod
     def from_points(cls, ctx: Context, pos_dev, shape_dev=None):
@@ -245,7 +246,7 @@ class PhotonMap:
         N.check(N.lib().rt_photon_map_from_points(ctx.handle, pos_dev.data_ptr(),
                                                   None if shape_dev is None else shape_dev.data_ptr(), n,
                                                   ctypes.byref(h)))
-        return cls(h)
+        return cls(h, owner=ctx)
 
     def build(self):
         N.check(N.lib().rt_photon_map_build(self.handle))
@@ -327,6 +328,7 @@ class Guide:
         N.check(N.lib().rt_guide_create(ctx.handle, ctypes.byref(o), ctypes.byref(h)))
         self.handle = h
         self.opts = o
+        self.ctx = ctx  # the context must outlive the guide
 
     @property
     def param_count(self) -> int:

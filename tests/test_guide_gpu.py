@@ -249,24 +249,24 @@ def test_guided_estimator_unbiased(core, gpu_ctx, nee):
 def test_trained_guide_lowers_error(core, gpu_ctx):
     """Light through a gap in a wall (mostly indirect): after online training, the guided
     estimator's error against a converged render is lower than BSDF sampling's at equal spp."""
-    import torch
-
-    sc, cam, cfg = C.build_config2(gpu_ctx, 256, 144)
+    sc, cam, cfg = C.build_config2(gpu_ctx, 512, 288)
     flags = N.RT_RENDER_NEE_AREA
     ref = None
-    for k in range(4):
-        ref, _ = sc.render(cam, spp=512, max_depth=16, seed=9, flags=flags, fp64=True, film=ref, sample_offset=512 * k)
+    for k in range(8):
+        ref, _ = sc.render(cam, spp=256, max_depth=16, seed=9, flags=flags, fp64=True, film=ref, sample_offset=256 * k)
     T = C.GUIDE_TRAINING
     g = core.Guide(gpu_ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=2)
-    GD.render_progressive(sc, cam, g, [1] * 24, max_depth=16, seed=300, flags=flags, train_passes=24,
-                          steps_per_pass=32, batch=1 << 16)
-    errs_g, errs_p = [], []
-    for k in range(4):
-        sc.set_guide(g, train=False)
-        fg, _ = sc.render(cam, spp=64, max_depth=16, seed=500 + k, flags=flags | N.RT_RENDER_GUIDE)
-        fp, _ = sc.render(cam, spp=64, max_depth=16, seed=600 + k, flags=flags)
-        errs_g.append(core.rmse(fg, ref))
-        errs_p.append(core.rmse(fp, ref))
-    assert np.mean(errs_g) < 0.9 * np.mean(errs_p), (errs_g, errs_p)
-    g.close()
-    del torch
+    try:
+        GD.render_progressive(sc, cam, g, [1] * 8, max_depth=16, seed=300, flags=flags, train_passes=8,
+                              steps_per_pass=32, batch=1 << 16)
+        errs_g, errs_p = [], []
+        for k in range(6):
+            sc.set_guide(g, train=False)
+            fg, _ = sc.render(cam, spp=64, max_depth=16, seed=500 + k, flags=flags | N.RT_RENDER_GUIDE)
+            fp, _ = sc.render(cam, spp=64, max_depth=16, seed=600 + k, flags=flags)
+            errs_g.append(core.rmse(fg, ref))
+            errs_p.append(core.rmse(fp, ref))
+        assert np.mean(errs_g) < 0.92 * np.mean(errs_p), (errs_g, errs_p)
+    finally:
+        sc.set_guide(None)
+        g.close()
