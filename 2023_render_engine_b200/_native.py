@@ -12,7 +12,8 @@ from pathlib import Path
 import numpy as np
 
 _HERE = Path(__file__).resolve().parent
-LIB_PATH = _HERE / "lib" / "librt_b200.so"
+# RT_B200_LIB overrides the library path (A/B comparisons of builds)
+LIB_PATH = Path(os.environ["RT_B200_LIB"]) if os.environ.get("RT_B200_LIB") else _HERE / "lib" / "librt_b200.so"
 
 RT_OK = 0
 RT_TRACE_SHADOW = 0x1

@@ -182,7 +182,13 @@ struct PhotonView {
     float radius;
 };
 
-__global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur, GuideView gv)
+// Resident blocks per SM k_shade is compiled for: more resident warps hide its scattered
+// loads better than the spills they cost. BVH-stress render, Mrays/s: 1465 / 1494 / 1507 for
+// 4 (127 registers, no bound) / 5 (96) / 6 (80).
+#ifndef RTB_SHADE_MIN_BLOCKS
+#define RTB_SHADE_MIN_BLOCKS 6
+#endif
+__global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView rv, Buffers bf, int cur, GuideView gv)
 {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = min(bf.cnt[cur], bf.cap);
@@ -423,7 +429,7 @@ __global__ void __launch_bounds__(kB) k_shade(RenderView rv, Buffers bf, int cur
 
 // Any-hit test of the wave's shadow rays (persistent warps, counter cnt[5]); an unoccluded
 // ray adds its contribution to the path it belongs to.
-__global__ void __launch_bounds__(kB) k_shadow(RenderView rv, Buffers bf, int nxt, GuideView gv)
+__global__ void __launch_bounds__(kB, RTB_TRAV_MIN_BLOCKS) k_shadow(RenderView rv, Buffers bf, int nxt, GuideView gv)
 {
     const uint32_t n = min(bf.cnt[2], bf.scap);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(cnt64(bf.cnt, 12), (unsigned long long)n);  // stats

@@ -71,7 +71,7 @@ __device__ __forceinline__ void closest_epilogue(const SceneView &v, uint64_t i,
 }
 
 // Persistent closest-hit kernel: warps fetch rays from counters[3] until all n are done.
-__global__ void __launch_bounds__(kBlock) k_trace_closest(SceneView v, const rt_ray *__restrict__ rays, uint64_t n,
+__global__ void __launch_bounds__(kBlock, RTB_TRAV_MIN_BLOCKS) k_trace_closest(SceneView v, const rt_ray *__restrict__ rays, uint64_t n,
                                                           const uint32_t *__restrict__ n_dev, rt_hit *__restrict__ hits,
                                                           uint32_t flags, uint32_t *__restrict__ queue,
                                                           uint32_t queue_cap, uint32_t *__restrict__ counters)
