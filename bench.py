@@ -187,6 +187,31 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def measure_reference_cuda(v, f, o, d, hits_d, N):
+    """The reference's BVH::intersectRay on the GPU (its thrust::transform path, built with its
+    own compile flags) over the same 2^24 rays: Mrays/s with the rays resident on the device,
+    Mrays/s of its per-call path with host copies, and id agreement with ours."""
+    try:
+        from oracle import bindings
+
+        rc = bindings.RefCuda()
+    except (FileNotFoundError, OSError) as e:
+        return {"unavailable": str(e)}
+    h = rc.build(v, f)
+    try:
+        ids, mk, ma = rc.trace(h, o, d, reps=3)
+    finally:
+        rc.free(h)
+    ours = hits_d.cpu().numpy().view(N.HIT_DTYPE)["prim"]
+    n = len(ids)
+    return {"value": n / (mk / 1000) / 1e6, "unit": "Mrays/s", "ms_per_call": mk,
+            "api_value": n / (ma / 1000) / 1e6, "api_ms_per_call": ma,
+            "id_agreement": float((ids == ours).mean()),
+            "build": "reference BVH::intersectRay + Triangle::intersects via thrust::transform, -O3 --use_fast_math "
+                     "-maxrregcount=64 (its compile.sh), sm_100a; api = its intersectRaysGpu path (rays to the "
+                     "device, transform, ids back, pageable host memory)"}
+
+
 def measure_guiding(args, core, N, cfgs, ctx, torch):
     """Time to RMSE <= args.guide_target on the guiding room (1280x720, max depth 16, area NEE):
     plain BSDF sampling vs the online-trained guide, against a converged FP64 render."""
@@ -332,6 +357,11 @@ def run_ours(args):
     if world == 1 and args.guide_ref_spp > 0:
         guiding = measure_guiding(args, core, N, cfgs, ctx, torch)
 
+    # ---- the reference's own CUDA traversal on the same rays (baseline, not a target)
+    ref_cuda = None
+    if world == 1 and not args.no_ref_cuda:
+        ref_cuda = measure_reference_cuda(v, f, o, d, hits_d, N)
+
     ms, ms_e2e, ms_trace = max_over_ranks([ms, ms_e2e, ms_trace], world)
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -365,6 +395,7 @@ def run_ours(args):
                          "note": f"peak {peak_kind}; traversal reads nodes/triangles from L2, see profiles/"},
             "clocks": clk.summary(),
             "guiding": guiding,
+            "reference_cuda": ref_cuda,
         }
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
@@ -392,6 +423,7 @@ def main():
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--guide-ref-spp", type=int, default=4096, help="0 skips the guiding measurement")
+    ap.add_argument("--no-ref-cuda", action="store_true", help="skip the reference CUDA traversal baseline")
     ap.add_argument("--guide-target", type=float, default=0.01)
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)

@@ -402,3 +402,43 @@ class RefCompat:
         if rc != 0:
             raise RuntimeError("compat render failed: " + self.L.refc_error().decode())
         return out
+
+
+class RefCuda:
+    """The reference's own GPU traversal (BVH::intersectRay via thrust::transform) built with
+    the flags of its compile.sh (oracle/_ref/libref_cuda.so): the reference-CUDA baseline."""
+
+    def __init__(self, path=HERE / "_ref" / "libref_cuda.so"):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+        L = ctypes.CDLL(str(path))
+        L.refg_build.argtypes = [P, ctypes.c_uint32, P, ctypes.c_uint32]
+        L.refg_build.restype = P
+        L.refg_free.argtypes = [P]
+        L.refg_trace.argtypes = [P, P, ctypes.c_uint64, ctypes.c_int32, P, P, P]
+        L.refg_trace.restype = I
+        L.refg_error.restype = ctypes.c_char_p
+        self.L = L
+
+    def build(self, verts, idx):
+        v = _np(verts, np.float32).reshape(-1, 3)
+        f = _np(idx, np.uint32).reshape(-1, 3)
+        h = self.L.refg_build(v.ctypes.data, v.shape[0], f.ctypes.data, f.shape[0])
+        if not h:
+            raise RuntimeError("reference GPU BVH build failed: " + self.L.refg_error().decode())
+        return h
+
+    def free(self, h):
+        self.L.refg_free(h)
+
+    def trace(self, h, o, d, reps=3):
+        """Returns (ids, ms per transform with device-resident rays, ms per API-style call)."""
+        od = np.ascontiguousarray(np.concatenate([_np(o, np.float32).reshape(-1, 3), _np(d, np.float32).reshape(-1, 3)],
+                                                 axis=1))
+        n = od.shape[0]
+        ids = np.zeros(n, np.int32)
+        mk, ma = ctypes.c_float(), ctypes.c_float()
+        rc = self.L.refg_trace(h, od.ctypes.data, n, reps, ids.ctypes.data, ctypes.byref(mk), ctypes.byref(ma))
+        if rc != 0:
+            raise RuntimeError("reference GPU trace failed: " + self.L.refg_error().decode())
+        return ids, mk.value, ma.value

@@ -208,3 +208,27 @@ def test_config1_full_ray_set_hash(core, gpu_ctx):
     tt = np.where(ids >= 0, t, -1.0).astype(np.float32)
     assert hashlib.sha256(tt.tobytes()).hexdigest() == info["t_sha256"]
     del torch
+
+
+def test_reference_cuda_build_agrees(core, gpu_ctx):
+    """The reference's own GPU traversal (its thrust path, fast-math build: the baseline in
+    bench.py) returns our reference-exact ids on all but a handful of near-edge rays."""
+    from oracle import bindings
+
+    try:
+        rc = bindings.RefCuda()
+    except FileNotFoundError as e:
+        pytest.skip(str(e))
+    S_ = importlib.import_module("2023_render_engine_b200.scenes")
+    v, f, _ = S_.flatten(S_.stress_scene(subdiv=5))
+    o, d = S_.random_rays(1 << 18, seed=11)
+    h = rc.build(v, f)
+    try:
+        ids, _, _ = rc.trace(h, o, d, reps=1)
+    finally:
+        rc.free(h)
+    sc = core.Scene(gpu_ctx)
+    sc.add_mesh(v, f)
+    sc.commit()
+    hits = sc.trace_closest_host(core.make_rays(o, d))
+    assert (ids == hits["prim"]).mean() > 0.9999
