@@ -58,6 +58,12 @@ class RenderOpts(ctypes.Structure):
                 ("max_paths", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
+class View(ctypes.Structure):
+    _fields_ = [("camera", Camera), ("spp", ctypes.c_uint32), ("sample_offset", ctypes.c_uint32),
+                ("max_depth", ctypes.c_uint32), ("rr_depth", ctypes.c_uint32), ("seed", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 3)]
+
+
 class RenderStats(ctypes.Structure):
     _fields_ = [("camera_rays", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64),
                 ("shadow_rays", ctypes.c_uint64), ("waves", ctypes.c_uint64), ("ms", ctypes.c_double)]
@@ -125,6 +131,7 @@ SIGNATURES = {
     "rt_scene_set_triangle_materials": [_P, _U32, _U32, _P],
     "rt_scene_add_point_light": [_P, _P, _P, _F32],
     "rt_render": [_P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), _P, _P, _P, ctypes.POINTER(RenderStats)],
+    "rt_render_batch": [_P, ctypes.POINTER(View), _U32, _U32, _U32, _P, _P, _P, ctypes.POINTER(RenderStats)],
     "rt_photons_trace": [_P, _U64, _U32, _U32, _U32, _U32, ctypes.POINTER(_P), ctypes.POINTER(PhotonTraceStats)],
     "rt_photon_map_from_points": [_P, _P, _P, _U64, ctypes.POINTER(_P)],
     "rt_photon_map_build": [_P],

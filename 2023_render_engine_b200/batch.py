@@ -1,0 +1,73 @@
+"""Batched multi-view rendering: capacity autotuning and the batched-vs-individual measurement.
+
+One rt_render_batch call renders all views of a scene in one wavefront. The queue capacity
+(paths in flight) is the tunable: larger queues keep more rays per traversal launch, smaller
+ones use less memory and finish the tail sooner. autotune_capacity times a reduced-spp copy
+of the batch at each candidate and keeps the fastest.
+"""
+from __future__ import annotations
+
+import time
+
+from . import _native as N
+
+CAPACITIES = (1 << 23, 1 << 22, 1 << 21, 1 << 20)
+
+
+def _timed(fn, sync):
+    sync()
+    t0 = time.perf_counter()
+    out = fn()
+    sync()
+    return time.perf_counter() - t0, out
+
+
+def autotune_capacity(scene, views, flags, sync, candidates=CAPACITIES, probe_spp=4):
+    """Fastest queue capacity for this batch, timed on a copy with spp capped at probe_spp
+    (each candidate twice; the second run counts, so buffer growth is not timed).
+    Returns (best capacity, [(capacity, seconds)])."""
+    probe = [dict(v, spp=min(v["spp"], probe_spp)) for v in views]
+    trials = []
+    for cap in candidates:
+        for rep in range(2):
+            t, _ = _timed(lambda: scene.render_batch(probe, flags=flags, max_paths=cap), sync)
+        trials.append((cap, t))
+    best = min(trials, key=lambda x: x[1])[0]
+    return best, trials
+
+
+def measure(groups, sync, autotune=True):
+    """Times every scene's views as one batch and as one rt_render call per view.
+
+    groups: [(name, scene, flags, views)]. Returns a dict with rays, samples and seconds of
+    both ways and the capacities chosen."""
+    res = {"groups": [], "batched_s": 0.0, "individual_s": 0.0, "rays": 0, "samples": 0, "views": 0}
+    for name, scene, flags, views in groups:
+        if not views:
+            continue
+        cap, trials = autotune_capacity(scene, views, flags, sync) if autotune else (0, [])
+        scene.render_batch(views[:1], flags=flags, max_paths=cap)  # warm
+        t_b, (film, st, off) = _timed(lambda: scene.render_batch(views, flags=flags, max_paths=cap), sync)
+        rays = st["extension_rays"] + st["shadow_rays"]
+        del film
+
+        def individual():
+            for v in views:
+                scene.render(v["camera"], spp=v["spp"], max_depth=v["max_depth"], rr_depth=v["rr_depth"],
+                             seed=v["seed"], flags=flags, max_paths=cap)
+
+        t_i, _ = _timed(individual, sync)
+        samples = sum(v["camera"].width * v["camera"].height * v["spp"] for v in views)
+        res["groups"].append({"scene": name, "views": len(views), "capacity": cap,
+                              "autotune": [(c, round(t, 4)) for c, t in trials], "batched_s": t_b,
+                              "individual_s": t_i, "rays": rays, "samples": samples})
+        res["batched_s"] += t_b
+        res["individual_s"] += t_i
+        res["rays"] += rays
+        res["samples"] += samples
+        res["views"] += len(views)
+    res["batched_mrays_s"] = res["rays"] / res["batched_s"] / 1e6
+    res["individual_mrays_s"] = res["rays"] / res["individual_s"] / 1e6
+    res["batched_msamples_s"] = res["samples"] / res["batched_s"] / 1e6
+    res["speedup"] = res["individual_s"] / res["batched_s"]
+    return res

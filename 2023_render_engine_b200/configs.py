@@ -102,3 +102,44 @@ def build_config2(ctx, width=1280, height=720, seed=3, target_triangles=200_000)
 # variance and their inference costs as much as the shallow ones).
 GUIDE_TRAINING = dict(learning_rate=1e-3, batch=1 << 16, train_passes=4, steps_per_pass=64, max_depth=2,
                       bbox_min=(-2.01, -0.01, -2.01), bbox_max=(2.01, 2.51, 2.01))
+
+
+def random_views(rng, n, eye_lo, eye_hi, target_lo, target_hi, max_depth_range=(8, 16)):
+    """n seeded views: eye uniform in a box, looking at a point uniform in another box;
+    resolution log-uniform in [128^2, 1024^2] pixels with aspect ratio in [0.5, 2];
+    spp in {4, 8, 16, 32, 64}; max depth uniform in max_depth_range."""
+    views = []
+    for _ in range(n):
+        eye = rng.uniform(eye_lo, eye_hi)
+        target = rng.uniform(target_lo, target_hi)
+        area = float(np.exp(rng.uniform(np.log(128 * 128), np.log(1024 * 1024))))
+        aspect = float(rng.uniform(0.5, 2.0))
+        w = int(np.clip(round(np.sqrt(area * aspect)), 16, 2048))
+        h = int(np.clip(round(np.sqrt(area / aspect)), 16, 2048))
+        cam = core.look_at_camera(tuple(eye), tuple(target), (0, 1, 0), float(rng.uniform(35, 70)), w, h)
+        views.append(dict(camera=cam, spp=int(rng.choice([4, 8, 16, 32, 64])),
+                          max_depth=int(rng.integers(max_depth_range[0], max_depth_range[1] + 1)), rr_depth=3,
+                          seed=int(rng.integers(0, 2 ** 31))))
+    return views
+
+
+def build_config3(ctx, n_views=64, seed=5):
+    """Config 3: n_views instances drawn from configs 0-2 with seeded camera poses,
+    resolutions, spp and depths. Returns [(name, scene, flags, views)], one entry per scene
+    (each is one rt_render_batch call)."""
+    rng = np.random.default_rng(seed)
+    counts = np.bincount(rng.integers(0, 3, n_views), minlength=3)
+    out = []
+    sc0, _, _ = build_config0(ctx, 16, 16)
+    out.append(("config 0 (Cornell box)", sc0, N.RT_RENDER_NEE_AREA,
+                random_views(rng, int(counts[0]), (-0.6, -0.6, 2.0), (0.6, 0.6, 4.0), (-0.4, -0.6, -0.5),
+                             (0.4, 0.3, 0.5))))
+    sc1, _, _ = build_config1(ctx, 16, 16)
+    out.append(("config 1 (BVH stress)", sc1, N.RT_RENDER_NEE_AREA,
+                random_views(rng, int(counts[1]), (-0.6, -0.6, 2.0), (0.6, 0.6, 4.0), (-0.3, -0.3, -0.3),
+                             (0.3, 0.3, 0.3))))
+    sc2, _, _ = build_config2(ctx, 16, 16)
+    out.append(("config 2 (guiding room)", sc2, N.RT_RENDER_NEE_AREA,
+                random_views(rng, int(counts[2]), (-1.7, 0.4, -1.7), (1.7, 2.2, 0.8), (-1.9, 0.0, -1.9),
+                             (1.9, 1.5, 0.5))))
+    return out

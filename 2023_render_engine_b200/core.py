@@ -141,6 +141,37 @@ class Scene:
                                   ctypes.byref(st)))
         return film, {f: getattr(st, f) for f, _ in N.RenderStats._fields_}
 
+    def render_batch(self, views, flags: int = 0, max_paths: int = 0, film=None, fp64: bool = False):
+        """Renders many views of this scene in one wavefront (rt_render_batch).
+
+        views: list of dicts with camera and spp, and optionally max_depth (8), rr_depth (3),
+        seed (0), sample_offset (0). The film holds the views' pixels back to back; returns
+        (film, stats, offsets) with view i's pixels at [offsets[i], offsets[i + 1])."""
+        import torch
+
+        arr = (N.View * len(views))()
+        offsets = [0]
+        for i, v in enumerate(views):
+            arr[i].camera = v["camera"]
+            arr[i].spp = v["spp"]
+            arr[i].sample_offset = v.get("sample_offset", 0)
+            arr[i].max_depth = v.get("max_depth", 8)
+            arr[i].rr_depth = v.get("rr_depth", 3)
+            arr[i].seed = v.get("seed", 0)
+            offsets.append(offsets[-1] + v["camera"].width * v["camera"].height)
+        npx = offsets[-1]
+        if film is None:
+            film = {"sum": torch.zeros(npx * 3, dtype=torch.float32, device="cuda"),
+                    "count": torch.zeros(npx, dtype=torch.int32, device="cuda")}
+            if fp64:
+                film["sum64"] = torch.zeros(npx * 3, dtype=torch.float64, device="cuda")
+        st = N.RenderStats()
+        s64 = film.get("sum64")
+        N.check(N.lib().rt_render_batch(self.handle, arr, len(views), flags, max_paths, film["sum"].data_ptr(),
+                                        film["count"].data_ptr(), None if s64 is None else s64.data_ptr(),
+                                        ctypes.byref(st)))
+        return film, {f: getattr(st, f) for f, _ in N.RenderStats._fields_}, offsets
+
     def set_photon_map(self, pmap, k: int = 100, radius: float = 100.0):
         """Photon map for RT_RENDER_PHOTON_MAP renders (MAX_NEIGHBOURS, PHOTON_SEARCH_RADIUS)."""
         N.check(N.lib().rt_render_set_photon_map(self.handle, None if pmap is None else pmap.handle, k,

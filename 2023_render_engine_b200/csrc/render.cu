@@ -100,28 +100,32 @@ __device__ __forceinline__ unsigned long long *cnt64(uint32_t *c, int i)
 // (ProjectiveCamera.cu:71-104).
 __device__ void start_path(const RenderView &rv, const Buffers &bf, int b, uint32_t q, uint64_t g)
 {
-    const uint32_t W = rv.cam.width, H = rv.cam.height;
-    const uint32_t pix = (uint32_t)(g / rv.spp);
-    const uint32_t j = rv.sample_offset + (uint32_t)(g % rv.spp);
+    const uint32_t vi = view_of_sample(rv, g);
+    const rt_view &vw = rv.views[vi];
+    const rt_camera &cam = vw.camera;
+    g -= rv.view_sample0[vi];
+    const uint32_t W = cam.width, H = cam.height;
+    const uint32_t pix = (uint32_t)(g / vw.spp);
+    const uint32_t j = vw.sample_offset + (uint32_t)(g % vw.spp);
     const uint32_t px = pix % W, py = pix / W;
-    Pcg r = pcg_init(pix, j, rv.seed);
+    Pcg r = pcg_init(pix, j, vw.seed);
     float fx = fminf(fmaxf((float)px + pcg_float(r), 0.f), (float)W);
     float fy = fminf(fmaxf((float)py + pcg_float(r), 0.f), (float)H);
     float l1 = pcg_float(r), l2 = pcg_float(r);
-    V3 pc = xform_point(rv.cam.raster_to_camera, v3(fx, fy, 0.f));
+    V3 pc = xform_point(cam.raster_to_camera, v3(fx, fy, 0.f));
     V3 oc = v3(0, 0, 0), dc = normalize(pc);
-    if (rv.cam.lens_radius > 0) {
+    if (cam.lens_radius > 0) {
         float lx, ly;
         concentric_disk(l1, l2, lx, ly);
-        lx *= rv.cam.lens_radius;
-        ly *= rv.cam.lens_radius;
-        float ft = rv.cam.focal_distance / pc.z;
+        lx *= cam.lens_radius;
+        ly *= cam.lens_radius;
+        float ft = cam.focal_distance / pc.z;
         V3 pf = pc * ft;
         oc = v3(lx, ly, 0);
         dc = normalize(pf - oc);
     }
-    V3 o = xform_point(rv.cam.camera_to_world, oc);
-    V3 d = normalize(xform_vec(rv.cam.camera_to_world, dc));
+    V3 o = xform_point(cam.camera_to_world, oc);
+    V3 d = normalize(xform_vec(cam.camera_to_world, dc));
     rt_ray ray;
     ray.ox = o.x;
     ray.oy = o.y;
@@ -134,7 +138,7 @@ __device__ void start_path(const RenderView &rv, const Buffers &bf, int b, uint3
     reinterpret_cast<float4 *>(bf.rays[b])[2 * q] = make_float4(ray.ox, ray.oy, ray.oz, ray.tmax);
     reinterpret_cast<float4 *>(bf.rays[b])[2 * q + 1] = make_float4(ray.dx, ray.dy, ray.dz, 0.f);
     bf.st0[b][q] = make_float4(1.f, 1.f, 1.f, 0.f);
-    bf.st1[b][q] = make_float4(0.f, 0.f, 0.f, __uint_as_float(pix));
+    bf.st1[b][q] = make_float4(0.f, 0.f, 0.f, __uint_as_float(rv.view_pixel0[vi] + pix));
     bf.st2[b][q] = make_uint4((uint32_t)r.state, (uint32_t)(r.state >> 32), j, kCameraRay | kRecBits);
 }
 
@@ -213,7 +217,8 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
     uint32_t rec = (flags >> kRecShift) & kRecNone;  // newest guide record of this path
     Pcg rng;
     rng.state = ((uint64_t)s2.y << 32) | s2.x;
-    rng.inc = ((((uint64_t)s2.z << 32) | rv.seed) << 1u) | 1u;
+    const rt_view &vw = rv.views[view_of_pixel(rv, pix)];
+    rng.inc = ((((uint64_t)s2.z << 32) | vw.seed) << 1u) | 1u;
 
     bool finished = h.prim < 0;  // missed: no environment light (Scene::getEnvironmentLight = 0)
     uint32_t target = 0;
@@ -325,14 +330,14 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
         // Russian roulette (pathTracing.cu:91-102) on the reference's brightness (luminance) in
         // compat mode; on the largest component otherwise, so that no channel of a surviving
         // path's throughput grows past 1 (luminance lets a saturated red path grow 4.7x)
-        if (!finished && scattering && depth > rv.rr_depth) {
+        if (!finished && scattering && depth > vw.rr_depth) {
             float qrr = fmaxf(0.05f, 1.f - (compat ? luminance(beta) : fmaxf(beta.x, fmaxf(beta.y, beta.z))));
             if (pcg_float(rng) < qrr)
                 finished = true;
             else
                 beta = beta * (1.f / (1.f - qrr));
         }
-        if (!finished && depth + 1 >= rv.max_depth) finished = true;  // loop bound (pathTracing.cu:296)
+        if (!finished && depth + 1 >= vw.max_depth) finished = true;  // loop bound (pathTracing.cu:296)
         // reserve the path's slot for the shadow contributions
         if (!finished) {
             uint32_t qn = append(bf.cnt + nxt);
@@ -638,7 +643,7 @@ namespace rtb {
 void RenderScratch::release()
 {
     for (DevBuf *b : {&rays[0], &rays[1], &st0[0], &st0[1], &st1[0], &st1[1], &st2[0], &st2[1], &hits, &srays,
-                      &scontrib, &retire, &cnt, &gather})
+                      &scontrib, &retire, &cnt, &gather, &views, &view_sample0, &view_pixel0})
         b->release();
     if (host_cnt) cudaFreeHost(host_cnt);
     host_cnt = nullptr;
@@ -747,24 +752,44 @@ int make_render_view(rt_scene *s, RenderView &rv)
 
 }  // namespace rtb
 
-extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts *opts, float *sum_rgb,
-                         uint32_t *count, double *sum64, rt_render_stats *stats)
+namespace rtb {
+namespace {
+
+// Renders the views of one scene in one wavefront (rt_render is a batch of one view).
+int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t flags, uint32_t max_paths,
+                 float *sum_rgb, uint32_t *count, double *sum64, rt_render_stats *stats, const char *who)
 {
-    if (!s || !cam || !opts || !sum_rgb || !count) return fail(RT_ERR_INVALID, "rt_render: null argument");
-    if (!s->committed) return fail(RT_ERR_STATE, "rt_render: scene not committed");
-    if (cam->width == 0 || cam->height == 0 || opts->spp == 0 || opts->max_depth == 0)
-        return fail(RT_ERR_INVALID, "rt_render: empty image, spp or depth");
-    if (opts->max_depth > 255) return fail(RT_ERR_INVALID, "rt_render: max_depth above 255");
+    const std::string name(who);
+    if (!s || !views || nviews == 0 || !sum_rgb || !count) return fail(RT_ERR_INVALID, name + ": null argument");
+    if (!s->committed) return fail(RT_ERR_STATE, name + ": scene not committed");
+    std::vector<uint64_t> sample0(nviews + 1, 0);
+    std::vector<uint32_t> pixel0(nviews + 1, 0);
+    uint32_t depth_max = 0;
+    uint64_t pixels = 0;
+    for (uint32_t i = 0; i < nviews; i++) {
+        const rt_view &v = views[i];
+        if (v.camera.width == 0 || v.camera.height == 0 || v.spp == 0 || v.max_depth == 0)
+            return fail(RT_ERR_INVALID, name + ": empty image, spp or depth");
+        if (v.max_depth > 255) return fail(RT_ERR_INVALID, name + ": max_depth above 255");
+        const uint64_t np = (uint64_t)v.camera.width * v.camera.height;
+        pixels += np;
+        if (pixels >= (1ull << 31)) return fail(RT_ERR_INVALID, name + ": images too large");
+        sample0[i + 1] = sample0[i] + np * v.spp;
+        pixel0[i + 1] = (uint32_t)pixels;
+        depth_max = std::max(depth_max, v.max_depth);
+    }
     RTB_CUDA(cudaSetDevice(s->ctx->device));
     cudaStream_t st = s->ctx->stream;
-    const uint64_t total = (uint64_t)cam->width * cam->height * opts->spp;
-    if ((uint64_t)cam->width * cam->height >= (1ull << 31)) return fail(RT_ERR_INVALID, "rt_render: image too large");
-    uint32_t cap = opts->max_paths ? opts->max_paths : (1u << 22);
+    const uint64_t total = sample0[nviews];
+    RenderScratch &rs = s->rscratch;
+    RTB_CHECK(rs.views.upload(views, sizeof(rt_view) * nviews, st));
+    RTB_CHECK(rs.view_sample0.upload(sample0.data(), 8ull * (nviews + 1), st));
+    RTB_CHECK(rs.view_pixel0.upload(pixel0.data(), 4ull * (nviews + 1), st));
+    uint32_t cap = max_paths ? max_paths : (1u << 22);
     cap = (uint32_t)std::min<uint64_t>(cap, std::max<uint64_t>(total, 1024));
     cap = (cap + kB - 1) / kB * kB;
-    const uint32_t per_path_shadow = (uint32_t)(s->plights.size() / 2) + ((opts->flags & RT_RENDER_NEE_AREA) ? 1 : 0);
+    const uint32_t per_path_shadow = (uint32_t)(s->plights.size() / 2) + ((flags & RT_RENDER_NEE_AREA) ? 1 : 0);
     const uint32_t scap = std::max<uint32_t>(cap * std::max<uint32_t>(per_path_shadow, 1), kB);
-    RenderScratch &rs = s->rscratch;
     RTB_CHECK(rs.rays[0].reserve(32ull * cap));
     RTB_CHECK(rs.rays[1].reserve(32ull * cap));
     for (int b = 0; b < 2; b++) {
@@ -776,18 +801,18 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
     RTB_CHECK(rs.srays.reserve(32ull * scap));
     RTB_CHECK(rs.scontrib.reserve(16ull * scap));
     RTB_CHECK(rs.retire.reserve(16ull * cap));
-    const bool photon_mode = (opts->flags & RT_RENDER_PHOTON_MAP) != 0;
+    const bool photon_mode = (flags & RT_RENDER_PHOTON_MAP) != 0;
     if (photon_mode) {
         if (!s->pmap || !s->pmap->built)
-            return fail(RT_ERR_STATE, "rt_render: RT_RENDER_PHOTON_MAP needs a built photon map (rt_render_set_photon_map)");
+            return fail(RT_ERR_STATE, name + ": RT_RENDER_PHOTON_MAP needs a built photon map (rt_render_set_photon_map)");
         RTB_CHECK(rs.gather.reserve(64ull * cap));
     }
-    const bool guided = (opts->flags & RT_RENDER_GUIDE) != 0;
+    const bool guided = (flags & RT_RENDER_GUIDE) != 0;
     GuideView gv{};
     rt_guide *guide = s->guide;
     if (guided) {
-        if (!guide) return fail(RT_ERR_STATE, "rt_render: RT_RENDER_GUIDE needs a guide (rt_render_set_guide)");
-        if (photon_mode) return fail(RT_ERR_UNSUPPORTED, "rt_render: RT_RENDER_GUIDE with RT_RENDER_PHOTON_MAP");
+        if (!guide) return fail(RT_ERR_STATE, name + ": RT_RENDER_GUIDE needs a guide (rt_render_set_guide)");
+        if (photon_mode) return fail(RT_ERR_UNSUPPORTED, name + ": RT_RENDER_GUIDE with RT_RENDER_PHOTON_MAP");
         gv.enabled = 1;
         gv.train = s->guide_train;
         gv.max_depth = guide->opts.max_depth ? guide->opts.max_depth : 0xFFFFFFFFu;
@@ -840,13 +865,11 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
 
     RenderView rv{};
     RTB_CHECK(make_render_view(s, rv));
-    rv.cam = *cam;
-    rv.spp = opts->spp;
-    rv.sample_offset = opts->sample_offset;
-    rv.max_depth = opts->max_depth;
-    rv.rr_depth = opts->rr_depth;
-    rv.seed = opts->seed;
-    rv.flags = opts->flags;
+    rv.views = rs.views.as<rt_view>();
+    rv.view_sample0 = rs.view_sample0.as<uint64_t>();
+    rv.view_pixel0 = rs.view_pixel0.as<uint32_t>();
+    rv.nviews = nviews;
+    rv.flags = flags;
     rv.total = total;
 
     cudaEvent_t e0, e1;
@@ -871,12 +894,13 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
     const GuideBox gbox = guided ? guide_box(guide) : GuideBox{};
     k_start<<<blocks, kB, 0, st>>>(rv, bf);
     RTB_CUDA(cudaGetLastError());
-    const uint32_t trace_flags = (opts->flags & RT_RENDER_EXACT_TRACE) ? 0u : RT_TRACE_FAST;
-    int cur = 0;
+    const uint32_t trace_flags = (flags & RT_RENDER_EXACT_TRACE) ? 0u : RT_TRACE_FAST;
     uint64_t waves = 0;
-    const uint64_t max_waves = (uint64_t)opts->max_depth * (total / std::max<uint32_t>(cap / 4, 1) + 8) + 64;
-    for (;;) {
-        const int nxt = cur ^ 1;
+    const uint64_t max_waves = (uint64_t)depth_max * (total / std::max<uint32_t>(cap / 4, 1) + 8) + 64;
+    // One group = 4 waves (cur 0, 1, 0, 1). The first group is launched directly; the rest
+    // replay it as a CUDA graph captured from the second group's launches.
+    auto wave_group = [&]() -> int {
+        int cur = 0;
         for (int k = 0; k < 4; k++) {
             RTB_CHECK(launch_trace_closest_dev(rv.sv, bf.rays[cur], bf.cnt + cur, cap, bf.hits, trace_flags,
                                                s->scratch.queue.as<uint32_t>(), s->scratch.counters.as<uint32_t>(),
@@ -899,17 +923,59 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
             k_retire<<<blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64, gv);
             RTB_CUDA(cudaGetLastError());
             cur ^= 1;
-            waves++;
         }
-        (void)nxt;
-        RTB_CUDA(cudaMemcpyAsync(rs.host_cnt, bf.cnt, 128, cudaMemcpyDeviceToHost, st));
-        RTB_CUDA(cudaStreamSynchronize(st));
+        return RT_OK;
+    };
+    cudaGraphExec_t graph = nullptr;
+    auto release_graph = [&]() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    };
+    for (uint64_t group = 0;; group++) {
+        int rc = RT_OK;
+        // the legacy default stream cannot be captured: there every group is launched directly
+        if (group == 1 && st != nullptr && st != cudaStreamLegacy &&
+            cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            rc = wave_group();
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(st, &g);
+            if (rc == RT_OK && ce == cudaSuccess && g) {
+                const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
+                cudaGraphDestroy(g);
+                if (ie != cudaSuccess) return cuda_status(ie, "cudaGraphInstantiate");
+            } else {
+                if (g) cudaGraphDestroy(g);
+                if (rc != RT_OK) return rc;
+                return cuda_status(ce, "cudaStreamEndCapture");
+            }
+        }
+        if (graph) {
+            const cudaError_t le = cudaGraphLaunch(graph, st);
+            if (le != cudaSuccess) {
+                release_graph();
+                return cuda_status(le, "cudaGraphLaunch");
+            }
+        } else {
+            rc = wave_group();
+            if (rc != RT_OK) return rc;
+        }
+        waves += 4;
+        cudaError_t ce = cudaMemcpyAsync(rs.host_cnt, bf.cnt, 128, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) {
+            release_graph();
+            return cuda_status(ce, "wave group");
+        }
         const uint32_t *hc = static_cast<const uint32_t *>(rs.host_cnt);
         uint64_t next_sample;
         std::memcpy(&next_sample, hc + 8, 8);
-        if (hc[cur] == 0 && next_sample >= total) break;
-        if (waves > max_waves) return fail(RT_ERR_TIMEOUT, "rt_render: wave cap exceeded");
+        if (hc[0] == 0 && next_sample >= total) break;
+        if (waves > max_waves) {
+            release_graph();
+            return fail(RT_ERR_TIMEOUT, name + ": wave cap exceeded");
+        }
     }
+    release_graph();
     RTB_CUDA(cudaEventRecord(e1, st));
     RTB_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
@@ -929,4 +995,27 @@ extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts
         stats->ms = ms;
     }
     return RT_OK;
+}
+
+}  // namespace
+}  // namespace rtb
+
+extern "C" int rt_render(rt_scene *s, const rt_camera *cam, const rt_render_opts *opts, float *sum_rgb,
+                         uint32_t *count, double *sum64, rt_render_stats *stats)
+{
+    if (!s || !cam || !opts) return fail(RT_ERR_INVALID, "rt_render: null argument");
+    rt_view v{};
+    v.camera = *cam;
+    v.spp = opts->spp;
+    v.sample_offset = opts->sample_offset;
+    v.max_depth = opts->max_depth;
+    v.rr_depth = opts->rr_depth;
+    v.seed = opts->seed;
+    return render_views(s, &v, 1, opts->flags, opts->max_paths, sum_rgb, count, sum64, stats, "rt_render");
+}
+
+extern "C" int rt_render_batch(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t flags, uint32_t max_paths,
+                               float *sum_rgb, uint32_t *count, double *sum64, rt_render_stats *stats)
+{
+    return render_views(s, views, nviews, flags, max_paths, sum_rgb, count, sum64, stats, "rt_render_batch");
 }

@@ -161,6 +161,7 @@ int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, uint8_t
 // Wavefront buffers of rt_render (grown on demand, kept between calls).
 struct RenderScratch {
     DevBuf rays[2], st0[2], st1[2], st2[2], hits, srays, scontrib, retire, cnt, gather;
+    DevBuf views, view_sample0, view_pixel0;  // the render's views and their prefix sums
     void *host_cnt = nullptr;  // pinned
     void release();
 };

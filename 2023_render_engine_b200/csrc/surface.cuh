@@ -26,10 +26,41 @@ struct RenderView {
     const float4 *plights;  // 2 per light: position, radiant intensity rgb
     uint32_t nplights;
     uint32_t nmats;
-    rt_camera cam;
-    uint32_t spp, sample_offset, max_depth, rr_depth, seed, flags;
-    uint64_t total;  // width * height * spp
+    // the views of the render (one for rt_render): camera and options, the first global
+    // sample index of each view (nviews + 1 entries) and its first pixel in the films
+    const rt_view *views;
+    const uint64_t *view_sample0;
+    const uint32_t *view_pixel0;
+    uint32_t nviews;
+    uint32_t flags;
+    uint64_t total;  // samples over all views
 };
+
+// view of global sample g / of global film pixel p (binary search over the prefix sums)
+__device__ __forceinline__ uint32_t view_of_sample(const RenderView &rv, uint64_t g)
+{
+    uint32_t lo = 0, hi = rv.nviews - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (rv.view_sample0[mid] <= g)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ uint32_t view_of_pixel(const RenderView &rv, uint32_t p)
+{
+    uint32_t lo = 0, hi = rv.nviews - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (rv.view_pixel0[mid] <= p)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
 
 // Warp-aggregated queue append: one atomic per group of active lanes.
 __device__ __forceinline__ uint32_t append(uint32_t *counter)

@@ -272,7 +272,8 @@ def run_ours(args):
     cfgs = importlib.import_module("2023_render_engine_b200.configs")
     dev = torch.cuda.current_device()
     ctx = core.Context(dev)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a stream of its own: the default stream cannot be captured
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
 
     def barrier():
@@ -357,6 +358,17 @@ def run_ours(args):
     if world == 1 and args.guide_ref_spp > 0:
         guiding = measure_guiding(args, core, N, cfgs, ctx, torch)
 
+    # ---- batched multi-view rendering (64 views of configs 0-2, one wavefront per scene)
+    batched = None
+    if world == 1 and not args.no_batch:
+        B = importlib.import_module("2023_render_engine_b200.batch")
+        groups = cfgs.build_config3(ctx, n_views=64, seed=5)
+        batched = B.measure(groups, torch.cuda.synchronize)
+        batched["workload"] = ("64 views drawn from configs 0-2 (seeded poses; resolution log-uniform 128^2-1024^2, "
+                               "aspect 0.5-2; spp in {4..64}; depth 8-16), area NEE; one rt_render_batch per "
+                               "scene vs one rt_render per view")
+        del groups
+
     # ---- the reference's own CUDA traversal on the same rays (baseline, not a target)
     ref_cuda = None
     if world == 1 and not args.no_ref_cuda:
@@ -396,6 +408,7 @@ def run_ours(args):
             "clocks": clk.summary(),
             "guiding": guiding,
             "reference_cuda": ref_cuda,
+            "batched": batched,
         }
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
@@ -424,6 +437,7 @@ def main():
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--guide-ref-spp", type=int, default=4096, help="0 skips the guiding measurement")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip the reference CUDA traversal baseline")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view measurement")
     ap.add_argument("--guide-target", type=float, default=0.01)
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)

@@ -244,6 +244,23 @@ typedef struct rt_render_stats {
 RT_API int rt_render(rt_scene *scene, const rt_camera *camera, const rt_render_opts *opts, float *sum_rgb,
                      uint32_t *count, double *sum_rgb64, rt_render_stats *stats);
 
+/* One view of a batch: the camera and per-view render options of rt_render_opts. */
+typedef struct rt_view {
+    rt_camera camera;
+    uint32_t spp, sample_offset, max_depth, rr_depth, seed;
+    uint32_t reserved[3];
+} rt_view;
+
+/* Many views of one scene in one wavefront (new in this build: the reference renders one
+ * camera per PathTracerIntegrator::render call, PathTracerIntegrator.cu:140-210). The views
+ * may differ in resolution, spp, depth and seed; their paths share the queues, so small views
+ * keep the GPU as busy as one large frame. Films lie back to back: view i's pixels start at
+ * pixel sum over k < i of width_k * height_k in sum_rgb (3 floats per pixel), count and sum64
+ * (nullable). A view renders exactly the samples rt_render would give it with the same
+ * options. flags: RT_RENDER_* for all views; max_paths: queue capacity (0: 4M). */
+RT_API int rt_render_batch(rt_scene *scene, const rt_view *views, uint32_t nviews, uint32_t flags, uint32_t max_paths,
+                           float *sum_rgb, uint32_t *count, double *sum64, rt_render_stats *stats);
+
 /* --------------------------------------------------------------- photons */
 
 typedef struct rt_photon_map rt_photon_map;
