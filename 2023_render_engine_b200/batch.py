@@ -71,3 +71,30 @@ def measure(groups, sync, autotune=True):
     res["batched_msamples_s"] = res["samples"] / res["batched_s"] / 1e6
     res["speedup"] = res["individual_s"] / res["batched_s"]
     return res
+
+
+def measure_guided(scene, flags, views, guide, sync, capacity=0, train_passes=4, steps_per_pass=64,
+                   batch=1 << 16):
+    """The views of one scene rendered with the learned guide: `train_passes` one-spp
+    recording passes over the whole batch (each followed by `steps_per_pass` training steps),
+    then the batch at its own spp with the guide, against the same batch without it."""
+    t0 = time.perf_counter()
+    sync()
+    for p in range(train_passes):
+        scene.set_guide(guide, train=True)
+        scene.render_batch([dict(v, spp=1, sample_offset=1000 + p) for v in views], flags=flags | N.RT_RENDER_GUIDE,
+                           max_paths=capacity)
+        guide.train_records(steps_per_pass, batch, seed=p)
+    sync()
+    t_train = time.perf_counter() - t0
+    scene.set_guide(guide, train=False)
+    t_g, (film, st, _) = _timed(lambda: scene.render_batch(views, flags=flags | N.RT_RENDER_GUIDE,
+                                                           max_paths=capacity), sync)
+    rays_g = st["extension_rays"] + st["shadow_rays"]
+    del film
+    t_p, (film, st, _) = _timed(lambda: scene.render_batch(views, flags=flags, max_paths=capacity), sync)
+    rays_p = st["extension_rays"] + st["shadow_rays"]
+    scene.set_guide(None)
+    return {"views": len(views), "train_s": t_train, "guided_s": t_g, "plain_s": t_p,
+            "guided_mrays_s": rays_g / t_g / 1e6, "plain_mrays_s": rays_p / t_p / 1e6,
+            "training": {"passes": train_passes, "steps": guide.steps, "batch": batch}}

@@ -364,6 +364,14 @@ def run_ours(args):
         B = importlib.import_module("2023_render_engine_b200.batch")
         groups = cfgs.build_config3(ctx, n_views=64, seed=5)
         batched = B.measure(groups, torch.cuda.synchronize)
+        T = cfgs.GUIDE_TRAINING
+        name, sc2, fl2, views2 = groups[2]
+        g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=2,
+                       max_depth=T["max_depth"])
+        batched["guided"] = B.measure_guided(sc2, fl2, views2, g, torch.cuda.synchronize,
+                                             capacity=batched["groups"][2]["capacity"])
+        batched["guided"]["scene"] = name
+        g.close()
         batched["workload"] = ("64 views drawn from configs 0-2 (seeded poses; resolution log-uniform 128^2-1024^2, "
                                "aspect 0.5-2; spp in {4..64}; depth 8-16), area NEE; one rt_render_batch per "
                                "scene vs one rt_render per view")
