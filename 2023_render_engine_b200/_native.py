@@ -132,6 +132,9 @@ SIGNATURES = {
     "rt_scene_add_point_light": [_P, _P, _P, _F32],
     "rt_render": [_P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), _P, _P, _P, ctypes.POINTER(RenderStats)],
     "rt_render_batch": [_P, ctypes.POINTER(View), _U32, _U32, _U32, _P, _P, _P, ctypes.POINTER(RenderStats)],
+    "rt_film_store_hdrbmp": [ctypes.c_char_p, _U32, _U32, _P, _P, _P, _U64],
+    "rt_film_load_hdrbmp": [ctypes.c_char_p, _U32, _U32, _P, ctypes.POINTER(_U64)],
+    "rt_film_rmse": [_P, _P, _P, _P, _P, _P, _U64, ctypes.POINTER(ctypes.c_double)],
     "rt_photons_trace": [_P, _U64, _U32, _U32, _U32, _U32, ctypes.POINTER(_P), ctypes.POINTER(PhotonTraceStats)],
     "rt_photon_map_from_points": [_P, _P, _P, _U64, ctypes.POINTER(_P)],
     "rt_photon_map_build": [_P],

@@ -452,3 +452,31 @@ class Guide:
             self.close()
         except Exception:
             pass
+
+
+def film_store_hdrbmp(path, film, width: int, height: int, samples: int):
+    """Film::storeContributionsToFile of a device film: writes `path`.hdrbmp."""
+    s64 = film.get("sum64")
+    N.check(N.lib().rt_film_store_hdrbmp(str(path).encode(), width, height,
+                                         None if s64 is not None else film["sum"].data_ptr(),
+                                         film["count"].data_ptr(), None if s64 is None else s64.data_ptr(),
+                                         samples))
+
+
+def film_load_hdrbmp(path, width: int, height: int):
+    """Film::loadContributionsFromFile: (per-pixel sums (h*w, 3) float64, samples per pixel)."""
+    out = np.zeros((width * height, 3), np.float64)
+    n = ctypes.c_uint64()
+    N.check(N.lib().rt_film_load_hdrbmp(str(path).encode(), width, height, out.ctypes.data, ctypes.byref(n)))
+    return out, n.value
+
+
+def film_rmse_gpu(film_a, film_b) -> float:
+    """computeRMSE of two device films on the GPU (rt_film_rmse)."""
+    out = ctypes.c_double()
+    a64, b64 = film_a.get("sum64"), film_b.get("sum64")
+    N.check(N.lib().rt_film_rmse(None if a64 is not None else film_a["sum"].data_ptr(), film_a["count"].data_ptr(),
+                                 None if a64 is None else a64.data_ptr(),
+                                 None if b64 is not None else film_b["sum"].data_ptr(), film_b["count"].data_ptr(),
+                                 None if b64 is None else b64.data_ptr(), film_a["count"].numel(), ctypes.byref(out)))
+    return out.value

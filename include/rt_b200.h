@@ -332,6 +332,25 @@ RT_API int rt_photon_knn(rt_photon_map *map, const float *queries_dev, const int
                          uint32_t k, float radius, int32_t *out_idx_dev, float *out_dist_dev,
                          uint32_t *out_count_dev);
 
+/* ------------------------------------------------------------ film files and RMSE */
+
+/* Film::storeContributionsToFile (camera/Film.cu:366-391): writes `path`.hdrbmp in the
+ * reference's format (text: "P6", resolution, "F", samples per pixel, then per pixel the RGB
+ * sum over its samples). The device film is rt_render's: sum_rgb (or sum64 when non-null) and
+ * count; a pixel's sum is written as sum * samples / count (NaN/Inf samples replaced by the
+ * mean of the valid ones, pathTracing.cu:457-490). */
+RT_API int rt_film_store_hdrbmp(const char *path, uint32_t width, uint32_t height, const float *sum_rgb_dev,
+                                const uint32_t *count_dev, const double *sum64_dev, uint64_t samples);
+/* Film::loadContributionsFromFile (camera/Film.cu:393-449): reads `path`.hdrbmp into host
+ * sums (3 doubles per pixel) and its samples per pixel. */
+RT_API int rt_film_load_hdrbmp(const char *path, uint32_t width, uint32_t height, double *sum_rgb_host,
+                               uint64_t *samples);
+/* computeRMSE (camera/Film.cu:611-632) of two device films on the GPU: sqrt(sum over pixels
+ * of |mean_a - mean_b|^2 / pixels), mean = sum / count per pixel (the FP64 sums when given). */
+RT_API int rt_film_rmse(const float *sum_a_dev, const uint32_t *count_a_dev, const double *sum64_a_dev,
+                        const float *sum_b_dev, const uint32_t *count_b_dev, const double *sum64_b_dev, uint64_t npix,
+                        double *rmse);
+
 /* ------------------------------------------------------------ path guide */
 
 /* Learned path-guiding proposal (new in this build; the reference has no counterpart).

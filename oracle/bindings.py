@@ -360,6 +360,32 @@ class RefRender:
         L.refr_config(ctypes.byref(w), ctypes.byref(h), ctypes.byref(s), ctypes.byref(d))
         self.width, self.height, self.spp, self.depth = w.value, h.value, s.value, d.value
 
+    def film_store(self, path, sums, samples):
+        """Film::storeContributionsToFile of a film with these per-pixel sums (h*w, 3)."""
+        a = _np(sums, np.float64).reshape(-1, 3)
+        L = self.L
+        L.refr_film_store.argtypes = [ctypes.c_char_p, P, ctypes.c_longlong]
+        L.refr_film_store(str(path).encode(), a.ctypes.data, samples)
+
+    def film_load(self, path):
+        """Film::loadContributionsFromFile: (sums (h*w, 3), samples)."""
+        L = self.L
+        L.refr_film_load.argtypes = [ctypes.c_char_p, P, P]
+        out = np.zeros((self.width * self.height, 3), np.float64)
+        n = ctypes.c_longlong()
+        if L.refr_film_load(str(path).encode(), out.ctypes.data, ctypes.byref(n)) != 0:
+            raise RuntimeError("reference film load failed")
+        return out, n.value
+
+    def film_rmse(self, a, na, b, nb):
+        """computeRMSE of two films given by per-pixel sums and samples per pixel."""
+        L = self.L
+        L.refr_film_rmse.argtypes = [P, ctypes.c_longlong, P, ctypes.c_longlong]
+        L.refr_film_rmse.restype = ctypes.c_double
+        a = _np(a, np.float64).reshape(-1, 3)
+        b = _np(b, np.float64).reshape(-1, 3)
+        return L.refr_film_rmse(a.ctypes.data, na, b.ctypes.data, nb)
+
     def render(self, obejota_path, planes, kd):
         """planes: (n, 12) Plane(corner, axisX, axisY, normal); kd: (n, 3). Returns
         (mean image (h*w, 3), cameraToWorld 4x4, rasterToCamera 4x4)."""

@@ -143,3 +143,47 @@ REFR_API int refr_render(const char *obejota, int nplanes, const float *planes, 
     for (auto *m : mats) delete m;
     return 0;
 }
+
+// Film accumulation files and computeRMSE (camera/Film.cu:366-449, 611-632) on films of the
+// harness resolution. sum: 3 doubles per pixel (the per-pixel sums over `samples` samples).
+namespace {
+struct FilmFill : public Film {
+    using Film::pixelLight;
+    using Film::samplesComputedPixel0;
+    using Film::samplesLoadedFromFile;
+};
+void fill(FilmFill &f, const double *sum, long long samples)
+{
+    for (int i = 0; i < resolutionX * resolutionY; i++) f.pixelLight[i] = Spectrum(sum[3 * i], sum[3 * i + 1], sum[3 * i + 2]);
+    f.samplesComputedPixel0 = samples;
+}
+}  // namespace
+
+REFR_API int refr_film_store(const char *path, const double *sum, long long samples)
+{
+    FilmFill f;
+    fill(f, sum, samples);
+    f.storeContributionsToFile(path);
+    return 0;
+}
+
+REFR_API int refr_film_load(const char *path, double *sum, long long *samples)
+{
+    FilmFill f;
+    if (!f.loadContributionsFromFile(path)) return 1;
+    for (int i = 0; i < resolutionX * resolutionY; i++) {
+        sum[3 * i] = f.pixelLight[i].getR();
+        sum[3 * i + 1] = f.pixelLight[i].getG();
+        sum[3 * i + 2] = f.pixelLight[i].getB();
+    }
+    *samples = f.samplesLoadedFromFile + f.samplesComputedPixel0;
+    return 0;
+}
+
+REFR_API double refr_film_rmse(const double *a, long long na, const double *b, long long nb)
+{
+    FilmFill fa, fb;
+    fill(fa, a, na);
+    fill(fb, b, nb);
+    return computeRMSE(fa, fb);
+}
