@@ -43,7 +43,7 @@ class SceneStats(ctypes.Structure):
 class Material(ctypes.Structure):
     _fields_ = [("type", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("color", ctypes.c_float * 3),
                 ("intensity", ctypes.c_float), ("eta", ctypes.c_float * 3), ("k", ctypes.c_float * 3),
-                ("roughness", ctypes.c_float * 2), ("ior", ctypes.c_float), ("pad", ctypes.c_float * 3)]
+                ("roughness", ctypes.c_float * 2), ("ior", ctypes.c_float), ("extra", ctypes.c_float * 3)]
 
 
 class Camera(ctypes.Structure):
@@ -70,12 +70,16 @@ class RenderStats(ctypes.Structure):
 
 
 RT_MAT_LAMBERTIAN, RT_MAT_TROWBRIDGE, RT_MAT_DIELECTRIC, RT_MAT_LIGHT, RT_MAT_MIRROR, RT_MAT_PLAIN = range(6)
+RT_MAT_PHONG = 6
+RT_MAT_SUBSURFACE = 7
 RT_MATF_TRANSPARENT = 0x1
 RT_RENDER_NEE_AREA = 0x1
 RT_RENDER_COMPAT = 0x2
 RT_RENDER_EXACT_TRACE = 0x4
 RT_RENDER_PHOTON_MAP = 0x8
 RT_RENDER_GUIDE = 0x10
+RT_RENDER_SUBSURFACE = 0x20
+RT_RENDER_HYBRID = 0x40
 
 
 class PhotonTraceStats(ctypes.Structure):
@@ -143,6 +147,7 @@ SIGNATURES = {
     "rt_photon_map_destroy": [_P],
     "rt_photon_knn": [_P, _P, _P, _U64, _U32, _F32, _P, _P, _P],
     "rt_photon_density": [_P, ctypes.POINTER(Material), _P, _P, _P, _P, _U64, _U32, _F32, _P],
+    "rt_photon_subsurface": [_P, ctypes.POINTER(Material), _P, _P, _P, _P, _U64, _F32, _U32, _P],
     "rt_render_set_photon_map": [_P, _P, _U32, _F32],
     "rt_guide_create": [_P, ctypes.POINTER(GuideOpts), ctypes.POINTER(_P)],
     "rt_guide_destroy": [_P],

@@ -214,8 +214,9 @@ def make_rays(o: np.ndarray, d: np.ndarray, tmax=None) -> np.ndarray:
 
 
 def material(type_, color=(0.8, 0.8, 0.8), intensity=0.0, eta=(1.5, 1.5, 1.5), k=(0.0, 0.0, 0.0),
-             roughness=(0.1, 0.1), ior=1.5, transparent=False) -> "N.Material":
+             roughness=(0.1, 0.1), ior=1.5, transparent=False, extra=(0.0, 0.0, 0.0)) -> "N.Material":
     m = N.Material()
+    m.extra[:] = [float(c) for c in extra]
     m.type = type_
     m.flags = N.RT_MATF_TRANSPARENT if transparent else 0
     m.color[:] = [float(c) for c in color]
@@ -225,6 +226,17 @@ def material(type_, color=(0.8, 0.8, 0.8), intensity=0.0, eta=(1.5, 1.5, 1.5), k
     m.roughness[:] = [float(c) for c in roughness]
     m.ior = float(ior)
     return m
+
+
+def phong_material(kd, ks, ns, transparent=False) -> "N.Material":
+    """PhongMaterial(ka, kd, ks, ke = 0, ni, ns) as the renderer's table entry."""
+    return material(N.RT_MAT_PHONG, color=kd, k=ks, roughness=(ns, 0.0), transparent=transparent)
+
+
+def subsurface_material(kd, ks, ns, eta, sigma_s, sigma_a, g=0.0, transparent=False) -> "N.Material":
+    """SSMaterial(ka, kd, ks, eta, ns, texture, transparent, sigmaS, sigmaA, g)."""
+    return material(N.RT_MAT_SUBSURFACE, color=kd, k=ks, roughness=(ns, g), ior=eta, eta=sigma_s, extra=sigma_a,
+                    transparent=transparent)
 
 
 def look_at_camera(eye, target, up, vfov_deg: float, width: int, height: int, focal=0.8,

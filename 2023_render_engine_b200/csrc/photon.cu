@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kPB) k_photon_shade(RenderView rv, PhotonBuffe
     Surface sf = surface_at(rv, h, o, d, compat);
     const rt_material &m = rv.mats[min(sf.mat, rv.nmats - 1)];
     Bsdf bs = load_bsdf(m);
-    if (is_scattering(bs.type)) {  // samplePhotonIntersections (photonDispersion.cu:40-54)
+    if (is_scattering(bs)) {  // samplePhotonIntersections (photonDispersion.cu:40-54)
         uint32_t slot = append(pb.cnt + 2);
         if (slot < pb.store_cap) {
             V3 pw = carry * beta;
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kPB) k_photon_shade(RenderView rv, PhotonBuffe
     carry = carry + beta * Le;  // photonDispersion.cu:64-65
     beta = beta * f;
     bool finished = is_black(f);
-    if (!finished && is_scattering(bs.type) && depth > rr_depth) {  // finishStep (pathTracing.cu:91-102)
+    if (!finished && is_scattering(bs) && depth > rr_depth) {  // finishStep (pathTracing.cu:91-102)
         float qrr = fmaxf(0.05f, 1.f - luminance(beta));
         if (pcg_float(rng) < qrr)
             finished = true;
@@ -223,6 +223,24 @@ __global__ void __launch_bounds__(128) k_density(const float4 *__restrict__ node
     V3 nn = normalize(v3(nrm[3 * qi], nrm[3 * qi + 1], nrm[3 * qi + 2]));
     V3 w = v3(wo[3 * qi], wo[3 * qi + 1], wo[3 * qi + 2]);
     V3 c = photon_density(node_pos, node_aux, photons, n, load_bsdf(mat), p, nn, w, shape ? shape[qi] : -1, k, radius);
+    out[3 * qi] = c.x;
+    out[3 * qi + 1] = c.y;
+    out[3 * qi + 2] = c.z;
+}
+
+__global__ void __launch_bounds__(128) k_subsurface(const float4 *__restrict__ node_pos, const int2 *__restrict__ node_aux,
+                                                    const rt_photon *__restrict__ photons, uint32_t n, rt_material mat,
+                                                    const float *__restrict__ pts, const float *__restrict__ nrm,
+                                                    const float *__restrict__ wo, const int32_t *__restrict__ shape,
+                                                    uint64_t nq, float radius, int compat, float *__restrict__ out)
+{
+    const uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= nq) return;
+    const V3 p = v3(pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]);
+    const V3 nn = v3(nrm[3 * qi], nrm[3 * qi + 1], nrm[3 * qi + 2]);
+    const V3 w = v3(wo[3 * qi], wo[3 * qi + 1], wo[3 * qi + 2]);
+    const V3 c = photon_subsurface(node_pos, node_aux, photons, n, mat, p, nn, w, shape ? shape[qi] : -1, radius,
+                                   compat != 0);
     out[3 * qi] = c.x;
     out[3 * qi + 1] = c.y;
     out[3 * qi + 2] = c.z;
@@ -390,6 +408,25 @@ int rt_photon_knn(rt_photon_map *m, const float *q, const int32_t *qs, uint64_t 
     k_knn<<<(unsigned)blocks, 128, 0, m->ctx->stream>>>(m->node_pos.as<float4>(), m->node_aux.as<int2>(),
                                                         (uint32_t)m->n, q, qs, nq, k, radius, out_idx, out_dist,
                                                         out_count);
+    RTB_CUDA(cudaGetLastError());
+    RTB_CUDA(cudaStreamSynchronize(m->ctx->stream));
+    return RT_OK;
+}
+
+int rt_photon_subsurface(rt_photon_map *m, const rt_material *mat, const float *pts, const float *nrm, const float *wo,
+                         const int32_t *shape, uint64_t nq, float radius, uint32_t flags, float *out_rgb)
+{
+    if (!m || !mat) return fail(RT_ERR_INVALID, "rt_photon_subsurface: null argument");
+    if (!m->built) return fail(RT_ERR_STATE, "rt_photon_subsurface: photon map not built");
+    if (mat->type != RT_MAT_SUBSURFACE) return fail(RT_ERR_INVALID, "rt_photon_subsurface: not a subsurface material");
+    if (nq == 0) return RT_OK;
+    if (!pts || !nrm || !wo || !out_rgb) return fail(RT_ERR_INVALID, "rt_photon_subsurface: null buffer");
+    RTB_CUDA(cudaSetDevice(m->ctx->device));
+    const uint64_t blocks = (nq + 127) / 128;
+    k_subsurface<<<(unsigned)blocks, 128, 0, m->ctx->stream>>>(m->node_pos.as<float4>(), m->node_aux.as<int2>(),
+                                                               m->photons.as<rt_photon>(), (uint32_t)m->n, *mat, pts, nrm,
+                                                               wo, shape, nq, radius, (flags & RT_RENDER_COMPAT) ? 1 : 0,
+                                                               out_rgb);
     RTB_CUDA(cudaGetLastError());
     RTB_CUDA(cudaStreamSynchronize(m->ctx->stream));
     return RT_OK;

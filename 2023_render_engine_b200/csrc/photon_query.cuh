@@ -168,4 +168,107 @@ __device__ __forceinline__ V3 photon_density(const float4 *__restrict__ node_pos
     return sum * kernel;
 }
 
+// nn::KDTree::nearest_neighbors with an unbounded k (kdtree.h:111-152, as
+// Scene::search_nearest(p, radius, (ulong)-1, shapeId) calls it, Scene.cu:808-813): every photon
+// at distance < radius on shape sid (-1: any) is passed to visit(photon index, distance).
+template <class F>
+__device__ __forceinline__ uint32_t radius_query(const float4 *__restrict__ node_pos, const int2 *__restrict__ node_aux,
+                                                 uint32_t n, float qx, float qy, float qz, int32_t sid, float radius,
+                                                 F &&visit)
+{
+    uint32_t cnt = 0;
+    uint32_t sl[64], sr[64];
+    float sd[64];
+    int sp = 1;
+    sl[0] = 0;
+    sr[0] = n;
+    sd[0] = 0.f;
+    while (sp > 0) {
+        sp--;
+        const uint32_t l = sl[sp], r = sr[sp];
+        if (!(sd[sp] < radius) || r <= l) continue;
+        const uint32_t m = (l + r) >> 1;
+        const float4 p = __ldg(node_pos + m);
+        const int2 aux = __ldg(node_aux + m);
+        const float dist = ref_dist(qx, qy, qz, p);
+        if (dist < radius && (sid == -1 || aux.x == sid)) {
+            visit(aux.y, dist);
+            cnt++;
+        }
+        if (r - l > 1) {
+            const uint32_t axis = __float_as_uint(p.w);
+            const float qa = axis == 0 ? qx : (axis == 1 ? qy : qz);
+            const float pa = axis == 0 ? p.x : (axis == 1 ? p.y : p.z);
+            const float diff = __fsub_rn(qa, pa);
+            const float pd = __fsqrt_rn(__fmul_rn(diff, diff));
+            uint32_t nl, nr, fl, fr;
+            if (qa < pa) {
+                nl = l, nr = m, fl = m + 1, fr = r;
+            } else {
+                nl = m + 1, nr = r, fl = l, fr = m;
+            }
+            if (sp + 2 <= 64) {
+                sl[sp] = fl, sr[sp] = fr, sd[sp] = pd, sp++;
+                sl[sp] = nl, sr[sp] = nr, sd[sp] = 0.f, sp++;
+            }
+        }
+    }
+    return cnt;
+}
+
+// Radius of the subsurface gather: th_photonSubsurfaceContributions' searchRadius (Scene.cu:802).
+constexpr float kSubsurfaceRadius = 0.3f;
+
+// impPaper_dipoleDiffusionAproximation (geometricMath.cu:455-490), one channel: the dipole
+// diffuse reflectance Rd at distance r with the reduced scattering coefficient (1 - g) sigma_s.
+__device__ __forceinline__ float dipole_rd(float r, float ss, float sa, float g, float eta)
+{
+    const float rs = (1 - g) * ss;
+    const float rt = rs + sa;
+    const float alpha = rs / rt;
+    const float tr = sqrtf(3 * sa * rt);
+    const float fdr = (-1.440f / (eta * eta)) + (0.710f / eta) + 0.668f + 0.0636f * eta;
+    const float A = (1 + fdr) / (1 - fdr);
+    const float zr = sqrtf(3 * (1 - alpha)) / tr;
+    const float zv = zr * A;
+    const float dr = sqrtf(r * r + zr * zr), dv = sqrtf(r * r + zv * zv);
+    const float trdr = tr * dr, trdv = tr * dv;
+    const float rd = (trdr + 1) * expf(-trdr) * zr / (dr * dr * dr) + (trdv + 1) * expf(-trdv) * zv / (dv * dv * dv);
+    const float c1 = zr * (tr + 1 / dr);
+    return c1 * rd * (1 - fdr) * alpha;
+}
+
+// Scene::combinePhotonsSubsurface (Scene.cu:667-701) at point p (shading normal nn, direction
+// to the camera wo_w) of an SSMaterial m: over the photons within `radius` on the same shape,
+// sum of power * kd * diffusionTermBSSRDF (geometricMath.cu:503-522:
+// Rd * (1 - F(cos_o)) * (1 - F(cos_i)) / pi) / (2 pi maxDist^2). With no photon the reference
+// divides 0 by 0 (a NaN sample, which the film drops); `compat` keeps that, otherwise 0.
+__device__ __forceinline__ V3 photon_subsurface(const float4 *__restrict__ node_pos,
+                                                const int2 *__restrict__ node_aux,
+                                                const rt_photon *__restrict__ photons, uint32_t n,
+                                                const rt_material &m, V3 p, V3 nn, V3 wo_w, int32_t sid, float radius,
+                                                bool compat)
+{
+    const float eta = m.ior, g = m.roughness[1];
+    const float cos_o = dot(nn, wo_w) / (length(nn) * length(wo_w));
+    const float ft_o = 1.f - fresnel_dielectric_ref(cos_o, 1.f, eta);
+    V3 sum = v3(0, 0, 0);
+    float maxd = 0.f;
+    const uint32_t cnt = radius_query(node_pos, node_aux, n, p.x, p.y, p.z, sid, radius, [&](int32_t idx, float) {
+        const rt_photon ph = photons[idx];
+        const V3 loc = v3(ph.pos[0], ph.pos[1], ph.pos[2]);
+        const float r = length(loc - p);
+        maxd = fmaxf(maxd, r);
+        const V3 pn = v3(ph.normal[0], ph.normal[1], ph.normal[2]);
+        const V3 wi = -v3(ph.dir[0], ph.dir[1], ph.dir[2]);
+        const float cos_i = dot(pn, wi) / (length(pn) * length(wi));
+        const float s = kInvPi * (1.f - fresnel_dielectric_ref(cos_i, 1.f, eta)) * ft_o;
+        const V3 rd = v3(dipole_rd(r, m.eta[0], m.extra[0], g, eta), dipole_rd(r, m.eta[1], m.extra[1], g, eta),
+                         dipole_rd(r, m.eta[2], m.extra[2], g, eta));
+        sum = sum + rd * s * v3(ph.power[0], ph.power[1], ph.power[2]) * v3(m.color[0], m.color[1], m.color[2]);
+    });
+    if (cnt == 0) return compat ? v3(NAN, NAN, NAN) : v3(0, 0, 0);
+    return sum * (1.f / (2.f * kPi * maxd * maxd));
+}
+
 }  // namespace rtb

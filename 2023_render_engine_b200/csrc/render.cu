@@ -56,7 +56,7 @@ struct Buffers {
     float4 *scontrib;  // rgb, target index bits (kRetireTarget: retire list)
     float4 *retire;    // L.xyz, pixel index bits
     float4 *gather;    // photon-map gather requests, 4 float4 each: p+shape, n+material, wo+target, beta
-    uint32_t cap, scap;
+    uint32_t cap, scap, gcap;
     // counters (uint32): [0],[1] queue sizes of buffers 0/1, [2] shadow count, [3] retire count,
     // [4] status, [5] shadow-kernel work counter, [6] gather requests; u64 at [8]: next sample,
     // [10] extension rays, [12] shadow rays
@@ -178,6 +178,22 @@ __device__ __forceinline__ void push_shadow(const Buffers &bf, V3 o, V3 d, float
     bf.scontrib[i] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(target));
 }
 
+constexpr uint32_t kGatherDensity = 0, kGatherSubsurface = 1;
+
+// Queues a photon-map gather at surface sf, weighted by `weight`, for the path whose radiance
+// lives at `target` (kRetireTarget: the retire list). Four float4: point + shape, normal +
+// material, direction to the previous vertex + target, weight + kind.
+__device__ __forceinline__ void push_gather(const Buffers &bf, const Surface &sf, V3 wo_w, V3 weight, uint32_t target,
+                                            uint32_t kind)
+{
+    const uint32_t gi = append(bf.cnt + 6);
+    if (gi >= bf.gcap) return;
+    bf.gather[4 * gi + 0] = make_float4(sf.p.x, sf.p.y, sf.p.z, __int_as_float(sf.shape));
+    bf.gather[4 * gi + 1] = make_float4(sf.n.x, sf.n.y, sf.n.z, __uint_as_float(sf.mat));
+    bf.gather[4 * gi + 2] = make_float4(wo_w.x, wo_w.y, wo_w.z, __uint_as_float(target));
+    bf.gather[4 * gi + 3] = make_float4(weight.x, weight.y, weight.z, __uint_as_float(kind));
+}
+
 struct PhotonView {
     const float4 *node_pos;
     const int2 *node_aux;
@@ -202,6 +218,8 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
     const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
     const bool nee_area = (rv.flags & RT_RENDER_NEE_AREA) != 0 && rv.nemit > 0;
     const bool photon_mode = (rv.flags & RT_RENDER_PHOTON_MAP) != 0;
+    const bool hybrid = (rv.flags & RT_RENDER_HYBRID) != 0;
+    const bool subsurface = (rv.flags & RT_RENDER_SUBSURFACE) != 0;
     float4 r0 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q];
     float4 r1 = reinterpret_cast<const float4 *>(bf.rays[cur])[2 * q + 1];
     float4 s0 = bf.st0[cur][q], s1 = bf.st1[cur][q];
@@ -234,7 +252,7 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
         onb(sf.n, t, bvec);
         V3 wo_w = -d;
         V3 wo = v3(dot(wo_w, t), dot(wo_w, bvec), dot(wo_w, sf.n));
-        const bool scattering = is_scattering(bs.type);
+        const bool scattering = is_scattering(bs);
         // where this path's radiance will live after this bounce: decided below, but shadow
         // rays need the target now, so reserve it first.
         // BSDF sample first (its outcome decides continue/retire), NEE uses beta before update.
@@ -316,13 +334,9 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
             // (Scene::getPhotonContributions, Scene.cu:822-840; finishStep, pathTracing.cu:85-89)
             finished = true;
             const uint32_t rt = kRetireTarget | append(bf.cnt + 3);
-            const uint32_t gi = append(bf.cnt + 6);
-            if (gi < bf.cap) {
-                bf.gather[4 * gi + 0] = make_float4(sf.p.x, sf.p.y, sf.p.z, __int_as_float(sf.shape));
-                bf.gather[4 * gi + 1] = make_float4(sf.n.x, sf.n.y, sf.n.z, __uint_as_float(sf.mat));
-                bf.gather[4 * gi + 2] = make_float4(wo_w.x, wo_w.y, wo_w.z, __uint_as_float(rt));
-                bf.gather[4 * gi + 3] = make_float4(beta_in.x, beta_in.y, beta_in.z, 0.f);
-            }
+            push_gather(bf, sf, wo_w, beta_in, rt, kGatherDensity);
+            if (subsurface && bs.type == RT_MAT_SUBSURFACE && (flags & kCameraRay))
+                push_gather(bf, sf, wo_w, beta_in, rt, kGatherSubsurface);
             bf.retire[rt & ~kRetireTarget] = make_float4(L.x, L.y, L.z, __uint_as_float(pix));
             regenerate(rv, bf, nxt);
             return;
@@ -347,12 +361,19 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
             next_d = wi_w;
             next_pdf = delta ? 0.f : pdf_b;
             next_flags = (depth + 1) | (delta ? kLastSpecular : 0u) |
-                         (((flags & kCameraRay) && is_specular(bs.type)) ? kCameraRay : 0u) | (rec << kRecShift);
+                         (((flags & kCameraRay) && is_specular(bs)) ? kCameraRay : 0u) | (rec << kRecShift);
         } else {
             target = kRetireTarget | append(bf.cnt + 3);
         }
-        // next-event estimation with beta before this bounce (pathTracing.cu:173-205)
+        // next-event estimation with beta before this bounce (pathTracing.cu:173-205). The
+        // direct-light term of a vertex (Scene::sampleDirectLight, Scene.cu:914-969) also holds
+        // the subsurface estimate at camera-ray hits and, in hybrid mode, the photon density,
+        // with the sum halved.
+        const float dscale = hybrid ? 0.5f : 1.0f;
         if (scattering) {
+            if (subsurface && bs.type == RT_MAT_SUBSURFACE && (flags & kCameraRay))
+                push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherSubsurface);
+            if (hybrid) push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherDensity);
             for (uint32_t li = 0; li < rv.nplights; li++) {  // Scene::estimateAllDirectLights, PointLight
                 float4 lp = rv.plights[2 * li], li4 = rv.plights[2 * li + 1];
                 V3 tol = v3(lp.x, lp.y, lp.z) - sf.p;
@@ -368,7 +389,7 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
                 V3 Li = v3(li4.x, li4.y, li4.z) * (1.0f / dist2);
                 if (is_black(fl) || is_black(Li)) continue;
                 float w = compat ? 1.0f / (1.0f + pb * pb) : 1.0f;  // powerHeuristic(1,1,1,pdf), Scene.cu:331
-                V3 c = beta_in * fl * Li * w;
+                V3 c = beta_in * fl * Li * (w * dscale);
                 V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
                 push_shadow(bf, so, wl, dist, c, target, compat, rec_in);
             }
@@ -408,7 +429,7 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
                              (1.f - alpha) * bsdf_sampling_pdf(bs, wo, wls);
                     if (!is_black(fl)) {
                         float w = (pl * pl) / (pl * pl + pb * pb);
-                        V3 c = beta_in * fl * Lel * (w / pl);
+                        V3 c = beta_in * fl * Lel * (w * dscale / pl);
                         V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
                         push_shadow(bf, so, wl, dist * (1.0f - 1e-4f), c, target, false, rec_in);
                     }
@@ -479,19 +500,31 @@ __global__ void __launch_bounds__(kB, RTB_TRAV_MIN_BLOCKS) k_shadow(RenderView r
 
 // Photon-map gathers queued by k_shade: the density estimate times the path throughput is
 // added to the finished path's radiance.
-__global__ void __launch_bounds__(kB) k_gather(RenderView rv, Buffers bf, PhotonView pv)
+// Photon-map gathers queued by k_shade: the density estimate (Scene::combinePhotonContributions,
+// zero on subsurface materials, Scene.cu:611-612) or the subsurface dipole estimate
+// (Scene::combinePhotonsSubsurface), times the request's weight, added to the path's radiance.
+__global__ void __launch_bounds__(kB) k_gather(RenderView rv, Buffers bf, PhotonView pv, int nxt)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = min(bf.cnt[6], bf.cap);
+    const uint32_t n = min(bf.cnt[6], bf.gcap);
     if (i >= n) return;
     const float4 a = bf.gather[4 * i], b = bf.gather[4 * i + 1], c = bf.gather[4 * i + 2], d = bf.gather[4 * i + 3];
     const rt_material &m = rv.mats[min(__float_as_uint(b.w), rv.nmats - 1)];
-    V3 e = photon_density(pv.node_pos, pv.node_aux, pv.photons, pv.n, load_bsdf(m), v3(a.x, a.y, a.z),
-                          v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), __float_as_int(a.w), pv.k, pv.radius,
-                          (rv.flags & RT_RENDER_COMPAT) != 0);
-    V3 contrib = v3(d.x, d.y, d.z) * e;
+    const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
+    const V3 p = v3(a.x, a.y, a.z), nn = v3(b.x, b.y, b.z), wo = v3(c.x, c.y, c.z);
+    V3 e;
+    if (__float_as_uint(d.w) == kGatherSubsurface)
+        e = photon_subsurface(pv.node_pos, pv.node_aux, pv.photons, pv.n, m, p, nn, wo, __float_as_int(a.w),
+                              kSubsurfaceRadius, compat);
+    else if (m.type == RT_MAT_SUBSURFACE)
+        e = v3(0, 0, 0);
+    else
+        e = photon_density(pv.node_pos, pv.node_aux, pv.photons, pv.n, load_bsdf(m), p, nn, wo, __float_as_int(a.w),
+                           pv.k, pv.radius, compat);
+    const V3 contrib = v3(d.x, d.y, d.z) * e;
     const uint32_t target = __float_as_uint(c.w);
-    float *dst = reinterpret_cast<float *>(bf.retire + (target & ~kRetireTarget));
+    float *dst = (target & kRetireTarget) ? reinterpret_cast<float *>(bf.retire + (target & ~kRetireTarget))
+                                          : reinterpret_cast<float *>(bf.st1[nxt] + target);
     atomicAdd(dst + 0, contrib.x);
     atomicAdd(dst + 1, contrib.y);
     atomicAdd(dst + 2, contrib.z);
@@ -599,7 +632,7 @@ int rt_scene_set_materials(rt_scene *s, const rt_material *table, uint32_t n)
 {
     if (!s || (!table && n)) return fail(RT_ERR_INVALID, "rt_scene_set_materials: null argument");
     for (uint32_t i = 0; i < n; i++)
-        if (table[i].type > RT_MAT_PLAIN) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_materials: unknown type");
+        if (table[i].type > RT_MAT_SUBSURFACE) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_materials: unknown type");
     s->materials.assign(table, table + n);
     s->render_dirty = true;
     return RT_OK;
@@ -802,17 +835,20 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     RTB_CHECK(rs.scontrib.reserve(16ull * scap));
     RTB_CHECK(rs.retire.reserve(16ull * cap));
     const bool photon_mode = (flags & RT_RENDER_PHOTON_MAP) != 0;
-    if (photon_mode) {
+    const bool gathers = (flags & (RT_RENDER_PHOTON_MAP | RT_RENDER_SUBSURFACE | RT_RENDER_HYBRID)) != 0;
+    // a path queues at most two gathers per wave (density, subsurface)
+    const uint32_t gcap = gathers ? 2 * cap : 0;
+    if (gathers) {
         if (!s->pmap || !s->pmap->built)
-            return fail(RT_ERR_STATE, name + ": RT_RENDER_PHOTON_MAP needs a built photon map (rt_render_set_photon_map)");
-        RTB_CHECK(rs.gather.reserve(64ull * cap));
+            return fail(RT_ERR_STATE, name + ": photon-map modes need a built photon map (rt_render_set_photon_map)");
+        RTB_CHECK(rs.gather.reserve(64ull * gcap));
     }
     const bool guided = (flags & RT_RENDER_GUIDE) != 0;
     GuideView gv{};
     rt_guide *guide = s->guide;
     if (guided) {
         if (!guide) return fail(RT_ERR_STATE, name + ": RT_RENDER_GUIDE needs a guide (rt_render_set_guide)");
-        if (photon_mode) return fail(RT_ERR_UNSUPPORTED, name + ": RT_RENDER_GUIDE with RT_RENDER_PHOTON_MAP");
+        if (gathers) return fail(RT_ERR_UNSUPPORTED, name + ": RT_RENDER_GUIDE with a photon-map mode");
         gv.enabled = 1;
         gv.train = s->guide_train;
         gv.max_depth = guide->opts.max_depth ? guide->opts.max_depth : 0xFFFFFFFFu;
@@ -851,7 +887,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     bf.retire = rs.retire.as<float4>();
     bf.gather = rs.gather.as<float4>();
     PhotonView pv{};
-    if (photon_mode) {
+    if (gathers) {
         pv.node_pos = s->pmap->node_pos.as<float4>();
         pv.node_aux = s->pmap->node_aux.as<int2>();
         pv.photons = s->pmap->photons.as<rt_photon>();
@@ -861,6 +897,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     }
     bf.cap = cap;
     bf.scap = scap;
+    bf.gcap = gcap;
     bf.cnt = rs.cnt.as<uint32_t>();
 
     RenderView rv{};
@@ -916,8 +953,8 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
             RTB_CUDA(cudaGetLastError());
             k_shadow<<<shadow_blocks, kB, 0, st>>>(rv, bf, cur ^ 1, gv);
             RTB_CUDA(cudaGetLastError());
-            if (photon_mode) {
-                k_gather<<<blocks, kB, 0, st>>>(rv, bf, pv);
+            if (gathers) {
+                k_gather<<<(gcap + kB - 1) / kB, kB, 0, st>>>(rv, bf, pv, cur ^ 1);
                 RTB_CUDA(cudaGetLastError());
             }
             k_retire<<<blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64, gv);

@@ -157,16 +157,38 @@ __device__ __forceinline__ Bsdf load_bsdf(const rt_material &m)
     b.eta = v3(m.eta[0], m.eta[1], m.eta[2]);
     b.k = v3(m.k[0], m.k[1], m.k[2]);
     b.ior = m.ior;
+    if (b.type == RT_MAT_PHONG || b.type == RT_MAT_SUBSURFACE) b.g.ax = m.roughness[0];  // ns, as given
     return b;
 }
 
-__device__ __forceinline__ bool is_scattering(uint32_t type)
+// Phong and subsurface surfaces keep ks in Bsdf::k and the exponent ns in g.ax.
+__device__ __forceinline__ bool is_phong(uint32_t type) { return type == RT_MAT_PHONG || type == RT_MAT_SUBSURFACE; }
+
+// Material::isScattering: PhongMaterial / SSMaterial scatter when kd is not black
+// (PhongMaterial.cu:45-48, SSMaterial.cu:55-58).
+__device__ __forceinline__ bool is_scattering(const Bsdf &b)
 {
-    return type == RT_MAT_LAMBERTIAN || type == RT_MAT_TROWBRIDGE || type == RT_MAT_PLAIN;
+    if (is_phong(b.type)) return fmaxf(b.color.x, fmaxf(b.color.y, b.color.z)) > 0.f;
+    return b.type == RT_MAT_LAMBERTIAN || b.type == RT_MAT_TROWBRIDGE || b.type == RT_MAT_PLAIN;
 }
-__device__ __forceinline__ bool is_specular(uint32_t type)
+__device__ __forceinline__ bool is_specular(const Bsdf &b)
 {
-    return type == RT_MAT_TROWBRIDGE || type == RT_MAT_DIELECTRIC;  // Material::isSpecular overrides
+    // Material::isSpecular overrides; PhongMaterial: ks not black (PhongMaterial.cu:55-58)
+    if (b.type == RT_MAT_PHONG) return fmaxf(b.k.x, fmaxf(b.k.y, b.k.z)) > 0.f;
+    return b.type == RT_MAT_TROWBRIDGE || b.type == RT_MAT_DIELECTRIC;
+}
+
+// PhongMaterial::lightReflected (PhongMaterial.cu:70-88): the Lambertian term plus
+// ks * max(0, cos(wo, mirror of wi))^ns when wi is above the surface (not weighted by cos).
+__device__ __forceinline__ V3 phong_eval(const Bsdf &b, V3 wo, V3 wi)
+{
+    V3 f = b.color * (kInvPi * abs_cos(wi));
+    if (wi.z / length(wi) > 0.f) {
+        const V3 r = v3(-wi.x, -wi.y, wi.z);
+        const float c = dot(wo, r) / (length(wo) * length(r));
+        f = f + b.k * powf(fmaxf(0.f, c), b.g.ax);
+    }
+    return f;
 }
 
 // f * |cos wi| and pdf, shading space.
@@ -177,6 +199,10 @@ __device__ __forceinline__ V3 bsdf_eval(const Bsdf &b, V3 wo, V3 wi, float &pdf)
     case RT_MAT_LAMBERTIAN:  // LambertianBSDF.cu:32-47
         pdf = (wo.z * wi.z > 0) ? fabsf(wi.z) * kInvPi : 0.f;
         return b.color * (kInvPi * abs_cos(wi));
+    case RT_MAT_PHONG:
+    case RT_MAT_SUBSURFACE:  // PhongMaterial::pdf: cosine(wi) / pi on wo's side (PhongMaterial.cu:94-100)
+        pdf = (wo.z * wi.z > 0) ? wi.z / length(wi) * kInvPi : 0.f;
+        return phong_eval(b, wo, wi);
     case RT_MAT_TROWBRIDGE:
         pdf = ggx_pdf(b.g, wo, wi);
         return ggx_eval(b.g, b.color, b.eta, b.k, wo, wi);
@@ -259,6 +285,14 @@ __device__ __forceinline__ V3 bsdf_sample(const Bsdf &b, V3 wo, Pcg &r, bool com
         float ct = sqrtf(fmaxf(0.f, 1 - s2t));
         wi = (-wo) * eta + n * (eta * co - ct);
         return b.color;
+    }
+    case RT_MAT_PHONG:
+    case RT_MAT_SUBSURFACE: {  // PhongMaterial::sampleDirection (PhongMaterial.cu:102-118)
+        float u1 = pcg_float(r), u2 = pcg_float(r);
+        wi = cosine_hemisphere(u1, u2);
+        pdf = wi.z / length(wi) * kInvPi;
+        if (!(pdf > 0)) return v3(0, 0, 0);
+        return phong_eval(b, wo, wi) * (1.0f / pdf);
     }
     case RT_MAT_MIRROR:  // PerfectReflectionBSDF
         delta = true;

@@ -168,7 +168,11 @@ typedef enum rt_material_type {
     RT_MAT_DIELECTRIC = 2, /* DielectricMaterial / GlassMaterial (DielectricMaterial.cu:12-83) */
     RT_MAT_LIGHT = 3,      /* LightMaterial: emitter, no scattering (LightMaterial.cu:10-60) */
     RT_MAT_MIRROR = 4,     /* perfect specular reflector (MirrorMaterial.cu) */
-    RT_MAT_PLAIN = 5       /* PlainMaterial: returns its colour on camera hits only */
+    RT_MAT_PLAIN = 5,      /* PlainMaterial: returns its colour on camera hits only */
+    RT_MAT_PHONG = 6,      /* PhongMaterial (PhongMaterial.cu): color = kd, k = ks, roughness[0] = ns */
+    RT_MAT_SUBSURFACE = 7  /* SSMaterial (SSMaterial.cu): a Phong surface (color = kd, k = ks, roughness[0] = ns)
+                              over a medium for the dipole photon estimate: ior = eta, eta = sigma_s,
+                              extra = sigma_a, roughness[1] = g (phase asymmetry) */
 } rt_material_type;
 
 #define RT_MATF_TRANSPARENT 0x1u /* ignored by shadow rays (Material::isTransparent) */
@@ -181,7 +185,7 @@ typedef struct rt_material {
     float eta[3], k[3];   /* conductor Fresnel (Trowbridge) */
     float roughness[2];   /* Trowbridge roughness x/y; alpha = sqrt(roughness) */
     float ior;            /* Dielectric index of refraction (Glass: 1.5) */
-    float pad[3];
+    float extra[3];       /* RT_MAT_SUBSURFACE: sigma_a */
 } rt_material;
 
 /* Replaces the Material* each Shape/Triangle points to (Triangle::setMaterial,
@@ -211,6 +215,12 @@ typedef struct rt_camera {
 #define RT_RENDER_COMPAT 0x2u   /* reference estimator quirks (delta-light MIS weight, 0.7/0.3 glass lobes
                                    without pdf, reference Fresnel); off = physically consistent */
 #define RT_RENDER_EXACT_TRACE 0x4u /* reference-exact closest-hit ids for extension rays */
+#define RT_RENDER_SUBSURFACE 0x20u /* CHECK_SUBSURFACE_SCATTERING: at camera-ray hits on RT_MAT_SUBSURFACE add
+                                      the dipole photon estimate (rt_photon_subsurface, radius 0.3);
+                                      needs the photon map of rt_render_set_photon_map */
+#define RT_RENDER_HYBRID 0x40u     /* RENDER_MODE HYBRID (Scene.cu:914-969): at every scattering vertex the
+                                      direct-light term is (photon density + next-event estimate) / 2 and
+                                      the path continues; needs the photon map */
 #define RT_RENDER_PHOTON_MAP 0x8u  /* photon-mapping mode (RENDER_MODE PHOTON_MAPPING): at the first
                                       scattering hit the photon density estimate replaces the rest
                                       of the path; needs rt_render_set_photon_map */
@@ -318,6 +328,15 @@ RT_API int rt_photon_map_destroy(rt_photon_map *map);
 RT_API int rt_photon_density(rt_photon_map *map, const rt_material *mat, const float *points_dev,
                              const float *normals_dev, const float *wo_dev, const int32_t *shape_ids_dev, uint64_t nq,
                              uint32_t k, float radius, float *out_rgb_dev);
+
+/* Scene::combinePhotonsSubsurface (Scene.cu:667-701) at nq points of an RT_MAT_SUBSURFACE
+ * material: over all photons within `radius` on the point's shape (0.3 in the reference,
+ * Scene.cu:802), sum of power * kd * diffusionTermBSSRDF / (2 pi maxDist^2). wo points to the
+ * camera. With no photon in range: NaN with RT_RENDER_COMPAT in flags (the reference's 0 / 0),
+ * otherwise 0. Device buffers, out_rgb 3 floats per point. */
+RT_API int rt_photon_subsurface(rt_photon_map *map, const rt_material *material, const float *points_dev,
+                                const float *normals_dev, const float *wo_dev, const int32_t *shape_ids_dev,
+                                uint64_t nq, float radius, uint32_t flags, float *out_rgb_dev);
 
 /* Photon map used by rt_render in RT_RENDER_PHOTON_MAP mode, with the gather size and radius
  * (the reference's MAX_NEIGHBOURS and PHOTON_SEARCH_RADIUS, types.h:57-60). NULL detaches. */

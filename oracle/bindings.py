@@ -240,6 +240,43 @@ class Restated:
         return idx, dist, cnt
 
 
+def restated_phong_eval(restated, material, wo, wi):
+    """The CPU restatement's Phong BSDF (f * |cos|, pdf) for pairs of shading-space directions."""
+    import importlib
+
+    N = importlib.import_module("2023_render_engine_b200._native")
+    L = restated.L
+    L.pto_phong_eval.argtypes = [ctypes.POINTER(N.Material), P, P, U32, P, P]
+    a, b = _np(wo, np.float32).reshape(-1, 3), _np(wi, np.float32).reshape(-1, 3)
+    f = np.zeros((a.shape[0], 3), np.float32)
+    pdf = np.zeros(a.shape[0], np.float32)
+    L.pto_phong_eval(ctypes.byref(material), a.ctypes.data, b.ctypes.data, a.shape[0], f.ctypes.data, pdf.ctypes.data)
+    return f, pdf
+
+
+def ref_phong_eval(refo, kd, ks, ns, wo, wi):
+    """The reference's PhongMaterial::lightReflected / pdf."""
+    L = refo.L
+    L.refo_phong_eval.argtypes = [P, P, ctypes.c_float, P, P, U32, P, P]
+    a, b = _np(wo, np.float32).reshape(-1, 3), _np(wi, np.float32).reshape(-1, 3)
+    kd_, ks_ = _np(kd, np.float32), _np(ks, np.float32)
+    f = np.zeros((a.shape[0], 3), np.float32)
+    pdf = np.zeros(a.shape[0], np.float32)
+    L.refo_phong_eval(kd_.ctypes.data, ks_.ctypes.data, ns, a.ctypes.data, b.ctypes.data, a.shape[0], f.ctypes.data,
+                      pdf.ctypes.data)
+    return f, pdf
+
+
+def ref_diffusion_term(refo, cam_p, cam_dir, cam_n, ph_loc, ph_dir, ph_n, sigma_s, sigma_a, g, eta):
+    """The reference's diffusionTermBSSRDF (geometricMath.cu:500-522) for one photon (rgb)."""
+    L = refo.L
+    L.refo_diffusion_term.argtypes = [P, P, P, P, P, P, P, P, ctypes.c_float, ctypes.c_float, P]
+    args = [_np(x, np.float32) for x in (cam_p, cam_dir, cam_n, ph_loc, ph_dir, ph_n, sigma_s, sigma_a)]
+    out = np.zeros(3, np.float64)
+    L.refo_diffusion_term(*[a.ctypes.data for a in args], g, eta, out.ctypes.data)
+    return out
+
+
 class RestatedBvh:
     def __init__(self, o: Restated, h, ntri):
         self.o, self.h, self.ntri = o, h, ntri

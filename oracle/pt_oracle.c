@@ -22,7 +22,7 @@
 #define PI_F 3.14159265358979323846f
 #define INV_PI_F 0.31830988618379067154f
 
-enum { M_LAMB = 0, M_GGX = 1, M_DIEL = 2, M_LIGHT = 3, M_MIRROR = 4, M_PLAIN = 5 };
+enum { M_LAMB = 0, M_GGX = 1, M_DIEL = 2, M_LIGHT = 3, M_MIRROR = 4, M_PLAIN = 5, M_PHONG = 6, M_SSS = 7 };
 enum { F_NEE_AREA = 1, F_COMPAT = 2 };
 
 typedef struct {
@@ -314,8 +314,19 @@ typedef struct {
     uint32_t pix_begin, pix_end;
 } ctx_t;
 
-static int is_scat(uint32_t t) { return t == M_LAMB || t == M_GGX || t == M_PLAIN; }
-static int is_spec(uint32_t t) { return t == M_GGX || t == M_DIEL; }
+static float maxc3(const float *c) { return fmaxf(c[0], fmaxf(c[1], c[2])); }
+/* Material::isScattering / isSpecular; Phong and subsurface: kd, ks not black
+ * (PhongMaterial.cu:45-58, SSMaterial.cu:55-58) */
+static int is_scat(const pto_material *m)
+{
+    if (m->type == M_PHONG || m->type == M_SSS) return maxc3(m->color) > 0.f;
+    return m->type == M_LAMB || m->type == M_GGX || m->type == M_PLAIN;
+}
+static int is_spec(const pto_material *m)
+{
+    if (m->type == M_PHONG) return maxc3(m->k) > 0.f;
+    return m->type == M_GGX || m->type == M_DIEL;
+}
 
 /* closest hit: triangles (reference order) then spheres (Scene::intersects, Scene.cu:108-150) */
 static int32_t closest(const ctx_t *c, v3 o, v3 d, float tmax, int shadow, float *t, float *b1, float *b2)
@@ -365,9 +376,26 @@ static v3 xvec(const float *m, v3 v)
 
 static v3 mat_color(const pto_material *m) { return V(m->color[0], m->color[1], m->color[2]); }
 
+/* PhongMaterial::lightReflected (PhongMaterial.cu:70-88): Lambertian term plus
+ * ks * max(0, cos(wo, mirror of wi))^ns when wi is above the surface */
+static v3 phong_eval(const pto_material *m, v3 wo, v3 wi)
+{
+    v3 f = mul(mat_color(m), INV_PI_F * acos1(wi));
+    if (wi.z / len3(wi) > 0.f) {
+        v3 r = V(-wi.x, -wi.y, wi.z);
+        float c = dot3(wo, r) / (len3(wo) * len3(r));
+        f = add(f, mul(V(m->k[0], m->k[1], m->k[2]), powf(fmaxf(0.f, c), m->roughness[0])));
+    }
+    return f;
+}
+
 static v3 bsdf_eval(const pto_material *m, v3 wo, v3 wi, float *pdf)
 {
     *pdf = 0.f;
+    if (m->type == M_PHONG || m->type == M_SSS) { /* PhongMaterial::pdf: cosine(wi) / pi */
+        *pdf = (wo.z * wi.z > 0) ? wi.z / len3(wi) * INV_PI_F : 0.f;
+        return phong_eval(m, wo, wi);
+    }
     if (m->type == M_LAMB) {
         *pdf = (wo.z * wi.z > 0) ? fabsf(wi.z) * INV_PI_F : 0.f;
         return mul(mat_color(m), INV_PI_F * acos1(wi));
@@ -456,6 +484,14 @@ static v3 bsdf_sample(const pto_material *m, v3 wo, pcg *r, int compat, v3 *wi, 
         *wi = add(mul(neg(wo), eta), mul(n, eta * co - ct));
         return col;
     }
+    case M_PHONG:
+    case M_SSS: { /* PhongMaterial::sampleDirection (PhongMaterial.cu:102-118) */
+        float u1 = pcg_f(r), u2 = pcg_f(r);
+        *wi = cos_hemi(u1, u2);
+        *pdf = wi->z / len3(*wi) * INV_PI_F;
+        if (!(*pdf > 0)) return V(0, 0, 0);
+        return mul(phong_eval(m, wo, *wi), 1.0f / *pdf);
+    }
     case M_MIRROR:
         *delta = 1;
         *wi = V(-wo.x, -wo.y, wo.z);
@@ -536,7 +572,7 @@ static v3 trace_sample(const ctx_t *c, uint32_t pix, uint32_t j)
         onb(n, &tt, &bb);
         v3 wow = neg(d);
         v3 wo = V(dot3(wow, tt), dot3(wow, bb), dot3(wow, n));
-        int scat = is_scat(m->type);
+        int scat = is_scat(m);
         v3 beta_in = beta;
         v3 Le = V(0, 0, 0);
         if (m->type == M_LIGHT)
@@ -630,7 +666,7 @@ static v3 trace_sample(const ctx_t *c, uint32_t pix, uint32_t j)
         d = wiw;
         last_pdf = delta ? 0.f : pdfb;
         last_spec = delta;
-        camera = camera && is_spec(m->type);
+        camera = camera && is_spec(m);
     }
     return L;
 }
@@ -808,7 +844,7 @@ uint64_t pto_trace_photons(const rto_bvh *bvh, const uint32_t *tri_mat, const in
             }
             if (mid >= nmat) mid = nmat - 1;
             const pto_material *m = &mats[mid];
-            if (is_scat(m->type)) {
+            if (is_scat(m)) {
                 if (stored < cap) {
                     float *ph = out + 16 * stored;
                     v3 pw = vmul(carry, beta);
@@ -836,7 +872,7 @@ uint64_t pto_trace_photons(const rto_bvh *bvh, const uint32_t *tri_mat, const in
             carry = add(carry, vmul(beta, Le));
             beta = vmul(beta, f);
             int finished = black(f);
-            if (!finished && is_scat(m->type) && depth > rr_depth) {
+            if (!finished && is_scat(m) && depth > rr_depth) {
                 float q = fmaxf(0.05f, 1.f - lum(beta));
                 if (pcg_f(&r) < q)
                     finished = 1;
@@ -853,4 +889,18 @@ uint64_t pto_trace_photons(const rto_bvh *bvh, const uint32_t *tri_mat, const in
     free(sel);
     free(perl);
     return stored;
+}
+
+
+/* The Phong BSDF of the estimator (eval and pdf) for n shading-space direction pairs. */
+void pto_phong_eval(const pto_material *m, const float *wo, const float *wi, uint32_t n, float *out_f, float *out_pdf)
+{
+    for (uint32_t i = 0; i < n; i++) {
+        float pdf;
+        v3 f = bsdf_eval(m, V(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), V(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), &pdf);
+        out_f[3 * i] = f.x;
+        out_f[3 * i + 1] = f.y;
+        out_f[3 * i + 2] = f.z;
+        out_pdf[i] = pdf;
+    }
 }

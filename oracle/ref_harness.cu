@@ -59,6 +59,7 @@
 #include "cuda_libraries/kdtree.h"
 #include "materials/LambertianMaterial.cu"
 #include "materials/GlassMaterial.cu"
+#include "materials/PhongMaterial.cu"
 #undef swap
 
 #define REFO_API extern "C" __attribute__((visibility("default")))
@@ -343,3 +344,39 @@ REFO_API void refo_kdtree_knn(void *h, const float *q, const int32_t *qShape, ui
 }
 
 REFO_API int refo_version() { return 1; }
+
+
+// diffusionTermBSSRDF (cuda_libraries/geometricMath.cu:500-522) for one photon: out = Sd (rgb).
+// camera: point, direction to the camera, shading normal; photon: location, incoming ray
+// direction, surface normal.
+REFO_API void refo_diffusion_term(const float *cam_p, const float *cam_dir, const float *cam_n, const float *ph_loc,
+                                  const float *ph_dir, const float *ph_n, const float *sigma_s, const float *sigma_a,
+                                  float g, float eta, double *out)
+{
+    Photon ph(Ray(Point3f(ph_loc[0], ph_loc[1], ph_loc[2]), Vector3f(ph_dir[0], ph_dir[1], ph_dir[2])),
+              Point3f(ph_loc[0], ph_loc[1], ph_loc[2]), Vector3f(ph_n[0], ph_n[1], ph_n[2]), Spectrum(1), 0,
+              Point2f(0, 0));
+    Spectrum s = diffusionTermBSSRDF(Point3f(cam_p[0], cam_p[1], cam_p[2]), Vector3f(cam_dir[0], cam_dir[1], cam_dir[2]),
+                                     Vector3f(cam_n[0], cam_n[1], cam_n[2]), ph,
+                                     Spectrum(sigma_s[0], sigma_s[1], sigma_s[2]),
+                                     Spectrum(sigma_a[0], sigma_a[1], sigma_a[2]), g, eta);
+    out[0] = s.getR();
+    out[1] = s.getG();
+    out[2] = s.getB();
+}
+
+// PhongMaterial::lightReflected and ::pdf (materials/PhongMaterial.cu:70-100) in shading space
+// for n direction pairs: out_f 3 floats per pair, out_pdf 1.
+REFO_API void refo_phong_eval(const float *kd, const float *ks, float ns, const float *wo, const float *wi, uint32_t n,
+                              float *out_f, float *out_pdf)
+{
+    PhongMaterial m(Spectrum(0), Spectrum(kd[0], kd[1], kd[2]), Spectrum(ks[0], ks[1], ks[2]), Spectrum(0), 1.5f, ns);
+    for (uint32_t i = 0; i < n; i++) {
+        Vector3f o(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), w(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        Spectrum f = m.lightReflected(o, w, Point2f(0, 0));
+        out_f[3 * i] = (float)f.getR();
+        out_f[3 * i + 1] = (float)f.getG();
+        out_f[3 * i + 2] = (float)f.getB();
+        out_pdf[i] = m.pdf(o, w);
+    }
+}

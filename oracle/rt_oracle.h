@@ -56,7 +56,7 @@ typedef struct pto_material { /* same layout as rt_material in include/rt_b200.h
     float eta[3], k[3];
     float roughness[2];
     float ior;
-    float pad[3];
+    float extra[3];
 } pto_material;
 
 typedef struct pto_sphere {
@@ -75,6 +75,9 @@ typedef struct pto_camera { /* same layout as rt_camera */
 
 /* Renders pixels [pix_begin, pix_end) with spp samples each into sum (3 doubles per
  * pixel, indexed by pixel) and count; flags: 1 = area-light NEE, 2 = reference quirks. */
+/* The estimator's Phong BSDF (f * |cos|, pdf) for n shading-space pairs (tests). */
+void pto_phong_eval(const pto_material *m, const float *wo, const float *wi, uint32_t n, float *out_f, float *out_pdf);
+
 int pto_render(const rto_bvh *bvh, const uint32_t *tri_mat, const pto_sphere *sph, uint32_t nsph,
                const pto_material *mats, uint32_t nmat, const float *plights, uint32_t npl, const pto_camera *cam,
                uint32_t spp, uint32_t sample_offset, uint32_t max_depth, uint32_t rr_depth, uint32_t seed,
