@@ -189,7 +189,9 @@ class Scene:
         st = N.PhotonTraceStats()
         N.check(N.lib().rt_photons_trace(self.handle, n, max_depth, rr_depth, seed, flags, ctypes.byref(h),
                                          ctypes.byref(st)))
-        return PhotonMap(h, owner=self), {f: getattr(st, f) for f, _ in N.PhotonTraceStats._fields_}
+        # the map keeps the context alive, not the scene: a scene holding its photon map
+        # (set_photon_map) would otherwise form a cycle whose finalisation order is arbitrary
+        return PhotonMap(h, owner=self.ctx), {f: getattr(st, f) for f, _ in N.PhotonTraceStats._fields_}
 
     def close(self):
         if self.handle:
