@@ -114,6 +114,22 @@ inline bool to_rt_material(const Material *m, rt_material &o)
     } else if (const auto *p = dynamic_cast<const PlainMaterial *>(m)) {
         o.type = RT_MAT_PLAIN;
         rgb(p->kd, o.color);
+    } else if (const auto *ss = dynamic_cast<const SSMaterial *>(m)) {
+        // Phong surface (SSMaterial.cu:29) over the dipole medium
+        o.type = RT_MAT_SUBSURFACE;
+        rgb(ss->kd, o.color);
+        rgb(ss->surfaceMaterial.ks, o.k);
+        o.roughness[0] = (float)ss->surfaceMaterial.ns;
+        o.roughness[1] = (float)ss->g;
+        o.ior = (float)ss->eta;
+        rgb(ss->sigmaS, o.eta);
+        rgb(ss->sigmaA, o.extra);
+    } else if (const auto *ph = dynamic_cast<const PhongMaterial *>(m)) {
+        if (ph->ke.maxComponent() > 0) return false;  // emissive Phong: not implemented by the core
+        o.type = RT_MAT_PHONG;
+        rgb(ph->kd, o.color);
+        rgb(ph->ks, o.k);
+        o.roughness[0] = (float)ph->ns;
     } else {
         return false;
     }
@@ -189,7 +205,8 @@ public:
 
     // generatePhotons (photonDispersion.cu:175-192) + Scene::buildPhotonStructures: traces
     // nPhotons from the point lights and builds the kd-tree gather structure.
-    void generatePhotons(uint64_t nPhotons, uint32_t maxDepth, uint32_t seed = 0, bool compat = true)
+    void generatePhotons(uint64_t nPhotons, uint32_t maxDepth, uint32_t seed = 0, bool compat = true,
+                         uint32_t k = 100, float radius = 100.f)
     {
         if (pmap_) {
             rt_photon_map_destroy(pmap_);
@@ -198,6 +215,7 @@ public:
         rt_photon_trace_stats st;
         check(rt_photons_trace(scene_, nPhotons, maxDepth, 3, seed, compat ? RT_RENDER_COMPAT : 0u, &pmap_, &st));
         check(rt_photon_map_build(pmap_));
+        check(rt_render_set_photon_map(scene_, pmap_, k, radius));  // MAX_NEIGHBOURS, PHOTON_SEARCH_RADIUS
         photons_.resize(0);
     }
 
@@ -365,6 +383,18 @@ private:
     std::vector<Shape *> shapes_;
     mutable std::vector<rt_photon> photons_;
 };
+
+// The estimator flags of the reference's compile-time configuration (types.h): its quirks,
+// CHECK_SUBSURFACE_SCATTERING and RENDER_MODE (PHOTON_MAPPING and HYBRID need the photon map of
+// Scene::generatePhotons).
+inline uint32_t reference_flags()
+{
+    uint32_t f = RT_RENDER_COMPAT;
+    if (CHECK_SUBSURFACE_SCATTERING) f |= RT_RENDER_SUBSURFACE;
+    if (RENDER_MODE == PHOTON_MAPPING) f |= RT_RENDER_PHOTON_MAP;
+    if (RENDER_MODE == HYBRID) f |= RT_RENDER_HYBRID;
+    return f;
+}
 
 // PathTracerIntegrator (PathTracerIntegrator.cu:140-210): renders the camera's film with
 // SAMPLES_PER_PIXEL samples and MAX_RAY_RECURSION_DEPTH bounces (the reference's compile-time

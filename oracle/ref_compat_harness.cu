@@ -70,6 +70,7 @@
 #include "materials/SSMaterial.cu"
 #include "materials/PlasticUnrealMaterial.cu"
 #include "materials/PlainMaterial.cu"
+#include "materials/PhongMaterial.cu"
 #include "textures/Texture.cu"
 #include "textures/SphericalTexture.cu"
 #include "cuda_libraries/FileImporting.cu"
