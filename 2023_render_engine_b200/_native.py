@@ -66,7 +66,8 @@ class View(ctypes.Structure):
 
 class RenderStats(ctypes.Structure):
     _fields_ = [("camera_rays", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64),
-                ("shadow_rays", ctypes.c_uint64), ("waves", ctypes.c_uint64), ("ms", ctypes.c_double)]
+                ("shadow_rays", ctypes.c_uint64), ("waves", ctypes.c_uint64), ("ms", ctypes.c_double),
+                ("gathers", ctypes.c_uint64)]
 
 
 RT_MAT_LAMBERTIAN, RT_MAT_TROWBRIDGE, RT_MAT_DIELECTRIC, RT_MAT_LIGHT, RT_MAT_MIRROR, RT_MAT_PLAIN = range(6)

@@ -8,6 +8,11 @@ materials and cameras per the configuration descriptions).
 * config1: BVH stress — the 1.31M-triangle displaced icosphere (GGX, F0 = 0.04 i.e.
   eta = 1.5, k = 0, roughness uniform in [0.05, 0.5] per block of 64 triangles) in the
   Cornell box; 1920x1080, 64 spp, max depth 12, NEE on the area light.
+* config2: the guiding room; config3: 64 seeded views of configs 0-2.
+* config4: photon mapping + subsurface scattering at 4K — the 2M-triangle displaced terrain,
+  16 glass spheres (IOR 1.5, radius 0.1-0.4), a subsurface slab (sigma_a = (0.01, 0.02, 0.05),
+  sigma_s = (1.0, 0.8, 0.6), g = 0), two point lights of 50 RGB; 10M photons, k = 50
+  nearest-photon gathers; 3840x2160, 256 spp, max depth 16.
 """
 from __future__ import annotations
 
@@ -143,3 +148,39 @@ def build_config3(ctx, n_views=64, seed=5):
                 random_views(rng, int(counts[2]), (-1.7, 0.4, -1.7), (1.7, 2.2, 0.8), (-1.9, 0.0, -1.9),
                              (1.9, 1.5, 0.5))))
     return out
+
+
+# Config 4 photon map and render modes: photons traced per map, the gather size, and the
+# render flags — RENDER_MODE HYBRID (at each scattering vertex the direct term is the mean of
+# the photon density and point-light NEE, and the path continues, so the guide has bounces to
+# sample) with CHECK_SUBSURFACE_SCATTERING (the dipole estimate at camera hits on the slab).
+CONFIG4_PHOTONS = 10_000_000
+CONFIG4_K = 50
+CONFIG4_FLAGS = N.RT_RENDER_HYBRID | N.RT_RENDER_SUBSURFACE
+
+
+def build_config4(ctx, width=3840, height=2160, seed=11, n=1000):
+    """Config 4 scene: terrain (Lambertian 0.6/0.55/0.45, shape 0), the slab (SSMaterial,
+    shape 1), 16 glass spheres (shapes 100-115), point lights of 50 RGB at (-1.6, 2.6, 1.4)
+    and (1.8, 3.2, -1.2); camera at (0, 2.4, 5.6) looking at (0, -0.1, 0), 45 degrees."""
+    (tv, tf), (sv, sf), spheres = scenes.photon_terrain(seed=seed, n=n)
+    mats = [core.material(N.RT_MAT_LAMBERTIAN, color=(0.6, 0.55, 0.45)),
+            core.material(N.RT_MAT_DIELECTRIC, color=(1, 1, 1), ior=1.5, transparent=True),
+            core.subsurface_material(kd=(0.9, 0.9, 0.9), ks=(0.04, 0.04, 0.04), ns=40.0, eta=1.3,
+                                     sigma_s=(1.0, 0.8, 0.6), sigma_a=(0.01, 0.02, 0.05), g=0.0)]
+    sc = core.Scene(ctx)
+    sc.set_materials(mats)
+    sc.add_mesh(tv, tf, material=0, shape_id=0)
+    sc.add_mesh(sv, sf, material=2, shape_id=1)
+    for j, (c, r) in enumerate(spheres):
+        o2w, w2o = scenes.sphere_matrices(c, r)
+        sc.add_sphere(o2w, w2o, r, material=1, shape_id=100 + j, transparent=True)
+    sc.add_point_light((-1.6, 2.6, 1.4), (1.0, 1.0, 1.0), 50.0)
+    sc.add_point_light((1.8, 3.2, -1.2), (1.0, 1.0, 1.0), 50.0)
+    sc.commit()
+    cam = core.look_at_camera((0.0, 2.4, 5.6), (0.0, -0.1, 0.0), (0, 1, 0), 45.0, width, height)
+    return sc, cam, dict(spp=256, max_depth=16, rr_depth=3)
+
+
+# The config-4 guide covers the terrain's bounding box (the slab and spheres lie inside it).
+CONFIG4_GUIDE = dict(GUIDE_TRAINING, bbox_min=(-4.01, -0.41, -4.01), bbox_max=(4.01, 1.21, 4.01))

@@ -208,42 +208,69 @@ __global__ void __launch_bounds__(128) k_knn(const float4 *__restrict__ node_pos
     out_count[qi] = cnt;
 }
 
+// One warp per query (the render's gather kernel uses the same warp functions).
+constexpr int kQueryBlock = 128;
+
+// The photons' shading attributes in tree-slot order, so that a query reads them with the
+// positions it scans: power and cos(normal, -direction) (the photon's factor of
+// diffusionTermBSSRDF, geometricMath.cu:503-522), and the arrival direction.
+__global__ void k_tree_attrs(const int2 *__restrict__ node_aux, const rt_photon *__restrict__ photons, uint64_t n,
+                             float4 *__restrict__ pw, float4 *__restrict__ dir)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const rt_photon ph = photons[node_aux[i].y];
+    const V3 pn = v3(ph.normal[0], ph.normal[1], ph.normal[2]);
+    const V3 wi = -v3(ph.dir[0], ph.dir[1], ph.dir[2]);
+    const float cos_i = dot(pn, wi) / (length(pn) * length(wi));
+    pw[i] = make_float4(ph.power[0], ph.power[1], ph.power[2], cos_i);
+    dir[i] = make_float4(ph.dir[0], ph.dir[1], ph.dir[2], 0.f);
+}
+
+
 // Scene::combinePhotonContributions (Scene.cu:607-635) per query: the k nearest photons on
 // the same shape within radius, sum of power * lightScattered(-photon direction), divided by
 // pi * (largest neighbour distance)^2.
-__global__ void __launch_bounds__(128) k_density(const float4 *__restrict__ node_pos, const int2 *__restrict__ node_aux,
-                                                 const rt_photon *__restrict__ photons, uint32_t n, rt_material mat,
-                                                 const float *__restrict__ pts, const float *__restrict__ nrm,
-                                                 const float *__restrict__ wo, const int32_t *__restrict__ shape,
-                                                 uint64_t nq, uint32_t k, float radius, float *__restrict__ out)
+__global__ void __launch_bounds__(kQueryBlock) k_density(PhotonTree tree, rt_material mat, const float *__restrict__ pts,
+                                                         const float *__restrict__ nrm, const float *__restrict__ wo,
+                                                         const int32_t *__restrict__ shape, uint64_t nq, uint32_t k,
+                                                         float radius, float *__restrict__ out)
 {
-    const uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (qi >= nq) return;
+    __shared__ PhotonWarpScratch scratch[kQueryBlock / 32];
+    const uint64_t qi = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (qi >= nq) return;  // warp-uniform
     V3 p = v3(pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]);
     V3 nn = normalize(v3(nrm[3 * qi], nrm[3 * qi + 1], nrm[3 * qi + 2]));
     V3 w = v3(wo[3 * qi], wo[3 * qi + 1], wo[3 * qi + 2]);
-    V3 c = photon_density(node_pos, node_aux, photons, n, load_bsdf(mat), p, nn, w, shape ? shape[qi] : -1, k, radius);
-    out[3 * qi] = c.x;
-    out[3 * qi + 1] = c.y;
-    out[3 * qi + 2] = c.z;
+    V3 c = warp_photon_density(tree, load_bsdf(mat), p, nn, w, shape ? shape[qi] : -1, k, radius, true,
+                               scratch[threadIdx.x >> 5]);
+    if ((threadIdx.x & 31u) == 0) {
+        out[3 * qi] = c.x;
+        out[3 * qi + 1] = c.y;
+        out[3 * qi + 2] = c.z;
+    }
 }
 
-__global__ void __launch_bounds__(128) k_subsurface(const float4 *__restrict__ node_pos, const int2 *__restrict__ node_aux,
-                                                    const rt_photon *__restrict__ photons, uint32_t n, rt_material mat,
-                                                    const float *__restrict__ pts, const float *__restrict__ nrm,
-                                                    const float *__restrict__ wo, const int32_t *__restrict__ shape,
-                                                    uint64_t nq, float radius, int compat, float *__restrict__ out)
+__global__ void __launch_bounds__(kQueryBlock) k_subsurface(PhotonTree tree, rt_material mat,
+                                                            const float *__restrict__ pts,
+                                                            const float *__restrict__ nrm,
+                                                            const float *__restrict__ wo,
+                                                            const int32_t *__restrict__ shape, uint64_t nq,
+                                                            float radius, int compat, float *__restrict__ out)
 {
-    const uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (qi >= nq) return;
+    __shared__ PhotonWarpScratch scratch[kQueryBlock / 32];
+    const uint64_t qi = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (qi >= nq) return;  // warp-uniform
     const V3 p = v3(pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]);
     const V3 nn = v3(nrm[3 * qi], nrm[3 * qi + 1], nrm[3 * qi + 2]);
     const V3 w = v3(wo[3 * qi], wo[3 * qi + 1], wo[3 * qi + 2]);
-    const V3 c = photon_subsurface(node_pos, node_aux, photons, n, mat, p, nn, w, shape ? shape[qi] : -1, radius,
-                                   compat != 0);
-    out[3 * qi] = c.x;
-    out[3 * qi + 1] = c.y;
-    out[3 * qi + 2] = c.z;
+    const V3 c = warp_photon_subsurface(tree, mat, p, nn, w, shape ? shape[qi] : -1, radius, compat != 0,
+                                        scratch[threadIdx.x >> 5]);
+    if ((threadIdx.x & 31u) == 0) {
+        out[3 * qi] = c.x;
+        out[3 * qi + 1] = c.y;
+        out[3 * qi + 2] = c.z;
+    }
 }
 
 // ---------------------------------------------------- host kd-tree build
@@ -302,6 +329,8 @@ int rt_photon_map_destroy(rt_photon_map *m)
     m->photons.release();
     m->node_pos.release();
     m->node_aux.release();
+    m->node_pw.release();
+    m->node_dir.release();
     delete m;
     return RT_OK;
 }
@@ -391,6 +420,13 @@ int rt_photon_map_build(rt_photon_map *m)
     }
     RTB_CHECK(m->node_pos.upload(np.data(), n * sizeof(float4), st));
     RTB_CHECK(m->node_aux.upload(na.data(), n * sizeof(int2), st));
+    RTB_CHECK(m->node_pw.reserve(std::max<uint64_t>(n, 1) * sizeof(float4)));
+    RTB_CHECK(m->node_dir.reserve(std::max<uint64_t>(n, 1) * sizeof(float4)));
+    if (n) {
+        k_tree_attrs<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(m->node_aux.as<int2>(), m->photons.as<rt_photon>(), n,
+                                                                 m->node_pw.as<float4>(), m->node_dir.as<float4>());
+        RTB_CUDA(cudaGetLastError());
+    }
     RTB_CUDA(cudaStreamSynchronize(st));
     m->built = true;
     return RT_OK;
@@ -422,11 +458,11 @@ int rt_photon_subsurface(rt_photon_map *m, const rt_material *mat, const float *
     if (nq == 0) return RT_OK;
     if (!pts || !nrm || !wo || !out_rgb) return fail(RT_ERR_INVALID, "rt_photon_subsurface: null buffer");
     RTB_CUDA(cudaSetDevice(m->ctx->device));
-    const uint64_t blocks = (nq + 127) / 128;
-    k_subsurface<<<(unsigned)blocks, 128, 0, m->ctx->stream>>>(m->node_pos.as<float4>(), m->node_aux.as<int2>(),
-                                                               m->photons.as<rt_photon>(), (uint32_t)m->n, *mat, pts, nrm,
-                                                               wo, shape, nq, radius, (flags & RT_RENDER_COMPAT) ? 1 : 0,
-                                                               out_rgb);
+    if (nq > (1ull << 31) / 32) return fail(RT_ERR_INVALID, "rt_photon_subsurface: nq must be at most 2^26");
+    const uint64_t blocks = (nq * 32 + kQueryBlock - 1) / kQueryBlock;
+    k_subsurface<<<(unsigned)blocks, kQueryBlock, 0, m->ctx->stream>>>(photon_tree(m), *mat, pts, nrm, wo, shape, nq,
+                                                                       radius, (flags & RT_RENDER_COMPAT) ? 1 : 0,
+                                                                       out_rgb);
     RTB_CUDA(cudaGetLastError());
     RTB_CUDA(cudaStreamSynchronize(m->ctx->stream));
     return RT_OK;
@@ -441,10 +477,10 @@ int rt_photon_density(rt_photon_map *m, const rt_material *mat, const float *pts
     if (k == 0 || k > kKnnMaxK) return fail(RT_ERR_INVALID, "rt_photon_density: k must be in [1, 128]");
     if (nq == 0) return RT_OK;
     RTB_CUDA(cudaSetDevice(m->ctx->device));
-    const uint64_t blocks = (nq + 127) / 128;
-    k_density<<<(unsigned)blocks, 128, 0, m->ctx->stream>>>(m->node_pos.as<float4>(), m->node_aux.as<int2>(),
-                                                            m->photons.as<rt_photon>(), (uint32_t)m->n, *mat, pts,
-                                                            nrm, wo, shape, nq, k, radius, out_rgb);
+    if (nq > (1ull << 31) / 32) return fail(RT_ERR_INVALID, "rt_photon_density: nq must be at most 2^26");
+    const uint64_t blocks = (nq * 32 + kQueryBlock - 1) / kQueryBlock;
+    k_density<<<(unsigned)blocks, kQueryBlock, 0, m->ctx->stream>>>(photon_tree(m), *mat, pts, nrm, wo, shape, nq, k,
+                                                                    radius, out_rgb);
     RTB_CUDA(cudaGetLastError());
     RTB_CUDA(cudaStreamSynchronize(m->ctx->stream));
     return RT_OK;

@@ -58,8 +58,9 @@ struct Buffers {
     float4 *gather;    // photon-map gather requests, 4 float4 each: p+shape, n+material, wo+target, beta
     uint32_t cap, scap, gcap;
     // counters (uint32): [0],[1] queue sizes of buffers 0/1, [2] shadow count, [3] retire count,
-    // [4] status, [5] shadow-kernel work counter, [6] gather requests; u64 at [8]: next sample,
-    // [10] extension rays, [12] shadow rays
+    // [4] status, [5] shadow-kernel work counter, [6] gather requests, [7] gather-kernel work
+    // counter; u64 at [8]: next sample,
+    // [10] extension rays, [12] shadow rays, [14] gathers
     uint32_t *cnt;
 };
 
@@ -182,23 +183,22 @@ constexpr uint32_t kGatherDensity = 0, kGatherSubsurface = 1;
 
 // Queues a photon-map gather at surface sf, weighted by `weight`, for the path whose radiance
 // lives at `target` (kRetireTarget: the retire list). Four float4: point + shape, normal +
-// material, direction to the previous vertex + target, weight + kind.
+// material, direction to the previous vertex + target, weight + (kind | guide record << 1).
+// rec: the guide record the estimate also belongs to (kRecNone: none).
 __device__ __forceinline__ void push_gather(const Buffers &bf, const Surface &sf, V3 wo_w, V3 weight, uint32_t target,
-                                            uint32_t kind)
+                                            uint32_t kind, uint32_t rec)
 {
     const uint32_t gi = append(bf.cnt + 6);
     if (gi >= bf.gcap) return;
     bf.gather[4 * gi + 0] = make_float4(sf.p.x, sf.p.y, sf.p.z, __int_as_float(sf.shape));
     bf.gather[4 * gi + 1] = make_float4(sf.n.x, sf.n.y, sf.n.z, __uint_as_float(sf.mat));
     bf.gather[4 * gi + 2] = make_float4(wo_w.x, wo_w.y, wo_w.z, __uint_as_float(target));
-    bf.gather[4 * gi + 3] = make_float4(weight.x, weight.y, weight.z, __uint_as_float(kind));
+    bf.gather[4 * gi + 3] = make_float4(weight.x, weight.y, weight.z, __uint_as_float(kind | (rec << 1)));
 }
 
 struct PhotonView {
-    const float4 *node_pos;
-    const int2 *node_aux;
-    const rt_photon *photons;
-    uint32_t n, k;
+    PhotonTree tree;
+    uint32_t k;
     float radius;
 };
 
@@ -334,9 +334,9 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
             // (Scene::getPhotonContributions, Scene.cu:822-840; finishStep, pathTracing.cu:85-89)
             finished = true;
             const uint32_t rt = kRetireTarget | append(bf.cnt + 3);
-            push_gather(bf, sf, wo_w, beta_in, rt, kGatherDensity);
+            push_gather(bf, sf, wo_w, beta_in, rt, kGatherDensity, rec_in);
             if (subsurface && bs.type == RT_MAT_SUBSURFACE && (flags & kCameraRay))
-                push_gather(bf, sf, wo_w, beta_in, rt, kGatherSubsurface);
+                push_gather(bf, sf, wo_w, beta_in, rt, kGatherSubsurface, rec_in);
             bf.retire[rt & ~kRetireTarget] = make_float4(L.x, L.y, L.z, __uint_as_float(pix));
             regenerate(rv, bf, nxt);
             return;
@@ -372,8 +372,8 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
         const float dscale = hybrid ? 0.5f : 1.0f;
         if (scattering) {
             if (subsurface && bs.type == RT_MAT_SUBSURFACE && (flags & kCameraRay))
-                push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherSubsurface);
-            if (hybrid) push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherDensity);
+                push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherSubsurface, rec_in);
+            if (hybrid) push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherDensity, rec_in);
             for (uint32_t li = 0; li < rv.nplights; li++) {  // Scene::estimateAllDirectLights, PointLight
                 float4 lp = rv.plights[2 * li], li4 = rv.plights[2 * li + 1];
                 V3 tol = v3(lp.x, lp.y, lp.z) - sf.p;
@@ -498,36 +498,55 @@ __global__ void __launch_bounds__(kB, RTB_TRAV_MIN_BLOCKS) k_shadow(RenderView r
         });
 }
 
-// Photon-map gathers queued by k_shade: the density estimate times the path throughput is
-// added to the finished path's radiance.
 // Photon-map gathers queued by k_shade: the density estimate (Scene::combinePhotonContributions,
 // zero on subsurface materials, Scene.cu:611-612) or the subsurface dipole estimate
-// (Scene::combinePhotonsSubsurface), times the request's weight, added to the path's radiance.
-__global__ void __launch_bounds__(kB) k_gather(RenderView rv, Buffers bf, PhotonView pv, int nxt)
+// (Scene::combinePhotonsSubsurface), times the request's weight, added to the path's radiance
+// and, while the guide trains, to the guide record of the vertex before it (as k_shadow does).
+// One warp per request; warps take requests from counter cnt[7] until the wave's are done.
+constexpr int kGatherBlock = 128;
+__global__ void __launch_bounds__(kGatherBlock) k_gather(RenderView rv, Buffers bf, PhotonView pv, int nxt,
+                                                         GuideView gv)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ PhotonWarpScratch scratch[kGatherBlock / 32];
+    PhotonWarpScratch &sm = scratch[threadIdx.x >> 5];
+    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n = min(bf.cnt[6], bf.gcap);
-    if (i >= n) return;
-    const float4 a = bf.gather[4 * i], b = bf.gather[4 * i + 1], c = bf.gather[4 * i + 2], d = bf.gather[4 * i + 3];
-    const rt_material &m = rv.mats[min(__float_as_uint(b.w), rv.nmats - 1)];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(cnt64(bf.cnt, 14), (unsigned long long)n);  // stats
     const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
-    const V3 p = v3(a.x, a.y, a.z), nn = v3(b.x, b.y, b.z), wo = v3(c.x, c.y, c.z);
-    V3 e;
-    if (__float_as_uint(d.w) == kGatherSubsurface)
-        e = photon_subsurface(pv.node_pos, pv.node_aux, pv.photons, pv.n, m, p, nn, wo, __float_as_int(a.w),
-                              kSubsurfaceRadius, compat);
-    else if (m.type == RT_MAT_SUBSURFACE)
-        e = v3(0, 0, 0);
-    else
-        e = photon_density(pv.node_pos, pv.node_aux, pv.photons, pv.n, load_bsdf(m), p, nn, wo, __float_as_int(a.w),
-                           pv.k, pv.radius, compat);
-    const V3 contrib = v3(d.x, d.y, d.z) * e;
-    const uint32_t target = __float_as_uint(c.w);
-    float *dst = (target & kRetireTarget) ? reinterpret_cast<float *>(bf.retire + (target & ~kRetireTarget))
-                                          : reinterpret_cast<float *>(bf.st1[nxt] + target);
-    atomicAdd(dst + 0, contrib.x);
-    atomicAdd(dst + 1, contrib.y);
-    atomicAdd(dst + 2, contrib.z);
+    for (;;) {
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(bf.cnt + 7, 1u);
+        i = __shfl_sync(kFullMask, i, 0);
+        if (i >= n) return;  // warp-uniform
+        const float4 a = bf.gather[4 * i], b = bf.gather[4 * i + 1], c = bf.gather[4 * i + 2],
+                     d = bf.gather[4 * i + 3];
+        const rt_material &m = rv.mats[min(__float_as_uint(b.w), rv.nmats - 1)];
+        const V3 p = v3(a.x, a.y, a.z), nn = v3(b.x, b.y, b.z), wo = v3(c.x, c.y, c.z);
+        const uint32_t kind = __float_as_uint(d.w) & 1u, rec = __float_as_uint(d.w) >> 1;
+        V3 e;
+        if (kind == kGatherSubsurface)
+            e = warp_photon_subsurface(pv.tree, m, p, nn, wo, __float_as_int(a.w), kSubsurfaceRadius, compat, sm);
+        else if (m.type == RT_MAT_SUBSURFACE)
+            e = v3(0, 0, 0);
+        else
+            e = warp_photon_density(pv.tree, load_bsdf(m), p, nn, wo, __float_as_int(a.w), pv.k, pv.radius, compat,
+                                    sm);
+        if (lane == 0) {
+            const V3 contrib = v3(d.x, d.y, d.z) * e;
+            const uint32_t target = __float_as_uint(c.w);
+            float *dst = (target & kRetireTarget) ? reinterpret_cast<float *>(bf.retire + (target & ~kRetireTarget))
+                                                  : reinterpret_cast<float *>(bf.st1[nxt] + target);
+            atomicAdd(dst + 0, contrib.x);
+            atomicAdd(dst + 1, contrib.y);
+            atomicAdd(dst + 2, contrib.z);
+            if (gv.train && rec != kRecNone && rec < gv.rec_cap) {
+                float4 *r = &gv.recs[rec].e;
+                atomicAdd(&r->x, contrib.x);
+                atomicAdd(&r->y, contrib.y);
+                atomicAdd(&r->z, contrib.z);
+            }
+        }
+    }
 }
 
 __device__ __forceinline__ float record_weight(const GuideRecord &r)
@@ -848,7 +867,10 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     rt_guide *guide = s->guide;
     if (guided) {
         if (!guide) return fail(RT_ERR_STATE, name + ": RT_RENDER_GUIDE needs a guide (rt_render_set_guide)");
-        if (gathers) return fail(RT_ERR_UNSUPPORTED, name + ": RT_RENDER_GUIDE with a photon-map mode");
+        // photon-mapping mode ends each path at its first scattering vertex, where the guide
+        // would sample: nothing is left to guide
+        if (flags & RT_RENDER_PHOTON_MAP)
+            return fail(RT_ERR_UNSUPPORTED, name + ": RT_RENDER_GUIDE with RT_RENDER_PHOTON_MAP");
         gv.enabled = 1;
         gv.train = s->guide_train;
         gv.max_depth = guide->opts.max_depth ? guide->opts.max_depth : 0xFFFFFFFFu;
@@ -888,10 +910,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     bf.gather = rs.gather.as<float4>();
     PhotonView pv{};
     if (gathers) {
-        pv.node_pos = s->pmap->node_pos.as<float4>();
-        pv.node_aux = s->pmap->node_aux.as<int2>();
-        pv.photons = s->pmap->photons.as<rt_photon>();
-        pv.n = (uint32_t)s->pmap->n;
+        pv.tree = photon_tree(s->pmap);
         pv.k = std::min<uint32_t>(std::max<uint32_t>(s->pm_k, 1u), kKnnMaxK);
         pv.radius = s->pm_radius;
     }
@@ -922,6 +941,15 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
         shadow_resident = (unsigned)std::max(1, s->ctx->sm_count * std::max(per_sm, 1));
     }
     const unsigned shadow_blocks = std::min<unsigned>(shadow_resident, (scap + kB - 1) / kB);
+    static unsigned gather_resident = 0;  // persistent gather warps: every resident block
+    if (gathers && !gather_resident) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather, kGatherBlock, 0);
+        gather_resident = (unsigned)std::max(1, s->ctx->sm_count * std::max(per_sm, 1));
+    }
+    const unsigned gather_blocks =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(gather_resident, ((uint64_t)gcap * 32 + kGatherBlock - 1) /
+                                                                                kGatherBlock));
     static bool infer_attr = false;
     if (gv.params && !infer_attr) {
         RTB_CUDA(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
@@ -948,13 +976,13 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
                 RTB_CUDA(cudaGetLastError());
             }
             RTB_CUDA(cudaMemsetAsync(bf.cnt + ((cur ^ 1)), 0, 4, st));
-            RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 20, st));
+            RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 24, st));
             k_shade<<<blocks, kB, 0, st>>>(rv, bf, cur, gv);
             RTB_CUDA(cudaGetLastError());
             k_shadow<<<shadow_blocks, kB, 0, st>>>(rv, bf, cur ^ 1, gv);
             RTB_CUDA(cudaGetLastError());
             if (gathers) {
-                k_gather<<<(gcap + kB - 1) / kB, kB, 0, st>>>(rv, bf, pv, cur ^ 1);
+                k_gather<<<gather_blocks, kGatherBlock, 0, st>>>(rv, bf, pv, cur ^ 1, gv);
                 RTB_CUDA(cudaGetLastError());
             }
             k_retire<<<blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64, gv);
@@ -1028,6 +1056,8 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
         stats->shadow_rays = v;
         std::memcpy(&v, hc + 8, 8);
         stats->camera_rays = std::min<uint64_t>(v, total);
+        std::memcpy(&v, hc + 14, 8);
+        stats->gathers = v;
         stats->waves = waves;
         stats->ms = ms;
     }

@@ -192,6 +192,8 @@ struct rt_photon_map {
     rtb::DevBuf photons;   // rt_photon[n], (path, depth) order
     rtb::DevBuf node_pos;  // float4 per tree slot: xyz, split axis (uint bits)
     rtb::DevBuf node_aux;  // int2 per tree slot: shape id, photon index
+    rtb::DevBuf node_pw;   // float4 per tree slot: power rgb, cos(normal, -direction)
+    rtb::DevBuf node_dir;  // float4 per tree slot: arrival direction xyz, 0
     bool built = false;
 };
 

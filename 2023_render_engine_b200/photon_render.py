@@ -1,0 +1,114 @@
+"""Photon mapping + subsurface scattering + guiding at 4K (config 4), measured end to end.
+
+The steps are the reference's photon pipeline (Scene::generatePhotons + computePhotons, the
+kd-tree build, then PathTracerIntegrator::render with the photon estimates,
+integration/Scene.cu:989-1026, 607-722, 914-969) on the GPU:
+
+1. trace the photons from the two point lights (rt_photons_trace);
+2. build the kd-tree over them (rt_photon_map_build);
+3. render in hybrid + subsurface mode with k-nearest-photon density gathers at every
+   scattering vertex and dipole gathers at camera hits on the slab — plain BSDF sampling, and
+   with a guide trained online on the same scene first.
+
+Each render step is timed with CUDA events on the context's stream; Mrays/s counts extension
+and shadow rays, and the gather rate counts photon-map estimates.
+"""
+from __future__ import annotations
+
+import importlib
+import time
+
+from . import _native as N
+from . import configs, core
+
+GD = importlib.import_module(__package__ + ".guiding")
+
+
+def _event_ms(torch, stream, fn):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def measure(ctx, torch, stream, width=3840, height=2160, spp=None, photons=None, k=None, seed=11,
+            guided=True, train_passes=4, train_steps=64, train_batch=1 << 16, terrain_n=1000):
+    """Runs config 4 once and returns a dict of its timings and rates."""
+    spp = spp or 256
+    photons = photons or configs.CONFIG4_PHOTONS
+    k = k or configs.CONFIG4_K
+    t0 = time.perf_counter()
+    sc, cam, p = configs.build_config4(ctx, width, height, seed=seed, n=terrain_n)
+    build_s = time.perf_counter() - t0
+    stats = sc.stats()
+    fl = configs.CONFIG4_FLAGS
+    out = {"workload": f"config 4: {stats['triangles']} triangles (displaced terrain) + 16 glass spheres + "
+                       f"subsurface slab, 2 point lights; {photons} photons, k={k}; {width}x{height}, {spp} spp, "
+                       f"max depth {p['max_depth']}, hybrid + subsurface",
+           "scene_build_s": build_s}
+
+    # warm the photon and render kernels on a small case (not timed)
+    pm_w, _ = sc.trace_photons(100_000, max_depth=16, seed=seed + 100)
+    pm_w.build()
+    sc.set_photon_map(pm_w, k, 100.0)
+    small = core.look_at_camera((0.0, 2.4, 5.6), (0.0, -0.1, 0.0), (0, 1, 0), 45.0, 64, 36)
+    sc.render(small, spp=1, max_depth=p["max_depth"], seed=1, flags=fl)
+    torch.cuda.synchronize()
+
+    # 1. photon trace
+    ms_trace, (pm, pst) = _event_ms(torch, stream,
+                                    lambda: sc.trace_photons(photons, max_depth=16, seed=seed + 1))
+    out["photon_trace"] = {"ms": ms_trace, "emitted": int(pst["emitted"]), "stored": len(pm),
+                           "rays": int(pst["rays"]), "emitted_per_s": pst["emitted"] / (ms_trace / 1000),
+                           "Mrays_per_s": pst["rays"] / (ms_trace / 1000) / 1e6}
+    # 2. kd-tree (host build over the device photons, then upload)
+    t0 = time.perf_counter()
+    pm.build()
+    out["kd_build_s"] = time.perf_counter() - t0
+    sc.set_photon_map(pm, k, 100.0)
+    pm_w.close()
+
+    def render(flags, film, rseed):
+        film["sum"].zero_()
+        film["count"].zero_()
+        return sc.render(cam, spp=spp, max_depth=p["max_depth"], rr_depth=p["rr_depth"], seed=rseed, flags=flags,
+                         film=film)[1]
+
+    W, H = cam.width, cam.height
+    film = {"sum": torch.zeros(H * W * 3, dtype=torch.float32, device="cuda"),
+            "count": torch.zeros(H * W, dtype=torch.int32, device="cuda")}
+
+    def line(ms, st):
+        rays = st["extension_rays"] + st["shadow_rays"]
+        return {"ms": ms, "Mrays_per_s": rays / (ms / 1000) / 1e6, "samples_per_s": W * H * spp / (ms / 1000),
+                "gathers_per_s": st["gathers"] / (ms / 1000), "extension_rays": int(st["extension_rays"]),
+                "shadow_rays": int(st["shadow_rays"]), "gathers": int(st["gathers"]), "waves": int(st["waves"])}
+
+    # 3a. plain
+    ms, st = _event_ms(torch, stream, lambda: render(fl, film, 5))
+    out["plain"] = line(ms, st)
+    if guided:
+        T = configs.CONFIG4_GUIDE
+        g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=2,
+                       max_depth=T["max_depth"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        GD.render_progressive(sc, cam, g, [1] * train_passes, max_depth=p["max_depth"], rr_depth=p["rr_depth"],
+                              seed=77, flags=fl, train_passes=train_passes, steps_per_pass=train_steps,
+                              batch=train_batch, sync=torch.cuda.synchronize)
+        out["guide_training_s"] = time.perf_counter() - t0
+        out["guide_training"] = {"passes": train_passes, "steps": g.steps, "batch": train_batch,
+                                 "learning_rate": T["learning_rate"], "guided_depths": T["max_depth"]}
+        sc.set_guide(g, train=False)
+        # 3b. guided
+        ms, st = _event_ms(torch, stream, lambda: render(fl | N.RT_RENDER_GUIDE, film, 6))
+        out["guided"] = line(ms, st)
+        sc.set_guide(None)
+        g.close()
+    sc.set_photon_map(None)
+    pm.close()
+    sc.close()
+    return out

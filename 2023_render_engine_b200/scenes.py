@@ -224,3 +224,48 @@ def guiding_room(seed=3, target_triangles=200_000):
         add(v, f, m)
         ntri += f.shape[0]
     return meshes, mats
+
+
+def terrain_grid(n=1000, half=4.0, amplitude=0.35, seed=11, octaves=5, base_freq=1.5):
+    """Height-field terrain over [-half, half]^2 in xz: an (n+1)^2 vertex grid, 2 n^2
+    triangles facing +y, heights amplitude * value noise of (x, z) / half. Returns (v, f, height)
+    with height(x, z) the same field at arbitrary points."""
+    g = np.linspace(-half, half, n + 1)
+    X, Z = np.meshgrid(g, g, indexing="ij")
+
+    def height(x, z):
+        x = np.asarray(x, np.float64).ravel()
+        z = np.asarray(z, np.float64).ravel()
+        p = np.stack([x / half, z / half, np.zeros_like(x)], 1)
+        return amplitude * value_noise(p, seed, octaves=octaves, base_freq=base_freq)
+
+    Y = height(X, Z).reshape(X.shape)
+    v = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    idx = np.arange((n + 1) * (n + 1)).reshape(n + 1, n + 1)
+    a, b, c, d = idx[:-1, :-1].ravel(), idx[1:, :-1].ravel(), idx[1:, 1:].ravel(), idx[:-1, 1:].ravel()
+    # (x, z) grid with x along the first index: (a, d, c) and (a, c, b) wind counter-clockwise
+    # seen from +y
+    f = np.concatenate([np.stack([a, d, c], 1), np.stack([a, c, b], 1)])
+    return v.astype(np.float32), f.astype(np.uint32), height
+
+
+def photon_terrain(seed=11, n=1000):
+    """Config 4 geometry: the displaced terrain (2 n^2 triangles; 2M at n = 1000), 16 glass
+    spheres of radius U[0.1, 0.4] resting on it without overlapping, and a 1.2 x 0.3 x 0.8
+    subsurface slab sunk 0.05 into it near the centre. Returns terrain (v, f), slab (v, f) and
+    the spheres [(centre, radius)]."""
+    rng = np.random.default_rng(seed + 1)
+    tv, tf, height = terrain_grid(n=n, seed=seed)
+    spheres = []
+    while len(spheres) < 16:
+        r = float(rng.uniform(0.1, 0.4))
+        x, z = rng.uniform(-2.5, 2.5, 2)
+        if abs(x) < 1.0 and abs(z) < 0.8:
+            continue  # keep the slab's footprint clear
+        if any((x - c[0]) ** 2 + (z - c[2]) ** 2 < (r + rr + 0.05) ** 2 for c, rr in spheres):
+            continue
+        y = float(height([x], [z])[0]) + r + 0.02
+        spheres.append(((float(x), y, float(z)), r))
+    h0 = float(height([0.0], [0.2])[0]) - 0.05
+    sv, sf = subdivided_box((-0.6, h0, -0.2), (0.6, h0 + 0.3, 0.6), 1)
+    return (tv, tf), (sv, sf), spheres

@@ -242,6 +242,7 @@ typedef struct rt_render_stats {
     uint64_t shadow_rays;
     uint64_t waves;
     double ms;               /* device time of the render call */
+    uint64_t gathers;        /* photon-map estimates (density and dipole) */
 } rt_render_stats;
 
 /* Path-traces spp samples per pixel and ADDS them to the caller's film (device
@@ -392,7 +393,10 @@ typedef struct rt_guide_opts {
 #define RT_GUIDE_INPUTS 144
 #define RT_GUIDE_OUTPUTS 48
 #define RT_GUIDE_LOBES 8
-#define RT_RENDER_GUIDE 0x10u /* rt_render_opts.flags: sample with the scene's guide (one-sample MIS) */
+#define RT_RENDER_GUIDE 0x10u /* rt_render_opts.flags: sample with the scene's guide (one-sample MIS).
+                               * Combines with RT_RENDER_SUBSURFACE and RT_RENDER_HYBRID (their photon
+                               * estimates also train the guide); RT_ERR_UNSUPPORTED with
+                               * RT_RENDER_PHOTON_MAP, whose paths end where the guide would sample. */
 
 RT_API int rt_guide_create(rt_context *ctx, const rt_guide_opts *opts, rt_guide **out);
 RT_API int rt_guide_destroy(rt_guide *g);

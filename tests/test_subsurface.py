@@ -141,6 +141,74 @@ def test_hybrid_mode_is_the_mean_of_photon_density_and_next_event(core, gpu_ctx)
     assert p.mean() > 0 and n.mean() > 0
 
 
+def covered_floor_scene(core, ctx):
+    """floor_scene with a 4x2 ceiling quad at z = 1.6 (shape 2) that paths bounce back from."""
+    sc = core.Scene(ctx)
+    sc.set_materials([core.material(N.RT_MAT_LAMBERTIAN, color=(0.7, 0.6, 0.5))])
+    quads = [np.array([[x0, -1, 0], [x0 + 2, -1, 0], [x0 + 2, 1, 0], [x0, 1, 0]], np.float32) for x0 in (-2.0, 0.0)]
+    quads.append(np.array([[-2, -1, 1.6], [-2, 1, 1.6], [2, 1, 1.6], [2, -1, 1.6]], np.float32))
+    for i, v in enumerate(quads):
+        sc.add_mesh(v, np.array([[0, 1, 2], [0, 2, 3]], np.uint32), material=0, shape_id=i)
+    sc.add_point_light((0.3, 0.2, 1.0), (1, 1, 1), 5.0)
+    sc.commit()
+    return sc
+
+
+@pytest.mark.gpu
+def test_guide_records_take_the_hybrid_photon_estimates(core, gpu_ctx):
+    """With the same samples, the guide records of a hybrid render hold half the next-event
+    radiance of a plain render plus half the photon density estimates: strictly more than
+    half, which they would be if the gathers did not reach the records."""
+    sc = covered_floor_scene(core, gpu_ctx)
+    pm, _ = sc.trace_photons(100000, max_depth=4, seed=6)
+    pm.build()
+    sc.set_photon_map(pm, 50, 1.0)
+    cam = core.look_at_camera((0.0, 0.0, 1.4), (0, 0, 0), (0, 1, 0), 70.0, 32, 32)
+    g = core.Guide(gpu_ctx, (-2.1, -1.1, -0.1), (2.1, 1.1, 1.7), learning_rate=1e-3, seed=1, max_depth=3)
+    sums = {}
+    for name, fl in (("plain", 0), ("hybrid", N.RT_RENDER_HYBRID)):
+        sc.set_guide(g, train=True)
+        sc.render(cam, spp=4, max_depth=4, seed=9, flags=fl | N.RT_RENDER_GUIDE)
+        r = g.records()
+        assert len(r) > 1000
+        sums[name] = r[:, 16:19].astype(np.float64).sum(0)
+    sc.set_guide(None)
+    g.close()
+    assert np.all(sums["plain"] > 0)
+    assert np.all(sums["hybrid"] > 0.5 * sums["plain"] * 1.05), sums
+
+
+@pytest.mark.gpu
+def test_guided_hybrid_subsurface_render_is_unbiased(core, gpu_ctx):
+    """A guide trained on hybrid + subsurface renders (its records hold the photon estimates)
+    leaves the image mean unchanged: one-sample MIS keeps the estimator unbiased."""
+    import torch
+
+    sc = covered_floor_scene(core, gpu_ctx)
+    pm, _ = sc.trace_photons(100000, max_depth=4, seed=6)
+    pm.build()
+    sc.set_photon_map(pm, 50, 1.0)
+    cam = core.look_at_camera((0.0, 0.0, 1.4), (0, 0, 0), (0, 1, 0), 70.0, 32, 32)
+    fl = N.RT_RENDER_HYBRID | N.RT_RENDER_SUBSURFACE
+    g = core.Guide(gpu_ctx, (-2.1, -1.1, -0.1), (2.1, 1.1, 1.7), learning_rate=1e-3, seed=1, max_depth=3)
+    for i in range(3):
+        sc.set_guide(g, train=True)
+        sc.render(cam, spp=4, max_depth=6, seed=20 + i, flags=fl | N.RT_RENDER_GUIDE)
+        assert g.record_count()[1] > 0
+        g.train_records(32, 1 << 14, seed=i)
+    sc.set_guide(g, train=False)
+    fg, _ = sc.render(cam, spp=1024, max_depth=6, seed=31, flags=fl | N.RT_RENDER_GUIDE, fp64=True)
+    fp, _ = sc.render(cam, spp=1024, max_depth=6, seed=32, flags=fl, fp64=True)
+    torch.cuda.synchronize()
+    mg, mp = core.film_mean(fg).mean(0), core.film_mean(fp).mean(0)
+    assert np.all(np.isfinite(mg)) and np.all(mp > 0)
+    assert np.allclose(mg, mp, rtol=0.02), (mg, mp)
+    with pytest.raises(N.RtError):
+        sc.render(cam, spp=1, max_depth=2, seed=1, flags=N.RT_RENDER_PHOTON_MAP | N.RT_RENDER_GUIDE)
+    sc.set_guide(None)
+    g.close()
+
+
 def ctypes_byref(x):
     import ctypes
 
