@@ -210,6 +210,11 @@ __global__ void __launch_bounds__(128) k_knn(const float4 *__restrict__ node_pos
 
 // One warp per query (the render's gather kernel uses the same warp functions).
 constexpr int kQueryBlock = 128;
+// Resident blocks per SM of the query kernels (64 registers): k_density 54 / 64 / 79 M queries/s
+// and k_subsurface 4.5 / 4.5 / 5.1 M/s for no bound (80 registers) / 6 / 8, on a 2.1M-photon map.
+#ifndef RTB_QUERY_MIN_BLOCKS
+#define RTB_QUERY_MIN_BLOCKS 8
+#endif
 
 // The photons' shading attributes in tree-slot order, so that a query reads them with the
 // positions it scans: power and cos(normal, -direction) (the photon's factor of
@@ -231,7 +236,7 @@ __global__ void k_tree_attrs(const int2 *__restrict__ node_aux, const rt_photon 
 // Scene::combinePhotonContributions (Scene.cu:607-635) per query: the k nearest photons on
 // the same shape within radius, sum of power * lightScattered(-photon direction), divided by
 // pi * (largest neighbour distance)^2.
-__global__ void __launch_bounds__(kQueryBlock) k_density(PhotonTree tree, rt_material mat, const float *__restrict__ pts,
+__global__ void __launch_bounds__(kQueryBlock, RTB_QUERY_MIN_BLOCKS) k_density(PhotonTree tree, rt_material mat, const float *__restrict__ pts,
                                                          const float *__restrict__ nrm, const float *__restrict__ wo,
                                                          const int32_t *__restrict__ shape, uint64_t nq, uint32_t k,
                                                          float radius, float *__restrict__ out)
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(kQueryBlock) k_density(PhotonTree tree, rt_mat
     }
 }
 
-__global__ void __launch_bounds__(kQueryBlock) k_subsurface(PhotonTree tree, rt_material mat,
+__global__ void __launch_bounds__(kQueryBlock, RTB_QUERY_MIN_BLOCKS) k_subsurface(PhotonTree tree, rt_material mat,
                                                             const float *__restrict__ pts,
                                                             const float *__restrict__ nrm,
                                                             const float *__restrict__ wo,

@@ -137,7 +137,9 @@ constexpr float kSubsurfaceRadius = 0.3f;
 // impPaper_dipoleDiffusionAproximation (geometricMath.cu:455-490), one channel: the dipole
 // diffuse reflectance Rd at distance r with the reduced scattering coefficient (1 - g) sigma_s.
 // The terms that do not depend on r are set up once per query (DipoleChannel); dipole_eval
-// evaluates the rest with the same operations in the same order.
+// evaluates the rest per photon, the hot loop of the subsurface gather, with reciprocal square
+// roots and the hardware exponential (relative error about 1e-6, against 1e-7 for the IEEE
+// operations): with d = sqrt(r^2 + z^2), 1/d and 1/d^3 come from one rsqrt.
 struct DipoleChannel {
     float tr, zr, zv, omf, alpha;  // sigma_tr, real and virtual source depths, 1 - Fdr, albedo
 };
@@ -157,13 +159,13 @@ __device__ __forceinline__ DipoleChannel dipole_setup(float ss, float sa, float 
     return c;
 }
 
-__device__ __forceinline__ float dipole_eval(const DipoleChannel &c, float r)
+__device__ __forceinline__ float dipole_eval(const DipoleChannel &c, float r2)
 {
-    const float dr = sqrtf(r * r + c.zr * c.zr), dv = sqrtf(r * r + c.zv * c.zv);
-    const float trdr = c.tr * dr, trdv = c.tr * dv;
-    const float rd =
-        (trdr + 1) * expf(-trdr) * c.zr / (dr * dr * dr) + (trdv + 1) * expf(-trdv) * c.zv / (dv * dv * dv);
-    const float c1 = c.zr * (c.tr + 1 / dr);
+    const float xr = r2 + c.zr * c.zr, xv = r2 + c.zv * c.zv;
+    const float ir = rsqrtf(xr), iv = rsqrtf(xv);  // 1/dr, 1/dv
+    const float trdr = c.tr * (xr * ir), trdv = c.tr * (xv * iv);
+    const float rd = (trdr + 1) * __expf(-trdr) * c.zr * (ir * ir * ir) + (trdv + 1) * __expf(-trdv) * c.zv * (iv * iv * iv);
+    const float c1 = c.zr * (c.tr + ir);
     return c1 * rd * c.omf * c.alpha;
 }
 
@@ -443,19 +445,19 @@ __device__ __forceinline__ V3 warp_photon_subsurface(const PhotonTree &t, const 
     V3 sum = v3(0, 0, 0);
     float maxd = 0.f;
     uint32_t cnt = 0;
-    auto add = [&](uint32_t s) {
-        const float4 pp = __ldg(t.pos + s), pw = __ldg(t.pw + s);
-        const float r = length(v3(pp.x, pp.y, pp.z) - p);
+    auto add = [&](uint32_t s, float r) {  // r: the photon's distance, as the search measured it
+        const float4 pw = __ldg(t.pw + s);
         maxd = fmaxf(maxd, r);
         const float sc = kInvPi * (1.f - fresnel_dielectric_ref(pw.w, 1.f, eta)) * ft_o;
-        const V3 rd = v3(dipole_eval(d0, r), dipole_eval(d1, r), dipole_eval(d2, r));
+        const float r2 = r * r;
+        const V3 rd = v3(dipole_eval(d0, r2), dipole_eval(d1, r2), dipole_eval(d2, r2));
         sum = sum + rd * sc * v3(pw.x, pw.y, pw.z) * kd;
     };
     warp_traverse<kRadiusScan>(t, p.x, p.y, p.z, sm, [&]() { return radius; },
                                [&](bool valid, float dist, int shape, uint32_t s) {
                                    const bool ok = valid && dist < radius && (sid == -1 || shape == sid);
                                    cnt += __popc(__ballot_sync(kFullMask, ok));
-                                   if (ok) add(s);
+                                   if (ok) add(s, dist);
                                });
     if (cnt == 0) return compat ? v3(NAN, NAN, NAN) : v3(0, 0, 0);
     sum = v3(warp_sum(sum.x), warp_sum(sum.y), warp_sum(sum.z));

@@ -504,7 +504,12 @@ __global__ void __launch_bounds__(kB, RTB_TRAV_MIN_BLOCKS) k_shadow(RenderView r
 // and, while the guide trains, to the guide record of the vertex before it (as k_shadow does).
 // One warp per request; warps take requests from counter cnt[7] until the wave's are done.
 constexpr int kGatherBlock = 128;
-__global__ void __launch_bounds__(kGatherBlock) k_gather(RenderView rv, Buffers bf, PhotonView pv, int nxt,
+// Resident blocks per SM k_gather is compiled for (64 registers). Config-4 render at 3840x2160,
+// 4 spp: 538 / 513 / 464 / 467 ms for no bound (118 registers) / 5 / 6 / 8.
+#ifndef RTB_GATHER_MIN_BLOCKS
+#define RTB_GATHER_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(kGatherBlock, RTB_GATHER_MIN_BLOCKS) k_gather(RenderView rv, Buffers bf, PhotonView pv, int nxt,
                                                          GuideView gv)
 {
     __shared__ PhotonWarpScratch scratch[kGatherBlock / 32];
@@ -853,7 +858,6 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     RTB_CHECK(rs.srays.reserve(32ull * scap));
     RTB_CHECK(rs.scontrib.reserve(16ull * scap));
     RTB_CHECK(rs.retire.reserve(16ull * cap));
-    const bool photon_mode = (flags & RT_RENDER_PHOTON_MAP) != 0;
     const bool gathers = (flags & (RT_RENDER_PHOTON_MAP | RT_RENDER_SUBSURFACE | RT_RENDER_HYBRID)) != 0;
     // a path queues at most two gathers per wave (density, subsurface)
     const uint32_t gcap = gathers ? 2 * cap : 0;
