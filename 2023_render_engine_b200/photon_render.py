@@ -10,8 +10,10 @@ integration/Scene.cu:989-1026, 607-722, 914-969) on the GPU:
    scattering vertex and dipole gathers at camera hits on the slab — plain BSDF sampling, and
    with a guide trained online on the same scene first.
 
-Each render step is timed with CUDA events on the context's stream; Mrays/s counts extension
-and shadow rays, and the gather rate counts photon-map estimates.
+Each render is timed with CUDA events on the context's stream; Mrays/s counts extension and
+shadow rays, and the gather rate counts photon-map estimates. A render is two halves with
+disjoint sample indices in two films, so that their difference measures the image noise of
+each mode without a converged reference at 4K.
 """
 from __future__ import annotations
 
@@ -71,25 +73,39 @@ def measure(ctx, torch, stream, width=3840, height=2160, spp=None, photons=None,
     sc.set_photon_map(pm, k, 100.0)
     pm_w.close()
 
-    def render(flags, film, rseed):
-        film["sum"].zero_()
-        film["count"].zero_()
-        return sc.render(cam, spp=spp, max_depth=p["max_depth"], rr_depth=p["rr_depth"], seed=rseed, flags=flags,
-                         film=film)[1]
-
     W, H = cam.width, cam.height
-    film = {"sum": torch.zeros(H * W * 3, dtype=torch.float32, device="cuda"),
-            "count": torch.zeros(H * W, dtype=torch.int32, device="cuda")}
+    half = max(spp // 2, 1)
+    films = [{"sum": torch.zeros(H * W * 3, dtype=torch.float32, device="cuda"),
+              "count": torch.zeros(H * W, dtype=torch.int32, device="cuda")} for _ in range(2)]
 
-    def line(ms, st):
+    def render_halves(flags, rseed):
+        """spp samples per pixel as two halves with disjoint sample indices, into two films;
+        returns the device time of both, their stats summed, and the noise estimate of the
+        full-spp image: RMSE(half a, half b) / 2 (each half has sqrt(2) times the noise of the
+        whole, and their difference sqrt(2) times that again)."""
+        for f in films:
+            f["sum"].zero_()
+            f["count"].zero_()
+        total = {}
+        ms = 0.0
+        for h, f in enumerate(films):
+            t, (_, st) = _event_ms(torch, stream, lambda: sc.render(
+                cam, spp=half, max_depth=p["max_depth"], rr_depth=p["rr_depth"], seed=rseed, flags=flags,
+                sample_offset=h * half, film=f))
+            ms += t
+            for key, v in st.items():
+                total[key] = total.get(key, 0) + v
+        return ms, total, core.film_rmse_gpu(films[0], films[1]) / 2.0
+
+    def line(ms, st, noise):
         rays = st["extension_rays"] + st["shadow_rays"]
-        return {"ms": ms, "Mrays_per_s": rays / (ms / 1000) / 1e6, "samples_per_s": W * H * spp / (ms / 1000),
+        return {"ms": ms, "Mrays_per_s": rays / (ms / 1000) / 1e6, "samples_per_s": W * H * 2 * half / (ms / 1000),
                 "gathers_per_s": st["gathers"] / (ms / 1000), "extension_rays": int(st["extension_rays"]),
-                "shadow_rays": int(st["shadow_rays"]), "gathers": int(st["gathers"]), "waves": int(st["waves"])}
+                "shadow_rays": int(st["shadow_rays"]), "gathers": int(st["gathers"]), "waves": int(st["waves"]),
+                "noise_rmse": noise}
 
     # 3a. plain
-    ms, st = _event_ms(torch, stream, lambda: render(fl, film, 5))
-    out["plain"] = line(ms, st)
+    out["plain"] = line(*render_halves(fl, 5))
     if guided:
         T = configs.CONFIG4_GUIDE
         g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=2,
@@ -104,10 +120,14 @@ def measure(ctx, torch, stream, width=3840, height=2160, spp=None, photons=None,
                                  "learning_rate": T["learning_rate"], "guided_depths": T["max_depth"]}
         sc.set_guide(g, train=False)
         # 3b. guided
-        ms, st = _event_ms(torch, stream, lambda: render(fl | N.RT_RENDER_GUIDE, film, 6))
-        out["guided"] = line(ms, st)
+        out["guided"] = line(*render_halves(fl | N.RT_RENDER_GUIDE, 6))
         sc.set_guide(None)
         g.close()
+        pl, gd = out["plain"], out["guided"]
+        if gd["noise_rmse"] > 0 and gd["ms"] > 0:
+            # time to equal error, plain over guided (error^2 falls as 1/time), training included
+            out["guided_efficiency"] = (pl["noise_rmse"] ** 2 * pl["ms"]) / (
+                gd["noise_rmse"] ** 2 * (gd["ms"] + 1000 * out["guide_training_s"]))
     sc.set_photon_map(None)
     pm.close()
     sc.close()

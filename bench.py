@@ -377,6 +377,14 @@ def run_ours(args):
                                "scene vs one rt_render per view")
         del groups
 
+    # ---- photon mapping + subsurface scattering + guiding at 4K (config 4)
+    photon_sss = None
+    if world == 1 and args.c4_spp > 0:
+        PR = importlib.import_module("2023_render_engine_b200.photon_render")
+        photon_sss = PR.measure(ctx, torch, stream, width=args.c4_width, height=args.c4_height, spp=args.c4_spp)
+        photon_sss["metric"] = ("Mrays/s, samples/s and photon-map gathers/s of hybrid + subsurface rendering; "
+                                "guided vs plain time to equal noise")
+
     # ---- the reference's own CUDA traversal on the same rays (baseline, not a target)
     ref_cuda = None
     if world == 1 and not args.no_ref_cuda:
@@ -417,6 +425,7 @@ def run_ours(args):
             "guiding": guiding,
             "reference_cuda": ref_cuda,
             "batched": batched,
+            "photon_sss": photon_sss,
         }
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
@@ -446,6 +455,9 @@ def main():
     ap.add_argument("--guide-ref-spp", type=int, default=4096, help="0 skips the guiding measurement")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip the reference CUDA traversal baseline")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view measurement")
+    ap.add_argument("--c4-spp", type=int, default=256, help="config-4 spp per mode (0 skips config 4)")
+    ap.add_argument("--c4-width", type=int, default=3840)
+    ap.add_argument("--c4-height", type=int, default=2160)
     ap.add_argument("--guide-target", type=float, default=0.01)
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)
