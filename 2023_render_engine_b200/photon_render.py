@@ -132,3 +132,31 @@ def measure(ctx, torch, stream, width=3840, height=2160, spp=None, photons=None,
     pm.close()
     sc.close()
     return out
+
+
+def main(argv=None):
+    """Command line: one config-4 measurement on cuda:0, printed as JSON."""
+    import argparse
+    import json
+
+    import torch
+
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--width", type=int, default=3840)
+    ap.add_argument("--height", type=int, default=2160)
+    ap.add_argument("--spp", type=int, default=256)
+    ap.add_argument("--photons", type=int, default=configs.CONFIG4_PHOTONS)
+    ap.add_argument("--plain", action="store_true", help="skip the guided render")
+    a = ap.parse_args(argv)
+    torch.cuda.set_device(0)
+    ctx = core.Context(0)
+    stream = torch.cuda.Stream()  # a stream of its own: the default stream cannot be captured
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    r = measure(ctx, torch, stream, width=a.width, height=a.height, spp=a.spp, photons=a.photons,
+                guided=not a.plain)
+    print(json.dumps(r, indent=1), flush=True)
+
+
+if __name__ == "__main__":
+    main()
