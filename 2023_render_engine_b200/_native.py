@@ -79,6 +79,7 @@ RT_RENDER_COMPAT = 0x2
 RT_RENDER_EXACT_TRACE = 0x4
 RT_RENDER_PHOTON_MAP = 0x8
 RT_RENDER_GUIDE = 0x10
+RT_BUILD_DEVICE, RT_BUILD_HOST = 0, 1
 RT_RENDER_SUBSURFACE = 0x20
 RT_RENDER_HYBRID = 0x40
 
@@ -126,6 +127,8 @@ SIGNATURES = {
     "rt_scene_add_mesh": [_P, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _I32, _INT, ctypes.POINTER(_U32)],
     "rt_scene_add_sphere": [_P, _P, _P, _F32, _U32, _I32, _INT, ctypes.POINTER(_U32)],
     "rt_scene_commit": [_P],
+    "rt_scene_set_build": [_P, _U32],
+    "rt_scene_export_bvh": [_P, _P, _P, _P, _P, _P, _P],
     "rt_scene_stats_get": [_P, ctypes.POINTER(SceneStats)],
     "rt_trace_closest": [_P, _P, _U64, _P, _U32],
     "rt_trace_closest_host": [_P, _P, _U64, _P, _U32],

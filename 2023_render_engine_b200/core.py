@@ -78,6 +78,25 @@ class Scene:
     def commit(self):
         N.check(N.lib().rt_scene_commit(self.handle))
 
+    def set_build(self, mode: int):
+        """Where commit() builds: N.RT_BUILD_DEVICE (default) or N.RT_BUILD_HOST (same bytes)."""
+        N.check(N.lib().rt_scene_set_build(self.handle, mode))
+
+    def export_bvh(self):
+        """The committed structures: (nodes (k, 80) uint8, records (n, 12) float32 whose w lanes
+        hold rank / triangle id / flags bits, reference-tree boxes (2n - 1, 6) float32)."""
+        nn, nr, nb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        N.check(N.lib().rt_scene_export_bvh(self.handle, None, None, None, ctypes.byref(nn), ctypes.byref(nr),
+                                            ctypes.byref(nb)))
+        nodes = np.zeros((nn.value, 80), np.uint8)
+        recs = np.zeros((nr.value, 12), np.float32)
+        boxes = np.zeros((nb.value, 6), np.float32)
+        N.check(N.lib().rt_scene_export_bvh(self.handle, nodes.ctypes.data if nodes.size else None,
+                                            recs.ctypes.data if recs.size else None,
+                                            boxes.ctypes.data if boxes.size else None, ctypes.byref(nn),
+                                            ctypes.byref(nr), ctypes.byref(nb)))
+        return nodes, recs, boxes
+
     def stats(self) -> dict:
         s = N.SceneStats()
         N.check(N.lib().rt_scene_stats_get(self.handle, ctypes.byref(s)))

@@ -6,6 +6,7 @@
 #include <mutex>
 #include <string>
 
+#include "bvh_common.cuh"
 #include "rt_internal.h"
 
 namespace rtb {
@@ -98,7 +99,7 @@ rtb::SceneView rt_scene::view() const
 uint64_t rt_scene::device_bytes() const
 {
     return d_nodes.bytes + d_tris.bytes + d_leafpos.bytes + d_ref_boxes.bytes + d_ref_sorted.bytes + d_ref_pos.bytes +
-           d_spheres.bytes + scratch.queue.bytes + scratch.counters.bytes;
+           d_spheres.bytes + scratch.queue.bytes + scratch.counters.bytes + d_tri_transp.bytes + d_mat_transp.bytes;
 }
 
 extern "C" {
@@ -239,6 +240,14 @@ int rt_scene_add_sphere(rt_scene *s, const float o2w[16], const float w2o[16], f
     return RT_OK;
 }
 
+int rt_scene_set_build(rt_scene *s, uint32_t mode)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_scene_set_build: null scene");
+    if (mode != RT_BUILD_DEVICE && mode != RT_BUILD_HOST) return fail(RT_ERR_INVALID, "rt_scene_set_build: bad mode");
+    s->build_mode = mode;
+    return RT_OK;
+}
+
 int rt_scene_commit(rt_scene *s)
 {
     if (!s) return fail(RT_ERR_INVALID, "rt_scene_commit: null scene");
@@ -246,44 +255,47 @@ int rt_scene_commit(rt_scene *s)
     cudaStream_t st = s->ctx->stream;
     auto t0 = std::chrono::steady_clock::now();
     const uint32_t n = (uint32_t)(s->tri9.size() / 9);
-    // conservative margin: 1e-5 of the largest coordinate magnitude
-    float maxabs = 0.f;
-    for (float x : s->tri9) maxabs = std::max(maxabs, std::fabs(x));
-    const float margin = std::max(1e-5f * maxabs, 1e-30f);
-    Bvh8Host bvh;
-    RefTreeHost ref;
-    build_bvh8(s->tri9.data(), n, margin, bvh);
-    build_ref_tree(s->tri9.data(), n, ref);
-    std::vector<TriRecord> recs(bvh.leaf_tris.size());
-    std::vector<uint32_t> leafpos(n, 0);
-    for (size_t r = 0; r < bvh.leaf_tris.size(); r++) {
-        uint32_t id = bvh.leaf_tris[r];
-        const float *p = s->tri9.data() + 9ull * id;
-        TriRecord &tr = recs[r];
-        uint32_t rank = ref.rank[id], flags = s->tri_transparent[id];
-        tr.v0 = make_float4(p[0], p[1], p[2], 0.f);
-        tr.v1 = make_float4(p[3], p[4], p[5], 0.f);
-        tr.v2 = make_float4(p[6], p[7], p[8], 0.f);
-        std::memcpy(&tr.v0.w, &rank, 4);
-        std::memcpy(&tr.v1.w, &id, 4);
-        std::memcpy(&tr.v2.w, &flags, 4);
-        leafpos[id] = (uint32_t)r;
+    if (n > 0 && s->build_mode == RT_BUILD_DEVICE) {
+        float margin = 0.f;
+        RTB_CHECK(build_scene_device(s, &margin));
+    } else {
+        // conservative margin: 1e-5 of the largest coordinate magnitude
+        float maxabs = 0.f;
+        for (float x : s->tri9) maxabs = std::max(maxabs, std::fabs(x));
+        const float margin = std::max(1e-5f * maxabs, 1e-30f);
+        Bvh8Host bvh;
+        RefTreeHost ref;
+        build_ref_tree(s->tri9.data(), n, ref);
+        build_bvh8(s->tri9.data(), n, margin, ref.sorted.data(), kPlocRadius, bvh);
+        std::vector<TriRecord> recs(bvh.leaf_tris.size());
+        std::vector<uint32_t> leafpos(n, 0);
+        for (size_t r = 0; r < bvh.leaf_tris.size(); r++) {
+            uint32_t id = bvh.leaf_tris[r];
+            const float *p = s->tri9.data() + 9ull * id;
+            TriRecord &tr = recs[r];
+            uint32_t rank = ref.rank[id], flags = s->tri_transparent[id];
+            tr.v0 = make_float4(p[0], p[1], p[2], 0.f);
+            tr.v1 = make_float4(p[3], p[4], p[5], 0.f);
+            tr.v2 = make_float4(p[6], p[7], p[8], 0.f);
+            std::memcpy(&tr.v0.w, &rank, 4);
+            std::memcpy(&tr.v1.w, &id, 4);
+            std::memcpy(&tr.v2.w, &flags, 4);
+            leafpos[id] = (uint32_t)r;
+        }
+        if (bvh.nodes.empty()) {
+            bvh.nodes.resize(1);
+            std::memset(bvh.nodes.data(), 0, sizeof(Bvh8Node));
+            std::memset(bvh.nodes[0].meta, 0xFF, 8);
+        }
+        s->nnodes = bvh.nodes.size();
+        RTB_CHECK(s->d_nodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(Bvh8Node), st));
+        RTB_CHECK(s->d_tris.upload(recs.data(), recs.size() * sizeof(TriRecord), st));
+        RTB_CHECK(s->d_leafpos.upload(leafpos.data(), leafpos.size() * 4, st));
+        RTB_CHECK(s->d_ref_boxes.upload(ref.boxes.data(), ref.boxes.size() * 4, st));
+        RTB_CHECK(s->d_ref_sorted.upload(ref.sorted.data(), ref.sorted.size() * 4, st));
+        RTB_CHECK(s->d_ref_pos.upload(ref.pos.data(), ref.pos.size() * 4, st));
     }
-    if (bvh.nodes.empty()) {
-        bvh.nodes.resize(1);
-        std::memset(bvh.nodes.data(), 0, sizeof(Bvh8Node));
-        std::memset(bvh.nodes[0].meta, 0xFF, 8);
-    }
-    s->nnodes = bvh.nodes.size();
-    s->recs = recs;
-    s->leaf_tris = bvh.leaf_tris;
     s->render_dirty = true;
-    RTB_CHECK(s->d_nodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(Bvh8Node), st));
-    RTB_CHECK(s->d_tris.upload(recs.data(), recs.size() * sizeof(TriRecord), st));
-    RTB_CHECK(s->d_leafpos.upload(leafpos.data(), leafpos.size() * 4, st));
-    RTB_CHECK(s->d_ref_boxes.upload(ref.boxes.data(), ref.boxes.size() * 4, st));
-    RTB_CHECK(s->d_ref_sorted.upload(ref.sorted.data(), ref.sorted.size() * 4, st));
-    RTB_CHECK(s->d_ref_pos.upload(ref.pos.data(), ref.pos.size() * 4, st));
     RTB_CHECK(s->d_spheres.upload(s->spheres.data(), s->spheres.size() * sizeof(SphereRecord), st));
     RTB_CHECK(s->scratch.counters.reserve(64));
     RTB_CHECK(refresh_transparency(s));
@@ -293,13 +305,34 @@ int rt_scene_commit(rt_scene *s)
     return RT_OK;
 }
 
+int rt_scene_export_bvh(rt_scene *s, void *nodes, void *records, float *ref_boxes, uint64_t *nnodes,
+                        uint64_t *nrecords, uint64_t *nref_nodes)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_scene_export_bvh: null scene");
+    if (!s->committed) return fail(RT_ERR_STATE, "rt_scene_export_bvh: scene not committed");
+    RTB_CUDA(cudaSetDevice(s->ctx->device));
+    cudaStream_t st = s->ctx->stream;
+    const uint64_t n = s->tri9.size() / 9;
+    const uint64_t nref = n ? 2 * n - 1 : 0;
+    if (nnodes) *nnodes = s->nnodes;
+    if (nrecords) *nrecords = n;
+    if (nref_nodes) *nref_nodes = nref;
+    if (nodes && s->nnodes)
+        RTB_CUDA(cudaMemcpyAsync(nodes, s->d_nodes.ptr, s->nnodes * sizeof(Bvh8Node), cudaMemcpyDeviceToHost, st));
+    if (records && n) RTB_CUDA(cudaMemcpyAsync(records, s->d_tris.ptr, n * sizeof(TriRecord), cudaMemcpyDeviceToHost, st));
+    if (ref_boxes && nref)
+        RTB_CUDA(cudaMemcpyAsync(ref_boxes, s->d_ref_boxes.ptr, nref * 24, cudaMemcpyDeviceToHost, st));
+    RTB_CUDA(cudaStreamSynchronize(st));
+    return RT_OK;
+}
+
 int rt_scene_stats_get(rt_scene *s, rt_scene_stats *out)
 {
     if (!s || !out) return fail(RT_ERR_INVALID, "rt_scene_stats_get: null argument");
     out->triangles = s->tri9.size() / 9;
     out->spheres = s->spheres.size();
     out->bvh8_nodes = s->nnodes;
-    out->bvh8_leaf_triangles = s->d_tris.bytes / sizeof(TriRecord);
+    out->bvh8_leaf_triangles = s->committed ? s->tri9.size() / 9 : 0;
     out->device_bytes = s->device_bytes();
     out->build_ms = s->build_ms;
     return RT_OK;

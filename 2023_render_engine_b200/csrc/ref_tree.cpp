@@ -18,27 +18,11 @@
 #include <cmath>
 #include <thread>
 
+#include "bvh_common.cuh"
 #include "rt_internal.h"
 
 namespace rtb {
 namespace {
-
-uint32_t expand_bits(uint32_t v)
-{
-    v = (v * 0x00010001u) & 0xFF0000FFu;
-    v = (v * 0x00000101u) & 0x0F00F00Fu;
-    v = (v * 0x00000011u) & 0xC30C30C3u;
-    v = (v * 0x00000005u) & 0x49249249u;
-    return v;
-}
-
-uint32_t morton3d(float x, float y, float z)
-{
-    x = (float)std::fmin(std::fmax((double)x * 1024.0, 0.0), 1023.0);
-    y = (float)std::fmin(std::fmax((double)y * 1024.0, 0.0), 1023.0);
-    z = (float)std::fmin(std::fmax((double)z * 1024.0, 0.0), 1023.0);
-    return expand_bits((uint32_t)x) * 4 + expand_bits((uint32_t)y) * 2 + expand_bits((uint32_t)z);
-}
 
 template <typename F>
 void parallel_chunks(uint32_t n, F &&f)
@@ -75,18 +59,9 @@ void build_ref_tree(const float *tri9, uint32_t n, RefTreeHost &out)
         hi[c] = fmaxf(hi[c], tri9[i]);
     }
     const float diag[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
-    const float third = (float)1 / 3.0f;
     std::vector<uint64_t> keys(n);
     parallel_chunks(n, [&](uint32_t b, uint32_t e) {
-        for (uint32_t t = b; t < e; t++) {
-            const float *p = tri9 + 9 * (size_t)t;
-            float u[3];
-            for (int c = 0; c < 3; c++) {
-                float cen = third * ((p[c] + p[3 + c]) + p[6 + c]);
-                u[c] = (cen - lo[c]) / diag[c];
-            }
-            keys[t] = ((uint64_t)morton3d(u[0], u[1], u[2]) << 32) | t;
-        }
+        for (uint32_t t = b; t < e; t++) keys[t] = ref_sort_key(tri9 + 9 * (size_t)t, t, lo, diag);
     });
     std::sort(keys.begin(), keys.end());
     for (uint32_t i = 0; i < n; i++) {

@@ -712,18 +712,7 @@ int refresh_transparency(rt_scene *s)
     auto mat_transparent = [&](uint32_t m) {
         return m < s->materials.size() && (s->materials[m].flags & RT_MATF_TRANSPARENT) != 0;
     };
-    bool changed = false;
-    for (size_t r = 0; r < s->recs.size(); r++) {
-        uint32_t id = s->leaf_tris[r];
-        uint32_t f = (s->tri_transparent[id] || mat_transparent(s->tri_material[id])) ? 1u : 0u;
-        uint32_t old;
-        std::memcpy(&old, &s->recs[r].v2.w, 4);
-        if (old != f) {
-            std::memcpy(&s->recs[r].v2.w, &f, 4);
-            changed = true;
-        }
-    }
-    if (changed) RTB_CHECK(s->d_tris.upload(s->recs.data(), s->recs.size() * sizeof(TriRecord), st));
+    RTB_CHECK(refresh_record_flags(s));
     bool schanged = false;
     for (auto &sp : s->spheres) {
         uint32_t f = ((sp.flags & 2u) || mat_transparent(sp.material)) ? 1u : 0u;

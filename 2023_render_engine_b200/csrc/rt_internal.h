@@ -129,8 +129,11 @@ struct Bvh8Host {
     std::vector<uint32_t> leaf_tris;  // record index -> triangle id
 };
 
-// Builds the 8-wide BVH over `n` triangles (9 floats each). `margin` enlarges every box.
-void build_bvh8(const float *tri9, uint32_t n, float margin, Bvh8Host &out);
+// Builds the 8-wide BVH over `n` triangles (9 floats each) on the host: PLOC over the
+// Morton order `sorted` of the reference-order tree (radius: clusters searched on each side),
+// boxes enlarged by `margin` (bvh8_build.cpp).
+void build_bvh8(const float *tri9, uint32_t n, float margin, const uint32_t *sorted, uint32_t radius,
+                Bvh8Host &out);
 
 // Reference-order tree (cuda_libraries/BVH.cu:314-341): sorted ids, node boxes and
 // each triangle's rank in the tree's static traversal order.
@@ -175,6 +178,12 @@ int upload_render_data(rt_scene *s);
 // Re-derives the shadow-ray transparency of triangle records / spheres from the
 // mesh flags and the material table; re-uploads what changed.
 int refresh_transparency(rt_scene *s);
+// Sets the records' shadow transparency bits on the device from the triangles' flags and
+// materials (build_gpu.cu).
+int refresh_record_flags(rt_scene *s);
+// Builds the reference-order tree and the 8-wide BVH of a scene's triangles on the device,
+// byte for byte the host build's (build_gpu.cu); the margin used is returned.
+int build_scene_device(rt_scene *s, float margin_out[1]);
 }  // namespace rtb
 
 // ------------------------------------------------------------- handles
@@ -227,6 +236,7 @@ struct rt_scene {
     std::vector<float> normals;
     std::vector<rtb::SphereRecord> spheres;
     bool committed = false;
+    uint32_t build_mode = RT_BUILD_DEVICE;
     double build_ms = 0;
     uint64_t nnodes = 0;
     // device
@@ -241,8 +251,6 @@ struct rt_scene {
         float r, g, b, i;
     };
     std::vector<PL> plight_rgbi;
-    std::vector<rtb::TriRecord> recs;  // host copy of the leaf-ordered triangle records
-    std::vector<uint32_t> leaf_tris;   // record index -> triangle id
     bool render_dirty = true;
     bool has_normals = false;
     uint32_t nemit = 0;
@@ -252,6 +260,7 @@ struct rt_scene {
     int guide_train = 0;            // record training samples while rendering
     uint32_t pm_k = 100;
     float pm_radius = 100.f;
+    rtb::DevBuf d_tri_transp, d_mat_transp;  // per-triangle / per-material transparency (record flags)
     rtb::DevBuf d_mats, d_tri_mat, d_tri_shape, d_tri_nidx, d_normals, d_emit_tri, d_emit_cdf, d_plights;
     rtb::RenderScratch rscratch;
     rtb::SceneView view() const;

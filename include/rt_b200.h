@@ -84,8 +84,25 @@ RT_API int rt_scene_add_sphere(rt_scene *scene, const float object_to_world[16],
 
 /* Builds the acceleration structures: the 8-wide compressed BVH used for traversal
  * and the reference-order tree (BVH::BVH, cuda_libraries/BVH.cu:314-341) whose
- * static order breaks exact distance ties like the reference does. */
+ * static order breaks exact distance ties like the reference does. Replaces
+ * Scene::build (integration/Scene.cu:56-95), whose BVH the reference builds on the host.
+ * The 8-wide BVH is a PLOC tree over the reference tree's Morton order, collapsed to 8-wide
+ * nodes. Both are built on the GPU unless rt_scene_set_build chose the host. */
 RT_API int rt_scene_commit(rt_scene *scene);
+
+#define RT_BUILD_DEVICE 0u /* rt_scene_set_build: build on the GPU (default) */
+#define RT_BUILD_HOST 1u   /* build on the host threads; the same bytes as RT_BUILD_DEVICE */
+/* Where rt_scene_commit builds. Both produce identical structures. */
+RT_API int rt_scene_set_build(rt_scene *scene, uint32_t mode);
+
+/* Copies the committed acceleration structures to host memory, for inspection and
+ * serialisation: nodes (80 bytes each), triangle records (48 bytes each: vertices, with
+ * the reference traversal rank, the triangle id and the flags in the w lanes) and the
+ * reference tree's boxes (6 floats per node, 2n - 1 nodes). Any output may be NULL; a
+ * non-NULL one must hold the count the call reports (query the counts with NULL outputs
+ * first). */
+RT_API int rt_scene_export_bvh(rt_scene *scene, void *nodes, void *records, float *ref_boxes, uint64_t *nnodes,
+                               uint64_t *nrecords, uint64_t *nref_nodes);
 
 typedef struct rt_scene_stats {
     uint64_t triangles;
@@ -93,7 +110,7 @@ typedef struct rt_scene_stats {
     uint64_t bvh8_nodes;
     uint64_t bvh8_leaf_triangles; /* triangle records in BVH8 leaf order */
     uint64_t device_bytes;        /* device memory held by the scene */
-    double build_ms;              /* host build time of the last commit */
+    double build_ms;              /* wall time of the last commit (build and upload) */
 } rt_scene_stats;
 RT_API int rt_scene_stats_get(rt_scene *scene, rt_scene_stats *out);
 
