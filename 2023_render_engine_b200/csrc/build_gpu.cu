@@ -443,8 +443,8 @@ int build_scene_device(rt_scene *s, float margin_out[1])
     }
 
     // 5. collapse, level by level
-    RTB_CHECK(s->d_nodes.reserve(sizeof(Bvh8Node) * (uint64_t)n));
-    Bvh8Node *nodes = s->d_nodes.as<Bvh8Node>();
+    DevBuf d_wide;  // room for the most nodes n triangles can need; copied to its size below
+    Bvh8Node *nodes = buf<Bvh8Node>(d_wide, n, rc);
     uint32_t *leaf_tris = buf<uint32_t>(d_leaf_tris, n, rc), *cur = buf<uint32_t>(d_cur, n, rc),
              *next = buf<uint32_t>(d_next, n, rc), *chbuf = buf<uint32_t>(d_chbuf, 8ull * n, rc);
     uint64_t *counts = buf<uint64_t>(d_counts, n, rc), *offs = buf<uint64_t>(d_offs, n, rc);
@@ -474,6 +474,8 @@ int build_scene_device(rt_scene *s, float margin_out[1])
     }
     if (tstart != n) return fail(RT_ERR_STATE, "build_scene_device: leaf triangles lost");
     s->nnodes = wstart;
+    RTB_CHECK(s->d_nodes.reserve(sizeof(Bvh8Node) * (uint64_t)wstart));
+    RTB_CUDA(cudaMemcpyAsync(s->d_nodes.ptr, nodes, sizeof(Bvh8Node) * (uint64_t)wstart, cudaMemcpyDeviceToDevice, st));
 
     // 6. records
     RTB_CHECK(s->d_tris.reserve(sizeof(TriRecord) * (uint64_t)n));

@@ -197,19 +197,42 @@ def measure_reference_cuda(v, f, o, d, hits_d, N):
         rc = bindings.RefCuda()
     except (FileNotFoundError, OSError) as e:
         return {"unavailable": str(e)}
+    t0 = time.perf_counter()
     h = rc.build(v, f)
+    build_ms = (time.perf_counter() - t0) * 1e3
     try:
         ids, mk, ma = rc.trace(h, o, d, reps=3)
     finally:
         rc.free(h)
     ours = hits_d.cpu().numpy().view(N.HIT_DTYPE)["prim"]
     n = len(ids)
-    return {"value": n / (mk / 1000) / 1e6, "unit": "Mrays/s", "ms_per_call": mk,
+    return {"value": n / (mk / 1000) / 1e6, "unit": "Mrays/s", "ms_per_call": mk, "build_ms": build_ms,
             "api_value": n / (ma / 1000) / 1e6, "api_ms_per_call": ma,
             "id_agreement": float((ids == ours).mean()),
             "build": "reference BVH::intersectRay + Triangle::intersects via thrust::transform, -O3 --use_fast_math "
                      "-maxrregcount=64 (its compile.sh), sm_100a; api = its intersectRaysGpu path (rays to the "
                      "device, transform, ids back, pageable host memory)"}
+
+
+def measure_scene_build(core, N, ctx, v, f, reps=3):
+    """rt_scene_commit of the BVH-stress mesh: the device build (after one warm-up commit that
+    loads the kernels; median of reps) and the host build (the same bytes)."""
+    out = {"triangles": int(f.shape[0])}
+    for name, mode, k in (("device", N.RT_BUILD_DEVICE, reps + 1), ("host", N.RT_BUILD_HOST, 1)):
+        ms = []
+        for _ in range(k):
+            sc = core.Scene(ctx)
+            sc.add_mesh(v, f)
+            sc.set_build(mode)
+            sc.commit()
+            ms.append(sc.stats()["build_ms"])
+            nodes = sc.stats()["bvh8_nodes"]
+            sc.close()
+        out[name + "_ms"] = float(np.median(ms[1:] if k > 1 else ms))
+        out["bvh8_nodes"] = int(nodes)
+    out["note"] = ("commit wall time (build + upload); both builds give the same PLOC 8-wide BVH and "
+                   "reference-order tree")
+    return out
 
 
 def measure_guiding(args, core, N, cfgs, ctx, torch):
@@ -390,6 +413,11 @@ def run_ours(args):
     if world == 1 and not args.no_ref_cuda:
         ref_cuda = measure_reference_cuda(v, f, o, d, hits_d, N)
 
+    # ---- scene commit: device vs host build of the same structures
+    scene_build = measure_scene_build(core, N, ctx, v, f) if world == 1 else None
+    if scene_build is not None and ref_cuda is not None:
+        scene_build["reference_ms"] = ref_cuda["build_ms"]
+
     ms, ms_e2e, ms_trace = max_over_ranks([ms, ms_e2e, ms_trace], world)
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -426,6 +454,7 @@ def run_ours(args):
             "reference_cuda": ref_cuda,
             "batched": batched,
             "photon_sss": photon_sss,
+            "scene_build": scene_build,
         }
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
