@@ -191,6 +191,12 @@ __global__ void k_ploc_merge(BBox *__restrict__ bx, const uint32_t *__restrict__
 
 // ---------------------------------------------------------- depth-first numbering, leaves
 
+__global__ void k_fill(uint32_t *__restrict__ v, uint64_t n, uint32_t x)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * kT + threadIdx.x;
+    if (i < n) v[i] = x;
+}
+
 __global__ void k_sizes(const uint32_t *__restrict__ c0, const uint32_t *__restrict__ c1, uint32_t b, uint32_t e,
                         uint32_t *__restrict__ size)
 {
@@ -317,9 +323,12 @@ int build_scene_device(rt_scene *s, float margin_out[1])
     cudaStream_t st = s->ctx->stream;
     const uint32_t n = (uint32_t)(s->tri9.size() / 9);
     if (n == 0) return fail(RT_ERR_INVALID, "build_scene_device: no triangles");
-    DevBuf d_tri, d_part, d_keys, d_keys2, d_cnt, d_start, d_rank, d_bx, d_c0, d_c1, d_cl, d_cl2, d_nn, d_flags,
-        d_pos, d_tot, d_size, d_first, d_ids, d_leaf, d_cur, d_next, d_chbuf, d_counts, d_offs, d_leaf_tris, d_tt,
-        d_tmp;
+    DevBuf *B = s->ctx->build;
+    DevBuf &d_tri = B[0], &d_part = B[1], &d_keys = B[2], &d_keys2 = B[3], &d_cnt = B[4], &d_start = B[5],
+           &d_rank = B[6], &d_bx = B[7], &d_c0 = B[8], &d_c1 = B[9], &d_cl = B[10], &d_cl2 = B[11], &d_nn = B[12],
+           &d_flags = B[13], &d_pos = B[14], &d_tot = B[15], &d_size = B[16], &d_first = B[17], &d_ids = B[18],
+           &d_leaf = B[19], &d_cur = B[20], &d_next = B[21], &d_chbuf = B[22], &d_counts = B[23], &d_offs = B[24],
+           &d_leaf_tris = B[25], &d_tt = B[26], &d_tmp = B[27], &d_tmp2 = B[28], &d_tmp3 = B[29], &d_wide = B[30];
     int rc = RT_OK;
     float *tri = buf<float>(d_tri, 9ull * n, rc);
     RTB_CHECK(rc);
@@ -397,7 +406,7 @@ int build_scene_device(rt_scene *s, float margin_out[1])
     k_ploc_leaves<<<blocks_for(n), kT, 0, st>>>(tri, sorted, n, margin, bx, cl);
     tmp_bytes = 0;
     RTB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, flags, pos, (int)n, st));
-    tmp = buf<uint8_t>(d_tmp, tmp_bytes, rc);
+    tmp = buf<uint8_t>(d_tmp2, tmp_bytes, rc);
     RTB_CHECK(rc);
     std::vector<uint32_t> batches{0};  // internal nodes made per round: [batches[t], batches[t + 1])
     uint32_t m = n, made = 0;
@@ -428,8 +437,7 @@ int build_scene_device(rt_scene *s, float margin_out[1])
     RTB_CHECK(rc);
     RTB_CUDA(cudaMemsetAsync(ids, 0, 4ull * n, st));
     {
-        std::vector<uint32_t> ones(nb, 1);  // leaf sizes; internal sizes overwritten below
-        RTB_CUDA(cudaMemcpyAsync(size, ones.data(), 4ull * nb, cudaMemcpyHostToDevice, st));
+        k_fill<<<blocks_for(nb), kT, 0, st>>>(size, nb, 1u);  // leaf sizes; internal sizes overwritten below
         RTB_CUDA(cudaMemsetAsync(first, 0, 4ull * nb, st));
         for (size_t t = 0; t + 1 < batches.size(); t++)
             k_sizes<<<blocks_for(batches[t + 1] - batches[t]), kT, 0, st>>>(c0, c1, batches[t], batches[t + 1],
@@ -439,19 +447,17 @@ int build_scene_device(rt_scene *s, float margin_out[1])
                                                                              batches[t], first);
         k_leaf_setup<<<blocks_for(n), kT, 0, st>>>(sorted, first, bx, c0, c1, size, n, ids, leaf);
         RTB_CUDA(cudaGetLastError());
-        RTB_CUDA(cudaStreamSynchronize(st));  // `ones` goes out of scope
     }
 
     // 5. collapse, level by level
-    DevBuf d_wide;  // room for the most nodes n triangles can need; copied to its size below
-    Bvh8Node *nodes = buf<Bvh8Node>(d_wide, n, rc);
+    Bvh8Node *nodes = buf<Bvh8Node>(d_wide, n, rc);  // room for the most nodes n triangles can need
     uint32_t *leaf_tris = buf<uint32_t>(d_leaf_tris, n, rc), *cur = buf<uint32_t>(d_cur, n, rc),
              *next = buf<uint32_t>(d_next, n, rc), *chbuf = buf<uint32_t>(d_chbuf, 8ull * n, rc);
     uint64_t *counts = buf<uint64_t>(d_counts, n, rc), *offs = buf<uint64_t>(d_offs, n, rc);
     RTB_CHECK(rc);
     tmp_bytes = 0;
     RTB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, counts, offs, (int)n, st));
-    tmp = buf<uint8_t>(d_tmp, tmp_bytes, rc);
+    tmp = buf<uint8_t>(d_tmp3, tmp_bytes, rc);
     RTB_CHECK(rc);
     RTB_CUDA(cudaMemcpyAsync(cur, &root, 4, cudaMemcpyHostToDevice, st));
     RTB_CUDA(cudaMemsetAsync(leaf_tris, 0, 4ull * n, st));

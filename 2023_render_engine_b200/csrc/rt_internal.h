@@ -193,6 +193,10 @@ struct rt_context {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int sm_count = 0;
+    // scratch of the device scene build, kept for the next commit (about 330 bytes per
+    // triangle of the largest scene committed): allocating and freeing it per commit cost
+    // more than the build
+    rtb::DevBuf build[32];
 };
 
 struct rt_photon_map {
