@@ -80,6 +80,8 @@ RT_RENDER_EXACT_TRACE = 0x4
 RT_RENDER_PHOTON_MAP = 0x8
 RT_RENDER_GUIDE = 0x10
 RT_BUILD_DEVICE, RT_BUILD_HOST = 0, 1
+(RT_TONEMAP_EQUALIZE, RT_TONEMAP_REINHARD, RT_TONEMAP_REINHARD_JODIE, RT_TONEMAP_ACES, RT_TONEMAP_UNCHARTED2,
+ RT_TONEMAP_GAMMA_CLAMP) = range(6)
 RT_RENDER_SUBSURFACE = 0x20
 RT_RENDER_HYBRID = 0x40
 
@@ -128,6 +130,9 @@ SIGNATURES = {
     "rt_scene_add_sphere": [_P, _P, _P, _F32, _U32, _I32, _INT, ctypes.POINTER(_U32)],
     "rt_scene_commit": [_P],
     "rt_scene_set_build": [_P, _U32],
+    "rt_film_tonemap": [_P, _P, _P, ctypes.c_uint64, ctypes.c_uint64, _U32, _P],
+    "rt_image_write_bmp": [ctypes.c_char_p, _P, _U32, _U32],
+    "rt_image_write_ppm": [ctypes.c_char_p, _P, _U32, _U32],
     "rt_scene_export_bvh": [_P, _P, _P, _P, _P, _P, _P],
     "rt_scene_stats_get": [_P, ctypes.POINTER(SceneStats)],
     "rt_trace_closest": [_P, _P, _U64, _P, _U32],

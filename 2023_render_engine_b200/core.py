@@ -504,6 +504,28 @@ def film_load_hdrbmp(path, width: int, height: int):
     return out, n.value
 
 
+def film_tonemap(film, samples: int, mode: int, use_count: bool = True):
+    """Film::toneMaxPixel of a device film (rt_film_tonemap): (H*W, 3) uint8 torch tensor on the
+    device, film order. samples: the samples per pixel the film holds."""
+    import torch
+
+    npix = film["count"].numel()
+    out = torch.empty(npix * 3, dtype=torch.uint8, device="cuda")
+    s64 = film.get("sum64")
+    N.check(N.lib().rt_film_tonemap(None if s64 is not None else film["sum"].data_ptr(),
+                                    film["count"].data_ptr() if use_count else None,
+                                    None if s64 is None else s64.data_ptr(), npix, int(samples), mode,
+                                    out.data_ptr()))
+    return out.view(npix, 3)
+
+
+def image_write(path, rgb8, width: int, height: int, fmt: str = "bmp"):
+    """Writes (H*W, 3) uint8 RGB (host) as the reference's BMP or PPM file."""
+    a = np.ascontiguousarray(np.asarray(rgb8, dtype=np.uint8))
+    fn = N.lib().rt_image_write_bmp if fmt == "bmp" else N.lib().rt_image_write_ppm
+    N.check(fn(str(path).encode(), a.ctypes.data, width, height))
+
+
 def film_rmse_gpu(film_a, film_b) -> float:
     """computeRMSE of two device films on the GPU (rt_film_rmse)."""
     out = ctypes.c_double()

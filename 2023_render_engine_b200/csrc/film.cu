@@ -1,12 +1,16 @@
 // Film output and comparison: the reference's .hdrbmp accumulation files
-// (Film::storeContributionsToFile / loadContributionsFromFile, camera/Film.cu:366-449) and its
-// computeRMSE (camera/Film.cu:611-632), for films the renderer accumulates on the device.
+// (Film::storeContributionsToFile / loadContributionsFromFile, camera/Film.cu:366-449), its
+// computeRMSE (camera/Film.cu:611-632), and its tone mapping to 8-bit images with the BMP and
+// PPM writers (Film::toneMaxPixel, writeToBMP, writeToPPM, camera/Film.cu:120-360,
+// camera/BMP_Format.cu), for films the renderer accumulates on the device.
 #include <cmath>
+#include <cstring>
 #include <fstream>
 #include <string>
 #include <vector>
 
 #include "rt_internal.h"
+#include "tonemap.cuh"
 
 namespace rtb {
 namespace {
@@ -38,6 +42,81 @@ __global__ void k_film_sqdiff(const float *sa, const uint32_t *ca, const double 
 }
 
 constexpr int kRmseBlocks = 592;
+
+// The film pixel as the reference holds it: the sum over `samples` samples, the invalid ones
+// replaced by the mean of the valid ones (pathTracing.cu:457-490), as rt_film_store_hdrbmp
+// writes it.
+__device__ __forceinline__ D3 film_pixel(const float *s, const uint32_t *c, const double *s64, uint64_t i,
+                                         double samples)
+{
+    D3 p = s64 ? D3{s64[3 * i], s64[3 * i + 1], s64[3 * i + 2]} : D3{s[3 * i], s[3 * i + 1], s[3 * i + 2]};
+    if (c) {
+        const double k = c[i] ? td_div(samples, (double)c[i]) : 0.0;
+        p = p * k;
+    }
+    return p;
+}
+
+constexpr int kTmBlocks = 592, kTmThreads = 256;
+
+// Film::getMaxChannel / getMaxLuminance (Film.cu:120-153) before their division by the
+// sample count: per-block maxima of the channels and of Spectrum::brightness, from 0.
+__global__ void __launch_bounds__(kTmThreads) k_tm_max(const float *s, const uint32_t *c, const double *s64,
+                                                       uint64_t npix, double samples, double *partial)
+{
+    __shared__ double red[2][kTmThreads];
+    double mc = 0.0, ml = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)kTmThreads + threadIdx.x; i < npix; i += (uint64_t)gridDim.x * kTmThreads) {
+        const D3 p = film_pixel(s, c, s64, i, samples);
+        if (p.r > mc) mc = p.r;
+        if (p.g > mc) mc = p.g;
+        if (p.b > mc) mc = p.b;
+        const double l = tm_brightness(p);
+        if (l > ml) ml = l;
+    }
+    red[0][threadIdx.x] = mc;
+    red[1][threadIdx.x] = ml;
+    __syncthreads();
+    for (int o = kTmThreads / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            if (red[0][threadIdx.x + o] > red[0][threadIdx.x]) red[0][threadIdx.x] = red[0][threadIdx.x + o];
+            if (red[1][threadIdx.x + o] > red[1][threadIdx.x]) red[1][threadIdx.x] = red[1][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 2) partial[2 * blockIdx.x + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// the film maxima over the blocks' partial maxima, divided by the sample count
+__global__ void k_tm_final(const double *partial, int nblocks, double samples, double *mm)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double mc = 0.0, ml = 0.0;
+    for (int b = 0; b < nblocks; b++) {
+        if (partial[2 * b] > mc) mc = partial[2 * b];
+        if (partial[2 * b + 1] > ml) ml = partial[2 * b + 1];
+    }
+    mm[0] = td_div(mc, samples);
+    mm[1] = td_div(ml, samples);
+}
+
+__global__ void __launch_bounds__(kTmThreads) k_tm_map(const float *s, const uint32_t *c, const double *s64,
+                                                       uint64_t npix, double samples, uint32_t mode,
+                                                       const double *mm, uint8_t *rgb)
+{
+    const uint64_t i = blockIdx.x * (uint64_t)kTmThreads + threadIdx.x;
+    if (i >= npix) return;
+    const D3 q = tonemap_pixel(film_pixel(s, c, s64, i, samples), samples, mm[0], mm[1], mode);
+    rgb[3 * i] = tm_byte(q.r);
+    rgb[3 * i + 1] = tm_byte(q.g);
+    rgb[3 * i + 2] = tm_byte(q.b);
+}
+
+template <class T>
+void put(std::ofstream &f, T v)  // little-endian field, as BitmapImage writes it on x86
+{
+    f.write(reinterpret_cast<const char *>(&v), sizeof(T));
+}
 
 }  // namespace
 }  // namespace rtb
@@ -96,6 +175,78 @@ int rt_film_store_hdrbmp(const char *path, uint32_t width, uint32_t height, cons
     }
     file.close();
     if (!file) return fail(RT_ERR_INVALID, "rt_film_store_hdrbmp: write failed");
+    return RT_OK;
+}
+
+int rt_film_tonemap(const float *sum_rgb, const uint32_t *count, const double *sum64, uint64_t npix, uint64_t samples,
+                    uint32_t mode, uint8_t *rgb8)
+{
+    if ((!sum_rgb && !sum64) || !rgb8) return fail(RT_ERR_INVALID, "rt_film_tonemap: null argument");
+    if (npix == 0 || samples == 0) return fail(RT_ERR_INVALID, "rt_film_tonemap: empty film");
+    if (mode > RT_TONEMAP_GAMMA_CLAMP) return fail(RT_ERR_INVALID, "rt_film_tonemap: unknown mode");
+    double *scratch = nullptr;  // per-block maxima, then the two film maxima
+    RTB_CUDA(cudaMalloc(&scratch, sizeof(double) * (2 * kTmBlocks + 2)));
+    const double ns = (double)samples;
+    k_tm_max<<<kTmBlocks, kTmThreads>>>(sum_rgb, count, sum64, npix, ns, scratch);
+    k_tm_final<<<1, 32>>>(scratch, kTmBlocks, ns, scratch + 2 * kTmBlocks);
+    k_tm_map<<<(unsigned)((npix + kTmThreads - 1) / kTmThreads), kTmThreads>>>(sum_rgb, count, sum64, npix, ns, mode,
+                                                                              scratch + 2 * kTmBlocks, rgb8);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(scratch);
+    if (e != cudaSuccess) return cuda_status(e, "rt_film_tonemap");
+    return RT_OK;
+}
+
+int rt_image_write_bmp(const char *path, const uint8_t *rgb8, uint32_t width, uint32_t height)
+{
+    if (!path || !rgb8 || !width || !height) return fail(RT_ERR_INVALID, "rt_image_write_bmp: bad argument");
+    std::ofstream f(path, std::ios::binary);
+    if (!f.is_open()) return fail(RT_ERR_INVALID, std::string("rt_image_write_bmp: cannot open ") + path);
+    // BitmapImage (camera/BMP_Format.cu): 14-byte file header, 40-byte info header whose image
+    // size field is (width + 4 - width % 4) * height, then bottom-up rows of BGR bytes, each
+    // padded with zero bytes to a multiple of 4
+    const uint32_t image_size = (width + 4 - (width % 4)) * height;
+    f.write("BM", 2);
+    put<uint32_t>(f, 14 + 40 + image_size);
+    put<uint16_t>(f, 0);
+    put<uint16_t>(f, 0);
+    put<uint32_t>(f, 14 + 40);
+    put<uint32_t>(f, 40);
+    put<int32_t>(f, (int32_t)width);
+    put<int32_t>(f, (int32_t)height);
+    put<uint16_t>(f, 1);
+    put<uint16_t>(f, 24);
+    put<uint32_t>(f, 0);
+    put<uint32_t>(f, image_size);
+    put<uint32_t>(f, 3780);
+    put<uint32_t>(f, 3780);
+    put<uint32_t>(f, 0);
+    put<uint32_t>(f, 0);
+    std::vector<char> row(((3 * (size_t)width + 3) / 4) * 4, 0);
+    for (uint32_t i = 0; i < height; i++) {
+        const uint8_t *src = rgb8 + 3 * (size_t)width * (height - 1 - i);  // film rows top to bottom
+        for (uint32_t j = 0; j < width; j++) {
+            row[3 * j] = (char)src[3 * j + 2];
+            row[3 * j + 1] = (char)src[3 * j + 1];
+            row[3 * j + 2] = (char)src[3 * j];
+        }
+        f.write(row.data(), (std::streamsize)row.size());
+    }
+    f.close();
+    if (!f) return fail(RT_ERR_INVALID, "rt_image_write_bmp: write failed");
+    return RT_OK;
+}
+
+int rt_image_write_ppm(const char *path, const uint8_t *rgb8, uint32_t width, uint32_t height)
+{
+    if (!path || !rgb8 || !width || !height) return fail(RT_ERR_INVALID, "rt_image_write_ppm: bad argument");
+    std::ofstream f(path, std::ios::binary);
+    if (!f.is_open()) return fail(RT_ERR_INVALID, std::string("rt_image_write_ppm: cannot open ") + path);
+    f << "P6\n" << width << " " << height << "\n255\n";  // Film::writeToPPM
+    f.write(reinterpret_cast<const char *>(rgb8), (std::streamsize)(3 * (size_t)width * height));
+    f.close();
+    if (!f) return fail(RT_ERR_INVALID, "rt_image_write_ppm: write failed");
     return RT_OK;
 }
 

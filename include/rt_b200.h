@@ -380,6 +380,27 @@ RT_API int rt_film_store_hdrbmp(const char *path, uint32_t width, uint32_t heigh
                                 const uint32_t *count_dev, const double *sum64_dev, uint64_t samples);
 /* Film::loadContributionsFromFile (camera/Film.cu:393-449): reads `path`.hdrbmp into host
  * sums (3 doubles per pixel) and its samples per pixel. */
+/* Tone mapping of a film to 8-bit RGB (device output, 3 bytes per pixel, film order: the top
+ * row first): Film::toneMaxPixel (camera/Film.cu:156-282) with the film's maximum channel
+ * and maximum luminance (getMaxChannel / getMaxLuminance, Film.cu:120-153), then
+ * (unsigned char)(v * 255) (Film::toneMapBMP / toneMapPPM). The film pixel is the sum over
+ * `samples` samples; with `count` (nullable) the sum is first scaled by samples / count, the
+ * film rt_film_store_hdrbmp writes. Device pointers; sum_rgb or sum64 (FP64, preferred when
+ * given). Runs on the legacy default stream and returns when done. */
+#define RT_TONEMAP_EQUALIZE 0u       /* ToneMappingType equalize: p / max */
+#define RT_TONEMAP_REINHARD 1u       /* reinhard with the film's maximum luminance */
+#define RT_TONEMAP_REINHARD_JODIE 2u /* reinhardJodie */
+#define RT_TONEMAP_ACES 3u           /* ACESfilmic */
+#define RT_TONEMAP_UNCHARTED2 4u     /* uncharted2 (not clamped, as the reference) */
+#define RT_TONEMAP_GAMMA_CLAMP 5u    /* gammaClamp: (p / max)^(1/2.2) */
+RT_API int rt_film_tonemap(const float *sum_rgb, const uint32_t *count, const double *sum64, uint64_t npix,
+                           uint64_t samples, uint32_t mode, uint8_t *rgb8_dev);
+/* 8-bit RGB images (host memory, film order) written as Film::writeToBMP writes them
+ * (BitmapImage, camera/BMP_Format.cu: bottom-up BGR rows padded to 4 bytes) and as
+ * Film::writeToPPM (camera/Film.cu:339-351). `path` is used as given (the reference appends
+ * ".bmp" / ".ppm" to its argument). */
+RT_API int rt_image_write_bmp(const char *path, const uint8_t *rgb8, uint32_t width, uint32_t height);
+RT_API int rt_image_write_ppm(const char *path, const uint8_t *rgb8, uint32_t width, uint32_t height);
 RT_API int rt_film_load_hdrbmp(const char *path, uint32_t width, uint32_t height, double *sum_rgb_host,
                                uint64_t *samples);
 /* computeRMSE (camera/Film.cu:611-632) of two device films on the GPU: sqrt(sum over pixels

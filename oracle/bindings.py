@@ -414,6 +414,20 @@ class RefRender:
             raise RuntimeError("reference film load failed")
         return out, n.value
 
+    def film_write(self, path, sums, samples, mode, bmp=True):
+        """Film::writeToBMP / writeToPPM of a film with these sums: writes path + '.bmp' / '.ppm'."""
+        a = _np(sums, np.float64).reshape(-1, 3)
+        L = self.L
+        L.refr_film_write.argtypes = [ctypes.c_char_p, P, ctypes.c_longlong, I, I]
+        L.refr_film_write(str(path).encode(), a.ctypes.data, samples, mode, int(bmp))
+
+    def bmp_write(self, path, bgr_rows, width, height):
+        """BitmapImage::write_image of (height, width, 3) BGR bytes, file row order (bottom-up)."""
+        a = np.ascontiguousarray(bgr_rows, np.uint8)
+        L = self.L
+        L.refr_bmp_write.argtypes = [ctypes.c_char_p, P, I, I]
+        L.refr_bmp_write(str(path).encode(), a.ctypes.data, width, height)
+
     def film_rmse(self, a, na, b, nb):
         """computeRMSE of two films given by per-pixel sums and samples per pixel."""
         L = self.L

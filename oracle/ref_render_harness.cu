@@ -180,6 +180,31 @@ REFR_API int refr_film_load(const char *path, double *sum, long long *samples)
     return 0;
 }
 
+// Film::writeToBMP / writeToPPM (camera/Film.cu:285-360): the reference's tone mapping of a
+// film with these sums and its 8-bit image files (path without extension; the reference
+// appends ".bmp" or ".ppm").
+REFR_API int refr_film_write(const char *path, const double *sum, long long samples, int mode, int bmp)
+{
+    FilmFill f;
+    fill(f, sum, samples);
+    if (bmp)
+        f.writeToBMP(path, (ToneMappingType)mode);
+    else
+        f.writeToPPM(path, (ToneMappingType)mode);
+    return 0;
+}
+
+// BitmapImage::write_image (camera/BMP_Format.cu) of an image given in its own byte order:
+// row i of image_bytes is row i of the file (bottom-up), BGR.
+REFR_API int refr_bmp_write(const char *path, const unsigned char *bgr_rows, int width, int height)
+{
+    BitmapImage img(width, height);
+    std::memcpy(img.image_bytes, bgr_rows, 3ull * width * height);
+    std::ofstream file(path, std::ios::binary);
+    img.write_image(file);
+    return 0;
+}
+
 REFR_API double refr_film_rmse(const double *a, long long na, const double *b, long long nb)
 {
     FilmFill fa, fb;

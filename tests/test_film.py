@@ -66,3 +66,48 @@ def test_writer_and_gpu_rmse_match_reference(core, gpu_ctx, refr, tmp_path):
     got = core.film_rmse_gpu(fa, fb)
     ref = refr.film_rmse(core.film_mean(fa) * 8, 8, core.film_mean(fb) * 8, 8)
     assert abs(got - ref) <= 1e-6 * ref  # computeRMSE returns a float
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (5, 3), (6, 2), (7, 9), (48, 48)])
+def test_bmp_and_ppm_writers_match_reference_layout(core, refr, tmp_path, w, h):
+    """rt_image_write_bmp against the reference's BitmapImage::write_image on the same pixels
+    (odd widths exercise the row padding and the quirky image-size field); the PPM header."""
+    rng = np.random.default_rng(w * 31 + h)
+    rgb = rng.integers(0, 256, size=(h * w, 3), dtype=np.uint8)
+    core.image_write(tmp_path / "ours.bmp", rgb, w, h, "bmp")
+    bgr_rows = rgb.reshape(h, w, 3)[::-1, :, ::-1]  # file row i = film row h - 1 - i, BGR
+    refr.bmp_write(tmp_path / "ref.bmp", bgr_rows, w, h)
+    assert (tmp_path / "ours.bmp").read_bytes() == (tmp_path / "ref.bmp").read_bytes()
+    core.image_write(tmp_path / "ours.ppm", rgb, w, h, "ppm")
+    assert (tmp_path / "ours.ppm").read_bytes() == f"P6\n{w} {h}\n255\n".encode() + rgb.tobytes()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", range(6))
+@pytest.mark.parametrize("fmt", ["bmp", "ppm"])
+def test_tonemap_files_match_reference(core, refr, tmp_path, mode, fmt):
+    """rt_film_tonemap + the writers against Film::writeToBMP / writeToPPM on the same sums
+    (FP64 film): identical files, except that gammaClamp's pow may round a value that lands
+    within an ulp of a byte boundary the other way."""
+    import torch
+
+    rng = np.random.default_rng(100 + mode)
+    npix = refr.width * refr.height
+    s = random_sums(rng, npix)
+    s[:40] *= 1e4  # values above the white point: uncharted2 goes past 1 (not clamped)
+    samples = 16
+    film = {"sum64": torch.from_numpy(s.reshape(-1)).cuda(),
+            "count": torch.full((npix,), samples, dtype=torch.int32, device="cuda"),
+            "sum": torch.zeros(npix * 3, dtype=torch.float32, device="cuda")}
+    rgb = core.film_tonemap(film, samples, mode).cpu().numpy()
+    ours = tmp_path / f"ours.{fmt}"
+    core.image_write(ours, rgb, refr.width, refr.height, fmt)
+    refr.film_write(tmp_path / "ref", s, samples, mode, bmp=(fmt == "bmp"))
+    a = np.frombuffer(ours.read_bytes(), np.uint8)
+    b = np.frombuffer((tmp_path / f"ref.{fmt}").read_bytes(), np.uint8)
+    assert a.shape == b.shape
+    diff = np.nonzero(a != b)[0]
+    if mode == N.RT_TONEMAP_GAMMA_CLAMP:
+        assert diff.size <= 3 and np.all(np.abs(a[diff].astype(int) - b[diff].astype(int)) == 1), diff
+    else:
+        assert diff.size == 0, (diff[:10], a[diff[:10]], b[diff[:10]])
