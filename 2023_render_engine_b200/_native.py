@@ -71,6 +71,7 @@ class RenderStats(ctypes.Structure):
 
 
 RT_MAT_LAMBERTIAN, RT_MAT_TROWBRIDGE, RT_MAT_DIELECTRIC, RT_MAT_LIGHT, RT_MAT_MIRROR, RT_MAT_PLAIN = range(6)
+RT_MAT_BECKMANN, RT_MAT_TROWBRIDGE_BASIC, RT_MAT_FRESNEL_BLEND, RT_MAT_PLASTIC = 8, 9, 10, 11
 RT_MAT_PHONG = 6
 RT_MAT_SUBSURFACE = 7
 RT_MATF_TRANSPARENT = 0x1
@@ -130,6 +131,8 @@ SIGNATURES = {
     "rt_scene_add_sphere": [_P, _P, _P, _F32, _U32, _I32, _INT, ctypes.POINTER(_U32)],
     "rt_scene_commit": [_P],
     "rt_scene_set_build": [_P, _U32],
+    "rt_material_eval": [_P, _P, _P, ctypes.c_uint64, _P, _P],
+    "rt_material_sample": [_P, _P, ctypes.c_uint64, _U32, _U32, _P, _P, _P, _P],
     "rt_film_tonemap": [_P, _P, _P, ctypes.c_uint64, ctypes.c_uint64, _U32, _P],
     "rt_image_write_bmp": [ctypes.c_char_p, _P, _U32, _U32],
     "rt_image_write_ppm": [ctypes.c_char_p, _P, _U32, _U32],

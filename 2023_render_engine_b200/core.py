@@ -504,6 +504,35 @@ def film_load_hdrbmp(path, width: int, height: int):
     return out, n.value
 
 
+def material_eval(mat, wo, wi):
+    """rt_material_eval on (n, 3) host arrays: (f (n, 3), pdf (n,)) as numpy."""
+    import torch
+
+    a = torch.from_numpy(np.ascontiguousarray(wo, np.float32).reshape(-1)).cuda()
+    b = torch.from_numpy(np.ascontiguousarray(wi, np.float32).reshape(-1)).cuda()
+    n = a.numel() // 3
+    f = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    pdf = torch.empty(n, dtype=torch.float32, device="cuda")
+    N.check(N.lib().rt_material_eval(ctypes.byref(mat), a.data_ptr(), b.data_ptr(), n, f.data_ptr(), pdf.data_ptr()))
+    return f.cpu().numpy().reshape(n, 3), pdf.cpu().numpy()
+
+
+def material_sample(mat, wo, seed: int = 0, flags: int = 0):
+    """rt_material_sample on (n, 3) host arrays: (wi, value, pdf, delta) as numpy."""
+    import torch
+
+    a = torch.from_numpy(np.ascontiguousarray(wo, np.float32).reshape(-1)).cuda()
+    n = a.numel() // 3
+    wi = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    val = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    pdf = torch.empty(n, dtype=torch.float32, device="cuda")
+    dl = torch.empty(n, dtype=torch.uint8, device="cuda")
+    N.check(N.lib().rt_material_sample(ctypes.byref(mat), a.data_ptr(), n, seed, flags, wi.data_ptr(), val.data_ptr(),
+                                       pdf.data_ptr(), dl.data_ptr()))
+    return (wi.cpu().numpy().reshape(n, 3), val.cpu().numpy().reshape(n, 3), pdf.cpu().numpy(),
+            dl.cpu().numpy().astype(bool))
+
+
 def film_tonemap(film, samples: int, mode: int, use_count: bool = True):
     """Film::toneMaxPixel of a device film (rt_film_tonemap): (H*W, 3) uint8 torch tensor on the
     device, film order. samples: the samples per pixel the film holds."""

@@ -266,6 +266,8 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
             Le = bs.color * m.intensity;
         } else if (bs.type == RT_MAT_PLAIN && (flags & kCameraRay)) {
             Le = bs.color;  // PlainMaterial::getEmittedRadiance on camera rays
+        } else if (bs.type == RT_MAT_FRESNEL_BLEND) {
+            Le = v3(m.extra[0], m.extra[1], m.extra[2]);  // FresnelBlendMaterial::getEmittedRadiance: ke
         }
         if (!is_black(Le)) {
             float w = 1.f;
@@ -656,7 +658,7 @@ int rt_scene_set_materials(rt_scene *s, const rt_material *table, uint32_t n)
 {
     if (!s || (!table && n)) return fail(RT_ERR_INVALID, "rt_scene_set_materials: null argument");
     for (uint32_t i = 0; i < n; i++)
-        if (table[i].type > RT_MAT_SUBSURFACE) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_materials: unknown type");
+        if (table[i].type > RT_MAT_PLASTIC) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_materials: unknown type");
     s->materials.assign(table, table + n);
     s->render_dirty = true;
     return RT_OK;

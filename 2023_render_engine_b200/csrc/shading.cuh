@@ -225,8 +225,9 @@ __device__ __forceinline__ float ggx_pdf_h(const Ggx &g, V3 wo, V3 h)
     return (1.0f / (1 + ggx_lambda(g, wo))) / abs_cos(wo) * ggx_D(g, h) * abs_cos2(wo, h);
 }
 
-// lightReflected: D F G / (4 cos_i cos_o) * kd * |cos_i|
-__device__ __forceinline__ V3 ggx_eval(const Ggx &g, V3 kd, V3 eta, V3 k, V3 wo, V3 wi)
+// lightReflected: D F G / (4 cos_i cos_o) * kd * |cos_i| (F = 1 for TrowbridgeBasicBSDF,
+// TrowbridgeBasicBSDF.cu:185-186)
+__device__ __forceinline__ V3 ggx_eval(const Ggx &g, V3 kd, V3 eta, V3 k, V3 wo, V3 wi, bool unit_fresnel = false)
 {
     wo = normalize(wo);
     wi = normalize(wi);
@@ -238,7 +239,9 @@ __device__ __forceinline__ V3 ggx_eval(const Ggx &g, V3 kd, V3 eta, V3 k, V3 wo,
     if (dot(h, h) == 0) return v3(0, 0, 0);
     h = normalize(h);
     float c = abs_cos2(wo, h);
-    V3 F = v3(fresnel_conductor(c, eta.x, k.x), fresnel_conductor(c, eta.y, k.y), fresnel_conductor(c, eta.z, k.z));
+    V3 F = unit_fresnel ? v3(1, 1, 1)
+                        : v3(fresnel_conductor(c, eta.x, k.x), fresnel_conductor(c, eta.y, k.y),
+                             fresnel_conductor(c, eta.z, k.z));
     float D = ggx_D(g, h);
     float G = 1.0f / (1 + ggx_lambda(g, wo) + ggx_lambda(g, wi));
     return F * (D * G / (4 * ci * co)) * kd * ci;
@@ -274,6 +277,90 @@ __device__ __forceinline__ V3 ggx_sample_h(const Ggx &g, V3 wo, float u1, float 
     float pz = sqrtf(fmaxf(0.f, 1 - (px * px + py * py)));
     V3 nh = T1 * px + T2 * py + wh * pz;
     return normalize(v3(g.ax * nh.x, g.ay * nh.y, fmaxf(1e-6f, nh.z)));
+}
+
+// Beckmann distribution and Smith lambda (geometricMath.cu:377-421) of a direction as given:
+// the reference also evaluates D at unnormalised sums of directions (BeckmannBSDF::pdf,
+// FresnelBlendMaterial::pdf), where cos2t is h.z^2 of the raw vector.
+__device__ __forceinline__ float beckmann_D(V3 h, float ax, float ay)
+{
+    const float t2 = tan2t(h);
+    if (isinf(t2)) return 0.f;
+    const float c4 = cos2t(h) * cos2t(h);
+    const float denom = kPi * ax * ay * c4;
+    const float cp = cosphi(h), sp = sinphi(h);
+    const float p = fabsf(cp * cp) / (ax * ax) + fabsf(sp * sp) / (ay * ay);
+    return expf(-t2 * p) / denom;
+}
+__device__ __forceinline__ float beckmann_lambda(V3 w, float ax, float ay)
+{
+    const float tt = fabsf(sqrtf(sin2t(w)) / (w.z / length(w)));
+    if (isinf(tt)) return 0.f;
+    const float cp = cosphi(w), sp = sinphi(w);
+    const float alpha = sqrtf(fabsf(cp * cp) * ax * ax + fabsf(sp * sp) * ay * ay);
+    const double a = 1.0 / (alpha * tt);
+    if (a >= 1.6) return 0.f;
+    return (float)((1 - 1.259 * a + 0.396 * a * a) / (3.535 * a + 2.181 * a * a));
+}
+// sampleHalfBeckman (BeckmannBSDF.cu:89-110): tan^2 = -ax ay log(1 - u1), phi = 2 pi u2, on
+// wo's side
+__device__ __forceinline__ V3 beckmann_sample_h(V3 wo, float ax, float ay, float u1, float u2)
+{
+    float lg = logf(1 - u1);
+    if (isinf(lg)) lg = 0.f;
+    const float t2 = -ax * ay * lg;
+    const float phi = 2 * kPi * u2;
+    const float c = 1 / sqrtf(1 + t2);
+    const float s = sqrtf(fmaxf(0.f, 1 - c * c));
+    float sn, cs;
+    sincosf(phi, &sn, &cs);
+    V3 h = v3(s * cs, s * sn, c);
+    if (!(wo.z * h.z > 0)) h = -h;
+    return h;
+}
+// BeckmannBSDF::lightReflected (BeckmannBSDF.cu:53-87), |cos wi| included
+__device__ __forceinline__ V3 beckmann_eval(const Ggx &g, V3 kd, V3 eta, V3 k, V3 wo, V3 wi)
+{
+    if (!(wo.z * wi.z > 0)) return v3(0, 0, 0);
+    if (fmaxf(g.ax, g.ay) < 1e-3f) return v3(0, 0, 0);
+    const float co = abs_cos(wo), ci = abs_cos(wi);
+    V3 h = wi + wo;
+    if (ci == 0 || co == 0) return v3(0, 0, 0);
+    if (h.x == 0 && h.y == 0 && h.z == 0) return v3(0, 0, 0);
+    h = normalize(h);
+    const float c = dot(wi, h) / (length(wi) * length(h));
+    const V3 F = v3(fresnel_conductor(c, eta.x, k.x), fresnel_conductor(c, eta.y, k.y), fresnel_conductor(c, eta.z, k.z));
+    const float D = beckmann_D(h, g.ax, g.ay);
+    const float G = 1 / (1 + beckmann_lambda(wo, g.ax, g.ay) + beckmann_lambda(wi, g.ax, g.ay));
+    return kd * D * G * F * (1.0f / (4 * ci * co)) * ci;
+}
+// BeckmannBSDF::pdf (BeckmannBSDF.cu:118-122): D(h) |cos h| / (4 |cos(wo, h)|) at the
+// unnormalised h = wi + wo
+__device__ __forceinline__ float beckmann_pdf(const Ggx &g, V3 wo, V3 wi)
+{
+    const V3 h = wi + wo;
+    return beckmann_D(h, g.ax, g.ay) * abs_cos(h) / (4 * abs_cos2(wo, h));
+}
+// FresnelBlendMaterial::lightReflected (FresnelBlendMaterial.cu:111-135) with its kd = 1,
+// ks = 0, alpha = 0.5: a diffuse lobe plus Schlick(R0 = 0) x Beckmann over
+// 4 |cos(wi, h)| max(|cos wi|, |cos wo|); not weighted by |cos wi|
+__device__ __forceinline__ V3 fresnel_blend_eval(V3 wo, V3 wi)
+{
+    auto pow5 = [](float x) { return (x * x) * (x * x) * x; };
+    const float diffuse = (28.f / (23.f * kPi)) * (1 - pow5(1 - 0.5f * abs_cos(wi))) * (1 - pow5(1 - 0.5f * abs_cos(wo)));
+    V3 h = wi + wo;
+    if (h.x == 0 && h.y == 0 && h.z == 0) return v3(0, 0, 0);
+    h = normalize(h);
+    const float num = pow5(1 - dot(wi, h) / (length(wi) * length(h))) * beckmann_D(h, 0.5f, 0.5f);
+    const float denom = 4 * abs_cos2(wi, h) * fmaxf(abs_cos(wi), abs_cos(wo));
+    const float s = diffuse + num / denom;
+    return v3(s, s, s);
+}
+// FresnelBlendMaterial::pdf (FresnelBlendMaterial.cu:137-141): D(h) |cos h| at h = wi + wo
+__device__ __forceinline__ float fresnel_blend_pdf(V3 wo, V3 wi)
+{
+    const V3 h = wi + wo;
+    return beckmann_D(h, 0.5f, 0.5f) * abs_cos(h);
 }
 
 // ------------------------------------------------------------- ONB / frames

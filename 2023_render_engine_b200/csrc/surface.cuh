@@ -166,16 +166,21 @@ __device__ __forceinline__ bool is_phong(uint32_t type) { return type == RT_MAT_
 
 // Material::isScattering: PhongMaterial / SSMaterial scatter when kd is not black
 // (PhongMaterial.cu:45-48, SSMaterial.cu:55-58).
+// FresnelBlendMaterial scatters (its kd is always 1, FresnelBlendMaterial.cu:33-36).
 __device__ __forceinline__ bool is_scattering(const Bsdf &b)
 {
     if (is_phong(b.type)) return fmaxf(b.color.x, fmaxf(b.color.y, b.color.z)) > 0.f;
-    return b.type == RT_MAT_LAMBERTIAN || b.type == RT_MAT_TROWBRIDGE || b.type == RT_MAT_PLAIN;
+    return b.type == RT_MAT_LAMBERTIAN || b.type == RT_MAT_TROWBRIDGE || b.type == RT_MAT_PLAIN ||
+           b.type == RT_MAT_BECKMANN || b.type == RT_MAT_TROWBRIDGE_BASIC || b.type == RT_MAT_FRESNEL_BLEND ||
+           b.type == RT_MAT_PLASTIC;
 }
 __device__ __forceinline__ bool is_specular(const Bsdf &b)
 {
-    // Material::isSpecular overrides; PhongMaterial: ks not black (PhongMaterial.cu:55-58)
+    // Material::isSpecular overrides; PhongMaterial: ks not black (PhongMaterial.cu:55-58);
+    // Beckmann, TrowbridgeBasic and PlasticUnreal: true; FresnelBlend: its ks (0) not black
     if (b.type == RT_MAT_PHONG) return fmaxf(b.k.x, fmaxf(b.k.y, b.k.z)) > 0.f;
-    return b.type == RT_MAT_TROWBRIDGE || b.type == RT_MAT_DIELECTRIC;
+    return b.type == RT_MAT_TROWBRIDGE || b.type == RT_MAT_DIELECTRIC || b.type == RT_MAT_BECKMANN ||
+           b.type == RT_MAT_TROWBRIDGE_BASIC || b.type == RT_MAT_PLASTIC;
 }
 
 // PhongMaterial::lightReflected (PhongMaterial.cu:70-88): the Lambertian term plus
@@ -196,8 +201,8 @@ __device__ __forceinline__ V3 bsdf_eval(const Bsdf &b, V3 wo, V3 wi, float &pdf)
 {
     pdf = 0.f;
     switch (b.type) {
-    case RT_MAT_LAMBERTIAN:  // LambertianBSDF.cu:32-47
-        pdf = (wo.z * wi.z > 0) ? fabsf(wi.z) * kInvPi : 0.f;
+    case RT_MAT_LAMBERTIAN:  // LambertianBSDF.cu:32-47: cosine(wi) / pi on wo's side (signed)
+        pdf = (wo.z * wi.z > 0) ? wi.z / length(wi) * kInvPi : 0.f;
         return b.color * (kInvPi * abs_cos(wi));
     case RT_MAT_PHONG:
     case RT_MAT_SUBSURFACE:  // PhongMaterial::pdf: cosine(wi) / pi on wo's side (PhongMaterial.cu:94-100)
@@ -206,6 +211,17 @@ __device__ __forceinline__ V3 bsdf_eval(const Bsdf &b, V3 wo, V3 wi, float &pdf)
     case RT_MAT_TROWBRIDGE:
         pdf = ggx_pdf(b.g, wo, wi);
         return ggx_eval(b.g, b.color, b.eta, b.k, wo, wi);
+    case RT_MAT_TROWBRIDGE_BASIC:  // TrowbridgeBasicBSDF.cu:155-210
+        pdf = ggx_pdf(b.g, wo, wi);
+        return ggx_eval(b.g, b.color, b.eta, b.k, wo, wi, true);
+    case RT_MAT_BECKMANN:  // BeckmannBSDF.cu:53-122
+        pdf = beckmann_pdf(b.g, wo, wi);
+        return beckmann_eval(b.g, b.color, b.eta, b.k, wo, wi);
+    case RT_MAT_FRESNEL_BLEND:  // FresnelBlendMaterial.cu:111-141
+        pdf = fresnel_blend_pdf(wo, wi);
+        return fresnel_blend_eval(wo, wi);
+    case RT_MAT_PLASTIC:  // PlasticUnrealMaterial.cu:49-59: the Lambertian lobe, pdf 0
+        return b.color * (kInvPi * abs_cos(wi));
     default:
         return v3(0, 0, 0);
     }
@@ -298,6 +314,66 @@ __device__ __forceinline__ V3 bsdf_sample(const Bsdf &b, V3 wo, Pcg &r, bool com
         delta = true;
         wi = v3(-wo.x, -wo.y, wo.z);
         return b.color;
+    case RT_MAT_TROWBRIDGE_BASIC: {  // TrowbridgeBasicBSDF.cu:213-246: Trowbridge with F = 1
+        V3 won = normalize(wo);
+        if (fmaxf(b.g.ax, b.g.ay) < 1e-3f) {
+            wi = v3(-won.x, -won.y, won.z);
+            delta = true;
+            return v3(1, 1, 1);
+        }
+        float u1 = pcg_float(r), u2 = pcg_float(r);
+        V3 h = ggx_sample_h(b.g, won, u1, u2);
+        wi = h * (2 * dot(won, h)) - won;
+        pdf = ggx_pdf_h(b.g, won, h) / (4 * abs_cos2(won, h));
+        V3 f = ggx_eval(b.g, b.color, b.eta, b.k, won, wi, true);
+        if (!(pdf > 0)) return v3(0, 0, 0);
+        return f * (1.0f / pdf);
+    }
+    case RT_MAT_BECKMANN: {  // BeckmannBSDF.cu:125-148
+        if (fmaxf(b.g.ax, b.g.ay) < 1e-3f) {
+            wi = v3(-wo.x, -wo.y, wo.z);
+            delta = true;
+            const float c = abs_cos(wi);
+            return v3(fresnel_conductor(c, b.eta.x, b.k.x), fresnel_conductor(c, b.eta.y, b.k.y),
+                      fresnel_conductor(c, b.eta.z, b.k.z));
+        }
+        pcg_float(r);  // the reference draws a 2D sample it does not use
+        pcg_float(r);
+        const float u1 = pcg_float(r), u2 = pcg_float(r);
+        const V3 h = beckmann_sample_h(wo, b.g.ax, b.g.ay, u1, u2);
+        wi = h * (2 * dot(wo, h)) - wo;  // reflect (geometricMath.cu:197-200)
+        const float sp = beckmann_D(h, b.g.ax, b.g.ay) * abs_cos(h) / (4 * abs_cos2(wo, h));
+        pdf = beckmann_pdf(b.g, wo, wi);  // the pdf the next-event side evaluates (MIS pairs)
+        if (!(sp > 0)) return v3(0, 0, 0);
+        return beckmann_eval(b.g, b.color, b.eta, b.k, wo, wi) * (1.0f / sp);
+    }
+    case RT_MAT_FRESNEL_BLEND: {  // FresnelBlendMaterial.cu:143-176: its roulette always takes
+                                  // this branch; the sample is h - wo, divided by pdf(wo, wi)
+        pcg_float(r);  // roulette
+        pcg_float(r);  // unused 2D sample
+        pcg_float(r);
+        const float u1 = pcg_float(r), u2 = pcg_float(r);
+        const V3 h = beckmann_sample_h(wo, 0.5f, 0.5f, u1, u2);
+        const V3 raw = h - wo;
+        pdf = fresnel_blend_pdf(wo, raw);
+        if (!(pdf > 0) || dot(raw, raw) == 0) {
+            wi = v3(0, 0, 1);
+            return v3(0, 0, 0);
+        }
+        wi = normalize(raw);  // the ray direction; the value uses the raw vector, as the reference
+        return fresnel_blend_eval(wo, raw) * (1.0f / pdf);
+    }
+    case RT_MAT_PLASTIC: {  // PlasticUnrealMaterial.cu:61-76: Lambertian (0.7) or mirror (0.3),
+                            // each returning its own value undivided; pdf() is 0
+        if (pcg_float(r) < 0.7f) {
+            float u1 = pcg_float(r), u2 = pcg_float(r);
+            wi = cosine_hemisphere(u1, u2);
+            return b.color;
+        }
+        delta = true;
+        wi = v3(-wo.x, -wo.y, wo.z);
+        return b.color;
+    }
     default:  // Light (NullBSDF) and Plain: no scattering
         wi = v3(0, 0, 0);
         return v3(0, 0, 0);

@@ -187,9 +187,15 @@ typedef enum rt_material_type {
     RT_MAT_MIRROR = 4,     /* perfect specular reflector (MirrorMaterial.cu) */
     RT_MAT_PLAIN = 5,      /* PlainMaterial: returns its colour on camera hits only */
     RT_MAT_PHONG = 6,      /* PhongMaterial (PhongMaterial.cu): color = kd, k = ks, roughness[0] = ns */
-    RT_MAT_SUBSURFACE = 7  /* SSMaterial (SSMaterial.cu): a Phong surface (color = kd, k = ks, roughness[0] = ns)
+    RT_MAT_SUBSURFACE = 7, /* SSMaterial (SSMaterial.cu): a Phong surface (color = kd, k = ks, roughness[0] = ns)
                               over a medium for the dipole photon estimate: ior = eta, eta = sigma_s,
                               extra = sigma_a, roughness[1] = g (phase asymmetry) */
+    RT_MAT_BECKMANN = 8,         /* BeckmannMaterial (BeckmannBSDF.cu): color = kd, eta, k, roughness x/y
+                                    (alpha = sqrt(roughness)) */
+    RT_MAT_TROWBRIDGE_BASIC = 9, /* TrowbridgeBasicMaterial: RT_MAT_TROWBRIDGE with Fresnel 1 */
+    RT_MAT_FRESNEL_BLEND = 10,   /* FresnelBlendMaterial: extra = ke (emission); its constructor fixes
+                                    kd = 1, ks = 0 and alpha = 0.5 */
+    RT_MAT_PLASTIC = 11,         /* PlasticUnrealMaterial(color, ior): kd = ks = color */
 } rt_material_type;
 
 #define RT_MATF_TRANSPARENT 0x1u /* ignored by shadow rays (Material::isTransparent) */
@@ -204,6 +210,19 @@ typedef struct rt_material {
     float ior;            /* Dielectric index of refraction (Glass: 1.5) */
     float extra[3];       /* RT_MAT_SUBSURFACE: sigma_a */
 } rt_material;
+
+/* A material's BSDF for n direction pairs in the shading frame (normal +z), device arrays of
+ * 3 floats per direction: f = what Material::lightReflected returns (f |cos wi| for most
+ * materials; Phong and FresnelBlend leave out the cosine, as the reference does) and
+ * pdf = Material::pdf (nullable). The renderer's own code (materials/*.cu). Runs on the
+ * legacy default stream and returns when done. */
+RT_API int rt_material_eval(const rt_material *m, const float *wo, const float *wi, uint64_t n, float *f, float *pdf);
+/* Material::sampleDirection for n outgoing directions: wi, the value it returns (f |cos| / pdf
+ * in the reference's convention), the pdf the renderer pairs with it (nullable) and whether the
+ * sample is a delta (nullable, 1 byte each). Sample i uses the random stream (i, seed).
+ * flags: RT_RENDER_COMPAT selects the reference's dielectric estimator. */
+RT_API int rt_material_sample(const rt_material *m, const float *wo, uint64_t n, uint32_t seed, uint32_t flags, float *wi,
+                              float *value, float *pdf, uint8_t *delta);
 
 /* Replaces the Material* each Shape/Triangle points to (Triangle::setMaterial,
  * Shape::setMaterial): a table indexed by the `material` ids given at add time. */

@@ -99,6 +99,26 @@ inline bool to_rt_material(const Material *m, rt_material &o)
         // TrowbridgeBSDF keeps alpha = sqrt(roughness) (TrowbridgeBSDF.cu:56-59)
         o.roughness[0] = (float)(t->bsdf.alphaX * t->bsdf.alphaX);
         o.roughness[1] = (float)(t->bsdf.alphaY * t->bsdf.alphaY);
+    } else if (const auto *tb = dynamic_cast<const TrowbridgeBasicMaterial *>(m)) {
+        o.type = RT_MAT_TROWBRIDGE_BASIC;  // TrowbridgeBasicBSDF keeps alpha = sqrt(roughness) too
+        rgb(tb->bsdf.kd, o.color);
+        rgb(tb->bsdf.eta, o.eta);
+        rgb(tb->bsdf.k, o.k);
+        o.roughness[0] = (float)(tb->bsdf.alphaX * tb->bsdf.alphaX);
+        o.roughness[1] = (float)(tb->bsdf.alphaY * tb->bsdf.alphaY);
+    } else if (const auto *bk = dynamic_cast<const BeckmannMaterial *>(m)) {
+        o.type = RT_MAT_BECKMANN;  // BeckmannBSDF: alpha = sqrt(roughness) (BeckmannBSDF.cu:30-37)
+        rgb(bk->bsdf.kd, o.color);
+        rgb(bk->bsdf.eta, o.eta);
+        rgb(bk->bsdf.k, o.k);
+        o.roughness[0] = (float)(bk->bsdf.alphaX * bk->bsdf.alphaX);
+        o.roughness[1] = (float)(bk->bsdf.alphaY * bk->bsdf.alphaY);
+    } else if (const auto *fb = dynamic_cast<const FresnelBlendMaterial *>(m)) {
+        o.type = RT_MAT_FRESNEL_BLEND;  // kd = 1, ks = 0, alpha = 0.5 fixed by its constructor
+        rgb(fb->ke, o.extra);
+    } else if (const auto *pu = dynamic_cast<const PlasticUnrealMaterial *>(m)) {
+        o.type = RT_MAT_PLASTIC;
+        rgb(pu->kd, o.color);
     } else if (const auto *d = dynamic_cast<const DielectricMaterial *>(m)) {
         o.type = RT_MAT_DIELECTRIC;
         rgb(d->ks, o.color);

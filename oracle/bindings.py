@@ -254,6 +254,21 @@ def restated_phong_eval(restated, material, wo, wi):
     return f, pdf
 
 
+def ref_material_eval(refo, kind, kd, eta, k, rx, ry, wo, wi):
+    """Material::lightReflected / pdf of the reference's own class (kind: rt_material_type)."""
+    L = refo.L
+    L.refo_material_eval.argtypes = [I, P, P, P, ctypes.c_float, ctypes.c_float, P, P, U32, P, P]
+    L.refo_material_eval.restype = I
+    a, b = _np(wo, np.float32).reshape(-1, 3), _np(wi, np.float32).reshape(-1, 3)
+    p = [_np(x, np.float32) for x in (kd, eta, k)]
+    f = np.zeros((a.shape[0], 3), np.float32)
+    pdf = np.zeros(a.shape[0], np.float32)
+    if L.refo_material_eval(kind, *[x.ctypes.data for x in p], rx, ry, a.ctypes.data, b.ctypes.data, a.shape[0],
+                            f.ctypes.data, pdf.ctypes.data) != 0:
+        raise ValueError(f"unknown material kind {kind}")
+    return f, pdf
+
+
 def ref_phong_eval(refo, kd, ks, ns, wo, wi):
     """The reference's PhongMaterial::lightReflected / pdf."""
     L = refo.L
@@ -465,6 +480,8 @@ class RefCompat:
         L.refc_render.argtypes = [ctypes.c_char_p, I, P, P, ctypes.c_uint32, P]
         L.refc_render.restype = I
         L.refc_error.restype = ctypes.c_char_p
+        L.refc_map_material.argtypes = [I, P, P, P, ctypes.c_float, ctypes.c_float, P]
+        L.refc_map_material.restype = I
         self.L = L
         w, h, s, d = (ctypes.c_int() for _ in range(4))
         L.refc_config(ctypes.byref(w), ctypes.byref(h), ctypes.byref(s), ctypes.byref(d))

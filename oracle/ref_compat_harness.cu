@@ -71,6 +71,10 @@
 #include "materials/PlasticUnrealMaterial.cu"
 #include "materials/PlainMaterial.cu"
 #include "materials/PhongMaterial.cu"
+#include "materials/TrowbridgeMaterial.cu"
+#include "materials/TrowbridgeBasicMaterial.cu"
+#include "materials/BeckmannMaterial.cu"
+#include "materials/FresnelBlendMaterial.cu"
 #include "textures/Texture.cu"
 #include "textures/SphericalTexture.cu"
 #include "cuda_libraries/FileImporting.cu"
@@ -97,6 +101,25 @@ REFC_API int refc_config(int *w, int *h, int *spp, int *depth)
 }
 
 REFC_API const char *refc_error() { return g_error.c_str(); }
+
+// The drop-in layer's mapping of a reference material (rt_material_type numbering of `kind`:
+// 8 Beckmann, 9 TrowbridgeBasic, 10 FresnelBlend with emission ke = kd, 11 PlasticUnreal,
+// 1 Trowbridge) into `out`. Returns 0, or 1 when the layer does not map it.
+REFC_API int refc_map_material(int kind, const float *kd, const float *eta, const float *k, float rx, float ry,
+                               rt_material *out)
+{
+    const Spectrum s_kd(kd[0], kd[1], kd[2]), s_eta(eta[0], eta[1], eta[2]), s_k(k[0], k[1], k[2]);
+    std::unique_ptr<Material> m;
+    switch (kind) {
+    case 1: m.reset(new TrowbridgeMaterial(s_kd, s_eta, s_k, rx, ry)); break;
+    case 8: m.reset(new BeckmannMaterial(s_kd, s_eta, s_k, rx, ry)); break;
+    case 9: m.reset(new TrowbridgeBasicMaterial(s_kd, s_eta, s_k, rx, ry)); break;
+    case 10: m.reset(new FresnelBlendMaterial(Spectrum(0), Spectrum(1), Spectrum(0), s_kd, 1.5f, 1.f)); break;
+    case 11: m.reset(new PlasticUnrealMaterial(s_kd, 1.5f)); break;
+    default: return 1;
+    }
+    return rtb::compat_detail::to_rt_material(m.get(), *out) ? 0 : 1;
+}
 
 // planes: 12 floats each, Plane(corner, axisX, axisY, normal); kd: 3 floats each. out_mean:
 // the film's per-pixel sum / spp after rtb::PathTracerIntegrator::render. Returns 0, or 1

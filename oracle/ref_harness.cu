@@ -60,6 +60,11 @@
 #include "materials/LambertianMaterial.cu"
 #include "materials/GlassMaterial.cu"
 #include "materials/PhongMaterial.cu"
+#include "materials/TrowbridgeMaterial.cu"
+#include "materials/TrowbridgeBasicMaterial.cu"
+#include "materials/BeckmannMaterial.cu"
+#include "materials/FresnelBlendMaterial.cu"
+#include "materials/PlasticUnrealMaterial.cu"
 #undef swap
 
 #define REFO_API extern "C" __attribute__((visibility("default")))
@@ -363,6 +368,34 @@ REFO_API void refo_diffusion_term(const float *cam_p, const float *cam_dir, cons
     out[0] = s.getR();
     out[1] = s.getG();
     out[2] = s.getB();
+}
+
+// Material::lightReflected and ::pdf of the reference's own classes in shading space for n
+// direction pairs: kind 0 Lambertian, 1 Trowbridge, 8 Beckmann, 9 TrowbridgeBasic,
+// 10 FresnelBlend, 11 PlasticUnreal (the rt_material_type numbers); out_f 3 floats per pair.
+REFO_API int refo_material_eval(int kind, const float *kd, const float *eta, const float *k, float rx, float ry,
+                                const float *wo, const float *wi, uint32_t n, float *out_f, float *out_pdf)
+{
+    const Spectrum s_kd(kd[0], kd[1], kd[2]), s_eta(eta[0], eta[1], eta[2]), s_k(k[0], k[1], k[2]);
+    std::unique_ptr<Material> m;
+    switch (kind) {
+    case 0: m.reset(new LambertianMaterial(s_kd)); break;
+    case 1: m.reset(new TrowbridgeMaterial(s_kd, s_eta, s_k, rx, ry)); break;
+    case 8: m.reset(new BeckmannMaterial(s_kd, s_eta, s_k, rx, ry)); break;
+    case 9: m.reset(new TrowbridgeBasicMaterial(s_kd, s_eta, s_k, rx, ry)); break;
+    case 10: m.reset(new FresnelBlendMaterial(Spectrum(0), s_kd, s_k, Spectrum(0), 1.5f, 1.f)); break;
+    case 11: m.reset(new PlasticUnrealMaterial(s_kd, 1.5f)); break;
+    default: return 1;
+    }
+    for (uint32_t i = 0; i < n; i++) {
+        Vector3f o(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), w(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        Spectrum f = m->lightReflected(o, w, Point2f(0, 0));
+        out_f[3 * i] = (float)f.getR();
+        out_f[3 * i + 1] = (float)f.getG();
+        out_f[3 * i + 2] = (float)f.getB();
+        out_pdf[i] = m->pdf(o, w);
+    }
+    return 0;
 }
 
 // PhongMaterial::lightReflected and ::pdf (materials/PhongMaterial.cu:70-100) in shading space
