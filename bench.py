@@ -39,7 +39,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Mrays/s"
 WORKLOAD = ("BVH-stress render: 1920x1080, 64 spp, max depth 12, RR after depth 3, NEE on the area light; "
             "1,310,732 triangles (displaced icosphere subdiv 8, GGX F0=0.04 + Cornell box)")
-TRACE_WORKLOAD = "closest hit of 2^24 seeded rays (origins uniform in [-1,1]^3, directions uniform), reference-exact ids"
+TRACE_WORKLOAD = "closest hit of 2^{} seeded rays (origins uniform in [-1,1]^3, directions uniform), reference-exact ids"
 NRAYS = 1 << 24
 ALG_BYTES_PER_RAY = 48  # 32 B ray in + 16 B hit out (queue level)
 
@@ -442,7 +442,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": W * H * 16,
                     "note": "render call through the C ABI + film read back to pinned host memory; the inputs "
                             "of a step are the camera and options structs"},
-            "trace": {"workload": TRACE_WORKLOAD, "value": trace_rate, "unit": "Mrays/s", "ms_per_step": ms_trace,
+            "trace": {"workload": TRACE_WORKLOAD.format(NRAYS.bit_length() - 1), "value": trace_rate, "unit": "Mrays/s", "ms_per_step": ms_trace,
                       "exact_fallback_rays": int(fallback)},
             "gpu_launches": int(st_last["waves"]) * 5 + 1,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
