@@ -63,7 +63,10 @@ __global__ void k_select(RenderView rv, uint64_t n, uint32_t seed, const float *
         }
     }
     sel[i] = l;
-    atomicAdd(per_light + l, 1ull);
+    // one add per distinct light of the warp: every thread adding to one of a few counters
+    // serialised the kernel (1.9 ms for 10M photons and two lights)
+    const unsigned peers = __match_any_sync(__activemask(), l);
+    if ((int)(threadIdx.x & 31u) == __ffs(peers) - 1) atomicAdd(per_light + l, (unsigned long long)__popc(peers));
 }
 
 // PointLight::sampleLight(sampler, n) (PointLight.cu:68-95) and the selection-pdf division

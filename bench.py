@@ -42,6 +42,9 @@ WORKLOAD = ("BVH-stress render: 1920x1080, 64 spp, max depth 12, RR after depth 
 TRACE_WORKLOAD = "closest hit of 2^{} seeded rays (origins uniform in [-1,1]^3, directions uniform), reference-exact ids"
 NRAYS = 1 << 24
 ALG_BYTES_PER_RAY = 48  # 32 B ray in + 16 B hit out (queue level)
+# DRAM bytes (read + write) of one k_trace_closest launch of the 2^24-ray call, from one ncu
+# capture of the full-size launch (1 pass, --cache-control none; profiles/k_trace_closest_bvh_stress.md)
+TRACE_TRAFFIC_BYTES_2_24 = 2_457_002_240 + 976_186_368
 
 
 def dist_env():
@@ -446,9 +449,13 @@ def run_ours(args):
                       "exact_fallback_rays": int(fallback)},
             "gpu_launches": int(st_last["waves"]) * 5 + 1,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": (TRACE_TRAFFIC_BYTES_2_24 / (ms_trace / 1000) / 1e9) if NRAYS == 1 << 24 else None,
+                         "traffic_bytes_per_launch": TRACE_TRAFFIC_BYTES_2_24 if NRAYS == 1 << 24 else None,
                          "kernel": "k_trace_closest (2^24-ray closest-hit call, 48 B/ray queue-level bytes)",
-                         "note": f"peak {peak_kind}; traversal reads nodes/triangles from L2, see profiles/"},
+                         "note": f"peak {peak_kind}; traffic (GB/s over the same launch time) from the ncu capture "
+                                 "of the full launch: 4.3x the algorithmic bytes, the scene re-read past L2 and the "
+                                 "traversal stacks in local memory; see profiles/"},
             "clocks": clk.summary(),
             "guiding": guiding,
             "reference_cuda": ref_cuda,
