@@ -204,9 +204,10 @@ struct PhotonView {
 
 // Resident blocks per SM k_shade is compiled for: more resident warps hide its scattered
 // loads better than the spills they cost. BVH-stress render, Mrays/s: 1465 / 1494 / 1507 for
-// 4 (127 registers, no bound) / 5 (96) / 6 (80).
+// 4 (127 registers, no bound) / 5 (96) / 6 (80) with the binned-SAH tree; 1559 / 1583 / 1588
+// for 6 / 7 (72) / 8 (64) with the PLOC tree.
 #ifndef RTB_SHADE_MIN_BLOCKS
-#define RTB_SHADE_MIN_BLOCKS 6
+#define RTB_SHADE_MIN_BLOCKS 8
 #endif
 __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView rv, Buffers bf, int cur, GuideView gv)
 {

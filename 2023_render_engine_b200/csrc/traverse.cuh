@@ -13,7 +13,8 @@ constexpr int kStack = 48;
 
 // Resident blocks of 128 threads per SM the traversal kernels are compiled for (register cap
 // 65536 / (128 * N)): 9 gives 56 registers and 36 warps per SM (measured on the BVH-stress
-// ray set: 2294 / 2410 / 2490 Mrays/s for 7 / 8 / 9).
+// ray set: 2294 / 2410 / 2490 Mrays/s for 7 / 8 / 9 with the binned-SAH tree; 3134 / 2870 /
+// 2530 for 9 / 10 (48 registers) / 11 (40) with the PLOC tree).
 #ifndef RTB_TRAV_MIN_BLOCKS
 #define RTB_TRAV_MIN_BLOCKS 9
 #endif

@@ -130,7 +130,8 @@ def test_photon_trace_matches_cpu_restatement(core, gpu_ctx, restated):
     assert abs(gpu["power"].sum() - cpu["power"].sum()) / cpu["power"].sum() < 0.02
 
 
-def test_density_estimate_matches_formula(core, gpu_ctx, restated):
+@pytest.mark.parametrize("k", [1, 50, 128])
+def test_density_estimate_matches_formula(core, gpu_ctx, restated, k):
     """Scene::combinePhotonContributions on a traced photon map: sum over the k nearest
     same-shape photons of power * kd/pi * |cos| / (pi * maxDist^2), recomputed in numpy from
     the same photons and the brute-force neighbour sets."""
@@ -151,7 +152,7 @@ def test_density_estimate_matches_formula(core, gpu_ctx, restated):
     wo = np.tile(np.array([0.3, 0.9, 0.1], np.float32) / np.linalg.norm([0.3, 0.9, 0.1]), (300, 1)).astype(np.float32)
     kd = np.array([0.8, 0.8, 0.8])
     mat = core.material(N.RT_MAT_LAMBERTIAN, color=kd)
-    k, radius = 50, 0.5
+    radius = 0.5
     qs = np.zeros(300, np.int32)
     got = pm.density(mat, torch.from_numpy(q).cuda(), torch.from_numpy(nrm).cuda(), torch.from_numpy(wo).cuda(),
                           k, radius, torch.from_numpy(qs).cuda()).cpu().numpy()
