@@ -397,9 +397,9 @@ struct SampleSink {
 
 template <class Sink>
 __global__ void __launch_bounds__(kInferWarps * 32) k_guide_eval(const uint4 *img, GuideBox box, uint32_t n,
-                                                                  QuerySrc src, Sink sink)
+                                                                  QuerySrc src, Sink sink, uint32_t *werr)
 {
-    guide_infer_rows(img, box, n, src, sink);
+    guide_infer_rows(img, box, n, src, sink, werr);
 }
 
 // ------------------------------------------------------------------ training samples
@@ -670,9 +670,26 @@ static int guide_eval_common(rt_guide *g, uint64_t B, const char *who)
 
 static unsigned infer_grid(rt_guide *g, uint64_t B)
 {
-    const uint64_t tiles = (B + 31) / 32;
-    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((tiles + kInferWarps - 1) / kInferWarps,
-                                                              2ull * std::max(g->ctx->sm_count, 1)));
+    const uint64_t tiles = (B + kInferRows - 1) / kInferRows;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, 2ull * std::max(g->ctx->sm_count, 1)));
+}
+
+// zeroes the tensor-core wait flag before an evaluation launch
+static int guide_eval_begin(rt_guide *g)
+{
+    RTB_CHECK(g->werr.reserve(16));
+    RTB_CUDA(cudaMemsetAsync(g->werr.ptr, 0, 4, g->ctx->stream));
+    return RT_OK;
+}
+
+// waits for the evaluation and reports a tensor-core wait that ran out
+static int guide_eval_end(rt_guide *g, const char *who)
+{
+    uint32_t werr = 0;
+    RTB_CUDA(cudaMemcpyAsync(&werr, g->werr.ptr, 4, cudaMemcpyDeviceToHost, g->ctx->stream));
+    RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    if (werr) return fail(RT_ERR_TIMEOUT, std::string(who) + ": tensor-core completion wait timed out");
+    return RT_OK;
 }
 
 int rt_guide_eval(rt_guide *g, const float *queries, uint64_t B, float *out)
@@ -680,11 +697,11 @@ int rt_guide_eval(rt_guide *g, const float *queries, uint64_t B, float *out)
     RTB_CHECK(guide_eval_common(g, B, "rt_guide_eval"));
     if (B == 0) return RT_OK;
     if (!queries || !out) return fail(RT_ERR_INVALID, "rt_guide_eval: null buffer");
+    RTB_CHECK(guide_eval_begin(g));
     k_guide_eval<RawSink><<<infer_grid(g, B), kInferWarps * 32, kInferSmem, g->ctx->stream>>>(
-        g->img.as<uint4>(), guide_box(g), (uint32_t)B, QuerySrc{queries}, RawSink{out});
+        g->img.as<uint4>(), guide_box(g), (uint32_t)B, QuerySrc{queries}, RawSink{out}, g->werr.as<uint32_t>());
     RTB_CUDA(cudaGetLastError());
-    RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
-    return RT_OK;
+    return guide_eval_end(g, "rt_guide_eval");
 }
 
 int rt_guide_pdf(rt_guide *g, const float *queries, const float *dirs, const float *bsdf_pdf, uint64_t B, float *out)
@@ -692,11 +709,11 @@ int rt_guide_pdf(rt_guide *g, const float *queries, const float *dirs, const flo
     RTB_CHECK(guide_eval_common(g, B, "rt_guide_pdf"));
     if (B == 0) return RT_OK;
     if (!queries || !dirs || !bsdf_pdf || !out) return fail(RT_ERR_INVALID, "rt_guide_pdf: null buffer");
+    RTB_CHECK(guide_eval_begin(g));
     k_guide_eval<PdfSink><<<infer_grid(g, B), kInferWarps * 32, kInferSmem, g->ctx->stream>>>(
-        g->img.as<uint4>(), guide_box(g), (uint32_t)B, QuerySrc{queries}, PdfSink{dirs, bsdf_pdf, out});
+        g->img.as<uint4>(), guide_box(g), (uint32_t)B, QuerySrc{queries}, PdfSink{dirs, bsdf_pdf, out}, g->werr.as<uint32_t>());
     RTB_CUDA(cudaGetLastError());
-    RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
-    return RT_OK;
+    return guide_eval_end(g, "rt_guide_pdf");
 }
 
 int rt_guide_sample(rt_guide *g, const float *queries, const float *u3, uint64_t B, float *out_dirs, float *out_pdf)
@@ -704,11 +721,11 @@ int rt_guide_sample(rt_guide *g, const float *queries, const float *u3, uint64_t
     RTB_CHECK(guide_eval_common(g, B, "rt_guide_sample"));
     if (B == 0) return RT_OK;
     if (!queries || !u3 || !out_dirs || !out_pdf) return fail(RT_ERR_INVALID, "rt_guide_sample: null buffer");
+    RTB_CHECK(guide_eval_begin(g));
     k_guide_eval<SampleSink><<<infer_grid(g, B), kInferWarps * 32, kInferSmem, g->ctx->stream>>>(
-        g->img.as<uint4>(), guide_box(g), (uint32_t)B, QuerySrc{queries}, SampleSink{u3, out_dirs, out_pdf});
+        g->img.as<uint4>(), guide_box(g), (uint32_t)B, QuerySrc{queries}, SampleSink{u3, out_dirs, out_pdf}, g->werr.as<uint32_t>());
     RTB_CUDA(cudaGetLastError());
-    RTB_CUDA(cudaStreamSynchronize(g->ctx->stream));
-    return RT_OK;
+    return guide_eval_end(g, "rt_guide_sample");
 }
 
 int rt_guide_train_step(rt_guide *g, const float *queries, const float *dirs, const float *bsdf_pdf,

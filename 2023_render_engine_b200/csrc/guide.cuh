@@ -3,7 +3,8 @@
 // importance-sampling proposal, combined with BSDF sampling by one-sample MIS.
 //
 // Network: 144 encoded inputs -> 4 hidden layers of 64 (ReLU) -> 48 outputs, FP16 weights and
-// activations on the tensor cores (mma.sync m16n8k16, FP32 accumulation), FP32 master weights.
+// activations on the tensor cores with FP32 accumulation (inference: tcgen05.mma with TMEM
+// accumulators; training: mma.sync m16n8k16), FP32 master weights.
 // Input encoding of a shading point (position p, shading normal n, outgoing direction wo):
 //   [0, 72)    p normalised to the guide's box (u in [0, 1]), per axis 12 frequency bands:
 //              sin, cos(2^(k/2) pi u), k = 0..11 (half-octave steps: the finest band resolves
@@ -391,64 +392,253 @@ __device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, float pd
     return -wt * logV + wt * wt;
 }
 
+// ------------------------------------------------------------------ tcgen05 (UMMA) primitives
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor of a K-major FP16 operand without swizzle. The operand is a
+// grid of core matrices of 8 rows x 16 bytes (rows 16 bytes apart); `lbo` is the byte distance
+// between the two core matrices of one K = 16 step, `sbo` between consecutive groups of 8
+// rows. Fields: start address >> 4 in bits [0, 14), lbo >> 4 in [16, 30), sbo >> 4 in
+// [32, 46), descriptor version 1 (sm_100) in [46, 48), base offset 0, layout 0 (no swizzle).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           (1ull << 46);
+}
+
+// Instruction descriptor of tcgen05.mma kind::f16: A and B FP16, both K-major, FP32
+// accumulator (bits [4, 6) = 1), N >> 3 in bits [17, 23), M >> 4 in bits [24, 29).
+__host__ __device__ constexpr uint32_t umma_idesc_f16(int m, int n)
+{
+    return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T, one M x N x 16 step, issued by one thread
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+// arrive on the mbarrier once every tcgen05.mma this thread issued has completed
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n\tfence.mbarrier_init.release.cluster;" ::"r"(smem_u32(bar)),
+                 "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// waits for the phase of `parity` to complete, polling at most `limit` times; false: gave up
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t limit)
+{
+    for (uint32_t i = 0; i < limit; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// generic-proxy shared-memory writes become visible to the tensor core's (async proxy) reads
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// TMEM allocation: executed by one whole warp; the column base is written to *slot
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols)
+{
+    asm volatile(
+        "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n\t"
+        "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::"r"(smem_u32(slot)),
+        "r"(ncols)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane (the warp reads lanes 32 (warp % 4)
+// + 0..31); the wait is inside the same statement, so the values are complete on return
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];\n\ttcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
 // ------------------------------------------------------------------ batched inference
 
-constexpr int kInferWarps = 4;  // 32 rows per warp
-constexpr int kInferWarpBytes = 32 * 152 * 2;
-constexpr int kInferSmem = kGuideImgBytes + kInferWarps * kInferWarpBytes;
+// One CTA of 128 threads runs tiles of 128 rows through the network on the tensor cores:
+// tcgen05.mma (M = 128, FP16 operands from shared memory, FP32 accumulator in 64 TMEM
+// columns) per layer, one thread issuing, the CTA's threads reading their own row back from
+// TMEM for bias, ReLU and the FP16 store of the next layer's operand. Operands are K-major
+// without swizzle, in core matrices of 8 rows x 8 halves: row r, halves [8c, 8c + 8) of an
+// operand with KC chunks per row sit at byte (r / 8) * KC * 128 + c * 128 + (r % 8) * 16.
+constexpr int kInferWarps = 4;
+constexpr int kInferRows = 128;
+// byte offset of layer l's weight operand (W_l^T: guide_out(l) rows of guide_in(l) halves)
+__host__ __device__ constexpr int tc_w(int l) { return l == 0 ? 0 : tc_w(l - 1) + guide_out(l - 1) * guide_in(l - 1) * 2; }
+constexpr int kTcBias = tc_w(kGuideLayers);                // 304 FP32 biases
+constexpr int kTcA = 50432;                                // activations, 128 x 144 halves
+constexpr int kTcBar = kTcA + kInferRows * kGuideIn * 2;  // mbarrier, TMEM base
+constexpr int kInferSmem = kTcBar + 16;
+constexpr int kTmemCols = 64;
+constexpr uint32_t kUmmaWaitPolls = 1u << 22;
+static_assert(tc_w(1) == 18432 && tc_w(4) == 43008 && kTcBias == 49152, "operand sizes");
+static_assert(kTcBias + 4 * (4 * 64 + 48) <= kTcA && kTcA % 128 == 0 && kTcBar % 8 == 0, "shared layout");
+static_assert(2 * kInferSmem <= 227 * 1024, "two CTAs per SM");
+
+// byte offset of row r, chunk c (8 halves) in an operand of kc chunks per row
+__host__ __device__ constexpr uint32_t tc_chunk(uint32_t r, uint32_t c, uint32_t kc)
+{
+    return (r >> 3) * kc * 128u + c * 128u + (r & 7u) * 16u;
+}
+
+__device__ __forceinline__ uint32_t pack_half2(float a, float b)
+{
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
 
 // Forward pass over rows [0, n): src(row, q) fills the 9-float query and says whether the row
-// is guided; sink(row, valid, out) receives the 48 raw outputs (biases added). Persistent
-// warps, 32 rows per warp; the weight image is staged in shared memory once per block.
-// Launch with kInferWarps * 32 threads and kInferSmem bytes of dynamic shared memory.
+// is guided; sink(row, valid, out) receives the 48 raw outputs (biases added). Persistent CTAs
+// of kInferWarps warps and kInferSmem bytes of dynamic shared memory; the weight image is
+// staged once per CTA. A tensor-core wait that runs out of polls sets *werr (nullable) and
+// ends the CTA after freeing its TMEM.
 template <class Src, class Sink>
 __device__ __forceinline__ void guide_infer_rows(const uint4 *img, const GuideBox &box, uint32_t n, Src &src,
-                                                 Sink &sink)
+                                                 Sink &sink, uint32_t *werr)
 {
-    extern __shared__ uint4 guide_smem[];
-    for (int i = threadIdx.x; i < kGuideImgBytes / 16; i += blockDim.x) guide_smem[i] = img[i];
-    __syncthreads();
-    unsigned char *sm = reinterpret_cast<unsigned char *>(guide_smem);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __half *A = reinterpret_cast<__half *>(sm + kGuideImgBytes + warp * kInferWarpBytes);
-    float *O = reinterpret_cast<float *>(A);
-    const __half *W = reinterpret_cast<const __half *>(sm);
-    const float *bias = reinterpret_cast<const float *>(sm + kGuideImgBias);
-    const uint32_t stride = gridDim.x * kInferWarps;
-    for (uint32_t tile = blockIdx.x * kInferWarps + warp; tile * 32u < n; tile += stride) {
-        const uint32_t row = tile * 32u + lane;
-        float q[9];
-        bool valid = row < n && src(row, q);
-        if (!valid)
-#pragma unroll
-            for (int i = 0; i < 9; i++) q[i] = 0.f;
-        __half2 *arow = reinterpret_cast<__half2 *>(A + lane * 152);
-        guide_encode(0, q, box, arow);
-        guide_encode(1, q, box, arow);
-        __syncwarp();
-        {
-            float acc[2][8][4];
-            guide_gemm<2, kGuideIn, 64, 152, 152>(acc, A, W + guide_iw(0), lane);
-            __syncwarp();
-            guide_store_hidden<2, 64, 72>(acc, bias + guide_ib(0), A, lane);
-            __syncwarp();
+    extern __shared__ __align__(128) unsigned char guide_smem[];
+    unsigned char *sm = guide_smem;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kTcBar);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kTcBar + 8);
+    // weights: image rows (W_l^T, stride guide_stride(l) halves) to core-matrix chunks
+    const unsigned char *ib = reinterpret_cast<const unsigned char *>(img);
 #pragma unroll 1
-            for (int l = 1; l < 4; l++) {
-                guide_gemm<2, 64, 64, 72, 72>(acc, A, W + guide_iw(l), lane);
-                __syncwarp();
-                guide_store_hidden<2, 64, 72>(acc, bias + guide_ib(l), A, lane);
-                __syncwarp();
-            }
+    for (int l = 0; l < kGuideLayers; l++) {
+        const int kc = guide_in(l) / 8, nrows = guide_out(l);
+        for (int i = tid; i < nrows * kc; i += blockDim.x) {
+            const int r = i / kc, c = i - r * kc;
+            *reinterpret_cast<uint4 *>(sm + tc_w(l) + tc_chunk(r, c, kc)) =
+                *reinterpret_cast<const uint4 *>(ib + 2 * (guide_iw(l) + r * guide_stride(l)) + 16 * c);
         }
+    }
+    for (int i = tid; i < (4 * 64 + 48) / 4; i += blockDim.x)
+        reinterpret_cast<uint4 *>(sm + kTcBias)[i] = reinterpret_cast<const uint4 *>(ib + kGuideImgBias)[i];
+    if (tid == 0) mbar_init(bar, 1);
+    __syncwarp();
+    if (warp == 0) tmem_alloc(tslot, kTmemCols);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t tlane = tmem + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's 32 lanes
+    const float *bias = reinterpret_cast<const float *>(sm + kTcBias);
+    unsigned char *A = sm + kTcA;
+    uint32_t phase = 0;
+    bool failed = false;
+    for (uint32_t tile = blockIdx.x; !failed && (uint64_t)tile * kInferRows < n; tile += gridDim.x) {
+        const uint32_t row = tile * kInferRows + tid;
+        bool valid;
         {
-            float acc[2][6][4];
-            guide_gemm<2, 64, kGuideOut, 72, 72>(acc, A, W + guide_iw(4), lane);
-            __syncwarp();
-            guide_store_out<2, kGuideOut, 49>(acc, bias + guide_ib(4), O, lane);
+            float q[9];
+            valid = row < n && src(row, q);
+            if (!valid)
+#pragma unroll
+                for (int i = 0; i < 9; i++) q[i] = 0.f;
+            __half2 e[72];
+            guide_encode(0, q, box, e);
+            guide_encode(1, q, box, e);
+#pragma unroll
+            for (int c = 0; c < kGuideIn / 8; c++)
+                *reinterpret_cast<uint4 *>(A + tc_chunk(tid, c, kGuideIn / 8)) =
+                    *reinterpret_cast<const uint4 *>(&e[4 * c]);
         }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+#pragma unroll 1
+        for (int l = 0; l < kGuideLayers && !failed; l++) {
+            const int kc = guide_in(l) / 8;
+            if (tid == 0) {
+                tc_fence_after();
+                const uint32_t idesc = umma_idesc_f16(kInferRows, guide_out(l));
+                const uint32_t a0 = smem_u32(A), b0 = smem_u32(sm + tc_w(l));
+                for (int s = 0; s < kc / 2; s++)
+                    umma_f16(tmem, umma_desc(a0 + 256u * s, 128u, 128u * kc), umma_desc(b0 + 256u * s, 128u, 128u * kc),
+                             idesc, s > 0 ? 1u : 0u);
+                umma_commit(bar);
+            }
+            // warp-uniform, as the tcgen05.ld below is .sync.aligned
+            const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar, phase, kUmmaWaitPolls));
+            phase ^= 1u;
+            tc_fence_after();
+            if (ok && l < kGuideLayers - 1) {
+                const float *b = bias + guide_ib(l);
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    float v[16];
+                    tmem_ld16(tlane + 16u * h, v);
+                    uint32_t w[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++)
+                        w[j] = pack_half2(fmaxf(v[2 * j] + b[16 * h + 2 * j], 0.f),
+                                          fmaxf(v[2 * j + 1] + b[16 * h + 2 * j + 1], 0.f));
+                    *reinterpret_cast<uint4 *>(A + tc_chunk(tid, 2 * h, 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+                    *reinterpret_cast<uint4 *>(A + tc_chunk(tid, 2 * h + 1, 8)) = make_uint4(w[4], w[5], w[6], w[7]);
+                }
+                fence_async_smem();
+            } else if (ok) {
+                float o[kGuideOut];
+                const float *b = bias + guide_ib(l);
+#pragma unroll
+                for (int h = 0; h < kGuideOut / 16; h++) tmem_ld16(tlane + 16u * h, o + 16 * h);
+#pragma unroll
+                for (int j = 0; j < kGuideOut; j++) o[j] += b[j];
+                if (row < n) sink(row, valid, o);
+            }
+            tc_fence_before();
+            failed = __syncthreads_or(!ok) != 0;
+        }
+    }
+    if (failed) {
+        if (tid == 0 && werr) atomicExch(werr, 1u);
+        mbar_wait_bounded(bar, phase ^ 1u, kUmmaWaitPolls);  // the commit that timed out, if it ever completes
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) {
         __syncwarp();
-        if (row < n) sink(row, valid, O + lane * 49);
-        __syncwarp();
+        tmem_dealloc(tmem, kTmemCols);
     }
 }
 

@@ -610,6 +610,7 @@ __global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t 
 __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(RenderView rv, Buffers bf, int cur, const uint4 *img,
                                                                    GuideBox box, GuideParams *params, uint32_t max_depth)
 {
+    // cnt[16]: set when a tensor-core completion wait ran out (checked after every wave group)
     const uint32_t n = min(bf.cnt[cur], bf.cap);
     const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
     auto src = [&](uint32_t q, float *out) -> bool {
@@ -642,7 +643,7 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(RenderView rv,
         guide_decode(o, P);
         params[q] = P;
     };
-    guide_infer_rows(img, box, n, src, sink);
+    guide_infer_rows(img, box, n, src, sink, bf.cnt + 16);
 }
 
 }  // namespace
@@ -1030,6 +1031,10 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
         const uint32_t *hc = static_cast<const uint32_t *>(rs.host_cnt);
         uint64_t next_sample;
         std::memcpy(&next_sample, hc + 8, 8);
+        if (hc[16]) {
+            release_graph();
+            return fail(RT_ERR_TIMEOUT, name + ": guide tensor-core completion wait timed out");
+        }
         if (hc[0] == 0 && next_sample >= total) break;
         if (waves > max_waves) {
             release_graph();

@@ -225,6 +225,7 @@ struct rt_guide {
     // with nonzero weight, the open record of each retiring path, counters ([0] records,
     // [1] nonzero)
     rtb::DevBuf params, recs, nz, retire_rec, rcnt;
+    rtb::DevBuf werr;  // evaluation: set when a tensor-core completion wait ran out
     uint32_t rec_cap = 0;
     void *host_scal = nullptr;  // pinned
 };

@@ -45,9 +45,12 @@ def guide(core, gpu_ctx):
     g.close()
 
 
-def test_eval_matches_oracle(guide):
-    rng = np.random.default_rng(0)
-    q, _, _, _ = batch(rng, 3000)  # not a multiple of the 32-row warp tile
+@pytest.mark.parametrize("B", [1, 3000, 100003])
+def test_eval_matches_oracle(guide, B):
+    """Row counts that are not a multiple of the 128-row tile; 100003 rows give every
+    persistent CTA several tiles (the completion barrier's phase alternates across them)."""
+    rng = np.random.default_rng(B)
+    q, _, _, _ = batch(rng, B)
     out = guide.eval(cuda(q)).cpu().numpy()
     _, ref = G.forward(guide.params(), G.encode(q, BMIN, BMAX))
     assert np.all(np.isfinite(out))
