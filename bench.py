@@ -281,6 +281,42 @@ def measure_guiding(args, core, N, cfgs, ctx, torch):
     }
 
 
+def measure_guide_inference(core, cfgs, ctx, torch, stream, rows):
+    """rt_guide_eval on `rows` seeded queries (positions in the guiding room's box, unit normals
+    and directions): the network forward on the tensor cores (tcgen05), encoding and output
+    stores included. Inputs (36 B/row) and outputs (192 B/row) exceed L2 at 2^21 rows."""
+    T = cfgs.GUIDE_TRAINING
+    g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=3)
+    rng = np.random.default_rng(11)
+    lo, hi = np.asarray(T["bbox_min"], np.float64), np.asarray(T["bbox_max"], np.float64)
+    n = rng.normal(size=(rows, 3))
+    w = rng.normal(size=(rows, 3))
+    q = np.concatenate([rng.uniform(lo, hi, size=(rows, 3)), n / np.linalg.norm(n, axis=1, keepdims=True),
+                        w / np.linalg.norm(w, axis=1, keepdims=True)], 1).astype(np.float32)
+    qd = torch.from_numpy(q.reshape(-1)).cuda()
+    for _ in range(3):
+        g.eval(qd)
+    ms = []
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.eval(qd)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    g.close()
+    t = float(np.mean(ms))
+    flops = 49_776.0 * rows  # 2 x (144*64 + 3*64*64 + 64*48) multiply-adds per row
+    tf = flops / (t * 1e-3) / 1e12
+    pf = ROOT / "MEASURED_PEAKS.json"
+    peak = float(json.loads(pf.read_text())["bf16_tflops"]) if pf.exists() else 1590.0
+    return {"workload": f"rt_guide_eval of {rows} rows (144 -> 64 x4 -> 48, FP16 operands, FP32 accumulation)",
+            "ms": t, "rows_per_s": rows / (t * 1e-3), "network_tflops": tf,
+            "tensor_frac": tf / peak, "tensor_peak": peak,
+            "tensor_peak_kind": "measured bf16 burst" if pf.exists() else "fallback",
+            "bytes_per_row": 36 + 192, "gbs": rows * 228 / (t * 1e-3) / 1e9}
+
+
 def run_ours(args):
     import torch
 
@@ -383,6 +419,9 @@ def run_ours(args):
     guiding = None
     if world == 1 and args.guide_ref_spp > 0:
         guiding = measure_guiding(args, core, N, cfgs, ctx, torch)
+    guide_inference = None
+    if world == 1 and args.guide_eval_rows > 0:
+        guide_inference = measure_guide_inference(core, cfgs, ctx, torch, stream, args.guide_eval_rows)
 
     # ---- batched multi-view rendering (64 views of configs 0-2, one wavefront per scene)
     batched = None
@@ -458,6 +497,7 @@ def run_ours(args):
                                  "traversal stacks in local memory; see profiles/"},
             "clocks": clk.summary(),
             "guiding": guiding,
+            "guide_inference": guide_inference,
             "reference_cuda": ref_cuda,
             "batched": batched,
             "photon_sss": photon_sss,
@@ -500,6 +540,7 @@ def main():
     ap.add_argument("--guide-train-passes", type=int, default=4)
     ap.add_argument("--guide-steps", type=int, default=64)
     ap.add_argument("--guide-batch", type=int, default=1 << 16)
+    ap.add_argument("--guide-eval-rows", type=int, default=1 << 21, help="guide inference rows (0 skips)")
     args = ap.parse_args()
     global NRAYS
     NRAYS = 1 << args.rays_log2
