@@ -350,6 +350,7 @@ __global__ void k_guide_adam(const float *grad, const float *scal, float *master
 
 // ------------------------------------------------------------------ batched evaluation
 
+// every query row is evaluated (the sinks below see valid = true for each of their rows)
 struct QuerySrc {
     const float *q;
     __device__ bool operator()(uint32_t row, float *o) const
@@ -362,8 +363,9 @@ struct QuerySrc {
 
 struct RawSink {
     float *out;
-    __device__ void operator()(uint32_t row, bool, const float *o) const
+    __device__ void operator()(uint32_t row, bool valid, const float *o) const
     {
+        if (!valid) return;
         for (int i = 0; i < kGuideOut; i++) out[(uint64_t)row * kGuideOut + i] = o[i];
     }
 };
@@ -371,8 +373,9 @@ struct RawSink {
 struct PdfSink {
     const float *dir, *pdfb;
     float *out;
-    __device__ void operator()(uint32_t row, bool, const float *o) const
+    __device__ void operator()(uint32_t row, bool valid, const float *o) const
     {
+        if (!valid) return;
         GuideParams P;
         guide_decode(o, P);
         const V3 w = v3(dir[3ull * row], dir[3ull * row + 1], dir[3ull * row + 2]);
@@ -383,8 +386,9 @@ struct PdfSink {
 struct SampleSink {
     const float *u;
     float *dirs, *pdf;
-    __device__ void operator()(uint32_t row, bool, const float *o) const
+    __device__ void operator()(uint32_t row, bool valid, const float *o) const
     {
+        if (!valid) return;
         GuideParams P;
         guide_decode(o, P);
         const V3 w = guide_sample(P, u[3ull * row], u[3ull * row + 1], u[3ull * row + 2]);
@@ -396,7 +400,7 @@ struct SampleSink {
 };
 
 template <class Sink>
-__global__ void __launch_bounds__(kInferWarps * 32) k_guide_eval(const uint4 *img, GuideBox box, uint32_t n,
+__global__ void __launch_bounds__(kInferWarps * 32, 1) k_guide_eval(const uint4 *img, GuideBox box, uint32_t n,
                                                                   QuerySrc src, Sink sink, uint32_t *werr)
 {
     guide_infer_rows(img, box, n, src, sink, werr);
@@ -671,7 +675,8 @@ static int guide_eval_common(rt_guide *g, uint64_t B, const char *who)
 static unsigned infer_grid(rt_guide *g, uint64_t B)
 {
     const uint64_t tiles = (B + kInferRows - 1) / kInferRows;
-    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, 2ull * std::max(g->ctx->sm_count, 1)));
+    return (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((tiles + kInferGroups - 1) / kInferGroups, (uint64_t)std::max(g->ctx->sm_count, 1)));
 }
 
 // zeroes the tensor-core wait flag before an evaluation launch

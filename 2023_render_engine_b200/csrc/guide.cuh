@@ -221,10 +221,12 @@ __device__ __forceinline__ void guide_store_out(const float (&acc)[MT][N / 8][4]
 
 // ------------------------------------------------------------------ encoding
 
+// one-blob Gaussian: |d| > 6 bins gives exp(-18) < 2^-25, which rounds to FP16 zero, so the
+// fast exponential's flush of tiny results changes no encoded value
 __device__ __forceinline__ float guide_blob(float x, int i)
 {
     const float d = x * 32.f - ((float)i + 0.5f);
-    return expf(-0.5f * d * d);
+    return __expf(-0.5f * d * d);
 }
 
 // part 0: position bands (half2 0..35); part 1: direction blobs, normal, zero pad (36..71)
@@ -234,16 +236,23 @@ __device__ __forceinline__ void guide_encode(int part, const float *q, const Gui
         const float u[3] = {fminf(fmaxf((q[0] - bx.lo.x) * bx.inv_ext.x, 0.f), 1.f),
                             fminf(fmaxf((q[1] - bx.lo.y) * bx.inv_ext.y, 0.f), 1.f),
                             fminf(fmaxf((q[2] - bx.lo.z) * bx.inv_ext.z, 0.f), 1.f)};
-        const float scale[12] = {1.f, 1.41421356f, 2.f, 2.82842712f, 4.f, 5.65685425f,
-                                 8.f, 11.3137085f, 16.f, 22.6274170f, 32.f, 45.2548340f};
+        // band k + 2 doubles the angle of band k: sin 2x = 2 sin x cos x, cos 2x = cos^2 x -
+        // sin^2 x, from sincospi(u) and sincospi(sqrt(2) u); five doublings grow the absolute
+        // error to ~2e-6, far below the FP16 step of the encoded value
 #pragma unroll
-        for (int a = 0; a < 3; a++)
+        for (int a = 0; a < 3; a++) {
+            float s0, c0, s1, c1;
+            sincospif(u[a], &s0, &c0);
+            sincospif(u[a] * 1.41421356f, &s1, &c1);
 #pragma unroll
-            for (int k = 0; k < 12; k++) {
-                float s, c;
-                sincospif(u[a] * scale[k], &s, &c);
-                row[a * 12 + k] = __floats2half2_rn(s, c);
+            for (int k = 0; k < 12; k += 2) {
+                row[a * 12 + k] = __floats2half2_rn(s0, c0);
+                row[a * 12 + k + 1] = __floats2half2_rn(s1, c1);
+                const float s0n = 2.f * s0 * c0, c0n = fmaf(c0, c0, -s0 * s0);
+                const float s1n = 2.f * s1 * c1, c1n = fmaf(c1, c1, -s1 * s1);
+                s0 = s0n, c0 = c0n, s1 = s1n, c1 = c1n;
             }
+        }
     } else {
         const float th = acosf(fminf(fmaxf(q[8], -1.f), 1.f)) * (1.f / 3.14159265358979f);
         const float ph = atan2f(q[7], q[6]) * (1.f / 6.28318530717959f) + 0.5f;
@@ -261,6 +270,9 @@ __device__ __forceinline__ void guide_encode(int part, const float *q, const Gui
 // ------------------------------------------------------------------ vMF mixture
 
 __device__ __forceinline__ float guide_sigmoid(float x) { return 1.f / (1.f + expf(-x)); }
+// the decode's sigmoid: the mixture is decoded once per hit and both the sampling and the
+// density use the decoded lobes, so a few ulp here only move the network's function
+__device__ __forceinline__ float guide_sigmoid_fast(float x) { return __fdividef(1.f, 1.f + __expf(-x)); }
 
 // kappa / (2 pi (1 - exp(-2 kappa))): the vMF density is norm * exp(kappa (mu.w - 1))
 __device__ __forceinline__ float vmf_norm(float k) { return k / (6.28318530717959f * (-expm1f(-2.f * k))); }
@@ -273,15 +285,15 @@ __device__ __forceinline__ void guide_decode(const float *o, GuideParams &P)
     float e[kGuideLobes], se = 0.f;
 #pragma unroll
     for (int j = 0; j < kGuideLobes; j++) {
-        e[j] = expf(o[4 * j + 3] - lmax);
+        e[j] = __expf(o[4 * j + 3] - lmax);
         se += e[j];
     }
     const float inv = 1.f / se;
 #pragma unroll
     for (int j = 0; j < kGuideLobes; j++) {
-        const float th = 3.14159265358979f * guide_sigmoid(o[4 * j]);
-        const float ph = 6.28318530717959f * guide_sigmoid(o[4 * j + 1]);
-        const float k = expf(kGuideLogKappaMin + kGuideLogKappaSpan * guide_sigmoid(o[4 * j + 2]));
+        const float th = 3.14159265358979f * guide_sigmoid_fast(o[4 * j]);
+        const float ph = 6.28318530717959f * guide_sigmoid_fast(o[4 * j + 1]);
+        const float k = __expf(kGuideLogKappaMin + kGuideLogKappaSpan * guide_sigmoid_fast(o[4 * j + 2]));
         float st, ct, sp, cp;
         sincosf(th, &st, &ct);
         sincosf(ph, &sp, &cp);
@@ -289,7 +301,7 @@ __device__ __forceinline__ void guide_decode(const float *o, GuideParams &P)
         P.lam[j] = e[j] * inv;
         P.lamn[j] = P.lam[j] * vmf_norm(k);
     }
-    P.alpha = kGuideAlphaMin + kGuideAlphaSpan * guide_sigmoid(o[32]);
+    P.alpha = kGuideAlphaMin + kGuideAlphaSpan * guide_sigmoid_fast(o[32]);
 }
 
 // mixture density of the vMF lobes at world direction w (unit)
@@ -493,25 +505,32 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
 
 // ------------------------------------------------------------------ batched inference
 
-// One CTA of 128 threads runs tiles of 128 rows through the network on the tensor cores:
-// tcgen05.mma (M = 128, FP16 operands from shared memory, FP32 accumulator in 64 TMEM
-// columns) per layer, one thread issuing, the CTA's threads reading their own row back from
-// TMEM for bias, ReLU and the FP16 store of the next layer's operand. Operands are K-major
-// without swizzle, in core matrices of 8 rows x 8 halves: row r, halves [8c, 8c + 8) of an
-// operand with KC chunks per row sit at byte (r / 8) * KC * 128 + c * 128 + (r % 8) * 16.
-constexpr int kInferWarps = 4;
+// Tiles of 128 rows run through the network on the tensor cores: per layer, tcgen05.mma
+// (M = 128, FP16 operands from shared memory, FP32 accumulator in 64 TMEM columns) issued by
+// one thread, then the 128 threads of the tile read their own row back from TMEM for bias,
+// ReLU and the FP16 store of the next layer's operand. A CTA holds one copy of the weights
+// and kInferGroups independent 128-thread groups, each with its own activation tile, TMEM
+// columns, mbarrier and named barrier, so 16 warps per SM hide each other's latency.
+// Operands are K-major without swizzle, in core matrices of 8 rows x 8 halves: row r, halves
+// [8c, 8c + 8) of an operand with KC chunks per row sit at byte (r / 8) * KC * 128 + c * 128 +
+// (r % 8) * 16.
 constexpr int kInferRows = 128;
+constexpr int kInferGroups = 4;
+constexpr int kInferWarps = 4 * kInferGroups;
 // byte offset of layer l's weight operand (W_l^T: guide_out(l) rows of guide_in(l) halves)
 __host__ __device__ constexpr int tc_w(int l) { return l == 0 ? 0 : tc_w(l - 1) + guide_out(l - 1) * guide_in(l - 1) * 2; }
-constexpr int kTcBias = tc_w(kGuideLayers);                // 304 FP32 biases
-constexpr int kTcA = 50432;                                // activations, 128 x 144 halves
-constexpr int kTcBar = kTcA + kInferRows * kGuideIn * 2;  // mbarrier, TMEM base
-constexpr int kInferSmem = kTcBar + 16;
-constexpr int kTmemCols = 64;
+constexpr int kTcBias = tc_w(kGuideLayers);                                 // 304 FP32 biases
+constexpr int kTcA = 50432;                                                 // activation tiles
+constexpr int kTcATile = kInferRows * kGuideIn * 2;                         // 128 x 144 halves
+constexpr int kTcBar = kTcA + kInferGroups * kTcATile;                      // mbarriers, TMEM base
+constexpr int kInferSmem = kTcBar + 8 * kInferGroups + 16;
+constexpr int kTmemColsPerGroup = 64;
+constexpr int kTmemCols = kTmemColsPerGroup * kInferGroups;  // a power of 2 in [32, 512]
 constexpr uint32_t kUmmaWaitPolls = 1u << 22;
 static_assert(tc_w(1) == 18432 && tc_w(4) == 43008 && kTcBias == 49152, "operand sizes");
 static_assert(kTcBias + 4 * (4 * 64 + 48) <= kTcA && kTcA % 128 == 0 && kTcBar % 8 == 0, "shared layout");
-static_assert(2 * kInferSmem <= 227 * 1024, "two CTAs per SM");
+static_assert(kInferSmem <= 227 * 1024, "shared memory per CTA");
+static_assert(kTmemCols == 256, "TMEM allocation");
 
 // byte offset of row r, chunk c (8 halves) in an operand of kc chunks per row
 __host__ __device__ constexpr uint32_t tc_chunk(uint32_t r, uint32_t c, uint32_t kc)
@@ -519,17 +538,31 @@ __host__ __device__ constexpr uint32_t tc_chunk(uint32_t r, uint32_t c, uint32_t
     return (r >> 3) * kc * 128u + c * 128u + (r & 7u) * 16u;
 }
 
-__device__ __forceinline__ uint32_t pack_half2(float a, float b)
+__device__ __forceinline__ uint32_t relu_half2(float a, float b)
 {
-    const __half2 h = __floats2half2_rn(a, b);
+    const __half2 h = __hmax2(__floats2half2_rn(a, b), __float2half2_rn(0.f));
     return *reinterpret_cast<const uint32_t *>(&h);
 }
 
+// barrier of the 128 threads of a group (named barrier `id`); returns whether any of them
+// passed `v`
+__device__ __forceinline__ bool group_sync_or(uint32_t id, bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, %2, 128, q;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return r != 0;
+}
+
 // Forward pass over rows [0, n): src(row, q) fills the 9-float query and says whether the row
-// is guided; sink(row, valid, out) receives the 48 raw outputs (biases added). Persistent CTAs
-// of kInferWarps warps and kInferSmem bytes of dynamic shared memory; the weight image is
-// staged once per CTA. A tensor-core wait that runs out of polls sets *werr (nullable) and
-// ends the CTA after freeing its TMEM.
+// is guided; sink(row, valid, out) receives the 48 raw outputs (biases added; meaningless
+// where valid is false). Persistent CTAs
+// of kInferWarps warps and kInferSmem bytes of dynamic shared memory, one per SM; the weight
+// image is staged once per CTA. A tensor-core wait that runs out of polls sets *werr
+// (nullable) and ends the group; the CTA frees its TMEM on exit.
 template <class Src, class Sink>
 __device__ __forceinline__ void guide_infer_rows(const uint4 *img, const GuideBox &box, uint32_t n, Src &src,
                                                  Sink &sink, uint32_t *werr)
@@ -537,8 +570,9 @@ __device__ __forceinline__ void guide_infer_rows(const uint4 *img, const GuideBo
     extern __shared__ __align__(128) unsigned char guide_smem[];
     unsigned char *sm = guide_smem;
     const int tid = threadIdx.x, warp = tid >> 5;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kTcBar);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kTcBar + 8);
+    const int grp = tid >> 7, gt = tid & 127;  // group, thread within the group
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kTcBar) + grp;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kTcBar + 8 * kInferGroups);
     // weights: image rows (W_l^T, stride guide_stride(l) halves) to core-matrix chunks
     const unsigned char *ib = reinterpret_cast<const unsigned char *>(img);
 #pragma unroll 1
@@ -552,43 +586,46 @@ __device__ __forceinline__ void guide_infer_rows(const uint4 *img, const GuideBo
     }
     for (int i = tid; i < (4 * 64 + 48) / 4; i += blockDim.x)
         reinterpret_cast<uint4 *>(sm + kTcBias)[i] = reinterpret_cast<const uint4 *>(ib + kGuideImgBias)[i];
-    if (tid == 0) mbar_init(bar, 1);
+    if (gt == 0) mbar_init(bar, 1);
     __syncwarp();
     if (warp == 0) tmem_alloc(tslot, kTmemCols);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *tslot;
-    const uint32_t tlane = tmem + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's 32 lanes
+    const uint32_t tmem = *tslot + (uint32_t)(kTmemColsPerGroup * grp);  // this group's columns
+    const uint32_t tlane = tmem + ((uint32_t)(32 * (warp & 3)) << 16);    // this warp's 32 lanes
+    const uint32_t bar_id = 1u + (uint32_t)grp;                           // 0 is __syncthreads
     const float *bias = reinterpret_cast<const float *>(sm + kTcBias);
-    unsigned char *A = sm + kTcA;
+    unsigned char *A = sm + kTcA + grp * kTcATile;
     uint32_t phase = 0;
     bool failed = false;
-    for (uint32_t tile = blockIdx.x; !failed && (uint64_t)tile * kInferRows < n; tile += gridDim.x) {
-        const uint32_t row = tile * kInferRows + tid;
-        bool valid;
-        {
-            float q[9];
-            valid = row < n && src(row, q);
-            if (!valid)
-#pragma unroll
-                for (int i = 0; i < 9; i++) q[i] = 0.f;
+    const uint32_t stride = gridDim.x * kInferGroups;
+    for (uint32_t tile = blockIdx.x * kInferGroups + grp; !failed && (uint64_t)tile * kInferRows < n; tile += stride) {
+        const uint32_t row = tile * kInferRows + gt;
+        // rows that are not guided keep whatever their operand row holds: a row of the
+        // product depends on its own operand row only, and their outputs are not used
+        float q[9];
+        const bool valid = row < n && src(row, q);
+        if (valid) {
             __half2 e[72];
             guide_encode(0, q, box, e);
             guide_encode(1, q, box, e);
 #pragma unroll
             for (int c = 0; c < kGuideIn / 8; c++)
-                *reinterpret_cast<uint4 *>(A + tc_chunk(tid, c, kGuideIn / 8)) =
+                *reinterpret_cast<uint4 *>(A + tc_chunk(gt, c, kGuideIn / 8)) =
                     *reinterpret_cast<const uint4 *>(&e[4 * c]);
         }
         fence_async_smem();
         tc_fence_before();
-        __syncthreads();
+        if (!group_sync_or(bar_id, valid)) {  // no guided row in the tile: no network pass
+            if (row < n) sink(row, false, q);
+            continue;
+        }
 #pragma unroll 1
         for (int l = 0; l < kGuideLayers && !failed; l++) {
             const int kc = guide_in(l) / 8;
-            if (tid == 0) {
+            if (gt == 0) {
                 tc_fence_after();
                 const uint32_t idesc = umma_idesc_f16(kInferRows, guide_out(l));
                 const uint32_t a0 = smem_u32(A), b0 = smem_u32(sm + tc_w(l));
@@ -609,11 +646,10 @@ __device__ __forceinline__ void guide_infer_rows(const uint4 *img, const GuideBo
                     tmem_ld16(tlane + 16u * h, v);
                     uint32_t w[8];
 #pragma unroll
-                    for (int j = 0; j < 8; j++)
-                        w[j] = pack_half2(fmaxf(v[2 * j] + b[16 * h + 2 * j], 0.f),
-                                          fmaxf(v[2 * j + 1] + b[16 * h + 2 * j + 1], 0.f));
-                    *reinterpret_cast<uint4 *>(A + tc_chunk(tid, 2 * h, 8)) = make_uint4(w[0], w[1], w[2], w[3]);
-                    *reinterpret_cast<uint4 *>(A + tc_chunk(tid, 2 * h + 1, 8)) = make_uint4(w[4], w[5], w[6], w[7]);
+                    for (int j = 0; j < 8; j++)  // ReLU after rounding: the same FP16 value
+                        w[j] = relu_half2(v[2 * j] + b[16 * h + 2 * j], v[2 * j + 1] + b[16 * h + 2 * j + 1]);
+                    *reinterpret_cast<uint4 *>(A + tc_chunk(gt, 2 * h, 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+                    *reinterpret_cast<uint4 *>(A + tc_chunk(gt, 2 * h + 1, 8)) = make_uint4(w[4], w[5], w[6], w[7]);
                 }
                 fence_async_smem();
             } else if (ok) {
@@ -626,11 +662,11 @@ __device__ __forceinline__ void guide_infer_rows(const uint4 *img, const GuideBo
                 if (row < n) sink(row, valid, o);
             }
             tc_fence_before();
-            failed = __syncthreads_or(!ok) != 0;
+            failed = group_sync_or(bar_id, !ok);
         }
     }
     if (failed) {
-        if (tid == 0 && werr) atomicExch(werr, 1u);
+        if (gt == 0 && werr) atomicExch(werr, 1u);
         mbar_wait_bounded(bar, phase ^ 1u, kUmmaWaitPolls);  // the commit that timed out, if it ever completes
     }
     tc_fence_before();
@@ -638,7 +674,7 @@ __device__ __forceinline__ void guide_infer_rows(const uint4 *img, const GuideBo
     tc_fence_after();
     if (warp == 0) {
         __syncwarp();
-        tmem_dealloc(tmem, kTmemCols);
+        tmem_dealloc(*tslot, kTmemCols);
     }
 }
 

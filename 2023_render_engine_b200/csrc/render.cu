@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t 
 
 // Guide network at the wave's hits (queue slots of buffer `cur`); writes the decoded mixture
 // per slot, alpha = 0 where the vertex is not guided.
-__global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(RenderView rv, Buffers bf, int cur, const uint4 *img,
+__global__ void __launch_bounds__(kInferWarps * 32, 1) k_guide_infer(RenderView rv, Buffers bf, int cur, const uint4 *img,
                                                                    GuideBox box, GuideParams *params, uint32_t max_depth)
 {
     // cnt[16]: set when a tensor-core completion wait ran out (checked after every wave group)
@@ -952,7 +952,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
         RTB_CUDA(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
         infer_attr = true;
     }
-    const unsigned infer_blocks = (unsigned)std::max(1, 2 * s->ctx->sm_count);
+    const unsigned infer_blocks = (unsigned)std::max(1, s->ctx->sm_count);  // one CTA of 4 tile groups per SM
     const GuideBox gbox = guided ? guide_box(guide) : GuideBox{};
     k_start<<<blocks, kB, 0, st>>>(rv, bf);
     RTB_CUDA(cudaGetLastError());
