@@ -43,7 +43,8 @@ class SceneStats(ctypes.Structure):
 class Material(ctypes.Structure):
     _fields_ = [("type", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("color", ctypes.c_float * 3),
                 ("intensity", ctypes.c_float), ("eta", ctypes.c_float * 3), ("k", ctypes.c_float * 3),
-                ("roughness", ctypes.c_float * 2), ("ior", ctypes.c_float), ("extra", ctypes.c_float * 3)]
+                ("roughness", ctypes.c_float * 2), ("ior", ctypes.c_float), ("extra", ctypes.c_float * 3),
+                ("texture", ctypes.c_uint32)]
 
 
 class Camera(ctypes.Structure):
@@ -145,6 +146,9 @@ SIGNATURES = {
     "rt_trace_stats_get": [_P, ctypes.POINTER(TraceStats)],
     "rt_scene_set_materials": [_P, _P, _U32],
     "rt_scene_set_triangle_materials": [_P, _U32, _U32, _P],
+    "rt_scene_add_texture": [_P, _P, _U32, _U32, _P],
+    "rt_scene_set_triangle_uvs": [_P, _U32, _U32, _P],
+    "rt_texture_lookup": [_P, _U32, _P, _U64, _P],
     "rt_scene_add_point_light": [_P, _P, _P, _F32],
     "rt_render": [_P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), _P, _P, _P, ctypes.POINTER(RenderStats)],
     "rt_render_batch": [_P, ctypes.POINTER(View), _U32, _U32, _U32, _P, _P, _P, ctypes.POINTER(RenderStats)],

@@ -135,6 +135,29 @@ class Scene:
         m = np.ascontiguousarray(mat_ids, dtype=np.uint32)
         N.check(N.lib().rt_scene_set_triangle_materials(self.handle, first, m.shape[0], m.ctypes.data))
 
+    def add_texture(self, rgb) -> int:
+        """rgb: (height, width, 3) texels, rows in Texture::pixelMatrix order. Returns the id."""
+        a = np.ascontiguousarray(rgb, dtype=np.float32)
+        if a.ndim != 3 or a.shape[2] != 3:
+            raise ValueError("texture must be (height, width, 3)")
+        tid = ctypes.c_uint32()
+        N.check(N.lib().rt_scene_add_texture(self.handle, a.ctypes.data, a.shape[1], a.shape[0], ctypes.byref(tid)))
+        return tid.value
+
+    def set_triangle_uvs(self, first: int, uv):
+        """uv: (n, 3, 2) texture coordinates of triangles [first, first + n)."""
+        a = np.ascontiguousarray(uv, dtype=np.float32).reshape(-1, 6)
+        N.check(N.lib().rt_scene_set_triangle_uvs(self.handle, first, a.shape[0], a.ctypes.data))
+
+    def texture_lookup(self, tid: int, uv_dev):
+        """Texture::getColor of texture tid at the (n, 2) device points; returns (n, 3)."""
+        import torch
+
+        n = uv_dev.numel() // 2
+        out = torch.empty(3 * n, dtype=torch.float32, device=uv_dev.device)
+        N.check(N.lib().rt_texture_lookup(self.handle, tid, uv_dev.data_ptr(), n, out.data_ptr()))
+        return out.view(n, 3)
+
     def add_point_light(self, pos, rgb, intensity: float):
         p = np.ascontiguousarray(pos, dtype=np.float32)
         c = np.ascontiguousarray(rgb, dtype=np.float32)
@@ -235,8 +258,10 @@ def make_rays(o: np.ndarray, d: np.ndarray, tmax=None) -> np.ndarray:
 
 
 def material(type_, color=(0.8, 0.8, 0.8), intensity=0.0, eta=(1.5, 1.5, 1.5), k=(0.0, 0.0, 0.0),
-             roughness=(0.1, 0.1), ior=1.5, transparent=False, extra=(0.0, 0.0, 0.0)) -> "N.Material":
+             roughness=(0.1, 0.1), ior=1.5, transparent=False, extra=(0.0, 0.0, 0.0), texture=None) -> "N.Material":
+    """texture: a scene texture id (Scene.add_texture) or None."""
     m = N.Material()
+    m.texture = 0 if texture is None else int(texture) + 1
     m.extra[:] = [float(c) for c in extra]
     m.type = type_
     m.flags = N.RT_MATF_TRANSPARENT if transparent else 0

@@ -122,7 +122,12 @@ __global__ void __launch_bounds__(kPB) k_photon_shade(RenderView rv, PhotonBuffe
     Surface sf = surface_at(rv, h, o, d, compat);
     const rt_material &m = rv.mats[min(sf.mat, rv.nmats - 1)];
     Bsdf bs = load_bsdf(m);
-    if (is_scattering(bs)) {  // samplePhotonIntersections (photonDispersion.cu:40-54)
+    const bool scattering = is_scattering(bs);  // from the material's own kd
+    if (m.texture) {
+        const float2 uv = surface_uv(rv, h, sf);
+        texture_bsdf(bs, tex_color(rv, m.texture - 1u, uv.x, uv.y));
+    }
+    if (scattering) {  // samplePhotonIntersections (photonDispersion.cu:40-54)
         uint32_t slot = append(pb.cnt + 2);
         if (slot < pb.store_cap) {
             V3 pw = carry * beta;
@@ -159,7 +164,7 @@ __global__ void __launch_bounds__(kPB) k_photon_shade(RenderView rv, PhotonBuffe
     carry = carry + beta * Le;  // photonDispersion.cu:64-65
     beta = beta * f;
     bool finished = is_black(f);
-    if (!finished && is_scattering(bs) && depth > rr_depth) {  // finishStep (pathTracing.cu:91-102)
+    if (!finished && scattering && depth > rr_depth) {  // finishStep (pathTracing.cu:91-102)
         float qrr = fmaxf(0.05f, 1.f - luminance(beta));
         if (pcg_float(rng) < qrr)
             finished = true;
@@ -272,8 +277,8 @@ __global__ void __launch_bounds__(kQueryBlock, RTB_QUERY_MIN_BLOCKS) k_subsurfac
     const V3 p = v3(pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]);
     const V3 nn = v3(nrm[3 * qi], nrm[3 * qi + 1], nrm[3 * qi + 2]);
     const V3 w = v3(wo[3 * qi], wo[3 * qi + 1], wo[3 * qi + 2]);
-    const V3 c = warp_photon_subsurface(tree, mat, p, nn, w, shape ? shape[qi] : -1, radius, compat != 0,
-                                        scratch[threadIdx.x >> 5]);
+    const V3 c = warp_photon_subsurface(tree, mat, v3(mat.color[0], mat.color[1], mat.color[2]), p, nn, w,
+                                        shape ? shape[qi] : -1, radius, compat != 0, scratch[threadIdx.x >> 5]);
     if ((threadIdx.x & 31u) == 0) {
         out[3 * qi] = c.x;
         out[3 * qi + 1] = c.y;

@@ -426,20 +426,21 @@ __device__ __forceinline__ V3 warp_photon_density(const PhotonTree &t, const Bsd
 }
 
 // Scene::combinePhotonsSubsurface (Scene.cu:667-701) at point p (shading normal nn, direction
-// to the camera wo_w) of an SSMaterial m, for a warp. Over the photons within `radius` on the
+// to the camera wo_w) of an SSMaterial m with diffuse colour kd (m's kd, times its texel at
+// the point when it has a texture: SSMaterial::getBSSDFparameters, SSMaterial.cu:245-263), for a warp. Over the photons within `radius` on the
 // same shape (nn::KDTree::nearest_neighbors with an unbounded k, as
 // Scene::search_nearest(p, radius, (ulong)-1, shapeId) calls it, Scene.cu:808-813): sum of
 // power * kd * diffusionTermBSSRDF (geometricMath.cu:503-522:
 // Rd * (1 - F(cos_o)) * (1 - F(cos_i)) / pi) / (2 pi maxDist^2). With no photon the reference
 // divides 0 by 0 (a NaN sample, which the film drops); `compat` keeps that, otherwise 0. The
 // terms are summed lane-parallel. Returns the estimate on every lane.
-__device__ __forceinline__ V3 warp_photon_subsurface(const PhotonTree &t, const rt_material &m, V3 p, V3 nn, V3 wo_w,
-                                                     int32_t sid, float radius, bool compat, PhotonWarpScratch &sm)
+__device__ __forceinline__ V3 warp_photon_subsurface(const PhotonTree &t, const rt_material &m, V3 kd, V3 p, V3 nn,
+                                                     V3 wo_w, int32_t sid, float radius, bool compat,
+                                                     PhotonWarpScratch &sm)
 {
     const float eta = m.ior, g = m.roughness[1];
     const float cos_o = dot(nn, wo_w) / (length(nn) * length(wo_w));
     const float ft_o = 1.f - fresnel_dielectric_ref(cos_o, 1.f, eta);
-    const V3 kd = v3(m.color[0], m.color[1], m.color[2]);
     const DipoleChannel d0 = dipole_setup(m.eta[0], m.extra[0], g, eta), d1 = dipole_setup(m.eta[1], m.extra[1], g, eta),
                         d2 = dipole_setup(m.eta[2], m.extra[2], g, eta);
     V3 sum = v3(0, 0, 0);

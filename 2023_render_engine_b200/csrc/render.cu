@@ -182,18 +182,22 @@ __device__ __forceinline__ void push_shadow(const Buffers &bf, V3 o, V3 d, float
 constexpr uint32_t kGatherDensity = 0, kGatherSubsurface = 1;
 
 // Queues a photon-map gather at surface sf, weighted by `weight`, for the path whose radiance
-// lives at `target` (kRetireTarget: the retire list). Four float4: point + shape, normal +
-// material, direction to the previous vertex + target, weight + (kind | guide record << 1).
+// lives at `target` (kRetireTarget: the retire list). Five float4: point + shape, normal +
+// material, direction to the previous vertex + target, weight + (kind | guide record << 1),
+// the material's kd at the point (its texture applied).
 // rec: the guide record the estimate also belongs to (kRecNone: none).
+constexpr int kGatherWords = 5;
 __device__ __forceinline__ void push_gather(const Buffers &bf, const Surface &sf, V3 wo_w, V3 weight, uint32_t target,
-                                            uint32_t kind, uint32_t rec)
+                                            uint32_t kind, uint32_t rec, V3 kd)
 {
     const uint32_t gi = append(bf.cnt + 6);
     if (gi >= bf.gcap) return;
-    bf.gather[4 * gi + 0] = make_float4(sf.p.x, sf.p.y, sf.p.z, __int_as_float(sf.shape));
-    bf.gather[4 * gi + 1] = make_float4(sf.n.x, sf.n.y, sf.n.z, __uint_as_float(sf.mat));
-    bf.gather[4 * gi + 2] = make_float4(wo_w.x, wo_w.y, wo_w.z, __uint_as_float(target));
-    bf.gather[4 * gi + 3] = make_float4(weight.x, weight.y, weight.z, __uint_as_float(kind | (rec << 1)));
+    float4 *g = bf.gather + (uint64_t)kGatherWords * gi;
+    g[0] = make_float4(sf.p.x, sf.p.y, sf.p.z, __int_as_float(sf.shape));
+    g[1] = make_float4(sf.n.x, sf.n.y, sf.n.z, __uint_as_float(sf.mat));
+    g[2] = make_float4(wo_w.x, wo_w.y, wo_w.z, __uint_as_float(target));
+    g[3] = make_float4(weight.x, weight.y, weight.z, __uint_as_float(kind | (rec << 1)));
+    g[4] = make_float4(kd.x, kd.y, kd.z, 0.f);
 }
 
 struct PhotonView {
@@ -253,7 +257,14 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
         onb(sf.n, t, bvec);
         V3 wo_w = -d;
         V3 wo = v3(dot(wo_w, t), dot(wo_w, bvec), dot(wo_w, sf.n));
+        // the reference decides these from the material's own kd, before any texture
         const bool scattering = is_scattering(bs);
+        const bool specular = is_specular(bs);
+        const bool guide_ok = guide_vertex(bs, wo.z);
+        if (m.texture) {
+            const float2 uv = surface_uv(rv, h, sf);
+            texture_bsdf(bs, tex_color(rv, m.texture - 1u, uv.x, uv.y));
+        }
         // where this path's radiance will live after this bounce: decided below, but shadow
         // rays need the target now, so reserve it first.
         // BSDF sample first (its outcome decides continue/retire), NEE uses beta before update.
@@ -286,7 +297,7 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
                 e.z += beta_in.z * Le.z * w;
             }
         }
-        const bool guided = gv.enabled && depth < gv.max_depth && guide_vertex(bs, wo.z);
+        const bool guided = gv.enabled && depth < gv.max_depth && guide_ok;
         const uint32_t rec_in = rec;  // this vertex's NEE belongs to the previous record
         float alpha = 0.f;
         const GuideParams *gp = nullptr;
@@ -337,9 +348,9 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
             // (Scene::getPhotonContributions, Scene.cu:822-840; finishStep, pathTracing.cu:85-89)
             finished = true;
             const uint32_t rt = kRetireTarget | append(bf.cnt + 3);
-            push_gather(bf, sf, wo_w, beta_in, rt, kGatherDensity, rec_in);
+            push_gather(bf, sf, wo_w, beta_in, rt, kGatherDensity, rec_in, bs.color);
             if (subsurface && bs.type == RT_MAT_SUBSURFACE && (flags & kCameraRay))
-                push_gather(bf, sf, wo_w, beta_in, rt, kGatherSubsurface, rec_in);
+                push_gather(bf, sf, wo_w, beta_in, rt, kGatherSubsurface, rec_in, bs.color);
             bf.retire[rt & ~kRetireTarget] = make_float4(L.x, L.y, L.z, __uint_as_float(pix));
             regenerate(rv, bf, nxt);
             return;
@@ -364,7 +375,7 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
             next_d = wi_w;
             next_pdf = delta ? 0.f : pdf_b;
             next_flags = (depth + 1) | (delta ? kLastSpecular : 0u) |
-                         (((flags & kCameraRay) && is_specular(bs)) ? kCameraRay : 0u) | (rec << kRecShift);
+                         (((flags & kCameraRay) && specular) ? kCameraRay : 0u) | (rec << kRecShift);
         } else {
             target = kRetireTarget | append(bf.cnt + 3);
         }
@@ -375,8 +386,8 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
         const float dscale = hybrid ? 0.5f : 1.0f;
         if (scattering) {
             if (subsurface && bs.type == RT_MAT_SUBSURFACE && (flags & kCameraRay))
-                push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherSubsurface, rec_in);
-            if (hybrid) push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherDensity, rec_in);
+                push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherSubsurface, rec_in, bs.color);
+            if (hybrid) push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherDensity, rec_in, bs.color);
             for (uint32_t li = 0; li < rv.nplights; li++) {  // Scene::estimateAllDirectLights, PointLight
                 float4 lp = rv.plights[2 * li], li4 = rv.plights[2 * li + 1];
                 V3 tol = v3(lp.x, lp.y, lp.z) - sf.p;
@@ -526,19 +537,21 @@ __global__ void __launch_bounds__(kGatherBlock, RTB_GATHER_MIN_BLOCKS) k_gather(
         if (lane == 0) i = atomicAdd(bf.cnt + 7, 1u);
         i = __shfl_sync(kFullMask, i, 0);
         if (i >= n) return;  // warp-uniform
-        const float4 a = bf.gather[4 * i], b = bf.gather[4 * i + 1], c = bf.gather[4 * i + 2],
-                     d = bf.gather[4 * i + 3];
+        const float4 *g = bf.gather + (uint64_t)kGatherWords * i;
+        const float4 a = g[0], b = g[1], c = g[2], d = g[3], k = g[4];
         const rt_material &m = rv.mats[min(__float_as_uint(b.w), rv.nmats - 1)];
-        const V3 p = v3(a.x, a.y, a.z), nn = v3(b.x, b.y, b.z), wo = v3(c.x, c.y, c.z);
+        const V3 p = v3(a.x, a.y, a.z), nn = v3(b.x, b.y, b.z), wo = v3(c.x, c.y, c.z), kd = v3(k.x, k.y, k.z);
         const uint32_t kind = __float_as_uint(d.w) & 1u, rec = __float_as_uint(d.w) >> 1;
         V3 e;
-        if (kind == kGatherSubsurface)
-            e = warp_photon_subsurface(pv.tree, m, p, nn, wo, __float_as_int(a.w), kSubsurfaceRadius, compat, sm);
-        else if (m.type == RT_MAT_SUBSURFACE)
+        if (kind == kGatherSubsurface) {
+            e = warp_photon_subsurface(pv.tree, m, kd, p, nn, wo, __float_as_int(a.w), kSubsurfaceRadius, compat, sm);
+        } else if (m.type == RT_MAT_SUBSURFACE) {
             e = v3(0, 0, 0);
-        else
-            e = warp_photon_density(pv.tree, load_bsdf(m), p, nn, wo, __float_as_int(a.w), pv.k, pv.radius, compat,
-                                    sm);
+        } else {
+            Bsdf bs = load_bsdf(m);
+            bs.color = kd;  // the textured kd the shading point saw
+            e = warp_photon_density(pv.tree, bs, p, nn, wo, __float_as_int(a.w), pv.k, pv.radius, compat, sm);
+        }
         if (lane == 0) {
             const V3 contrib = v3(d.x, d.y, d.z) * e;
             const uint32_t target = __float_as_uint(c.w);
@@ -646,6 +659,16 @@ __global__ void __launch_bounds__(kInferWarps * 32, 1) k_guide_infer(RenderView 
     guide_infer_rows(img, box, n, src, sink, bf.cnt + 16);
 }
 
+__global__ void k_texture_lookup(RenderView rv, uint32_t id, const float *uv, uint64_t n, float *rgb)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const V3 c = tex_color(rv, id, uv[2 * i], uv[2 * i + 1]);
+    rgb[3 * i] = c.x;
+    rgb[3 * i + 1] = c.y;
+    rgb[3 * i + 2] = c.z;
+}
+
 }  // namespace
 
 }  // namespace rtb
@@ -683,6 +706,63 @@ int rt_render_set_photon_map(rt_scene *s, rt_photon_map *m, uint32_t k, float ra
     s->pmap = m;
     s->pm_k = k;
     s->pm_radius = radius;
+    return RT_OK;
+}
+
+int rt_scene_add_texture(rt_scene *s, const float *rgb, uint32_t width, uint32_t height, uint32_t *id)
+{
+    if (!s || !rgb || !id) return fail(RT_ERR_INVALID, "rt_scene_add_texture: null argument");
+    if (width == 0 || height == 0 || width >= (1u << 24) || height >= (1u << 24) ||
+        (uint64_t)width * height >= (1ull << 32))
+        return fail(RT_ERR_INVALID, "rt_scene_add_texture: size must be in [1, 2^24) per axis, < 2^32 texels");
+    if (s->texels.size() + (uint64_t)width * height >= (1ull << 32))
+        return fail(RT_ERR_INVALID, "rt_scene_add_texture: more than 2^32 texels in the scene");
+    const uint32_t first = (uint32_t)s->texels.size();
+    s->texels.reserve(s->texels.size() + (size_t)width * height);
+    for (uint64_t i = 0; i < (uint64_t)width * height; i++)
+        s->texels.push_back(make_float4(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2], 0.f));
+    *id = (uint32_t)s->tex_info.size();
+    s->tex_info.push_back(make_uint4(first, width, height, 0u));
+    s->tex_dirty = true;
+    s->render_dirty = true;
+    return RT_OK;
+}
+
+int rt_scene_set_triangle_uvs(rt_scene *s, uint32_t first, uint32_t n, const float *uv)
+{
+    if (!s || (!uv && n)) return fail(RT_ERR_INVALID, "rt_scene_set_triangle_uvs: null argument");
+    const uint64_t ntri = s->tri9.size() / 9;
+    if ((uint64_t)first + n > ntri) return fail(RT_ERR_INVALID, "rt_scene_set_triangle_uvs: range out of bounds");
+    if (s->tri_uv.size() < 6 * ntri) {
+        const size_t old = s->tri_uv.size() / 6;
+        s->tri_uv.resize(6 * ntri);
+        for (size_t t = old; t < ntri; t++) {
+            float *u = s->tri_uv.data() + 6 * t;
+            u[0] = 0.f, u[1] = 0.f, u[2] = 1.f, u[3] = 0.f, u[4] = 1.f, u[5] = 1.f;
+        }
+    }
+    std::memcpy(s->tri_uv.data() + 6ull * first, uv, 24ull * n);
+    s->render_dirty = true;
+    return RT_OK;
+}
+
+int rt_texture_lookup(rt_scene *s, uint32_t id, const float *uv, uint64_t n, float *rgb)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_texture_lookup: null scene");
+    if (id >= s->tex_info.size()) return fail(RT_ERR_INVALID, "rt_texture_lookup: unknown texture");
+    if (n == 0) return RT_OK;
+    if (!uv || !rgb) return fail(RT_ERR_INVALID, "rt_texture_lookup: null buffer");
+    RTB_CUDA(cudaSetDevice(s->ctx->device));
+    RTB_CHECK(upload_textures(s));
+    RenderView rv{};
+    rv.texels = s->d_texels.as<float4>();
+    rv.tex_info = s->d_tex_info.as<uint4>();
+    rv.ntex = (uint32_t)s->tex_info.size();
+    const uint64_t blocks = (n + 255) / 256;
+    if (blocks >= (1ull << 31)) return fail(RT_ERR_INVALID, "rt_texture_lookup: n too large");
+    k_texture_lookup<<<(unsigned)blocks, 256, 0, s->ctx->stream>>>(rv, id, uv, n, rgb);
+    RTB_CUDA(cudaGetLastError());
+    RTB_CUDA(cudaStreamSynchronize(s->ctx->stream));
     return RT_OK;
 }
 
@@ -730,6 +810,19 @@ int refresh_transparency(rt_scene *s)
     return RT_OK;
 }
 
+// texels and texture table, when textures were added since the last upload
+int upload_textures(rt_scene *s)
+{
+    if (!s->tex_dirty) return RT_OK;
+    cudaStream_t st = s->ctx->stream;
+    if (!s->texels.empty()) {
+        RTB_CHECK(s->d_texels.upload(s->texels.data(), sizeof(float4) * s->texels.size(), st));
+        RTB_CHECK(s->d_tex_info.upload(s->tex_info.data(), sizeof(uint4) * s->tex_info.size(), st));
+    }
+    s->tex_dirty = false;
+    return RT_OK;
+}
+
 int upload_render_data(rt_scene *s)
 {
     if (!s->render_dirty) return RT_OK;
@@ -741,6 +834,18 @@ int upload_render_data(rt_scene *s)
         if (m >= s->materials.size()) return fail(RT_ERR_INVALID, "rt_render: triangle material id out of range");
     for (const auto &sp : s->spheres)
         if (sp.material >= s->materials.size()) return fail(RT_ERR_INVALID, "rt_render: sphere material out of range");
+    for (const auto &m : s->materials)
+        if (m.texture > s->tex_info.size()) return fail(RT_ERR_INVALID, "rt_render: material texture id out of range");
+    if (!s->tri_uv.empty() && s->tri_uv.size() < 6ull * n) {  // triangles added after the coordinates
+        const size_t old = s->tri_uv.size() / 6;
+        s->tri_uv.resize(6ull * n);
+        for (size_t t = old; t < n; t++) {
+            float *u = s->tri_uv.data() + 6 * t;
+            u[0] = 0.f, u[1] = 0.f, u[2] = 1.f, u[3] = 0.f, u[4] = 1.f, u[5] = 1.f;
+        }
+    }
+    if (!s->tri_uv.empty()) RTB_CHECK(s->d_tri_uv.upload(s->tri_uv.data(), 4ull * 6 * n, st));
+    RTB_CHECK(upload_textures(s));
     RTB_CHECK(s->d_mats.upload(s->materials.data(), s->materials.size() * sizeof(rt_material), st));
     RTB_CHECK(s->d_tri_mat.upload(s->tri_material.data(), 4ull * n, st));
     bool any_normals = false;
@@ -797,6 +902,10 @@ int make_render_view(rt_scene *s, RenderView &rv)
     rv.emit_total = s->emit_total;
     rv.plights = s->d_plights.as<float4>();
     rv.nplights = (uint32_t)(s->plights.size() / 2);
+    rv.texels = s->d_texels.as<float4>();
+    rv.tex_info = s->d_tex_info.as<uint4>();
+    rv.ntex = (uint32_t)s->tex_info.size();
+    rv.tri_uv = s->tri_uv.empty() ? nullptr : s->d_tri_uv.as<float>();
     return RT_OK;
 }
 
@@ -857,7 +966,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     if (gathers) {
         if (!s->pmap || !s->pmap->built)
             return fail(RT_ERR_STATE, name + ": photon-map modes need a built photon map (rt_render_set_photon_map)");
-        RTB_CHECK(rs.gather.reserve(64ull * gcap));
+        RTB_CHECK(rs.gather.reserve(16ull * kGatherWords * gcap));
     }
     const bool guided = (flags & RT_RENDER_GUIDE) != 0;
     GuideView gv{};

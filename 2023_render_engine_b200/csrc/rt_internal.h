@@ -175,6 +175,7 @@ struct rt_scene;
 namespace rtb {
 // Uploads materials, per-triangle data, emitters and lights when they changed.
 int upload_render_data(rt_scene *s);
+int upload_textures(rt_scene *s);  // texels and texture table, when textures were added
 // Re-derives the shadow-ray transparency of triangle records / spheres from the
 // mesh flags and the material table; re-uploads what changed.
 int refresh_transparency(rt_scene *s);
@@ -266,6 +267,14 @@ struct rt_scene {
     uint32_t pm_k = 100;
     float pm_radius = 100.f;
     rtb::DevBuf d_tri_transp, d_mat_transp;  // per-triangle / per-material transparency (record flags)
+    // textures: texels (rgb in xyz), per texture (first texel, width, height, 0); texture
+    // coordinates, 6 per triangle (empty until rt_scene_set_triangle_uvs; triangles added
+    // later get the defaults at upload)
+    std::vector<float4> texels;
+    std::vector<uint4> tex_info;
+    std::vector<float> tri_uv;
+    rtb::DevBuf d_texels, d_tex_info, d_tri_uv;
+    bool tex_dirty = false;
     rtb::DevBuf d_mats, d_tri_mat, d_tri_shape, d_tri_nidx, d_normals, d_emit_tri, d_emit_cdf, d_plights;
     rtb::RenderScratch rscratch;
     rtb::SceneView view() const;

@@ -34,6 +34,12 @@ struct RenderView {
     uint32_t nviews;
     uint32_t flags;
     uint64_t total;  // samples over all views
+    // textures: texels (rgb), per texture (first texel, width, height, 0); texture
+    // coordinates, 6 per triangle (null: every triangle uses the default ones)
+    const float4 *texels;
+    const uint4 *tex_info;
+    const float *tri_uv;
+    uint32_t ntex;
 };
 
 // view of global sample g / of global film pixel p (binary search over the prefix sums)
@@ -139,6 +145,50 @@ __device__ __forceinline__ Surface surface_at(const RenderView &rv, const rt_hit
     return s;
 }
 
+// ------------------------------------------------------------------ textures
+
+// Texel index along one axis as Texture::getColor computes it (Texture.cu:179-192):
+// `unsigned int x = point.x * getWidth()` converts the float product the way the reference's
+// x86-64 build does (truncation to a 64-bit integer, low 32 bits kept; NaN and out-of-range
+// values give 0), then clamp(x, 0, size - 1) picks the float overload of clamp, which for
+// these non-negative values is min(x, size - 1).
+__host__ __device__ __forceinline__ uint32_t tex_index(float c, uint32_t size)
+{
+    const float x = c * (float)size;
+    const long long i = (fabsf(x) < 9.22337204e18f) ? (long long)x : (long long)(1ull << 63);
+    const uint32_t u = (uint32_t)(unsigned long long)i;
+    return u < size - 1 ? u : size - 1;
+}
+
+// Texture::getColor of texture `id` at surface point (u, v): pixelMatrix[y][x]
+__device__ __forceinline__ V3 tex_color(const RenderView &rv, uint32_t id, float u, float v)
+{
+    const uint4 t = rv.tex_info[id];
+    const float4 c = rv.texels[t.x + (uint64_t)tex_index(v, t.z) * t.y + tex_index(u, t.y)];
+    return v3(c.x, c.y, c.z);
+}
+
+// Surface point of a hit: the barycentric blend of the triangle's texture coordinates
+// (Triangle.cu:355-358; without coordinates (0,0), (1,0), (1,1), Triangle.cu:134-151), or a
+// sphere's (theta, phi) in degrees from its object-space hit point (Sphere::localToSurface,
+// to_spherical, geometricMath.cu:49-57; degrees() rounds radians * 180.0 / PI in double).
+__device__ __forceinline__ float2 surface_uv(const RenderView &rv, const rt_hit &h, const Surface &s)
+{
+    if (h.prim & RT_PRIM_SHAPE) {
+        const float *m = rv.sv.spheres[h.prim & ~RT_PRIM_SHAPE].w2o;
+        const float x = m[0] * s.p.x + m[1] * s.p.y + m[2] * s.p.z + m[3];
+        const float y = m[4] * s.p.x + m[5] * s.p.y + m[6] * s.p.z + m[7];
+        const float z = m[8] * s.p.x + m[9] * s.p.y + m[10] * s.p.z + m[11];
+        const float th = atan2f(sqrtf(x * x + y * y), z), ph = atan2f(y, x);
+        const double deg = 180.0 / (double)3.14159265358979f;
+        return make_float2((float)((double)th * deg), (float)((double)ph * deg));
+    }
+    const float b1 = h.b1, b2 = h.b2, b0 = 1.f - b1 - b2;
+    if (!rv.tri_uv) return make_float2(b1 + b2, b2);  // (0,0) b0 + (1,0) b1 + (1,1) b2
+    const float *t = rv.tri_uv + 6ull * (uint32_t)h.prim;
+    return make_float2(b0 * t[0] + b1 * t[2] + b2 * t[4], b0 * t[1] + b1 * t[3] + b2 * t[5]);
+}
+
 struct Bsdf {
     uint32_t type;
     V3 color;
@@ -159,6 +209,26 @@ __device__ __forceinline__ Bsdf load_bsdf(const rt_material &m)
     b.ior = m.ior;
     if (b.type == RT_MAT_PHONG || b.type == RT_MAT_SUBSURFACE) b.g.ax = m.roughness[0];  // ns, as given
     return b;
+}
+
+// The texel's effect on a material (the reference's materials read their Texture in these
+// places only): Lambertian (LambertianBSDF.cu:22-28, 66-70), Phong and the surface of
+// SSMaterial (through their LambertianBRDF, PhongMaterial.cu:95) and Plain's emission
+// (PlainMaterial.cu:66-67) multiply kd by it; Trowbridge, TrowbridgeBasic and Beckmann replace
+// kd with it (TrowbridgeBSDF.cu:167-169, TrowbridgeBasicBSDF.cu:167-169, BeckmannBSDF.cu:61-63).
+// FresnelBlend's LambertianBRDF is never evaluated, so its texture has no effect.
+__device__ __forceinline__ void texture_bsdf(Bsdf &b, V3 texel)
+{
+    switch (b.type) {
+    case RT_MAT_LAMBERTIAN:
+    case RT_MAT_PHONG:
+    case RT_MAT_SUBSURFACE:
+    case RT_MAT_PLAIN: b.color = b.color * texel; break;
+    case RT_MAT_TROWBRIDGE:
+    case RT_MAT_TROWBRIDGE_BASIC:
+    case RT_MAT_BECKMANN: b.color = texel; break;
+    default: break;
+    }
 }
 
 // Phong and subsurface surfaces keep ks in Bsdf::k and the exponent ns in g.ax.

@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define RT_B200_ABI_VERSION 1
+#define RT_B200_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define RT_API __attribute__((visibility("default")))
@@ -209,6 +209,11 @@ typedef struct rt_material {
     float roughness[2];   /* Trowbridge roughness x/y; alpha = sqrt(roughness) */
     float ior;            /* Dielectric index of refraction (Glass: 1.5) */
     float extra[3];       /* RT_MAT_SUBSURFACE: sigma_a */
+    uint32_t texture;     /* 1 + id of a scene texture (rt_scene_add_texture); 0: none. Applied
+                             where the reference's materials read their Texture: Lambertian,
+                             Phong, Subsurface (surface and dipole kd) and Plain multiply kd by
+                             the texel; Trowbridge, TrowbridgeBasic and Beckmann replace kd by
+                             it; the other materials ignore it */
 } rt_material;
 
 /* A material's BSDF for n direction pairs in the shading frame (normal +z), device arrays of
@@ -230,6 +235,23 @@ RT_API int rt_scene_set_materials(rt_scene *scene, const rt_material *table, uin
 
 /* Per-triangle material ids for triangles [first, first+n) (overrides the mesh id). */
 RT_API int rt_scene_set_triangle_materials(rt_scene *scene, uint32_t first, uint32_t n, const uint32_t *materials);
+
+/* A texture (textures/Texture.cu: Texture::pixelMatrix): width x height RGB texels, 3 floats
+ * each, rows in the order Texture::loadBmpImage stores them (row 0 = the BMP's first stored
+ * row). Host memory, copied. *id receives the texture's id; materials name it as 1 + id.
+ * Takes effect at the next render. */
+RT_API int rt_scene_add_texture(rt_scene *scene, const float *rgb, uint32_t width, uint32_t height, uint32_t *id);
+/* Texture coordinates of triangles [first, first+n): 6 floats each, the (u, v) of vertices 0,
+ * 1 and 2 (TriangleMesh::textureCoords through Triangle::textureIndices). Triangles without
+ * them use (0,0), (1,0), (1,1) (Triangle::getSurfaceCoordinates, Triangle.cu:134-151). The
+ * hit's surface point is the barycentric blend (Triangle.cu:355-358); a sphere's is its
+ * (theta, phi) in degrees (Sphere::localToSurface, Sphere.cu:269-275). */
+RT_API int rt_scene_set_triangle_uvs(rt_scene *scene, uint32_t first, uint32_t n, const float *uv);
+/* Texture::getColor (Texture.cu:179-192) of texture `id` at n surface points: device arrays,
+ * 2 floats in, 3 floats out per point. The texel index is the point times the size, converted
+ * to unsigned as the reference's x86-64 build converts it (through a 64-bit integer) and
+ * clamped to the last row and column. */
+RT_API int rt_texture_lookup(rt_scene *scene, uint32_t id, const float *uv_dev, uint64_t n, float *rgb_dev);
 
 /* PointLight(lightToWorld = translate(pos), color, intensity) (light/PointLight.cu:15-96). */
 RT_API int rt_scene_add_point_light(rt_scene *scene, const float pos[3], const float rgb[3], float intensity);
@@ -361,7 +383,8 @@ RT_API int rt_photon_map_destroy(rt_photon_map *map);
  * buffers, 3 floats each: position, shading normal, outgoing direction toward the viewer;
  * shape ids nullable): sum over the k nearest photons on the same shape within radius of
  * power * f(wo, -photon direction)|cos| for material `mat`, divided by pi * (largest
- * neighbour distance)^2. out_rgb: 3 floats per point. */
+ * neighbour distance)^2. out_rgb: 3 floats per point. The points carry no surface
+ * coordinates: `mat`'s texture is not applied (give the textured kd in `mat` instead). */
 RT_API int rt_photon_density(rt_photon_map *map, const rt_material *mat, const float *points_dev,
                              const float *normals_dev, const float *wo_dev, const int32_t *shape_ids_dev, uint64_t nq,
                              uint32_t k, float radius, float *out_rgb_dev);

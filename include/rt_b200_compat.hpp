@@ -85,14 +85,19 @@ inline void rgb(const Spectrum &s, float out[3])
 }
 
 // Material* -> rt_material (materials/*.cu); false for a class the core does not implement.
-inline bool to_rt_material(const Material *m, rt_material &o)
+// *tex receives the Texture the material reads (null: none); the caller registers it and sets
+// o.texture.
+inline bool to_rt_material(const Material *m, rt_material &o, const Texture **tex)
 {
     o = rt_material{};
+    *tex = nullptr;
     if (const auto *l = dynamic_cast<const LambertianMaterial *>(m)) {
         o.type = RT_MAT_LAMBERTIAN;
         rgb(l->bsdf.color, o.color);
+        *tex = l->bsdf.texture;
     } else if (const auto *t = dynamic_cast<const TrowbridgeMaterial *>(m)) {
         o.type = RT_MAT_TROWBRIDGE;
+        *tex = t->bsdf.text;
         rgb(t->bsdf.kd, o.color);
         rgb(t->bsdf.eta, o.eta);
         rgb(t->bsdf.k, o.k);
@@ -101,6 +106,7 @@ inline bool to_rt_material(const Material *m, rt_material &o)
         o.roughness[1] = (float)(t->bsdf.alphaY * t->bsdf.alphaY);
     } else if (const auto *tb = dynamic_cast<const TrowbridgeBasicMaterial *>(m)) {
         o.type = RT_MAT_TROWBRIDGE_BASIC;  // TrowbridgeBasicBSDF keeps alpha = sqrt(roughness) too
+        *tex = tb->bsdf.text;
         rgb(tb->bsdf.kd, o.color);
         rgb(tb->bsdf.eta, o.eta);
         rgb(tb->bsdf.k, o.k);
@@ -108,6 +114,7 @@ inline bool to_rt_material(const Material *m, rt_material &o)
         o.roughness[1] = (float)(tb->bsdf.alphaY * tb->bsdf.alphaY);
     } else if (const auto *bk = dynamic_cast<const BeckmannMaterial *>(m)) {
         o.type = RT_MAT_BECKMANN;  // BeckmannBSDF: alpha = sqrt(roughness) (BeckmannBSDF.cu:30-37)
+        *tex = bk->bsdf.text;
         rgb(bk->bsdf.kd, o.color);
         rgb(bk->bsdf.eta, o.eta);
         rgb(bk->bsdf.k, o.k);
@@ -133,10 +140,12 @@ inline bool to_rt_material(const Material *m, rt_material &o)
         rgb(r->color, o.color);
     } else if (const auto *p = dynamic_cast<const PlainMaterial *>(m)) {
         o.type = RT_MAT_PLAIN;
+        *tex = p->texture;
         rgb(p->kd, o.color);
     } else if (const auto *ss = dynamic_cast<const SSMaterial *>(m)) {
         // Phong surface (SSMaterial.cu:29) over the dipole medium
         o.type = RT_MAT_SUBSURFACE;
+        *tex = ss->text;
         rgb(ss->kd, o.color);
         rgb(ss->surfaceMaterial.ks, o.k);
         o.roughness[0] = (float)ss->surfaceMaterial.ns;
@@ -147,6 +156,7 @@ inline bool to_rt_material(const Material *m, rt_material &o)
     } else if (const auto *ph = dynamic_cast<const PhongMaterial *>(m)) {
         if (ph->ke.maxComponent() > 0) return false;  // emissive Phong: not implemented by the core
         o.type = RT_MAT_PHONG;
+        *tex = ph->text;
         rgb(ph->kd, o.color);
         rgb(ph->ks, o.k);
         o.roughness[0] = (float)ph->ns;
@@ -300,11 +310,34 @@ private:
         for (size_t i = 0; i < material_ptrs_.size(); i++)
             if (material_ptrs_[i] == m) return (uint32_t)i;
         rt_material rm;
-        if (!m || !compat_detail::to_rt_material(m, rm))
+        const Texture *tex = nullptr;
+        if (!m || !compat_detail::to_rt_material(m, rm, &tex))
             check_unsupported(std::string("material class ") + (m ? typeid(*m).name() : "(null)"));
+        if (tex) rm.texture = 1u + texture_index(tex);
         material_ptrs_.push_back(m);
         materials_.push_back(rm);
         return (uint32_t)(materials_.size() - 1);
+    }
+
+    // a Texture's texels, read through Texture::getColor at the texel centres (its pixelMatrix
+    // is not public), registered once per Texture object
+    uint32_t texture_index(const Texture *t)
+    {
+        for (size_t i = 0; i < texture_ptrs_.size(); i++)
+            if (texture_ptrs_[i] == t) return texture_ids_[i];
+        const uint32_t w = t->getWidth(), h = t->getHeight();
+        std::vector<float> rgb(3ull * w * h);
+        for (uint32_t y = 0; y < h; y++)
+            for (uint32_t x = 0; x < w; x++) {
+                const Spectrum c = t->getColor(Point2f(((float)x + 0.5f) / (float)w, ((float)y + 0.5f) / (float)h));
+                float *o = rgb.data() + 3ull * ((size_t)y * w + x);
+                compat_detail::rgb(c, o);
+            }
+        uint32_t id = 0;
+        check(rt_scene_add_texture(scene_, rgb.data(), w, h, &id));
+        texture_ptrs_.push_back(t);
+        texture_ids_.push_back(id);
+        return id;
     }
 
     [[noreturn]] static void check_unsupported(const std::string &what)
@@ -329,11 +362,20 @@ private:
         }
         std::vector<uint32_t> idx(3 * tris.size()), nidx;
         if (!mesh.normals.empty()) nidx.resize(3 * tris.size());
+        // texture coordinates per triangle through its textureIndices (Triangle.cu:134-151)
+        std::vector<float> uv;
+        if (!mesh.textureCoords.empty()) uv.resize(6 * tris.size());
+        const uint32_t first = (uint32_t)tri_material_.size();
         bool transparent = false;
         for (size_t t = 0; t < tris.size(); t++) {
             for (int k = 0; k < 3; k++) {
                 idx[3 * t + k] = tris[t].vertexIndices[k];
                 if (!nidx.empty()) nidx[3 * t + k] = tris[t].normalIndices[k];
+                if (!uv.empty()) {
+                    const Point2f &c = mesh.textureCoords[tris[t].textureIndices[k]];
+                    uv[6 * t + 2 * k] = (float)c.x;
+                    uv[6 * t + 2 * k + 1] = (float)c.y;
+                }
             }
             transparent = transparent || tris[t].isTransparent;
             tri_material_.push_back(material_index(tris[t].material));
@@ -342,6 +384,7 @@ private:
                                 nrm.empty() ? nullptr : nrm.data(), (uint32_t)mesh.normals.size(),
                                 nidx.empty() ? nullptr : nidx.data(), tri_material_.back(), shape_id, transparent,
                                 nullptr));
+        if (!uv.empty()) check(rt_scene_set_triangle_uvs(scene_, first, (uint32_t)tris.size(), uv.data()));
     }
 
     void add_shape(const Shape *s, int32_t index)
@@ -366,9 +409,14 @@ private:
                 xyz[3 * c + 2] = (float)w.z;
             }
             const uint32_t idx[6] = {0, 1, 2, 0, 2, 3};
+            const uint32_t first = (uint32_t)tri_material_.size();
             check(rt_scene_add_mesh(scene_, xyz, 4, idx, 2, nullptr, 0, nullptr, mat, index, transparent, nullptr));
             tri_material_.push_back(mat);
             tri_material_.push_back(mat);
+            // the plane's surface point is its object-space (x, y) (Plane.cu:82): the corners'
+            // coordinates, blended barycentrically, give the same point
+            const float uv[12] = {0, 0, 1, 0, 1, 1, 0, 0, 1, 1, 0, 1};
+            check(rt_scene_set_triangle_uvs(scene_, first, 2, uv));
         } else {
             check_unsupported(std::string("shape class ") + typeid(*s).name());
         }
@@ -399,6 +447,8 @@ private:
     rt_photon_map *pmap_ = nullptr;
     std::vector<const Material *> material_ptrs_;
     std::vector<rt_material> materials_;
+    std::vector<const Texture *> texture_ptrs_;
+    std::vector<uint32_t> texture_ids_;
     std::vector<uint32_t> tri_material_;
     std::vector<Shape *> shapes_;
     mutable std::vector<rt_photon> photons_;

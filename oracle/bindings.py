@@ -269,6 +269,54 @@ def ref_material_eval(refo, kind, kd, eta, k, rx, ry, wo, wi):
     return f, pdf
 
 
+def write_bmp24(path, rgb_rows):
+    """A 24-bit BMP as Texture::loadBmpImage (textures/Texture.cu:38-121) reads it: `rgb_rows`
+    (height, width, 3) uint8, row i = the i-th row stored in the file, BGR on disk. The width
+    must make a row a multiple of 4 bytes (the reader does not skip row padding)."""
+    a = np.ascontiguousarray(rgb_rows, dtype=np.uint8)
+    h, w, _ = a.shape
+    if (3 * w) % 4:
+        raise ValueError("row bytes must be a multiple of 4")
+    import struct
+
+    data = a[:, :, ::-1].tobytes()
+    hdr = struct.pack("<2sIHHIIiiHHIIiiII", b"BM", 54 + len(data), 0, 0, 54, 40, w, h, 1, 24, 0, len(data), 2835, 2835,
+                      0, 0)
+    Path(path).write_bytes(hdr + data)
+
+
+def ref_texture_lookup(refo, bmp_path, uv):
+    """Texture::getColor of the reference's own Texture read from bmp_path."""
+    L = refo.L
+    L.refo_texture_lookup.argtypes = [ctypes.c_char_p, P, U32, P]
+    L.refo_texture_lookup.restype = I
+    u = _np(uv, np.float32).reshape(-1, 2)
+    out = np.zeros((u.shape[0], 3), np.float32)
+    if L.refo_texture_lookup(str(bmp_path).encode(), u.ctypes.data, u.shape[0], out.ctypes.data) != 0:
+        raise FileNotFoundError(bmp_path)
+    return out
+
+
+def ref_material_eval_tex(refo, kind, kd, eta, k, rx, ry, bmp_path, uv, wo, wi):
+    """lightReflected / pdf of the reference's class with a Texture, pair i at surface point uv[i]
+    (kind: 0 Lambertian, 1 Trowbridge, 5 Phong with ks = eta and ns = rx, 8 Beckmann, 9
+    TrowbridgeBasic)."""
+    L = refo.L
+    L.refo_material_eval_tex.argtypes = [I, P, P, P, ctypes.c_float, ctypes.c_float, ctypes.c_char_p, P, P, P, U32,
+                                         P, P]
+    L.refo_material_eval_tex.restype = I
+    a, b = _np(wo, np.float32).reshape(-1, 3), _np(wi, np.float32).reshape(-1, 3)
+    u = _np(uv, np.float32).reshape(-1, 2)
+    p = [_np(x, np.float32) for x in (kd, eta, k)]
+    f = np.zeros((a.shape[0], 3), np.float32)
+    pdf = np.zeros(a.shape[0], np.float32)
+    rc = L.refo_material_eval_tex(kind, *[x.ctypes.data for x in p], rx, ry, str(bmp_path).encode(), u.ctypes.data,
+                                  a.ctypes.data, b.ctypes.data, a.shape[0], f.ctypes.data, pdf.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"reference textured material eval failed ({rc})")
+    return f, pdf
+
+
 def ref_phong_eval(refo, kd, ks, ns, wo, wi):
     """The reference's PhongMaterial::lightReflected / pdf."""
     L = refo.L
@@ -452,16 +500,23 @@ class RefRender:
         b = _np(b, np.float64).reshape(-1, 3)
         return L.refr_film_rmse(a.ctypes.data, na, b.ctypes.data, nb)
 
-    def render(self, obejota_path, planes, kd):
-        """planes: (n, 12) Plane(corner, axisX, axisY, normal); kd: (n, 3). Returns
-        (mean image (h*w, 3), cameraToWorld 4x4, rasterToCamera 4x4)."""
+    def render(self, obejota_path, planes, kd, bmp_path=None, textured=None):
+        """planes: (n, 12) Plane(corner, axisX, axisY, normal); kd: (n, 3); textured: per plane
+        whether its material carries the Texture read from bmp_path. Returns (mean image
+        (h*w, 3), cameraToWorld 4x4, rasterToCamera 4x4)."""
         pl = _np(planes, np.float32).reshape(-1, 12)
         k = _np(kd, np.float32).reshape(-1, 3)
         out = np.zeros((self.width * self.height, 3), np.float32)
         c2w = np.zeros(16, np.float32)
         r2c = np.zeros(16, np.float32)
-        rc = self.L.refr_render(str(obejota_path).encode(), pl.shape[0], pl.ctypes.data, k.ctypes.data,
-                                out.ctypes.data, c2w.ctypes.data, r2c.ctypes.data)
+        L = self.L
+        L.refr_render_tex.argtypes = [ctypes.c_char_p, I, P, P, ctypes.c_char_p, P, P, P, P]
+        L.refr_render_tex.restype = I
+        tx = None if textured is None else _np(textured, np.int32)
+        rc = L.refr_render_tex(str(obejota_path).encode(), pl.shape[0], pl.ctypes.data, k.ctypes.data,
+                               None if bmp_path is None else str(bmp_path).encode(),
+                               None if tx is None else tx.ctypes.data, out.ctypes.data, c2w.ctypes.data,
+                               r2c.ctypes.data)
         if rc != 0:
             raise RuntimeError("reference render failed")
         return out, c2w.reshape(4, 4), r2c.reshape(4, 4)
@@ -487,12 +542,17 @@ class RefCompat:
         L.refc_config(ctypes.byref(w), ctypes.byref(h), ctypes.byref(s), ctypes.byref(d))
         self.width, self.height, self.spp, self.depth = w.value, h.value, s.value, d.value
 
-    def render(self, obejota_path, planes, kd, seed):
+    def render(self, obejota_path, planes, kd, seed, bmp_path=None, textured=None):
         pl = _np(planes, np.float32).reshape(-1, 12)
         k = _np(kd, np.float32).reshape(-1, 3)
         out = np.zeros((self.width * self.height, 3), np.float32)
-        rc = self.L.refc_render(str(obejota_path).encode(), pl.shape[0], pl.ctypes.data, k.ctypes.data, seed,
-                                out.ctypes.data)
+        L = self.L
+        L.refc_render_tex.argtypes = [ctypes.c_char_p, I, P, P, ctypes.c_char_p, P, U32, P]
+        L.refc_render_tex.restype = I
+        tx = None if textured is None else _np(textured, np.int32)
+        rc = L.refc_render_tex(str(obejota_path).encode(), pl.shape[0], pl.ctypes.data, k.ctypes.data,
+                               None if bmp_path is None else str(bmp_path).encode(),
+                               None if tx is None else tx.ctypes.data, seed, out.ctypes.data)
         if rc != 0:
             raise RuntimeError("compat render failed: " + self.L.refc_error().decode())
         return out

@@ -118,25 +118,31 @@ REFC_API int refc_map_material(int kind, const float *kd, const float *eta, cons
     case 11: m.reset(new PlasticUnrealMaterial(s_kd, 1.5f)); break;
     default: return 1;
     }
-    return rtb::compat_detail::to_rt_material(m.get(), *out) ? 0 : 1;
+    const Texture *tex = nullptr;
+    return rtb::compat_detail::to_rt_material(m.get(), *out, &tex) ? 0 : 1;
 }
 
 // planes: 12 floats each, Plane(corner, axisX, axisY, normal); kd: 3 floats each. out_mean:
 // the film's per-pixel sum / spp after rtb::PathTracerIntegrator::render. Returns 0, or 1
 // with refc_error() set.
-REFC_API int refc_render(const char *obejota, int nplanes, const float *planes, const float *kd, uint32_t seed,
-                         float *out_mean)
+// bmp_path / textured (nullable): per plane nonzero when its material carries the reference's
+// own Texture read from bmp_path.
+REFC_API int refc_render_tex(const char *obejota, int nplanes, const float *planes, const float *kd,
+                             const char *bmp_path, const int *textured, uint32_t seed, float *out_mean)
 {
     std::vector<Plane *> pl;
     std::vector<LambertianMaterial *> mats;
     std::vector<Shape *> shapes;
+    std::unique_ptr<Texture> tex;
     int rc = 0;
     try {
+        if (bmp_path && textured) tex.reset(new Texture(bmp_path));
         for (int i = 0; i < nplanes; i++) {
             const float *p = planes + 12 * i;
             Plane *s = new Plane(Point3f(p[0], p[1], p[2]), Vector3f(p[3], p[4], p[5]), Vector3f(p[6], p[7], p[8]),
                                  Vector3f(p[9], p[10], p[11]));
-            LambertianMaterial *m = new LambertianMaterial(Spectrum(kd[3 * i], kd[3 * i + 1], kd[3 * i + 2]));
+            LambertianMaterial *m = new LambertianMaterial(Spectrum(kd[3 * i], kd[3 * i + 1], kd[3 * i + 2]),
+                                                           Spectrum(0), (tex && textured[i]) ? tex.get() : nullptr);
             s->setMaterial(m);
             pl.push_back(s);
             mats.push_back(m);
@@ -165,4 +171,10 @@ REFC_API int refc_render(const char *obejota, int nplanes, const float *planes, 
     for (auto *s : pl) delete s;
     for (auto *m : mats) delete m;
     return rc;
+}
+
+REFC_API int refc_render(const char *obejota, int nplanes, const float *planes, const float *kd, uint32_t seed,
+                         float *out_mean)
+{
+    return refc_render_tex(obejota, nplanes, planes, kd, nullptr, nullptr, seed, out_mean);
 }

@@ -398,6 +398,60 @@ REFO_API int refo_material_eval(int kind, const float *kd, const float *eta, con
     return 0;
 }
 
+// Texture::getColor (textures/Texture.cu:179-192) of the reference's own Texture, loaded by
+// its own BMP reader (Texture::loadBmpImage) from `bmp_path`, at n surface points (2 floats
+// each); out_rgb 3 floats per point. Returns 1 when the file cannot be read.
+REFO_API int refo_texture_lookup(const char *bmp_path, const float *uv, uint32_t n, float *out_rgb)
+{
+    std::unique_ptr<Texture> t;
+    try {
+        t.reset(new Texture(bmp_path));
+    } catch (const std::exception &) {
+        return 1;
+    }
+    for (uint32_t i = 0; i < n; i++) {
+        const Spectrum c = t->getColor(Point2f(uv[2 * i], uv[2 * i + 1]));
+        out_rgb[3 * i] = (float)c.getR();
+        out_rgb[3 * i + 1] = (float)c.getG();
+        out_rgb[3 * i + 2] = (float)c.getB();
+    }
+    return 0;
+}
+
+// Material::lightReflected and ::pdf of the reference's classes built with a Texture (read
+// from `bmp_path` as above), each direction pair i evaluated at surface point uv[i]: kind 0
+// Lambertian, 1 Trowbridge, 5 Phong (kd, ks = eta, ns = rx), 8 Beckmann, 9 TrowbridgeBasic.
+REFO_API int refo_material_eval_tex(int kind, const float *kd, const float *eta, const float *k, float rx, float ry,
+                                    const char *bmp_path, const float *uv, const float *wo, const float *wi,
+                                    uint32_t n, float *out_f, float *out_pdf)
+{
+    std::unique_ptr<Texture> t;
+    try {
+        t.reset(new Texture(bmp_path));
+    } catch (const std::exception &) {
+        return 1;
+    }
+    const Spectrum s_kd(kd[0], kd[1], kd[2]), s_eta(eta[0], eta[1], eta[2]), s_k(k[0], k[1], k[2]);
+    std::unique_ptr<Material> m;
+    switch (kind) {
+    case 0: m.reset(new LambertianMaterial(s_kd, Spectrum(0), t.get())); break;
+    case 1: m.reset(new TrowbridgeMaterial(s_kd, s_eta, s_k, rx, ry, t.get())); break;
+    case 5: m.reset(new PhongMaterial(Spectrum(0), s_kd, s_eta, Spectrum(0), 1.5f, rx, t.get())); break;
+    case 8: m.reset(new BeckmannMaterial(s_kd, s_eta, s_k, rx, ry, t.get())); break;
+    case 9: m.reset(new TrowbridgeBasicMaterial(s_kd, s_eta, s_k, rx, ry, t.get())); break;
+    default: return 2;
+    }
+    for (uint32_t i = 0; i < n; i++) {
+        Vector3f o(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), w(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        Spectrum f = m->lightReflected(o, w, Point2f(uv[2 * i], uv[2 * i + 1]));
+        out_f[3 * i] = (float)f.getR();
+        out_f[3 * i + 1] = (float)f.getG();
+        out_f[3 * i + 2] = (float)f.getB();
+        out_pdf[i] = m->pdf(o, w);
+    }
+    return 0;
+}
+
 // PhongMaterial::lightReflected and ::pdf (materials/PhongMaterial.cu:70-100) in shading space
 // for n direction pairs: out_f 3 floats per pair, out_pdf 1.
 REFO_API void refo_phong_eval(const float *kd, const float *ks, float ns, const float *wo, const float *wi, uint32_t n,

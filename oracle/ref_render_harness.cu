@@ -101,9 +101,21 @@ REFR_API int refr_config(int *w, int *h, int *spp, int *depth)
 // Plane(Point3f, Vector3f, Vector3f, Vector3f) (Plane.cu:26-50); kd: 3 floats per plane.
 // out_mean: per-pixel mean radiance (Film sum / spp), row-major, 3 floats per pixel.
 // out_c2w / out_r2c: the camera's cameraToWorld and rasterToCamera matrices (row-major).
-REFR_API int refr_render(const char *obejota, int nplanes, const float *planes, const float *kd, float *out_mean,
-                         float *out_c2w, float *out_r2c)
+// textured: nullable, per plane nonzero when its Lambertian material carries the Texture read
+// from bmp_path (Texture::Texture, textures/Texture.cu); the plane's surface point is its
+// object-space (x, y) (Plane.cu:82).
+REFR_API int refr_render_tex(const char *obejota, int nplanes, const float *planes, const float *kd,
+                             const char *bmp_path, const int *textured, float *out_mean, float *out_c2w,
+                             float *out_r2c)
 {
+    std::unique_ptr<Texture> tex;
+    if (bmp_path && textured) {
+        try {
+            tex.reset(new Texture(bmp_path));
+        } catch (const std::exception &) {
+            return 2;
+        }
+    }
     std::vector<Plane *> pl;
     std::vector<LambertianMaterial *> mats;
     std::vector<Shape *> shapes;
@@ -111,7 +123,8 @@ REFR_API int refr_render(const char *obejota, int nplanes, const float *planes, 
         const float *p = planes + 12 * i;
         Plane *s = new Plane(Point3f(p[0], p[1], p[2]), Vector3f(p[3], p[4], p[5]), Vector3f(p[6], p[7], p[8]),
                              Vector3f(p[9], p[10], p[11]));
-        LambertianMaterial *m = new LambertianMaterial(Spectrum(kd[3 * i], kd[3 * i + 1], kd[3 * i + 2]));
+        LambertianMaterial *m = new LambertianMaterial(Spectrum(kd[3 * i], kd[3 * i + 1], kd[3 * i + 2]), Spectrum(0),
+                                                       (tex && textured[i]) ? tex.get() : nullptr);
         s->setMaterial(m);
         pl.push_back(s);
         mats.push_back(m);
@@ -142,6 +155,12 @@ REFR_API int refr_render(const char *obejota, int nplanes, const float *planes, 
     for (auto *s : pl) delete s;
     for (auto *m : mats) delete m;
     return 0;
+}
+
+REFR_API int refr_render(const char *obejota, int nplanes, const float *planes, const float *kd, float *out_mean,
+                         float *out_c2w, float *out_r2c)
+{
+    return refr_render_tex(obejota, nplanes, planes, kd, nullptr, nullptr, out_mean, out_c2w, out_r2c);
 }
 
 // Film accumulation files and computeRMSE (camera/Film.cu:366-449, 611-632) on films of the

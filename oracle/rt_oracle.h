@@ -57,6 +57,7 @@ typedef struct pto_material { /* same layout as rt_material in include/rt_b200.h
     float roughness[2];
     float ior;
     float extra[3];
+    uint32_t texture; /* not restated here: texture parity is checked against the reference's Texture */
 } pto_material;
 
 typedef struct pto_sphere {

@@ -43,7 +43,7 @@ def test_python_binding_covers_declarations():
 
 def test_abi_version_and_errors_without_gpu():
     lib = N.load()
-    assert lib.rt_abi_version() == 1
+    assert lib.rt_abi_version() == 2
     # null arguments are rejected before any device work
     assert lib.rt_scene_commit(None) == 1
     assert "null" in N.last_error()
