@@ -147,6 +147,7 @@ SIGNATURES = {
     "rt_scene_set_materials": [_P, _P, _U32],
     "rt_scene_set_triangle_materials": [_P, _U32, _U32, _P],
     "rt_scene_add_texture": [_P, _P, _U32, _U32, _P],
+    "rt_material_single_scattering": [_P, _P, _P, _P, _U64, _P, _P, _P],
     "rt_scene_set_triangle_uvs": [_P, _U32, _U32, _P],
     "rt_texture_lookup": [_P, _U32, _P, _U64, _P],
     "rt_scene_add_point_light": [_P, _P, _P, _F32],

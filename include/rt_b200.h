@@ -228,6 +228,14 @@ RT_API int rt_material_eval(const rt_material *m, const float *wo, const float *
  * flags: RT_RENDER_COMPAT selects the reference's dielectric estimator. */
 RT_API int rt_material_sample(const rt_material *m, const float *wo, uint64_t n, uint32_t seed, uint32_t flags, float *wi,
                               float *value, float *pdf, uint8_t *delta);
+/* SSMaterial::singleScattering (materials/SSMaterial.cu:108-181) of an RT_MAT_SUBSURFACE
+ * material for n cases in the shading frame (device arrays): wo toward the camera, L the light
+ * direction (3 floats each), u the sampler's sample in (0, 1) (1 float each). Out: the value (3
+ * floats), the refracted light direction Ti and the surface point Pi where the light enters
+ * (3 floats each, both nullable). L = 0 gives 0, as the reference's photon case. The reference
+ * defines the term but its integrator never calls it; neither does rt_render. */
+RT_API int rt_material_single_scattering(const rt_material *m, const float *wo, const float *L, const float *u, uint64_t n,
+                                         float *rgb, float *wi, float *point);
 
 /* Replaces the Material* each Shape/Triangle points to (Triangle::setMaterial,
  * Shape::setMaterial): a table indexed by the `material` ids given at add time. */

@@ -460,6 +460,23 @@ class RefRender:
         L.refr_config(ctypes.byref(w), ctypes.byref(h), ctypes.byref(s), ctypes.byref(d))
         self.width, self.height, self.spp, self.depth = w.value, h.value, s.value, d.value
 
+    def single_scattering(self, eta, ns, g, sigma_s, sigma_a, wo, L, seeds):
+        """SSMaterial::singleScattering of the reference's class: (value (n, 3), Ti (n, 3),
+        Pi (n, 3), the sample u each case drew (n,))."""
+        L_ = self.L
+        L_.refr_single_scattering.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_float, P, P, P, P, P, U32, P,
+                                              P, P, P]
+        L_.refr_single_scattering.restype = I
+        a, b = _np(wo, np.float32).reshape(-1, 3), _np(L, np.float32).reshape(-1, 3)
+        sd = _np(seeds, np.uint32)
+        ss, sa = _np(sigma_s, np.float32), _np(sigma_a, np.float32)
+        n = a.shape[0]
+        v, wi, pt, u = (np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32),
+                        np.zeros(n, np.float32))
+        L_.refr_single_scattering(eta, ns, g, ss.ctypes.data, sa.ctypes.data, a.ctypes.data, b.ctypes.data,
+                                  sd.ctypes.data, n, v.ctypes.data, wi.ctypes.data, pt.ctypes.data, u.ctypes.data)
+        return v, wi, pt, u
+
     def film_store(self, path, sums, samples):
         """Film::storeContributionsToFile of a film with these per-pixel sums (h*w, 3)."""
         a = _np(sums, np.float64).reshape(-1, 3)

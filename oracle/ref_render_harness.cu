@@ -163,6 +163,34 @@ REFR_API int refr_render(const char *obejota, int nplanes, const float *planes, 
     return refr_render_tex(obejota, nplanes, planes, kd, nullptr, nullptr, out_mean, out_c2w, out_r2c);
 }
 
+// SSMaterial::singleScattering (materials/SSMaterial.cu:108-181) of the reference's own class
+// for n cases: wo, L 3 floats each; the sampler's generator is seeded with seeds[i] and its
+// first sample (the one singleScattering draws) is returned in out_u. Out: value (3 floats),
+// sampleDirection and outgoingPoint (3 floats each).
+REFR_API int refr_single_scattering(float eta, float ns, float g, const float *sigma_s, const float *sigma_a,
+                                    const float *wo, const float *L, const uint32_t *seeds, uint32_t n, float *out_rgb,
+                                    float *out_wi, float *out_pt, float *out_u)
+{
+    SSMaterial m(Spectrum(0), Spectrum(0.5), Spectrum(0.1), eta, ns, nullptr, false,
+                 Spectrum(sigma_s[0], sigma_s[1], sigma_s[2]), Spectrum(sigma_a[0], sigma_a[1], sigma_a[2]), g);
+    for (uint32_t i = 0; i < n; i++) {
+        Sampler s;
+        s.rng = std::mt19937(seeds[i]);
+        Sampler peek(s);
+        out_u[i] = peek.get1Dsample();
+        Vector3f wi;
+        Point3f po;
+        const Spectrum v = m.singleScattering(Vector3f(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), s, wi, Point2f(0, 0), po,
+                                              Vector3f(L[3 * i], L[3 * i + 1], L[3 * i + 2]));
+        out_rgb[3 * i] = (float)v.getR();
+        out_rgb[3 * i + 1] = (float)v.getG();
+        out_rgb[3 * i + 2] = (float)v.getB();
+        out_wi[3 * i] = wi.x, out_wi[3 * i + 1] = wi.y, out_wi[3 * i + 2] = wi.z;
+        out_pt[3 * i] = po.x, out_pt[3 * i + 1] = po.y, out_pt[3 * i + 2] = po.z;
+    }
+    return 0;
+}
+
 // Film accumulation files and computeRMSE (camera/Film.cu:366-449, 611-632) on films of the
 // harness resolution. sum: 3 doubles per pixel (the per-pixel sums over `samples` samples).
 namespace {
