@@ -21,6 +21,7 @@
 extern "C" {
 #endif
 
+/* 2: rt_material gained `texture` (76 bytes); a caller built against 1 passes 72-byte entries */
 #define RT_B200_ABI_VERSION 2
 
 #if defined(__GNUC__)
@@ -220,7 +221,8 @@ typedef struct rt_material {
  * 3 floats per direction: f = what Material::lightReflected returns (f |cos wi| for most
  * materials; Phong and FresnelBlend leave out the cosine, as the reference does) and
  * pdf = Material::pdf (nullable). The renderer's own code (materials/*.cu). Runs on the
- * legacy default stream and returns when done. */
+ * legacy default stream and returns when done. The directions carry no surface point, so
+ * `texture` is not applied: pass the texel-applied kd in `color`. */
 RT_API int rt_material_eval(const rt_material *m, const float *wo, const float *wi, uint64_t n, float *f, float *pdf);
 /* Material::sampleDirection for n outgoing directions: wi, the value it returns (f |cos| / pdf
  * in the reference's convention), the pdf the renderer pairs with it (nullable) and whether the
