@@ -122,6 +122,38 @@ REFC_API int refc_map_material(int kind, const float *kd, const float *eta, cons
     return rtb::compat_detail::to_rt_material(m.get(), *out, &tex) ? 0 : 1;
 }
 
+// The drop-in layer's reading of a material built with the reference's own Texture (read from
+// bmp_path): kind 0 Lambertian, 1 Trowbridge, 3 Plain, 5 Phong, 6 SSMaterial, 8 Beckmann, 9
+// TrowbridgeBasic, 10 FresnelBlend. *has_texture = 1 when the layer reports the material's
+// Texture for registration. Returns 0, 1 when the layer does not map the class, 2 when the
+// file cannot be read, 3 for an unknown kind.
+REFC_API int refc_map_textured(int kind, const char *bmp_path, rt_material *out, int *has_texture)
+{
+    std::unique_ptr<Texture> t;
+    try {
+        t.reset(new Texture(bmp_path));
+    } catch (const std::exception &) {
+        return 2;
+    }
+    const Spectrum kd(0.6, 0.5, 0.4), eta(0.2, 0.9, 1.1), k(3.9, 2.4, 2.2);
+    std::unique_ptr<Material> m;
+    switch (kind) {
+    case 0: m.reset(new LambertianMaterial(kd, Spectrum(0), t.get())); break;
+    case 1: m.reset(new TrowbridgeMaterial(kd, eta, k, 0.3f, 0.1f, t.get())); break;
+    case 3: m.reset(new PlainMaterial(kd, Spectrum(0), t.get())); break;
+    case 5: m.reset(new PhongMaterial(Spectrum(0), kd, Spectrum(0.2), Spectrum(0), 1.5f, 20.f, t.get())); break;
+    case 6: m.reset(new SSMaterial(Spectrum(0), kd, Spectrum(0.2), 1.3f, 20.f, t.get(), false, Spectrum(1), Spectrum(0.1), 0.f)); break;
+    case 8: m.reset(new BeckmannMaterial(kd, eta, k, 0.3f, 0.1f, t.get())); break;
+    case 9: m.reset(new TrowbridgeBasicMaterial(kd, eta, k, 0.3f, 0.1f, t.get())); break;
+    case 10: m.reset(new FresnelBlendMaterial(Spectrum(0), kd, Spectrum(0), Spectrum(0), 1.5f, 1.f, t.get())); break;
+    default: return 3;
+    }
+    const Texture *tex = nullptr;
+    if (!rtb::compat_detail::to_rt_material(m.get(), *out, &tex)) return 1;
+    *has_texture = (tex == t.get()) ? 1 : 0;
+    return 0;
+}
+
 // planes: 12 floats each, Plane(corner, axisX, axisY, normal); kd: 3 floats each. out_mean:
 // the film's per-pixel sum / spp after rtb::PathTracerIntegrator::render. Returns 0, or 1
 // with refc_error() set.

@@ -43,3 +43,25 @@ def test_fresnel_blend_and_plastic(refc):
     assert fb.type == N.RT_MAT_FRESNEL_BLEND and np.allclose(list(fb.extra), (2.0, 1.0, 0.5))  # ke
     pu = mapped(refc, 11, (0.6, 0.5, 0.4), (1, 1, 1), (0, 0, 0), 0, 0)
     assert pu.type == N.RT_MAT_PLASTIC and np.allclose(list(pu.color), (0.6, 0.5, 0.4))
+
+
+@pytest.mark.parametrize("kind,type_,textured", [
+    (0, N.RT_MAT_LAMBERTIAN, True), (1, N.RT_MAT_TROWBRIDGE, True), (3, N.RT_MAT_PLAIN, True),
+    (5, N.RT_MAT_PHONG, True), (6, N.RT_MAT_SUBSURFACE, True), (8, N.RT_MAT_BECKMANN, True),
+    (9, N.RT_MAT_TROWBRIDGE_BASIC, True), (10, N.RT_MAT_FRESNEL_BLEND, False)])
+def test_drop_in_reports_each_material_texture(refc, tmp_path, kind, type_, textured):
+    """The layer hands every material's Texture (the member its class reads) to the scene for
+    registration; FresnelBlend's texture is never read by the reference, so it is not."""
+    from oracle import bindings
+
+    bmp = tmp_path / "tex.bmp"
+    bindings.write_bmp24(bmp, np.random.default_rng(kind).integers(0, 256, size=(4, 8, 3), dtype=np.uint8))
+    out = N.Material()
+    has = ctypes.c_int(-1)
+    L = refc.L
+    L.refc_map_textured.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.refc_map_textured.restype = ctypes.c_int
+    assert L.refc_map_textured(kind, str(bmp).encode(), ctypes.byref(out), ctypes.byref(has)) == 0
+    assert out.type == type_
+    assert has.value == (1 if textured else 0)
+    assert out.texture == 0  # the scene sets the id when it registers the texture
