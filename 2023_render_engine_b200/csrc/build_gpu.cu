@@ -183,7 +183,7 @@ __global__ void k_ploc_merge(BBox *__restrict__ bx, const uint32_t *__restrict__
         c1[k] = b;
         BBox u = bx[a];
         bbox_grow(u, bx[b]);
-        bx[k] = u;  // a new node: no thread of this round reads it
+        bx[k] = u;  // a new node: no thread of this merge pass reads it
     }
     if (f >> 32) next[(uint32_t)(pp >> 32)] = (f & 1u) ? k : cl[i];
     if (i == m - 1) *totals = pp + f;
