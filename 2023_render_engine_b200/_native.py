@@ -143,6 +143,7 @@ SIGNATURES = {
     "rt_trace_closest_host": [_P, _P, _U64, _P, _U32],
     "rt_trace_closest_noalloc": [_P, _P, _U64, _P, _U32],
     "rt_trace_any": [_P, _P, _U64, _P, _U32],
+    "rt_trace_any_bits": [_P, _P, _U64, _P, _U32],
     "rt_trace_stats_get": [_P, ctypes.POINTER(TraceStats)],
     "rt_scene_set_materials": [_P, _P, _U32],
     "rt_scene_set_triangle_materials": [_P, _U32, _U32, _P],

@@ -122,9 +122,17 @@ class Scene:
         return hits
 
     def trace_any(self, rays_dev, occluded_dev, n: int | None = None, flags: int = 0):
+        """Scene::isVisible's occlusion: occluded_dev gets one byte per ray (1: something is hit
+        no farther than the ray's tmax)."""
         if n is None:
             n = rays_dev.numel() // 8
         N.check(N.lib().rt_trace_any(self.handle, rays_dev.data_ptr(), n, occluded_dev.data_ptr(), flags))
+
+    def trace_any_bits(self, rays_dev, bits_dev, n: int | None = None, flags: int = 0):
+        """The same decisions as a bit mask: ray i is bit i % 32 of 32-bit word i // 32."""
+        if n is None:
+            n = rays_dev.numel() // 8
+        N.check(N.lib().rt_trace_any_bits(self.handle, rays_dev.data_ptr(), n, bits_dev.data_ptr(), flags))
 
     # ---- rendering ----
     def set_materials(self, mats):

@@ -1,5 +1,6 @@
 // C ABI entry points (include/rt_b200.h): contexts, scenes, tracing.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -28,6 +29,33 @@ int cuda_status(cudaError_t e, const char *what)
     if (e == cudaSuccess) return RT_OK;
     set_error(std::string(what) + ": " + cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? RT_ERR_OOM : RT_ERR_CUDA;
+}
+
+namespace {
+std::atomic<unsigned> g_device_slots[kMaxDevices][SLOT_COUNT];
+
+int current_device()
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return (dev >= 0 && dev < kMaxDevices) ? dev : 0;
+}
+}  // namespace
+
+unsigned device_slot(DeviceSlot slot) { return g_device_slots[current_device()][slot].load(); }
+void set_device_slot(DeviceSlot slot, unsigned value) { g_device_slots[current_device()][slot].store(value); }
+void or_device_slot(DeviceSlot slot, unsigned bits) { g_device_slots[current_device()][slot].fetch_or(bits); }
+
+unsigned device_sm_count()
+{
+    unsigned n = device_slot(SLOT_SM_COUNT);
+    if (!n) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, current_device());
+        n = (unsigned)std::max(sms, 1);
+        set_device_slot(SLOT_SM_COUNT, n);
+    }
+    return n;
 }
 
 int DevBuf::reserve(size_t n)
@@ -355,10 +383,12 @@ static int trace_common(rt_scene *s, const rt_ray *rays, uint64_t n, rt_hit *hit
 
 static int finish_trace(rt_scene *s, uint64_t n)
 {
+    s->last_rays = n;
+    s->last_fallback = 0;
+    if (n == 0) return RT_OK;  // nothing launched: the counters still hold an earlier call's
     uint32_t c[4] = {0, 0, 0, 0};
     RTB_CUDA(cudaMemcpyAsync(c, s->scratch.counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, s->ctx->stream));
     RTB_CUDA(cudaStreamSynchronize(s->ctx->stream));
-    s->last_rays = n;
     s->last_fallback = c[0];
     return check_device_status(c[1]);
 }
@@ -383,18 +413,45 @@ int rt_trace_closest_host(rt_scene *s, const rt_ray *rays, uint64_t n, rt_hit *h
     return finish_trace(s, n);
 }
 
-int rt_trace_any(rt_scene *s, const rt_ray *rays, uint64_t n, uint8_t *occluded, uint32_t flags)
+static int trace_any_common(rt_scene *s, const rt_ray *rays, uint64_t n, void *out, bool bits, uint32_t flags,
+                            const char *who)
 {
-    if (!s) return fail(RT_ERR_INVALID, "rt_trace_any: null scene");
-    if (!s->committed) return fail(RT_ERR_STATE, "rt_trace_any: scene not committed");
-    if (n && (!rays || !occluded)) return fail(RT_ERR_INVALID, "rt_trace_any: null buffer");
-    if (reinterpret_cast<uintptr_t>(rays) & 15u) return fail(RT_ERR_INVALID, "rt_trace_any: rays must be 16-byte aligned");
+    if (!s) return fail(RT_ERR_INVALID, std::string(who) + ": null scene");
+    if (!s->committed) return fail(RT_ERR_STATE, std::string(who) + ": scene not committed");
+    if (n && (!rays || !out)) return fail(RT_ERR_INVALID, std::string(who) + ": null buffer");
+    if (n >= 0x80000000ull) return fail(RT_ERR_INVALID, std::string(who) + ": at most 2^31-1 rays per call");
+    if (reinterpret_cast<uintptr_t>(rays) & 15u)
+        return fail(RT_ERR_INVALID, std::string(who) + ": rays must be 16-byte aligned");
+    if (bits && (reinterpret_cast<uintptr_t>(out) & 3u))
+        return fail(RT_ERR_INVALID, std::string(who) + ": the bit mask must be 4-byte aligned");
+    if (n == 0) return RT_OK;
     RTB_CUDA(cudaSetDevice(s->ctx->device));
-    RTB_CHECK(launch_trace_any(s->view(), rays, n, occluded, flags, s->scratch.counters.as<uint32_t>(), s->ctx->stream));
+    cudaStream_t st = s->ctx->stream;
+    if (flags & RT_TRACE_FAST) {
+        RTB_CHECK(launch_trace_any(s->view(), rays, n, out, bits, flags, s->scratch.counters.as<uint32_t>(), st));
+    } else {
+        // the reference's decision: its closest hit along the unbounded ray, then t <= tmax
+        RTB_CHECK(s->scratch.queue.reserve(n * 4));
+        RTB_CHECK(s->any_hits.reserve(n * sizeof(rt_hit)));
+        RTB_CHECK(launch_trace_closest(s->view(), rays, n, s->any_hits.as<rt_hit>(),
+                                       (flags & RT_TRACE_SHADOW) | kTraceUnbounded, s->scratch.queue.as<uint32_t>(),
+                                       (uint32_t)n, s->scratch.counters.as<uint32_t>(), st));
+        RTB_CHECK(launch_occlusion_from_hits(rays, n, s->any_hits.as<rt_hit>(), out, bits, st));
+    }
     uint32_t c[4] = {0, 0, 0, 0};
     RTB_CUDA(cudaMemcpyAsync(c, s->scratch.counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, s->ctx->stream));
     RTB_CUDA(cudaStreamSynchronize(s->ctx->stream));
     return check_device_status(c[1]);
+}
+
+int rt_trace_any(rt_scene *s, const rt_ray *rays, uint64_t n, uint8_t *occluded, uint32_t flags)
+{
+    return trace_any_common(s, rays, n, occluded, false, flags, "rt_trace_any");
+}
+
+int rt_trace_any_bits(rt_scene *s, const rt_ray *rays, uint64_t n, uint32_t *occluded_bits, uint32_t flags)
+{
+    return trace_any_common(s, rays, n, occluded_bits, true, flags, "rt_trace_any_bits");
 }
 
 int rt_trace_stats_get(rt_scene *s, rt_trace_stats *out)

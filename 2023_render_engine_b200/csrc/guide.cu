@@ -506,10 +506,9 @@ int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf,
     double *wpart = reinterpret_cast<double *>(g->scal.as<uint8_t>() + 64);
     k_guide_wsum<<<kWsumBlocks, 256, 0, st>>>(w, B, wpart, scal);
     RTB_CUDA(cudaGetLastError());
-    static bool attr = false;
-    if (!attr) {
+    if (!(device_slot(SLOT_SMEM_ATTRS) & SMEM_GUIDE_TRAIN)) {
         RTB_CUDA(cudaFuncSetAttribute(k_guide_train_fb, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem));
-        attr = true;
+        or_device_slot(SLOT_SMEM_ATTRS, SMEM_GUIDE_TRAIN);
     }
     TrainArgs a{q, dir, pdf, w, B, Bp, g->xt.as<__half>(), g->gt.as<__half>(), scal, wpart, guide_box(g)};
     const uint64_t tiles = Bp / 16;
@@ -661,13 +660,12 @@ static int guide_eval_common(rt_guide *g, uint64_t B, const char *who)
     if (!g) return fail(RT_ERR_INVALID, std::string(who) + ": null guide");
     if (B >= (1ull << 31)) return fail(RT_ERR_INVALID, std::string(who) + ": batch too large");
     RTB_CUDA(cudaSetDevice(g->ctx->device));
-    static bool attr = false;
-    if (!attr) {
+    if (!(device_slot(SLOT_SMEM_ATTRS) & SMEM_GUIDE_EVAL)) {
         RTB_CUDA(cudaFuncSetAttribute(k_guide_eval<RawSink>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
         RTB_CUDA(cudaFuncSetAttribute(k_guide_eval<PdfSink>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
         RTB_CUDA(
             cudaFuncSetAttribute(k_guide_eval<SampleSink>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
-        attr = true;
+        or_device_slot(SLOT_SMEM_ATTRS, SMEM_GUIDE_EVAL);
     }
     return RT_OK;
 }

@@ -11,7 +11,9 @@
 // The array is a file-scope __device__ array, so every GPU that loads the library holds
 // it (a little over 4 MiB) until the process exits. Host code cannot use the array's name
 // as a device address; its address is looked up once per device with
-// cudaGetSymbolAddress, with that device current.
+// cudaGetSymbolAddress, with that device current, and kept for the life of the process.
+// A cudaDeviceReset by the application destroys the module that holds the array, so the
+// kept address is stale afterwards: do not call this entry point after resetting a device.
 #include <mutex>
 
 #include "rt_internal.h"
@@ -58,6 +60,11 @@ extern "C" int rt_trace_closest_noalloc(rt_scene *s, const rt_ray *rays, uint64_
                                      "use rt_trace_closest)");
     if ((reinterpret_cast<uintptr_t>(rays) | reinterpret_cast<uintptr_t>(hits)) & 15u)
         return fail(RT_ERR_INVALID, "rt_trace_closest_noalloc: buffers must be 16-byte aligned");
+    if (n == 0) {  // nothing to launch; the shared counters may hold another call's values
+        s->last_rays = 0;
+        s->last_fallback = 0;
+        return RT_OK;
+    }
     RTB_CUDA(cudaSetDevice(s->ctx->device));
     uint32_t *scratch = nullptr;
     RTB_CHECK(scratch_for(s->ctx->device, &scratch));

@@ -1040,26 +1040,27 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     RTB_CUDA(cudaEventRecord(e0, st));
     RTB_CUDA(cudaMemsetAsync(bf.cnt, 0, 256, st));
     const unsigned blocks = cap / kB;
-    static unsigned shadow_resident = 0;
+    unsigned shadow_resident = device_slot(SLOT_SHADOW_RESIDENT);
     if (!shadow_resident) {
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shadow, kB, 0);
-        shadow_resident = (unsigned)std::max(1, s->ctx->sm_count * std::max(per_sm, 1));
+        shadow_resident = device_sm_count() * (unsigned)std::max(per_sm, 1);
+        set_device_slot(SLOT_SHADOW_RESIDENT, shadow_resident);
     }
     const unsigned shadow_blocks = std::min<unsigned>(shadow_resident, (scap + kB - 1) / kB);
-    static unsigned gather_resident = 0;  // persistent gather warps: every resident block
+    unsigned gather_resident = device_slot(SLOT_GATHER_RESIDENT);  // persistent gather warps: every resident block
     if (gathers && !gather_resident) {
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather, kGatherBlock, 0);
-        gather_resident = (unsigned)std::max(1, s->ctx->sm_count * std::max(per_sm, 1));
+        gather_resident = device_sm_count() * (unsigned)std::max(per_sm, 1);
+        set_device_slot(SLOT_GATHER_RESIDENT, gather_resident);
     }
     const unsigned gather_blocks =
         (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(gather_resident, ((uint64_t)gcap * 32 + kGatherBlock - 1) /
                                                                                 kGatherBlock));
-    static bool infer_attr = false;
-    if (gv.params && !infer_attr) {
+    if (gv.params && !(device_slot(SLOT_SMEM_ATTRS) & SMEM_RENDER_INFER)) {
         RTB_CUDA(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
-        infer_attr = true;
+        or_device_slot(SLOT_SMEM_ATTRS, SMEM_RENDER_INFER);
     }
     const unsigned infer_blocks = (unsigned)std::max(1, s->ctx->sm_count);  // one CTA of 4 tile groups per SM
     const GuideBox gbox = guided ? guide_box(guide) : GuideBox{};

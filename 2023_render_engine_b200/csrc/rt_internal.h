@@ -62,6 +62,25 @@ struct DevBuf {
     T *as() const { return static_cast<T *>(ptr); }
 };
 
+// Launch sizes derived from occupancy and per-kernel function attributes are properties of
+// a device, not of the process: each is cached per CUDA device id.
+constexpr int kMaxDevices = 64;
+enum DeviceSlot : int {
+    SLOT_TRACE_RESIDENT = 0,   // resident blocks of k_trace_closest (SM count x blocks per SM)
+    SLOT_SHADOW_RESIDENT = 1,  // resident blocks of the render's k_shadow
+    SLOT_GATHER_RESIDENT = 2,  // resident blocks of the render's k_gather
+    SLOT_SMEM_ATTRS = 3,       // bit mask of kernels whose dynamic shared-memory limit is raised (SMEM_*)
+    SLOT_SM_COUNT = 4,         // multiprocessor count
+    SLOT_COUNT = 5
+};
+enum SmemAttr : unsigned { SMEM_RENDER_INFER = 1u, SMEM_GUIDE_TRAIN = 2u, SMEM_GUIDE_EVAL = 4u };
+// Value of `slot` for the current device; 0 until set_device_slot stored one.
+unsigned device_slot(DeviceSlot slot);
+void set_device_slot(DeviceSlot slot, unsigned value);
+void or_device_slot(DeviceSlot slot, unsigned bits);
+// Multiprocessor count of the current device (cached).
+unsigned device_sm_count();
+
 // Error codes written by kernels into the status word (first failure wins).
 enum DevError : uint32_t {
     DEV_OK = 0,
@@ -158,7 +177,15 @@ int launch_trace_closest(const SceneView &v, const rt_ray *rays, uint64_t n, rt_
 // Same with the ray count read on the device (queues built by other kernels); cap bounds it.
 int launch_trace_closest_dev(const SceneView &v, const rt_ray *rays, const uint32_t *n_dev, uint32_t cap, rt_hit *hits,
                              uint32_t flags, uint32_t *queue, uint32_t *counters, cudaStream_t s);
-int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, uint8_t *occluded, uint32_t flags,
+// Internal trace flag (above the public RT_TRACE_* bits): trace every ray with tmax = inf,
+// as the reference's shadow rays are, whatever tmax the ray carries.
+constexpr uint32_t kTraceUnbounded = 0x80000000u;
+// Occlusion decided from closest hits: hit and t <= the ray's tmax (Scene::isVisible).
+int launch_occlusion_from_hits(const rt_ray *rays, uint64_t n, const rt_hit *hits, void *out, bool bits,
+                               cudaStream_t s);
+// Any-hit occlusion of n rays: one byte per ray, or (bits) bit i % 32 of word i / 32 (the last
+// word's bits past n are 0).
+int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, void *out, bool bits, uint32_t flags,
                      uint32_t *counters, cudaStream_t s);
 
 // Wavefront buffers of rt_render (grown on demand, kept between calls).
@@ -250,6 +277,7 @@ struct rt_scene {
     rtb::TraceScratch scratch;
     uint64_t last_rays = 0, last_fallback = 0;
     rtb::DevBuf h2d_rays, d2h_hits;  // device staging for the host-buffer entry points
+    rtb::DevBuf any_hits;            // closest hits behind rt_trace_any's reference-exact decision
     // rendering
     std::vector<rt_material> materials;
     std::vector<float4> plights;  // 2 per light: position, rgb * intensity

@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(kBlock, RTB_TRAV_MIN_BLOCKS) k_trace_closest(S
         [&](uint32_t i, Trav &T) {
             float4 ra, rb;
             load_ray(rays, i, ra, rb);
-            trav_init(T, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w);
+            trav_init(T, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, (flags & kTraceUnbounded) ? INFINITY : ra.w);
             T.shadow = shadow;
         },
         [&](uint32_t i, Trav &T) { closest_epilogue(v, i, T, flags, hits, queue, queue_cap, counters); });
@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(kBlock) k_trace_exact(SceneView v, const rt_ra
         const uint64_t i = entry & ~kQueueBlocker;
         float4 ra, rb;
         load_ray(rays, i, ra, rb);
+        if (flags & kTraceUnbounded) ra.w = INFINITY;
         WatertightRay w = make_watertight(ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w);
         const float ix = fdiv(1.0f, rb.x), iy = fdiv(1.0f, rb.y), iz = fdiv(1.0f, rb.z);
         rt_hit cand = hits[i];
@@ -135,46 +136,80 @@ __global__ void __launch_bounds__(kBlock) k_trace_exact(SceneView v, const rt_ra
     }
 }
 
+// One thread per ray; BITS: the warp's 32 results go out as one word (rays 32w .. 32w+31).
+template <bool BITS>
 __global__ void __launch_bounds__(kBlock) k_trace_any(SceneView v, const rt_ray *__restrict__ rays, uint64_t n,
-                                                      uint8_t *__restrict__ occluded, uint32_t flags,
+                                                      void *__restrict__ out, uint32_t flags,
                                                       uint32_t *__restrict__ counters)
 {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float4 ra, rb;
-    load_ray(rays, i, ra, rb);
-    const bool shadow = (flags & RT_TRACE_SHADOW) != 0;
-    WatertightRay w = make_watertight(ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w);
-    Best best{INFINITY, -1, 0u, 0.f, 0.f, INFINITY};
-    bool ok = true;
-    if (v.ntri > 0) ok = traverse_bvh8(v, w, rb.x, rb.y, rb.z, shadow, true, best);
-    if (!ok) atomicCAS(counters + 1, 0u, (uint32_t)DEV_STACK_OVERFLOW);
-    bool occ = best.prim >= 0 && best.t < ra.w;
-    if (!occ) {
-        float t = ra.w;
-        int32_t prim = -1;
-        float b1 = 0, b2 = 0;
-        intersect_spheres(v, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w, shadow, t, prim, b1, b2);
-        occ = prim >= 0 && t < ra.w;
+    bool occ = false;
+    if (i < n) {
+        float4 ra, rb;
+        load_ray(rays, i, ra, rb);
+        const bool shadow = (flags & RT_TRACE_SHADOW) != 0;
+        WatertightRay w = make_watertight(ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w);
+        Best best{INFINITY, -1, 0u, 0.f, 0.f, INFINITY};
+        bool ok = true;
+        if (v.ntri > 0) ok = traverse_bvh8(v, w, rb.x, rb.y, rb.z, shadow, true, best);
+        if (!ok) atomicCAS(counters + 1, 0u, (uint32_t)DEV_STACK_OVERFLOW);
+        occ = best.prim >= 0 && best.t < ra.w;
+        if (!occ) {
+            float t = ra.w;
+            int32_t prim = -1;
+            float b1 = 0, b2 = 0;
+            intersect_spheres(v, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w, shadow, t, prim, b1, b2);
+            occ = prim >= 0 && t < ra.w;
+        }
     }
-    occluded[i] = occ ? 1 : 0;
+    if (BITS) {
+        // the grid covers whole warps, so every lane of a warp reaches the ballot
+        const uint32_t word = __ballot_sync(0xFFFFFFFFu, occ);
+        if ((threadIdx.x & 31u) == 0 && i < n) static_cast<uint32_t *>(out)[i >> 5] = word;
+    } else if (i < n) {
+        static_cast<uint8_t *>(out)[i] = occ ? 1 : 0;
+    }
+}
+
+// Scene::isVisible's decision from the closest hits of an unbounded trace: a ray is
+// occluded when it hit something no farther than its tmax (visible = no hit or t > distance).
+template <bool BITS>
+__global__ void __launch_bounds__(kBlock) k_occlusion_from_hits(const rt_ray *__restrict__ rays, uint64_t n,
+                                                                const rt_hit *__restrict__ hits, void *__restrict__ out)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool occ = false;
+    if (i < n) {
+        const float4 h = __ldg(reinterpret_cast<const float4 *>(hits) + i);
+        const float tmax = __ldg(reinterpret_cast<const float *>(rays) + 8 * i + 3);
+        occ = __float_as_int(h.y) != RT_PRIM_NONE && h.x <= tmax;
+    }
+    if (BITS) {
+        const uint32_t word = __ballot_sync(0xFFFFFFFFu, occ);
+        if ((threadIdx.x & 31u) == 0 && i < n) static_cast<uint32_t *>(out)[i >> 5] = word;
+    } else if (i < n) {
+        static_cast<uint8_t *>(out)[i] = occ ? 1 : 0;
+    }
 }
 
 }  // namespace
 
-// Resident blocks of the persistent closest-hit kernel on this device (queried once).
+// Resident blocks of the persistent closest-hit kernel on the current device.
 static unsigned persistent_blocks()
 {
-    static unsigned cached = 0;
+    unsigned cached = device_slot(SLOT_TRACE_RESIDENT);
     if (!cached) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_closest, kBlock, 0);
-        cached = (unsigned)std::max(1, sms * std::max(per_sm, 1));
+        cached = device_sm_count() * (unsigned)std::max(per_sm, 1);
+        set_device_slot(SLOT_TRACE_RESIDENT, cached);
     }
     return cached;
 }
+
+// Grid of k_trace_exact: a grid-stride loop over the (usually tiny) replay queue, four
+// blocks per SM.
+static unsigned exact_blocks() { return 4 * device_sm_count(); }
 
 int launch_trace_closest(const SceneView &v, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags,
                          uint32_t *queue, uint32_t queue_cap, uint32_t *counters, cudaStream_t s)
@@ -186,7 +221,7 @@ int launch_trace_closest(const SceneView &v, const rt_ray *rays, uint64_t n, rt_
     RTB_CUDA(cudaGetLastError());
     // Always launched: stack-overflow rays are replayed even in RT_TRACE_FAST mode. It
     // reads the queue length on the device, so no host synchronisation is needed.
-    k_trace_exact<<<148 * 4, kBlock, 0, s>>>(v, rays, hits, flags, queue, queue_cap, counters);
+    k_trace_exact<<<exact_blocks(), kBlock, 0, s>>>(v, rays, hits, flags, queue, queue_cap, counters);
     RTB_CUDA(cudaGetLastError());
     return RT_OK;
 }
@@ -199,18 +234,33 @@ int launch_trace_closest_dev(const SceneView &v, const rt_ray *rays, const uint3
     const uint64_t blocks = std::min<uint64_t>(((uint64_t)cap + kBlock - 1) / kBlock, persistent_blocks());
     k_trace_closest<<<(unsigned)blocks, kBlock, 0, s>>>(v, rays, cap, n_dev, hits, flags, queue, cap, counters);
     RTB_CUDA(cudaGetLastError());
-    k_trace_exact<<<148 * 4, kBlock, 0, s>>>(v, rays, hits, flags, queue, cap, counters);
+    k_trace_exact<<<exact_blocks(), kBlock, 0, s>>>(v, rays, hits, flags, queue, cap, counters);
     RTB_CUDA(cudaGetLastError());
     return RT_OK;
 }
 
-int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, uint8_t *occluded, uint32_t flags,
+int launch_occlusion_from_hits(const rt_ray *rays, uint64_t n, const rt_hit *hits, void *out, bool bits, cudaStream_t s)
+{
+    if (n == 0) return RT_OK;
+    const uint64_t blocks = (n + kBlock - 1) / kBlock;
+    if (bits)
+        k_occlusion_from_hits<true><<<(unsigned)blocks, kBlock, 0, s>>>(rays, n, hits, out);
+    else
+        k_occlusion_from_hits<false><<<(unsigned)blocks, kBlock, 0, s>>>(rays, n, hits, out);
+    RTB_CUDA(cudaGetLastError());
+    return RT_OK;
+}
+
+int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, void *out, bool bits, uint32_t flags,
                      uint32_t *counters, cudaStream_t s)
 {
     if (n == 0) return RT_OK;
     RTB_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), s));
     const uint64_t blocks = (n + kBlock - 1) / kBlock;
-    k_trace_any<<<(unsigned)blocks, kBlock, 0, s>>>(v, rays, n, occluded, flags, counters);
+    if (bits)
+        k_trace_any<true><<<(unsigned)blocks, kBlock, 0, s>>>(v, rays, n, out, flags, counters);
+    else
+        k_trace_any<false><<<(unsigned)blocks, kBlock, 0, s>>>(v, rays, n, out, flags, counters);
     RTB_CUDA(cudaGetLastError());
     return RT_OK;
 }

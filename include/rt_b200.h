@@ -157,15 +157,26 @@ RT_API int rt_trace_closest_host(rt_scene *scene, const rt_ray *rays, uint64_t n
  * counters) is a fixed device array inside this library, about 4 MiB, held on every GPU
  * that loads the library until the process exits. At most 1048576 rays per call
  * (RT_ERR_CAPACITY above that). The first call on a device looks up the array's device
- * address (make that first call before any stream capture). All calls share the array:
+ * address (make that first call before any stream capture) and keeps it for the process's
+ * life, so do not call it after a cudaDeviceReset of that device. All calls share the array:
  * calls that overlap on the GPU (other threads or streams) race; serialise them. */
 RT_API int rt_trace_closest_noalloc(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, rt_hit *hits_dev,
                                     uint32_t flags);
 
-/* Occlusion test: occluded[i] = 1 when a primitive is hit at t < rays[i].tmax.
- * Replaces the shadow-ray use of Scene::intersects in Scene::isVisible
- * (Scene.cu:238-276). Device pointers. */
+/* Occlusion test, replacing the shadow-ray use of Scene::intersects in Scene::isVisible
+ * (Scene.cu:238-276): rays[i].tmax is the distance to the light. Device pointers.
+ * Default: the reference's decision, bit for bit. The ray is traced unbounded (the reference's
+ * shadow rays carry tMax = inf) to the closest hit rt_trace_closest reports, and
+ * occluded[i] = 1 when there is one at t <= tmax (isVisible: visible = no hit or t > distance).
+ * With RT_TRACE_FAST: any-hit traversal that stops at the first primitive hit at t < tmax (the
+ * renderer's shadow rays); it can differ from the reference where the reference's offset-update
+ * quirk hides an occluder (Triangle.cu:569-593) and at t == tmax.
+ * RT_TRACE_SHADOW: transparent primitives do not occlude (checkShadow, Triangle.cu:439-440). */
 RT_API int rt_trace_any(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, uint8_t *occluded_dev, uint32_t flags);
+/* The same decisions packed into a bit mask: ray i is bit i % 32 of occluded_bits[i / 32]
+ * (ceil(n / 32) words, 4-byte aligned; the last word's bits past n are 0). */
+RT_API int rt_trace_any_bits(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, uint32_t *occluded_bits_dev,
+                             uint32_t flags);
 
 /* Counters of the last rt_trace_closest call: rays that took the reference-order
  * exact traversal (distance ties resolved through the reference tree, grazing

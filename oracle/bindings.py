@@ -27,13 +27,21 @@ I = ctypes.c_int
 F = ctypes.c_float
 
 
+def reference_dir() -> Path | None:
+    """The reference source tree named by the REF_DIR environment variable, if it exists."""
+    d = os.environ.get("REF_DIR", "")
+    return Path(d) if d and Path(d).is_dir() else None
+
+
 def build(ref: bool = True):
-    """Builds the restatement (always) and the reference harness when the reference
-    tree is present. Returns the list of targets built."""
+    """Builds the restatement (always) and the reference harnesses when REF_DIR names the
+    reference tree. Returns the list of targets built."""
     targets = ["restate"]
-    if ref and Path(os.environ.get("REF_DIR", "/root/reference")).is_dir():
+    rd = reference_dir()
+    if ref and rd is not None:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+    env = dict(os.environ, REF_DIR=str(rd)) if rd is not None else None
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True, env=env)
     return targets
 
 

@@ -1,5 +1,4 @@
 import importlib
-import os
 import sys
 from pathlib import Path
 
@@ -42,10 +41,10 @@ def refo():
     from oracle import bindings
 
     if not bindings.REF_SO.exists():
-        if Path(os.environ.get("REF_DIR", "/root/reference")).is_dir():
+        if bindings.reference_dir() is not None:
             bindings.build(ref=True)
         else:
-            pytest.skip("reference harness library not built and reference tree absent")
+            pytest.skip("reference harness library not built and REF_DIR does not name the reference tree")
     return bindings.RefOracle()
 
 

@@ -232,3 +232,98 @@ def test_reference_cuda_build_agrees(core, gpu_ctx):
     sc.commit()
     hits = sc.trace_closest_host(core.make_rays(o, d))
     assert (ids == hits["prim"]).mean() > 0.9999
+
+
+def occlusion_gpu(sc, o, d, tmax, flags=0):
+    """rt_trace_any (bytes) and rt_trace_any_bits for the same rays; both must agree."""
+    import torch
+
+    n = o.shape[0]
+    rays = core_make_rays(o, d, tmax)
+    rd = torch.from_numpy(rays.view(np.float32).reshape(-1)).cuda()
+    occ = torch.full((n,), 7, dtype=torch.uint8, device="cuda")
+    bits = torch.full(((n + 31) // 32,), -1, dtype=torch.int32, device="cuda")
+    sc.trace_any(rd, occ, n, flags)
+    sc.trace_any_bits(rd, bits, n, flags)
+    torch.cuda.synchronize()
+    b = occ.cpu().numpy()
+    words = bits.cpu().numpy().view(np.uint32)
+    unpacked = ((words[:, None] >> np.arange(32, dtype=np.uint32)) & 1).reshape(-1).astype(np.uint8)
+    assert np.array_equal(unpacked[:n], b)
+    assert not unpacked[n:].any()  # bits past n are zero
+    return b.astype(bool)
+
+
+def distances_around(t_ref, hit, rng):
+    """Light distances for the isVisible test: for rays that hit, before, exactly at, one ulp
+    either side of, and beyond the reference's hit distance; for misses, anything."""
+    n = t_ref.shape[0]
+    pick = rng.integers(0, 6, n)
+    t = np.where(hit, t_ref, 1.0).astype(np.float32)
+    dist = np.select(
+        [pick == 0, pick == 1, pick == 2, pick == 3, pick == 4],
+        [t * np.float32(0.5), t, np.nextafter(t, np.float32(0)), np.nextafter(t, np.float32(np.inf)),
+         t * np.float32(3.0)],
+        rng.uniform(0.01, 5.0, n).astype(np.float32)).astype(np.float32)
+    return dist
+
+
+@pytest.mark.parametrize("key", ["soup1000", "soup20000", "grids"])
+def test_trace_any_is_reference_isvisible(core, gpu_ctx, key):
+    """rt_trace_any = Scene::isVisible's decision (Scene.cu:238-276) on the golden rays: the
+    reference's closest hit along the unbounded ray, occluded when it is no farther than the
+    light (visible = no hit or t > distance), with the light at, one ulp either side of, and
+    away from the reference's own hit distance."""
+    g = _unpack(np.load(GOLDEN / "trace_small.npz"), key)
+    sc = make_scene(core, gpu_ctx, g["v"], g["f"])
+    hit = g["ids"] >= 0
+    dist = distances_around(g["t"], hit, np.random.default_rng(5))
+    want = hit & (g["t"] <= dist)
+    got = occlusion_gpu(sc, g["o"], g["d"], dist)
+    assert np.array_equal(got, want)
+    assert 0.2 < want.mean() < 0.8  # both answers well represented
+    # any-hit mode (the renderer's shadow rays): same answer away from the boundary
+    fast = occlusion_gpu(sc, g["o"], g["d"], dist, N.RT_TRACE_FAST)
+    away = ~hit | (np.abs(dist - g["t"]) > 1e-5 * np.maximum(g["t"], 1))
+    assert (fast[away] == want[away]).mean() > 0.9999
+
+
+def test_trace_any_transparency_spheres_and_edges(core, gpu_ctx, restated):
+    """checkShadow semantics (transparent triangles and glass spheres do not occlude), the
+    analytic-shape loop of Scene::intersects and the edge rays (exact ties, axis-aligned rays,
+    offsets below the error bound) with the reference's decision taken from the pinned
+    restatement's closest hit."""
+    g = np.load(GOLDEN / "spheres_cornell.npz")
+    v, f = cases.stacked_grids()
+    tr = np.zeros(f.shape[0], np.uint8)
+    tr[-2:] = 1
+    spheres = [{"o2w": g[f"o2w{i}"], "w2o": g[f"w2o{i}"], "radius": float(g["radii"][i]), "glass": i == 1}
+               for i in range(len(g["radii"]))]
+    sc = make_scene(core, gpu_ctx, v, f, transparent=tr, spheres=spheres)
+    o, d = cases.edge_rays(9)
+    o2, d2 = S.random_rays(20000, seed=77, lo=-1.2, hi=1.2)
+    o, d = np.concatenate([o, o2]), np.concatenate([d, d2])
+    rng = np.random.default_rng(8)
+    ob = restated.bvh(v, f, tr)
+    for shadow in (False, True):
+        flags = N.RT_TRACE_SHADOW if shadow else 0
+        ids, t, _ = trace_gpu(sc, o, d, flags=flags)  # closest hit, pinned to the reference elsewhere
+        tri, ttri = ob.intersect(o, d, shadow=shadow)
+        hit = ids >= 0
+        assert np.array_equal(ids[ids < N.RT_PRIM_SHAPE], tri[ids < N.RT_PRIM_SHAPE])
+        dist = distances_around(t, hit, rng)
+        got = occlusion_gpu(sc, o, d, dist, flags)
+        assert np.array_equal(got, hit & (t <= dist))
+
+
+def test_trace_any_empty_and_invalid(core, gpu_ctx):
+    import torch
+
+    v, f = cases.soup(100, 3)
+    sc = make_scene(core, gpu_ctx, v, f)
+    rd = torch.zeros(8, dtype=torch.float32, device="cuda")
+    occ = torch.zeros(1, dtype=torch.uint8, device="cuda")
+    sc.trace_any(rd, occ, 0)
+    bits = torch.zeros(2, dtype=torch.int32, device="cuda")
+    with pytest.raises(N.RtError):  # a bit mask must be 4-byte aligned
+        N.check(N.lib().rt_trace_any_bits(sc.handle, rd.data_ptr(), 1, bits.data_ptr() + 2, 0))

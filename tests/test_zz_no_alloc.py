@@ -46,11 +46,21 @@ def test_noalloc_matches_allocating_entry_point(core, gpu_ctx):
         hits_d = torch.empty(n * 4, dtype=torch.float32, device="cuda")
         for flags in (0, N.RT_TRACE_SHADOW):
             ref = _trace(lib.rt_trace_closest, sc, rays_d, hits_d, n, flags)
+            ref_stats = sc.trace_stats()
             got = _trace(lib.rt_trace_closest_noalloc, sc, rays_d, hits_d, n, flags)
+            got_stats = sc.trace_stats()
             assert np.array_equal(got["prim"], ref["prim"])
             hit = ref["prim"] >= 0
             assert np.array_equal(got["t"][hit], ref["t"][hit])
             assert np.array_equal(got["b1"][hit], ref["b1"][hit])
+            assert np.array_equal(got["b2"][hit], ref["b2"][hit])
+            # the replay queue half of the shared array carried the same rays
+            assert got_stats == ref_stats
+            if call == 0:
+                assert got_stats["exact_fallback_rays"] > 0
+    # an empty call after calls that left counters behind reports nothing of theirs
+    N.check(lib.rt_trace_closest_noalloc(sc.handle, rays_d.data_ptr(), 0, hits_d.data_ptr(), 0))
+    assert sc.trace_stats() == {"rays": 0, "exact_fallback_rays": 0}
 
 
 def test_noalloc_rejects_batches_above_the_limit(core, gpu_ctx):
