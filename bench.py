@@ -15,9 +15,11 @@ roofline of the dominant kernel (k_trace_closest).
 N > 1 runs under torchrun: every rank renders its own image (different seed; independent
 replicas, weak scaling, no collective on the data path); the time is the max over ranks.
 
---impl reference times the reference renderer's own traversal (BVH::intersectRay,
-compiled from its sources into oracle/_ref) on this machine's host cores over a bounded
-sample of the BVH-stress ray set; rank 0 alone runs it.
+--impl reference times the reference renderer's own integrator (PathTracerIntegrator::render
+with Scene::build and its BVH, compiled from its sources into oracle/_ref with thrust's device
+system on OpenMP, so its whole render runs on this machine's host cores) on the same scene,
+camera and depth; each step renders a bounded sample of the frame (a lower-resolution image of
+the same view at 1 spp). Rank 0 alone runs it.
 """
 from __future__ import annotations
 
@@ -152,39 +154,88 @@ def cpu_reference_rate(v, f, o, d, threads):
     return o.shape[0] / dt / 1e6, dt
 
 
+def bench_config(args):
+    """The `config` both arms report: the workload this benchmark is quoted on."""
+    return {"workload": WORKLOAD, "width": args.width, "height": args.height, "spp": args.spp, "max_depth": 12,
+            "triangles": 1_310_732}
+
+
+def reference_scene(S):
+    """The BVH-stress scene in the reference harness's terms: one mesh, per-triangle materials
+    (the Cornell walls, the emitter, one Trowbridge material per 64-triangle block) and the
+    Cornell camera (pinhole at (0, 0, 3.5) looking down -z, 40 degree vertical field of view)."""
+    from oracle import bindings
+
+    R = bindings.RefIntegrator
+    sd = S.stress_scene()
+    v, f, m = S.flatten(sd)
+    table = [R.entry(R.LAMBERTIAN, (0.8, 0.8, 0.8)), R.entry(R.LAMBERTIAN, (0.8, 0.1, 0.1)),
+             R.entry(R.LAMBERTIAN, (0.1, 0.8, 0.1)), R.entry(R.LIGHT, (1, 1, 1), value=15.0)]
+    rough = sd["roughness"]
+    ggx = np.flatnonzero(m == S.MAT_GGX)
+    tri_mat = m.astype(np.uint32).copy()
+    for blk, r in enumerate(rough[::64][:(rough.shape[0] + 63) // 64]):
+        table.append(R.entry(R.TROWBRIDGE, (1, 1, 1), (1.5, 1.5, 1.5), (0, 0, 0), (float(r), float(r))))
+    tri_mat[ggx] = 4 + (np.arange(ggx.shape[0]) // 64)
+    return v, f, tri_mat, table
+
+
+REFERENCE_CAMERA = "camera\np 0 0 3.5\nlookat 0 0 0\nup 0 1 0\ncts 0 0 -0.8\nframeY 0.5823\n"
+
+
+def reference_render_rate(host, args, S, width, height, spp, runs=1, warmup=0):
+    """The reference integrator (host build, or its CUDA build) on the BVH-stress scene at
+    width x height (the bench camera's view), spp, depth 12: per run (seconds in
+    PathTracerIntegrator::render, rays it traced, build seconds). None if not built."""
+    import tempfile
+
+    from oracle import bindings
+
+    try:
+        R = bindings.RefIntegrator(host=host)
+    except (FileNotFoundError, OSError):
+        return None
+    v, f, tri_mat, table = reference_scene(S)
+    with tempfile.TemporaryDirectory() as td:
+        cam = Path(td) / "camera.obejota"
+        cam.write_text(REFERENCE_CAMERA)
+        out = []
+        for k in range(warmup + runs):
+            _, _, _, st = R.render(cam, width, height, spp, 12, table, v, f, tri_mat)
+            if k >= warmup:
+                out.append(st)
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
     S = importlib.import_module("2023_render_engine_b200.scenes")
-    sc_data = S.stress_scene()
-    v, f, _ = S.flatten(sc_data)
-    o, d = S.random_rays(NRAYS, seed=7)
     threads = os.cpu_count() or 1
-    sample = args.ref_sample
-    from oracle import bindings
-
-    R = bindings.RefOracle()
-    b = R.bvh(v, f)
-    for w in range(args.warmup):
-        b.intersect(o[:4096], d[:4096], threads=threads)
-    times = []
-    for k in range(args.steps):
-        s0 = (k * sample) % (NRAYS - sample)
-        t0 = time.perf_counter()
-        b.intersect(o[s0:s0 + sample], d[s0:s0 + sample], threads=threads)
-        times.append(time.perf_counter() - t0)
-    ms = 1000 * float(np.mean(times))
-    val = sample / (ms / 1000) / 1e6
+    w, h = args.ref_width, args.ref_height
+    runs = reference_render_rate(True, args, S, w, h, 1, runs=args.steps, warmup=args.warmup)
+    if runs is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_integrator_host.so not built "
+                                                              "(make -C oracle ref with REF_DIR set)"}))
+        return
+    secs = np.array([r["render_s"] for r in runs])
+    rays = np.array([r["extension_rays"] + r["shadow_rays"] for r in runs], np.float64)
+    ms = 1000 * float(secs.mean())
+    val = float(rays.sum() / secs.sum() / 1e6)
+    sample = (f"{w}x{h} image of the same view (camera, scene, depth 12), 1 spp per step; the reference's "
+              f"estimator traces no shadow rays here (it has no area-light NEE)")
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "Mrays/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "rays_per_step": sample,
-                   "reference_path": "BVH::intersectRay over the BVH-stress ray set (the reference's render loop "
-                                     "needs its GPU BVH; its traversal alone is timed, shading excluded)"},
-        "cpu_baseline": {"value": val, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-                         "sample": f"{sample} consecutive rays of the 2^24 set per step"},
+        "config": bench_config(args),
+        "sample": {"rays_per_step": float(rays.mean()), "what": sample,
+                   "reference_path": "PathTracerIntegrator::render + Scene::build of the reference, its BVH built "
+                                     "and traversed by its own code on the host cores (thrust OpenMP system), "
+                                     "shading on its 128 worker threads",
+                   "build_s": float(np.mean([r["build_s"] for r in runs]))},
+        "cpu_baseline": {"value": val, "unit": "Mrays/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": val, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -467,6 +518,16 @@ def run_ours(args):
     ref_cuda = None
     if world == 1 and not args.no_ref_cuda:
         ref_cuda = measure_reference_cuda(v, f, o, d, hits_d, N)
+        runs = reference_render_rate(False, args, S, args.ref_width, args.ref_height, 1, runs=2, warmup=1)
+        if runs:
+            secs = sum(r["render_s"] for r in runs)
+            rays_ref = sum(r["extension_rays"] + r["shadow_rays"] for r in runs)
+            ref_cuda["render"] = {
+                "value": rays_ref / secs / 1e6, "unit": "Mrays/s",
+                "workload": f"the reference's PathTracerIntegrator::render, its stock CUDA build (compile.sh flags: "
+                            f"BVH built and traversed on this GPU by thrust, shading on its host threads), on the "
+                            f"same scene and view at {args.ref_width}x{args.ref_height}, 1 spp, depth 12",
+                "rays_per_run": rays_ref / len(runs), "seconds_per_run": secs / len(runs)}
 
     # ---- scene commit: device vs host build of the same structures
     scene_build = measure_scene_build(core, N, ctx, v, f) if world == 1 else None
@@ -485,14 +546,13 @@ def run_ours(args):
             "metric": METRIC, "value": rate, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, camera and sample streams)",
-            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": args.spp,
-                       "max_depth": p["max_depth"], "triangles": int(f.shape[0]),
-                       "rays_per_step_per_gpu": rays_step,
-                       "extension_rays": int(st_last["extension_rays"]), "shadow_rays": int(st_last["shadow_rays"]),
-                       "camera_rays": int(st_last["camera_rays"]), "waves": int(st_last["waves"]),
-                       "samples_per_s": samples * world / (ms / 1000),
-                       "l2": "scene ~140 MB and path queues ~1 GB per step exceed the 126 MB L2",
-                       "parallelism": f"replicas x{world}"},
+            "config": bench_config(args),
+            "details": {"rays_per_step_per_gpu": rays_step,
+                        "extension_rays": int(st_last["extension_rays"]), "shadow_rays": int(st_last["shadow_rays"]),
+                        "camera_rays": int(st_last["camera_rays"]), "waves": int(st_last["waves"]),
+                        "samples_per_s": samples * world / (ms / 1000),
+                        "l2": "scene ~140 MB and path queues ~1 GB per step exceed the 126 MB L2",
+                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": rate_e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 144 + 32,
                     "d2h_bytes_per_step": W * H * 16,
                     "note": "render call through the C ABI + film read back to pinned host memory; the inputs "
@@ -518,11 +578,22 @@ def run_ours(args):
         }
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
+            w, h = args.ref_width, args.ref_height
+            runs = reference_render_rate(True, args, S, w, h, 1, runs=1)
+            if runs:
+                r = runs[0]
+                rays_ref = r["extension_rays"] + r["shadow_rays"]
+                line["cpu_baseline"] = {
+                    "value": rays_ref / r["render_s"] / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                    "sample": f"the reference's PathTracerIntegrator::render on the same scene and view at {w}x{h}, "
+                              f"1 spp, depth 12 ({rays_ref} rays in {r['render_s']:.1f} s; BVH built and traversed "
+                              f"by its own code on the host cores)"}
             ns = args.cpu_sample
             val, dt = cpu_reference_rate(v, f, o[:ns], d[:ns], threads)
-            line["cpu_baseline"] = {"value": val, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-                                    "sample": f"first {ns} rays of the BVH-stress ray set through the reference's "
-                                              f"BVH::intersectRay ({dt:.1f} s)"}
+            line["cpu_baseline_traversal"] = {
+                "value": val, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                "sample": f"first {ns} rays of the BVH-stress ray set through the reference's BVH::intersectRay "
+                          f"({dt:.1f} s); traversal only", "ours": trace_rate}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -536,7 +607,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1 << 20)
-    ap.add_argument("--ref-sample", type=int, default=1 << 18)
+    ap.add_argument("--ref-width", type=int, default=480, help="reference integrator sample image width")
+    ap.add_argument("--ref-height", type=int, default=270)
     ap.add_argument("--rays-log2", type=int, default=24, help="smaller ray sets for profiler captures")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)

@@ -49,6 +49,27 @@ def _np(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
+class _quiet_stdout:
+    """Sends file descriptor 1 to /dev/null for the duration (C code writing to stdout)."""
+
+    def __enter__(self):
+        import sys
+
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        import ctypes as _c
+
+        _c.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 class RefOracle:
     """The reference's own BVH / triangle / sphere / kd-tree code."""
 
@@ -621,3 +642,86 @@ class RefCuda:
         if rc != 0:
             raise RuntimeError("reference GPU trace failed: " + self.L.refg_error().decode())
         return ids, mk.value, ma.value
+
+
+class RefIntegrator:
+    """The reference's own PathTracerIntegrator::render (with Scene::build and its BVH) on
+    triangle meshes, spheres and planes (oracle/ref_integrator_harness.cu).
+
+    host=True: libref_integrator_host.so, the host-compiled integrator (thrust's device system
+    on OpenMP: its BVH build and traversal run on the host cores too). host=False:
+    libref_integrator_cuda.so, its stock CUDA build (BVH on the GPU, compile.sh flags)."""
+
+    # material kinds of the harness's 12-float table entries
+    LAMBERTIAN, TROWBRIDGE, LIGHT, DIELECTRIC, MIRROR = 0, 1, 2, 3, 4
+
+    def __init__(self, host: bool = True):
+        name = "libref_integrator_host.so" if host else "libref_integrator_cuda.so"
+        path = HERE / "_ref" / name
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+        L = ctypes.CDLL(str(path))
+        L.refi_error.restype = ctypes.c_char_p
+        L.refi_config.argtypes = [I, I, I, I]
+        L.refi_render.argtypes = [ctypes.c_char_p, U32, P, U32, P, P, P, U32, P, P, U32, P, P, U32, P, P, P, P, P]
+        L.refi_render.restype = I
+        L.refi_material_sample.argtypes = [P, P, P, U32, P, P, P]
+        L.refi_material_sample.restype = I
+        self.L = L
+        self.host = bool(L.refi_host_backend())
+
+    @staticmethod
+    def entry(kind, color=(1, 1, 1), eta=(0, 0, 0), k=(0, 0, 0), roughness=(0, 0), value=0.0):
+        """A material table entry: value is the Light intensity or the Dielectric IOR."""
+        e = np.zeros(12, np.float32)
+        e[0] = kind
+        e[1:4] = color
+        if kind == RefIntegrator.TROWBRIDGE:
+            e[4:7], e[7:10], e[10:12] = eta, k, roughness
+        else:
+            e[4] = value
+        return e
+
+    def render(self, obejota_path, width, height, spp, depth, materials, verts=None, idx=None, tri_mat=None,
+               tri_shape=None, spheres=(), planes=()):
+        """Returns (per-pixel mean (h*w, 3), camera_to_world (4, 4), raster_to_camera (4, 4), stats)
+        with stats = {render_s, extension_rays, shadow_rays, build_s}. spheres: (center, radius,
+        material); planes: (12 floats of Plane(corner, axisX, axisY, normal), material)."""
+        if self.L.refi_config(width, height, spp, depth) != 0:
+            raise ValueError("bad render configuration")
+        mats = _np(np.stack(list(materials)), np.float32).reshape(-1, 12)
+        if verts is None or idx is None or len(idx) == 0:
+            v = np.zeros((1, 3), np.float32)
+            f = np.zeros((0, 3), np.uint32)
+        else:
+            v, f = _np(verts, np.float32).reshape(-1, 3), _np(idx, np.uint32).reshape(-1, 3)
+        tm = _np(tri_mat if tri_mat is not None else np.zeros(f.shape[0]), np.uint32)
+        ts = _np(tri_shape if tri_shape is not None else np.zeros(f.shape[0]), np.int32)
+        sp = _np([[*c, r] for c, r, _ in spheres], np.float32).reshape(-1, 4)
+        spm = _np([m for _, _, m in spheres], np.uint32)
+        pl = _np([p for p, _ in planes], np.float32).reshape(-1, 12)
+        plm = _np([m for _, m in planes], np.uint32)
+        out = np.zeros((width * height, 3), np.float32)
+        c2w, r2c, st = np.zeros(16, np.float32), np.zeros(16, np.float32), np.zeros(4, np.float64)
+        with _quiet_stdout():  # the integrator printf()s progress lines
+            rc = self.L.refi_render(str(obejota_path).encode(), v.shape[0], v.ctypes.data, f.shape[0], f.ctypes.data,
+                                    tm.ctypes.data, ts.ctypes.data, sp.shape[0], sp.ctypes.data, spm.ctypes.data,
+                                    pl.shape[0], pl.ctypes.data, plm.ctypes.data, mats.shape[0], mats.ctypes.data,
+                                    out.ctypes.data, c2w.ctypes.data, r2c.ctypes.data, st.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("reference render failed: " + self.L.refi_error().decode())
+        stats = dict(render_s=float(st[0]), extension_rays=int(st[1]), shadow_rays=int(st[2]), build_s=float(st[3]))
+        return out, c2w.reshape(4, 4), r2c.reshape(4, 4), stats
+
+    def material_sample(self, entry, wo, seeds):
+        """Material::sampleDirection of the reference's class: (wi (n, 3), value (n, 3), the
+        first 1D sample each case drew (n,))."""
+        a = _np(wo, np.float32).reshape(-1, 3)
+        sd = _np(seeds, np.uint32)
+        n = a.shape[0]
+        wi, val, u = np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros(n, np.float32)
+        e = _np(entry, np.float32)
+        if self.L.refi_material_sample(e.ctypes.data, a.ctypes.data, sd.ctypes.data, n, wi.ctypes.data,
+                                       val.ctypes.data, u.ctypes.data) != 0:
+            raise RuntimeError(self.L.refi_error().decode())
+        return wi, val, u
