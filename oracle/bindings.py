@@ -667,6 +667,9 @@ class RefIntegrator:
         L.refi_render.restype = I
         L.refi_material_sample.argtypes = [P, P, P, U32, P, P, P]
         L.refi_material_sample.restype = I
+        L.refi_photons.argtypes = [ctypes.c_char_p, U32, P, U32, P, P, P, U32, P, P, U32, P, P, U32, P, U32, P, P, P,
+                                   U64, P]
+        L.refi_photons.restype = I
         self.L = L
         self.host = bool(L.refi_host_backend())
 
@@ -712,6 +715,43 @@ class RefIntegrator:
             raise RuntimeError("reference render failed: " + self.L.refi_error().decode())
         stats = dict(render_s=float(st[0]), extension_rays=int(st[1]), shadow_rays=int(st[2]), build_s=float(st[3]))
         return out, c2w.reshape(4, 4), r2c.reshape(4, 4), stats
+
+    @staticmethod
+    def _scene_args(materials, verts, idx, tri_mat, tri_shape, spheres, planes):
+        mats = _np(np.stack(list(materials)), np.float32).reshape(-1, 12)
+        if verts is None or idx is None or len(idx) == 0:
+            v, f = np.zeros((1, 3), np.float32), np.zeros((0, 3), np.uint32)
+        else:
+            v, f = _np(verts, np.float32).reshape(-1, 3), _np(idx, np.uint32).reshape(-1, 3)
+        tm = _np(tri_mat if tri_mat is not None else np.zeros(f.shape[0]), np.uint32)
+        ts = _np(tri_shape if tri_shape is not None else np.zeros(f.shape[0]), np.int32)
+        sp = _np([[*c, r] for c, r, _ in spheres], np.float32).reshape(-1, 4)
+        spm = _np([m for _, _, m in spheres], np.uint32)
+        pl = _np([p for p, _ in planes], np.float32).reshape(-1, 12)
+        plm = _np([m for _, m in planes], np.uint32)
+        keep = (mats, v, f, tm, ts, sp, spm, pl, plm)
+        args = [v.shape[0], v.ctypes.data, f.shape[0], f.ctypes.data, tm.ctypes.data, ts.ctypes.data, sp.shape[0],
+                sp.ctypes.data, spm.ctypes.data, pl.shape[0], pl.ctypes.data, plm.ctypes.data, mats.shape[0],
+                mats.ctypes.data]
+        return keep, args
+
+    def photons(self, obejota_path, nphotons, materials, verts=None, idx=None, tri_mat=None, tri_shape=None,
+                spheres=(), planes=(), cap=None):
+        """The reference's photon pass (generatePhotons) with nphotons emitted: the stored photons
+        as (positions (n, 3), power (n, 3), shape ids (n,))."""
+        keep, args = self._scene_args(materials, verts, idx, tri_mat, tri_shape, spheres, planes)
+        cap = cap or 8 * nphotons
+        pos, power = np.zeros((cap, 3), np.float32), np.zeros((cap, 3), np.float32)
+        shape = np.zeros(cap, np.int32)
+        count = ctypes.c_uint64()
+        with _quiet_stdout():
+            rc = self.L.refi_photons(str(obejota_path).encode(), *args, nphotons, pos.ctypes.data, power.ctypes.data,
+                                     shape.ctypes.data, cap, ctypes.byref(count))
+        del keep
+        if rc != 0:
+            raise RuntimeError("reference photon pass failed: " + self.L.refi_error().decode())
+        n = min(count.value, cap)
+        return pos[:n], power[:n], shape[:n]
 
     def material_sample(self, entry, wo, seeds):
         """Material::sampleDirection of the reference's class: (wi (n, 3), value (n, 3), the

@@ -81,6 +81,7 @@ namespace refi {
 // Render configuration read by the reference's compile-time macros below.
 struct Config {
     int w = 64, h = 64, spp = 4, depth = 8;
+    unsigned photons = 100000;  // N_PHOTON_SAMPLES of a photon pass
 };
 Config g_cfg;
 std::atomic<unsigned long long> g_ext_rays{0}, g_shadow_rays{0};
@@ -109,7 +110,9 @@ int count_shadow(const V &rays, const Rest &...)
 #undef MAX_RAY_RECURSION_DEPTH
 #undef CHECK_SUBSURFACE_SCATTERING
 #undef RENDER_MODE
+#undef N_PHOTON_SAMPLES
 #ifdef __CUDA_ARCH__
+#define N_PHOTON_SAMPLES 1
 // device pass: the reference's __device__ code that names these is never launched here
 #define resolutionX 640
 #define resolutionY 360
@@ -120,6 +123,7 @@ int count_shadow(const V &rays, const Rest &...)
 #define resolutionY (refi::g_cfg.h)
 #define SAMPLES_PER_PIXEL (refi::g_cfg.spp)
 #define MAX_RAY_RECURSION_DEPTH (refi::g_cfg.depth)
+#define N_PHOTON_SAMPLES (refi::g_cfg.photons)
 #endif
 #define CHECK_SUBSURFACE_SCATTERING false
 #define RENDER_MODE PATH_TRACING
@@ -164,6 +168,9 @@ struct FilmPeek : public Film {
 };
 struct CameraPeek : public ProjectiveCamera {
     using ProjectiveCamera::rasterToCamera;
+};
+struct ScenePeek : public Scene {
+    using Scene::photons;
 };
 thread_local std::string g_error;
 
@@ -223,6 +230,71 @@ REFI_API int refi_config(int w, int h, int spp, int depth)
 // out_c2w / out_r2c (nullable): the camera's cameraToWorld and rasterToCamera (row-major).
 // out_stats (nullable): [0] seconds in PathTracerIntegrator::render, [1] extension rays,
 //   [2] shadow rays, [3] seconds in Scene::build (the reference's BVH build).
+namespace {
+// The reference's scene objects for one call; owns what the reference leaves to its caller.
+struct SceneInput {
+    std::vector<std::unique_ptr<Material>> mats;
+    std::vector<std::unique_ptr<Shape>> owned;
+    std::vector<Shape *> shapes;
+    std::vector<Light *> lights;
+    Camera *camera = nullptr;
+    std::shared_ptr<std::vector<TriangleMesh>> meshes = std::make_shared<std::vector<TriangleMesh>>();
+    std::vector<std::vector<Triangle>> triangles;
+    ~SceneInput()
+    {
+        for (Light *l : lights) delete l;
+    }
+};
+
+// Fills `in` from the arrays refi_render documents; 0 or 1 with g_error set.
+int make_scene_input(SceneInput &in, const char *obejota, uint32_t nv, const float *xyz, uint32_t ntri,
+                     const uint32_t *idx, const uint32_t *tri_mat, const int32_t *tri_shape, uint32_t nspheres,
+                     const float *spheres, const uint32_t *sphere_mat, uint32_t nplanes, const float *planes,
+                     const uint32_t *plane_mat, uint32_t nmat, const float *materials)
+{
+    for (uint32_t i = 0; i < nmat; i++) {
+        in.mats.emplace_back(make_material(materials + 12 * i));
+        if (!in.mats.back()) return g_error = "unknown material kind", 1;
+    }
+    for (uint32_t i = 0; i < nspheres; i++) {
+        const float *sp = spheres + 4 * i;
+        if (sphere_mat[i] >= nmat) return g_error = "sphere material", 1;
+        Sphere *sh = new Sphere(Point3f(sp[0], sp[1], sp[2]), sp[3]);
+        sh->setMaterial(in.mats[sphere_mat[i]].get());
+        in.owned.emplace_back(sh);
+        in.shapes.push_back(sh);
+    }
+    for (uint32_t i = 0; i < nplanes; i++) {
+        const float *p = planes + 12 * i;
+        if (plane_mat[i] >= nmat) return g_error = "plane material", 1;
+        Plane *pl = new Plane(Point3f(p[0], p[1], p[2]), Vector3f(p[3], p[4], p[5]), Vector3f(p[6], p[7], p[8]),
+                              Vector3f(p[9], p[10], p[11]));
+        pl->setMaterial(in.mats[plane_mat[i]].get());
+        in.owned.emplace_back(pl);
+        in.shapes.push_back(pl);
+    }
+    loadObejota(obejota, in.lights, in.shapes, in.camera);
+    if (ntri > 0) {
+        TriangleMesh mesh;
+        thrust::host_vector<Point3f> hv(nv);
+        for (uint32_t i = 0; i < nv; i++) hv[i] = Point3f(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        mesh.vertices = hv;
+        std::vector<Triangle> tris(ntri);
+        for (uint32_t t = 0; t < ntri; t++) {
+            if (tri_mat[t] >= nmat) return g_error = "triangle material", 1;
+            Triangle face;
+            face.meshId = tri_shape ? tri_shape[t] : 0;
+            for (int k = 0; k < 3; k++) face.vertexIndices[k] = idx[3 * t + k];
+            face.setMaterial(in.mats[tri_mat[t]].get());
+            tris[t] = face;
+        }
+        in.meshes->push_back(mesh);
+        in.triangles.push_back(tris);
+    }
+    return 0;
+}
+}  // namespace
+
 REFI_API int refi_render(const char *obejota, uint32_t nv, const float *xyz, uint32_t ntri, const uint32_t *idx,
                          const uint32_t *tri_mat, const int32_t *tri_shape, uint32_t nspheres, const float *spheres,
                          const uint32_t *sphere_mat, uint32_t nplanes, const float *planes, const uint32_t *plane_mat,
@@ -230,61 +302,17 @@ REFI_API int refi_render(const char *obejota, uint32_t nv, const float *xyz, uin
                          double *out_stats)
 {
     try {
-        std::vector<std::unique_ptr<Material>> mats;
-        for (uint32_t i = 0; i < nmat; i++) {
-            mats.emplace_back(make_material(materials + 12 * i));
-            if (!mats.back()) {
-                g_error = "unknown material kind";
-                return 1;
-            }
-        }
-        std::vector<std::unique_ptr<Shape>> owned;
-        std::vector<Shape *> shapes;
-        for (uint32_t i = 0; i < nspheres; i++) {
-            const float *s = spheres + 4 * i;
-            if (sphere_mat[i] >= nmat) return g_error = "sphere material", 1;
-            Sphere *sp = new Sphere(Point3f(s[0], s[1], s[2]), s[3]);
-            sp->setMaterial(mats[sphere_mat[i]].get());
-            owned.emplace_back(sp);
-            shapes.push_back(sp);
-        }
-        for (uint32_t i = 0; i < nplanes; i++) {
-            const float *p = planes + 12 * i;
-            if (plane_mat[i] >= nmat) return g_error = "plane material", 1;
-            Plane *pl = new Plane(Point3f(p[0], p[1], p[2]), Vector3f(p[3], p[4], p[5]), Vector3f(p[6], p[7], p[8]),
-                                  Vector3f(p[9], p[10], p[11]));
-            pl->setMaterial(mats[plane_mat[i]].get());
-            owned.emplace_back(pl);
-            shapes.push_back(pl);
-        }
-        std::vector<Light *> lights;
-        Camera *camera = nullptr;
-        loadObejota(obejota, lights, shapes, camera);
+        SceneInput in;
+        if (make_scene_input(in, obejota, nv, xyz, ntri, idx, tri_mat, tri_shape, nspheres, spheres, sphere_mat,
+                             nplanes, planes, plane_mat, nmat, materials))
+            return 1;
+        Camera *camera = in.camera;
         if (!camera) return g_error = "no camera in the scene file", 1;
-        std::shared_ptr<std::vector<TriangleMesh>> meshes = std::make_shared<std::vector<TriangleMesh>>();
-        std::vector<std::vector<Triangle>> triangles;
-        if (ntri > 0) {
-            TriangleMesh mesh;
-            thrust::host_vector<Point3f> hv(nv);
-            for (uint32_t i = 0; i < nv; i++) hv[i] = Point3f(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
-            mesh.vertices = hv;
-            std::vector<Triangle> tris(ntri);
-            for (uint32_t t = 0; t < ntri; t++) {
-                if (tri_mat[t] >= nmat) return g_error = "triangle material", 1;
-                Triangle face;
-                face.meshId = tri_shape ? tri_shape[t] : 0;
-                for (int k = 0; k < 3; k++) face.vertexIndices[k] = idx[3 * t + k];
-                face.setMaterial(mats[tri_mat[t]].get());
-                tris[t] = face;
-            }
-            meshes->push_back(mesh);
-            triangles.push_back(tris);
-        }
         refi::g_ext_rays = 0;
         refi::g_shadow_rays = 0;
         auto t0 = std::chrono::steady_clock::now();
         Scene scene;
-        scene.build(shapes, lights, triangles, meshes);
+        scene.build(in.shapes, in.lights, in.triangles, in.meshes);
         auto t1 = std::chrono::steady_clock::now();
         PathTracerIntegrator integrator(camera);
         std::streambuf *old = std::cout.rdbuf(nullptr);  // the integrator prints progress lines
@@ -312,7 +340,45 @@ REFI_API int refi_render(const char *obejota, uint32_t nv, const float *xyz, uin
             out_stats[2] = (double)refi::g_shadow_rays.load();
             out_stats[3] = std::chrono::duration<double>(t1 - t0).count();
         }
-        for (Light *l : lights) delete l;
+        return 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+// The reference's photon pass, generatePhotons (photonDispersion.cu:175-192: Scene::generatePhotons,
+// Scene.cu:989-1018, then computePhotons), with `nphotons` emitted photons on the scene
+// refi_render takes (the scene file supplies the point lights; a camera in it is optional).
+// Out: the stored photons, up to cap: location (3 floats), radiance (3 floats, the reference's
+// double spectrum rounded to float) and shape id per photon, and their number (*count, which may
+// exceed cap).
+REFI_API int refi_photons(const char *obejota, uint32_t nv, const float *xyz, uint32_t ntri, const uint32_t *idx,
+                          const uint32_t *tri_mat, const int32_t *tri_shape, uint32_t nspheres, const float *spheres,
+                          const uint32_t *sphere_mat, uint32_t nplanes, const float *planes, const uint32_t *plane_mat,
+                          uint32_t nmat, const float *materials, uint32_t nphotons, float *out_pos, float *out_power,
+                          int32_t *out_shape, uint64_t cap, uint64_t *count)
+{
+    try {
+        SceneInput in;
+        if (make_scene_input(in, obejota, nv, xyz, ntri, idx, tri_mat, tri_shape, nspheres, spheres, sphere_mat,
+                             nplanes, planes, plane_mat, nmat, materials))
+            return 1;
+        refi::g_cfg.photons = nphotons;
+        ScenePeek scene;
+        scene.build(in.shapes, in.lights, in.triangles, in.meshes);
+        Sampler sampler;
+        generatePhotons(&scene, &sampler);
+        const auto &ph = scene.photons;
+        *count = ph.size();
+        for (uint64_t i = 0; i < ph.size() && i < cap; i++) {
+            const Photon &p = ph[i];
+            out_pos[3 * i] = p.location.x, out_pos[3 * i + 1] = p.location.y, out_pos[3 * i + 2] = p.location.z;
+            out_power[3 * i] = (float)p.radiance.getR();
+            out_power[3 * i + 1] = (float)p.radiance.getG();
+            out_power[3 * i + 2] = (float)p.radiance.getB();
+            out_shape[i] = p.shapeId;
+        }
         return 0;
     } catch (const std::exception &e) {
         g_error = e.what();
