@@ -153,6 +153,7 @@ SIGNATURES = {
     "rt_texture_lookup": [_P, _U32, _P, _U64, _P],
     "rt_scene_add_point_light": [_P, _P, _P, _F32],
     "rt_render": [_P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), _P, _P, _P, ctypes.POINTER(RenderStats)],
+    "rt_render_set_sort": [_P, _U32],
     "rt_render_batch": [_P, ctypes.POINTER(View), _U32, _U32, _U32, _P, _P, _P, ctypes.POINTER(RenderStats)],
     "rt_film_store_hdrbmp": [ctypes.c_char_p, _U32, _U32, _P, _P, _P, _U64],
     "rt_film_load_hdrbmp": [ctypes.c_char_p, _U32, _U32, _P, ctypes.POINTER(_U64)],

@@ -171,6 +171,10 @@ class Scene:
         c = np.ascontiguousarray(rgb, dtype=np.float32)
         N.check(N.lib().rt_scene_add_point_light(self.handle, p.ctypes.data, c.ctypes.data, float(intensity)))
 
+    def set_sort(self, chunk_log2: int):
+        """Material sort of the wavefront's shading order in chunks of 2^chunk_log2 slots (0: off)."""
+        N.check(N.lib().rt_render_set_sort(self.handle, int(chunk_log2)))
+
     def render(self, camera: "N.Camera", spp: int, max_depth: int, rr_depth: int = 3, seed: int = 0,
                flags: int = 0, sample_offset: int = 0, film=None, fp64: bool = False, max_paths: int = 0):
         """Adds spp samples per pixel into `film` (dict of torch tensors sum/count[/sum64]);

@@ -56,6 +56,7 @@ struct Buffers {
     float4 *scontrib;  // rgb, target index bits (kRetireTarget: retire list)
     float4 *retire;    // L.xyz, pixel index bits
     float4 *gather;    // photon-map gather requests, 4 float4 each: p+shape, n+material, wo+target, beta
+    const uint32_t *perm;  // shading order of the wave's queue slots (material sort), or null
     uint32_t cap, scap, gcap;
     // counters (uint32): [0],[1] queue sizes of buffers 0/1, [2] shadow count, [3] retire count,
     // [4] status, [5] shadow-kernel work counter, [6] gather requests, [7] gather-kernel work
@@ -206,6 +207,55 @@ struct PhotonView {
     float radius;
 };
 
+// Material sort: the shading order of a wave. Each block takes one chunk of 2^log2 queue slots
+// and orders it by the kind of surface its ray hit (a miss first, then rt_material_type), by
+// a counting sort in shared memory; k_shade's thread i then shades slot perm[i]. Lanes of a warp
+// then mostly run the same BSDF code, while the chunk keeps the state reads of a warp within a
+// few kilobytes. The chunk size is the sort granularity (rt_render_set_sort).
+constexpr int kSortBlock = 256;
+constexpr int kSortKeys = 16;  // 0: miss, 1 + rt_material_type
+constexpr uint32_t kSortMaxLog2 = 13;
+__device__ __forceinline__ uint32_t shade_key(const RenderView &rv, const Buffers &bf, uint32_t q)
+{
+    const int32_t prim = __float_as_int(__ldg(reinterpret_cast<const float *>(bf.hits) + 4 * (uint64_t)q + 1));
+    if (prim < 0) return 0;
+    uint32_t mat;
+    if (prim & RT_PRIM_SHAPE)
+        mat = rv.sv.spheres[prim & ~RT_PRIM_SHAPE].material;
+    else
+        mat = __ldg(rv.tri_mat + prim);
+    const uint32_t type = (uint32_t)rv.mats[min(mat, rv.nmats - 1)].type;
+    return min(1u + type, (uint32_t)kSortKeys - 1u);
+}
+
+__global__ void __launch_bounds__(kSortBlock) k_material_sort(RenderView rv, Buffers bf, int cur, uint32_t *perm,
+                                                               uint32_t log2)
+{
+    __shared__ uint32_t count[kSortKeys], start[kSortKeys];
+    __shared__ uint8_t key[1u << kSortMaxLog2];
+    const uint32_t n = min(bf.cnt[cur], bf.cap);
+    const uint32_t c0 = blockIdx.x << log2;
+    if (c0 >= n) return;
+    const uint32_t len = min(1u << log2, n - c0);
+    if (threadIdx.x < kSortKeys) count[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < len; j += kSortBlock) {
+        const uint32_t k = shade_key(rv, bf, c0 + j);
+        key[j] = (uint8_t)k;
+        atomicAdd(&count[k], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int k = 0; k < kSortKeys; k++) {
+            start[k] = acc;
+            acc += count[k];
+        }
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < len; j += kSortBlock) perm[c0 + atomicAdd(&start[key[j]], 1u)] = c0 + j;
+}
+
 // Resident blocks per SM k_shade is compiled for: more resident warps hide its scattered
 // loads better than the spills they cost. BVH-stress render, Mrays/s: 1465 / 1494 / 1507 for
 // 4 (127 registers, no bound) / 5 (96) / 6 (80) with the binned-SAH tree; 1559 / 1583 / 1588
@@ -215,10 +265,11 @@ struct PhotonView {
 #endif
 __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView rv, Buffers bf, int cur, GuideView gv)
 {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = min(bf.cnt[cur], bf.cap);
-    if (q == 0) atomicAdd(cnt64(bf.cnt, 10), (unsigned long long)n);  // extension rays of this wave
-    if (q >= n) return;
+    if (i == 0) atomicAdd(cnt64(bf.cnt, 10), (unsigned long long)n);  // extension rays of this wave
+    if (i >= n) return;
+    const uint32_t q = bf.perm ? __ldg(bf.perm + i) : i;  // the queue slot this thread shades
     const int nxt = cur ^ 1;
     const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
     const bool nee_area = (rv.flags & RT_RENDER_NEE_AREA) != 0 && rv.nemit > 0;
@@ -784,7 +835,7 @@ namespace rtb {
 void RenderScratch::release()
 {
     for (DevBuf *b : {&rays[0], &rays[1], &st0[0], &st0[1], &st1[0], &st1[1], &st2[0], &st2[1], &hits, &srays,
-                      &scontrib, &retire, &cnt, &gather, &views, &view_sample0, &view_pixel0})
+                      &scontrib, &retire, &cnt, &gather, &views, &view_sample0, &view_pixel0, &perm})
         b->release();
     if (host_cnt) cudaFreeHost(host_cnt);
     host_cnt = nullptr;
@@ -1023,6 +1074,11 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     bf.cap = cap;
     bf.scap = scap;
     bf.gcap = gcap;
+    // material sort of the shading order, chunks of 2^sort_log2 queue slots (0: off)
+    const uint32_t sort_log2 = s->sort_log2 ? std::min<uint32_t>(std::max<uint32_t>(s->sort_log2, 5u), kSortMaxLog2) : 0u;
+    const unsigned sort_blocks = sort_log2 ? (unsigned)((cap + (1u << sort_log2) - 1) >> sort_log2) : 0u;
+    if (sort_log2) RTB_CHECK(rs.perm.reserve(4ull * cap));
+    bf.perm = sort_log2 ? rs.perm.as<uint32_t>() : nullptr;
     bf.cnt = rs.cnt.as<uint32_t>();
 
     RenderView rv{};
@@ -1084,6 +1140,10 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
             }
             RTB_CUDA(cudaMemsetAsync(bf.cnt + ((cur ^ 1)), 0, 4, st));
             RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 24, st));
+            if (sort_log2) {
+                k_material_sort<<<sort_blocks, kSortBlock, 0, st>>>(rv, bf, cur, rs.perm.as<uint32_t>(), sort_log2);
+                RTB_CUDA(cudaGetLastError());
+            }
             k_shade<<<blocks, kB, 0, st>>>(rv, bf, cur, gv);
             RTB_CUDA(cudaGetLastError());
             k_shadow<<<shadow_blocks, kB, 0, st>>>(rv, bf, cur ^ 1, gv);
@@ -1196,4 +1256,13 @@ extern "C" int rt_render_batch(rt_scene *s, const rt_view *views, uint32_t nview
                                float *sum_rgb, uint32_t *count, double *sum64, rt_render_stats *stats)
 {
     return render_views(s, views, nviews, flags, max_paths, sum_rgb, count, sum64, stats, "rt_render_batch");
+}
+
+extern "C" int rt_render_set_sort(rt_scene *s, uint32_t chunk_log2)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_render_set_sort: null scene");
+    if (chunk_log2 != 0 && (chunk_log2 < 5 || chunk_log2 > kSortMaxLog2))
+        return fail(RT_ERR_INVALID, "rt_render_set_sort: chunk_log2 must be 0 (off) or 5..13");
+    s->sort_log2 = chunk_log2;
+    return RT_OK;
 }

@@ -192,6 +192,7 @@ int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, void *o
 struct RenderScratch {
     DevBuf rays[2], st0[2], st1[2], st2[2], hits, srays, scontrib, retire, cnt, gather;
     DevBuf views, view_sample0, view_pixel0;  // the render's views and their prefix sums
+    DevBuf perm;  // shading order of the wave (material sort)
     void *host_cnt = nullptr;  // pinned
     void release();
 };
@@ -293,6 +294,7 @@ struct rt_scene {
     rt_guide *guide = nullptr;      // RT_RENDER_GUIDE proposal
     int guide_train = 0;            // record training samples while rendering
     uint32_t pm_k = 100;
+    uint32_t sort_log2 = 0;  // material sort granularity of rt_render (log2 chunk; 0: off)
     float pm_radius = 100.f;
     rtb::DevBuf d_tri_transp, d_mat_transp;  // per-triangle / per-material transparency (record flags)
     // textures: texels (rgb in xyz), per texture (first texel, width, height, 0); texture

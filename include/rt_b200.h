@@ -351,6 +351,13 @@ typedef struct rt_view {
 RT_API int rt_render_batch(rt_scene *scene, const rt_view *views, uint32_t nviews, uint32_t flags, uint32_t max_paths,
                            float *sum_rgb, uint32_t *count, double *sum64, rt_render_stats *stats);
 
+/* Material sort of the wavefront (new in this build; the reference shades its samples in pixel
+ * order, pathTracing.cu:284-414): before each wave is shaded, every chunk of 2^chunk_log2 queue
+ * slots is ordered by the kind of surface its ray hit (a miss, then rt_material_type), so the
+ * lanes of a warp mostly run the same BSDF code. chunk_log2 is the sort granularity, 5..13;
+ * 0 turns the sort off. Results do not depend on it. Applies to rt_render and rt_render_batch. */
+RT_API int rt_render_set_sort(rt_scene *scene, uint32_t chunk_log2);
+
 /* --------------------------------------------------------------- photons */
 
 typedef struct rt_photon_map rt_photon_map;

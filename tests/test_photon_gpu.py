@@ -191,3 +191,48 @@ def test_photon_mapping_render_agrees_with_path_tracing(core, gpu_ctx):
     cf, _ = sc.render(cam, spp=16, max_depth=8, flags=N.RT_RENDER_PHOTON_MAP | N.RT_RENDER_COMPAT, fp64=True)
     ratio = core.film_mean(cf).mean() / pmimg.mean()
     assert 0.4 < ratio < 0.95
+
+
+def test_config4_knn_set_against_reference_kdtree(core, gpu_ctx, refo):
+    """The 4K photon-mapping configuration's gather: the photon map of 10M emitted photons over
+    the 2M-triangle terrain, the subsurface slab and 16 glass spheres, and 2^20 query points on
+    its surfaces with their shape ids (the stored photons of an independent trace), k = 50 nearest
+    on the same shape within the reference's default radius (100, types.h:58). Every neighbour
+    count equals the reference kd-tree's (nn::KDTree, kdtree.h:111-152); every neighbour set equals
+    it except for members tied at the k-th distance, which the reference's heap order decides.
+    The number of such tie-broken sets is reported."""
+    import torch
+    from oracle import bindings
+
+    cfgs = importlib.import_module("2023_render_engine_b200.configs")
+    sc, _, _ = cfgs.build_config4(gpu_ctx, 64, 36)
+    pm, st = sc.trace_photons(10_000_000, max_depth=16, seed=12)
+    pm.build()
+    ph = pm.photons()
+    qm, _ = sc.trace_photons(1_000_000, max_depth=16, seed=99)
+    qp = qm.photons()
+    nq = 1 << 20
+    assert len(qp) >= nq
+    q, qs = np.ascontiguousarray(qp["pos"][:nq]), np.ascontiguousarray(qp["shape_id"][:nq])
+    k, radius = 50, 100.0
+    gi, gd, gc = pm.knn(torch.from_numpy(q.reshape(-1)).cuda(), k, radius, torch.from_numpy(qs).cuda())
+    gi, gd, gc = gi.cpu().numpy(), gd.cpu().numpy(), gc.cpu().numpy()
+    pos, shp = np.ascontiguousarray(ph["pos"]), np.ascontiguousarray(ph["shape_id"])
+    kd = bindings.RefKdTree(refo, pos, shp)
+    import os
+
+    ri, rc = kd.knn(q, k, radius, qs, threads=os.cpu_count() or 8)
+    assert np.array_equal(gc, rc.astype(np.int32))
+    assert (gc == k).mean() > 0.99
+    col = np.arange(k)[None, :]
+    gs = np.sort(np.where(col < gc[:, None], gi, -1), axis=1)
+    rs = np.sort(np.where(col < rc[:, None].astype(np.int64), ri, -1), axis=1)
+    differ = np.flatnonzero(np.any(gs != rs, axis=1))
+    for i in differ:
+        a, b = set(gi[i, :gc[i]].tolist()), set(ri[i, :rc[i]].tolist())
+        kth = gd[i, gc[i] - 1]
+        dd = np.sqrt(((pos[list(a ^ b)].astype(np.float64) - q[i]) ** 2).sum(1))
+        assert np.allclose(dd, kth, rtol=1e-6, atol=0), (i, dd, kth)
+    print(f"config-4 k-NN: {len(ph)} photons, {nq} queries, {len(differ)} sets differ only by members tied "
+          f"at the k-th distance ({len(differ) / nq:.2e})")
+    assert len(differ) < 1e-3 * nq

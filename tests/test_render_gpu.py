@@ -121,3 +121,23 @@ def test_cornell_matches_cpu_restatement(core, gpu_ctx, restated, flags):
     assert np.median(rel) < 1e-4
     assert (rel < 1e-3).mean() > 0.8
     assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 0.02
+
+
+@pytest.mark.parametrize("log2", [5, 9, 13])
+def test_material_sort_leaves_the_image_unchanged(core, gpu_ctx, log2):
+    """The material sort only reorders which thread shades which path: every path keeps its own
+    random stream, so the image equals the unsorted one up to the order of film additions."""
+    cfgs = importlib.import_module("2023_render_engine_b200.configs")
+    sc, cam, p = cfgs.build_config0(gpu_ctx, 64, 64)
+    sc.add_point_light((0.0, 0.5, 0.0), (1.0, 1.0, 1.0), 2.0)
+    sc.commit()
+    flags = N.RT_RENDER_NEE_AREA
+    ref, st0 = sc.render(cam, spp=8, max_depth=8, seed=3, flags=flags, fp64=True, max_paths=1 << 14)
+    sc.set_sort(log2)
+    got, st1 = sc.render(cam, spp=8, max_depth=8, seed=3, flags=flags, fp64=True, max_paths=1 << 14)
+    sc.set_sort(0)
+    a, b = core.film_mean(ref), core.film_mean(got)
+    assert st0["extension_rays"] == st1["extension_rays"] and st0["shadow_rays"] == st1["shadow_rays"]
+    assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+    with pytest.raises(N.RtError):
+        sc.set_sort(20)
