@@ -1,9 +1,11 @@
-"""Batched multi-view rendering: capacity autotuning and the batched-vs-individual measurement.
+"""Batched multi-view rendering: autotuning and the batched-vs-individual measurement.
 
-One rt_render_batch call renders all views of a scene in one wavefront. The queue capacity
-(paths in flight) is the tunable: larger queues keep more rays per traversal launch, smaller
-ones use less memory and finish the tail sooner. autotune_capacity times a reduced-spp copy
-of the batch at each candidate and keeps the fastest.
+One rt_render_batch call renders all views of a scene in one wavefront. Two knobs are tuned:
+the queue capacity (paths in flight: larger queues keep more rays per traversal launch,
+smaller ones use less memory and finish the tail sooner) and the material-sort granularity
+(chunk of queue slots ordered by hit material before shading: larger chunks group more lanes
+by material, smaller ones keep a warp's state reads closer together). autotune times a
+reduced-spp copy of the batch at each candidate and keeps the fastest.
 """
 from __future__ import annotations
 
@@ -12,6 +14,7 @@ import time
 from . import _native as N
 
 CAPACITIES = (1 << 23, 1 << 22, 1 << 21, 1 << 20)
+SORT_LOG2 = (0, 8, 10, 12)
 
 
 def _timed(fn, sync):
@@ -36,6 +39,21 @@ def autotune_capacity(scene, views, flags, sync, candidates=CAPACITIES, probe_sp
     return best, trials
 
 
+def autotune_sort(scene, views, flags, capacity, sync, candidates=SORT_LOG2, probe_spp=4):
+    """Fastest material-sort granularity (log2 chunk, 0: off) for this batch at `capacity`,
+    timed like autotune_capacity; leaves the scene set to it. Returns (best, [(log2, seconds)])."""
+    probe = [dict(v, spp=min(v["spp"], probe_spp)) for v in views]
+    trials = []
+    for lg in candidates:
+        scene.set_sort(lg)
+        for rep in range(2):
+            t, _ = _timed(lambda: scene.render_batch(probe, flags=flags, max_paths=capacity), sync)
+        trials.append((lg, t))
+    best = min(trials, key=lambda x: x[1])[0]
+    scene.set_sort(best)
+    return best, trials
+
+
 def measure(groups, sync, autotune=True):
     """Times every scene's views as one batch and as one rt_render call per view.
 
@@ -46,6 +64,7 @@ def measure(groups, sync, autotune=True):
         if not views:
             continue
         cap, trials = autotune_capacity(scene, views, flags, sync) if autotune else (0, [])
+        sort_log2, sort_trials = autotune_sort(scene, views, flags, cap, sync) if autotune else (10, [])
         scene.render_batch(views[:1], flags=flags, max_paths=cap)  # warm
         t_b, (film, st, off) = _timed(lambda: scene.render_batch(views, flags=flags, max_paths=cap), sync)
         rays = st["extension_rays"] + st["shadow_rays"]
@@ -58,8 +77,9 @@ def measure(groups, sync, autotune=True):
 
         t_i, _ = _timed(individual, sync)
         samples = sum(v["camera"].width * v["camera"].height * v["spp"] for v in views)
-        res["groups"].append({"scene": name, "views": len(views), "capacity": cap,
-                              "autotune": [(c, round(t, 4)) for c, t in trials], "batched_s": t_b,
+        res["groups"].append({"scene": name, "views": len(views), "capacity": cap, "sort_log2": sort_log2,
+                              "autotune": [(c, round(t, 4)) for c, t in trials],
+                              "autotune_sort": [(c, round(t, 4)) for c, t in sort_trials], "batched_s": t_b,
                               "individual_s": t_i, "rays": rays, "samples": samples})
         res["batched_s"] += t_b
         res["individual_s"] += t_i

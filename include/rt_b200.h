@@ -355,7 +355,8 @@ RT_API int rt_render_batch(rt_scene *scene, const rt_view *views, uint32_t nview
  * order, pathTracing.cu:284-414): before each wave is shaded, every chunk of 2^chunk_log2 queue
  * slots is ordered by the kind of surface its ray hit (a miss, then rt_material_type), so the
  * lanes of a warp mostly run the same BSDF code. chunk_log2 is the sort granularity, 5..13;
- * 0 turns the sort off. Results do not depend on it. Applies to rt_render and rt_render_batch. */
+ * 0 turns the sort off; a new scene uses 10. Results do not depend on it. Applies to rt_render
+ * and rt_render_batch. */
 RT_API int rt_render_set_sort(rt_scene *scene, uint32_t chunk_log2);
 
 /* --------------------------------------------------------------- photons */
