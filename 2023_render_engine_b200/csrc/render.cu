@@ -61,7 +61,8 @@ struct Buffers {
     // counters (uint32): [0],[1] queue sizes of buffers 0/1, [2] shadow count, [3] retire count,
     // [4] status, [5] shadow-kernel work counter, [6] gather requests, [7] gather-kernel work
     // counter; u64 at [8]: next sample,
-    // [10] extension rays, [12] shadow rays, [14] gathers
+    // [10] extension rays, [12] shadow rays, [14] gathers; [16] guide wait timed out, [18] waves
+    // of the device-side loop, [19] wave cap reached
     uint32_t *cnt;
 };
 
@@ -254,6 +255,22 @@ __global__ void __launch_bounds__(kSortBlock) k_material_sort(RenderView rv, Buf
     }
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < len; j += kSortBlock) perm[c0 + atomicAdd(&start[key[j]], 1u)] = c0 + j;
+}
+
+// End of one 4-wave group of the device-side wave loop: counts the waves and sets the loop's
+// condition to 0 once every queue has drained and every camera sample has started (what the
+// host loop checks after each group), when the guide's tensor-core wait timed out, or at the
+// wave cap (cnt[19] = 1 then). cnt[18] counts the waves.
+__global__ void k_wave_check(uint32_t *cnt, uint64_t total, uint32_t max_waves, cudaGraphConditionalHandle loop)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t waves = cnt[18] + 4;
+    cnt[18] = waves;
+    const unsigned long long next = *reinterpret_cast<const unsigned long long *>(cnt + 8);
+    const bool done = cnt[0] == 0 && next >= total;
+    const bool capped = !done && waves >= max_waves;
+    if (capped) cnt[19] = 1;
+    cudaGraphSetConditional(loop, (done || capped || cnt[16] != 0) ? 0u : 1u);
 }
 
 // Resident blocks per SM k_shade is compiled for: more resident warps hide its scattered
@@ -1163,7 +1180,65 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
     };
-    for (uint64_t group = 0;; group++) {
+    // Device-side wave loop: one CUDA graph whose conditional WHILE node repeats the 4-wave
+    // group, ended by k_wave_check on the device, so the host waits once per frame instead of
+    // after every group. Where conditional graphs cannot be built (the legacy default stream
+    // cannot be captured) the host loop below runs instead.
+    bool device_loop = false;
+    const uint32_t wave_cap = (uint32_t)std::min<uint64_t>(max_waves, 0x7FFFFFF0u);
+    if (st != nullptr && st != cudaStreamLegacy) {
+        cudaGraph_t g = nullptr;
+        cudaGraphConditionalHandle loop_handle;
+        bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
+                  cudaGraphConditionalHandleCreate(&loop_handle, g, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+        cudaGraph_t body = nullptr;
+        if (ok) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = loop_handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t cn;
+            ok = cudaGraphAddNode(&cn, g, nullptr, 0, &cp) == cudaSuccess;
+            if (ok) body = cp.conditional.phGraph_out[0];
+        }
+        if (ok && cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                      cudaSuccess) {
+            int rc = wave_group();
+            if (rc == RT_OK) {
+                k_wave_check<<<1, 32, 0, st>>>(bf.cnt, total, wave_cap, loop_handle);
+                rc = cuda_status(cudaGetLastError(), "k_wave_check");
+            }
+            cudaGraph_t captured = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(st, &captured);
+            if (rc != RT_OK) {
+                cudaGraphDestroy(g);
+                return rc;
+            }
+            ok = ce == cudaSuccess && cudaGraphInstantiate(&graph, g, 0) == cudaSuccess;
+        } else {
+            ok = false;
+        }
+        if (g) cudaGraphDestroy(g);
+        if (ok) {
+            device_loop = true;
+        } else {
+            release_graph();
+            (void)cudaGetLastError();  // fall back to the host loop
+        }
+    }
+    if (device_loop) {
+        cudaError_t ce = cudaGraphLaunch(graph, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(rs.host_cnt, bf.cnt, 128, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        release_graph();
+        if (ce != cudaSuccess) return cuda_status(ce, "device wave loop");
+        const uint32_t *hc = static_cast<const uint32_t *>(rs.host_cnt);
+        waves = hc[18];
+        if (hc[16]) return fail(RT_ERR_TIMEOUT, name + ": guide tensor-core completion wait timed out");
+        if (hc[19]) return fail(RT_ERR_TIMEOUT, name + ": wave cap exceeded");
+    }
+    for (uint64_t group = 0; !device_loop; group++) {
         int rc = RT_OK;
         // the legacy default stream cannot be captured: there every group is launched directly
         if (group == 1 && st != nullptr && st != cudaStreamLegacy &&

@@ -141,3 +141,24 @@ def test_material_sort_leaves_the_image_unchanged(core, gpu_ctx, log2):
     assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
     with pytest.raises(N.RtError):
         sc.set_sort(20)
+
+
+def test_device_wave_loop_equals_host_loop(core, gpu_ctx):
+    """On a stream of its own a render runs its waves as one CUDA graph with a conditional WHILE
+    node ended on the device; on the legacy default stream (which cannot be captured) the host
+    checks after every 4-wave group. Both render the same samples: equal ray counts and images."""
+    cfgs = importlib.import_module("2023_render_engine_b200.configs")
+    out = []
+    for legacy in (False, True):
+        ctx = core.Context(0)
+        if legacy:
+            ctx.set_stream(0)
+        sc, cam, p = cfgs.build_config0(ctx, 48, 48)
+        film, st = sc.render(cam, spp=8, max_depth=8, seed=11, flags=N.RT_RENDER_NEE_AREA, fp64=True,
+                             max_paths=1 << 12)  # small queues: many wave groups
+        out.append((core.film_mean(film), st))
+        sc.close()
+    (a, sa), (b, sb) = out
+    assert sa["extension_rays"] == sb["extension_rays"] and sa["shadow_rays"] == sb["shadow_rays"]
+    assert sa["waves"] == sb["waves"] and sa["waves"] > 8
+    assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
