@@ -62,7 +62,7 @@ class RenderOpts(ctypes.Structure):
 class View(ctypes.Structure):
     _fields_ = [("camera", Camera), ("spp", ctypes.c_uint32), ("sample_offset", ctypes.c_uint32),
                 ("max_depth", ctypes.c_uint32), ("rr_depth", ctypes.c_uint32), ("seed", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 3)]
+                ("scene", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 2)]
 
 
 class RenderStats(ctypes.Structure):
@@ -154,6 +154,7 @@ SIGNATURES = {
     "rt_scene_add_point_light": [_P, _P, _P, _F32],
     "rt_render": [_P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), _P, _P, _P, ctypes.POINTER(RenderStats)],
     "rt_render_set_sort": [_P, _U32],
+    "rt_scene_merge": [_P, _P, _U32, ctypes.POINTER(_P)],
     "rt_render_batch": [_P, ctypes.POINTER(View), _U32, _U32, _U32, _P, _P, _P, ctypes.POINTER(RenderStats)],
     "rt_film_store_hdrbmp": [ctypes.c_char_p, _U32, _U32, _P, _P, _P, _U64],
     "rt_film_load_hdrbmp": [ctypes.c_char_p, _U32, _U32, _P, ctypes.POINTER(_U64)],

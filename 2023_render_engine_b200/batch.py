@@ -54,11 +54,12 @@ def autotune_sort(scene, views, flags, capacity, sync, candidates=SORT_LOG2, pro
     return best, trials
 
 
-def measure(groups, sync, autotune=True):
-    """Times every scene's views as one batch and as one rt_render call per view.
+def measure(groups, sync, autotune=True, merged=True):
+    """Times every scene's views as one batch and as one rt_render call per view, and (merged)
+    all views of all scenes as one batch of the merged scene.
 
     groups: [(name, scene, flags, views)]. Returns a dict with rays, samples and seconds of
-    both ways and the capacities chosen."""
+    each way and the capacities chosen."""
     res = {"groups": [], "batched_s": 0.0, "individual_s": 0.0, "rays": 0, "samples": 0, "views": 0}
     for name, scene, flags, views in groups:
         if not views:
@@ -90,7 +91,36 @@ def measure(groups, sync, autotune=True):
     res["individual_mrays_s"] = res["rays"] / res["individual_s"] / 1e6
     res["batched_msamples_s"] = res["samples"] / res["batched_s"] / 1e6
     res["speedup"] = res["individual_s"] / res["batched_s"]
+    if len(groups) > 1 and merged:
+        res["merged"] = measure_merged(groups, sync, autotune=autotune)
+        res["merged"]["speedup_vs_individual"] = res["individual_s"] / res["merged"]["seconds"]
     return res
+
+
+def measure_merged(groups, sync, autotune=True):
+    """All views of all groups in ONE rt_render_batch call on the merged scene (rt_scene_merge),
+    its capacity and sort granularity autotuned like a group's."""
+    from . import core
+
+    scenes = [sc for _, sc, _, views in groups if views]
+    flags = [fl for _, _, fl, views in groups if views]
+    if any(f != flags[0] for f in flags):
+        return {"unavailable": "groups render with different flags"}
+    views = [dict(v, scene=k) for k, (_, _, _, vs) in enumerate([g for g in groups if g[3]]) for v in vs]
+    merged = core.merge_scenes(scenes[0].ctx, scenes)
+    try:
+        cap, trials = autotune_capacity(merged, views, flags[0], sync) if autotune else (0, [])
+        sort_log2, sort_trials = autotune_sort(merged, views, flags[0], cap, sync) if autotune else (10, [])
+        merged.render_batch(views[:1], flags=flags[0], max_paths=cap)  # warm
+        t, (film, st, _) = _timed(lambda: merged.render_batch(views, flags=flags[0], max_paths=cap), sync)
+        del film
+        rays = st["extension_rays"] + st["shadow_rays"]
+        return {"views": len(views), "scenes": len(scenes), "capacity": cap, "sort_log2": sort_log2,
+                "autotune": [(c, round(x, 4)) for c, x in trials],
+                "autotune_sort": [(c, round(x, 4)) for c, x in sort_trials],
+                "seconds": t, "rays": rays, "mrays_s": rays / t / 1e6, "waves": st["waves"]}
+    finally:
+        merged.close()
 
 
 def measure_guided(scene, flags, views, guide, sync, capacity=0, train_passes=4, steps_per_pass=64,

@@ -48,11 +48,12 @@ class Context:
 class Scene:
     """Scene container; mirrors Scene::build (integration/Scene.cu:56-95) + intersects."""
 
-    def __init__(self, ctx: Context):
+    def __init__(self, ctx: Context, handle=None):
         self.ctx = ctx
-        h = ctypes.c_void_p()
-        N.check(N.lib().rt_scene_create(ctx.handle, ctypes.byref(h)))
-        self.handle = h
+        if handle is None:
+            handle = ctypes.c_void_p()
+            N.check(N.lib().rt_scene_create(ctx.handle, ctypes.byref(handle)))
+        self.handle = handle
 
     def add_mesh(self, vertices, indices, material: int = 0, shape_id: int = 0, transparent: bool = False,
                  normals=None, normal_indices=None) -> int:
@@ -199,8 +200,9 @@ class Scene:
         """Renders many views of this scene in one wavefront (rt_render_batch).
 
         views: list of dicts with camera and spp, and optionally max_depth (8), rr_depth (3),
-        seed (0), sample_offset (0). The film holds the views' pixels back to back; returns
-        (film, stats, offsets) with view i's pixels at [offsets[i], offsets[i + 1])."""
+        seed (0), sample_offset (0), scene (0: the view's scene in a merged scene). The film holds
+        the views' pixels back to back; returns (film, stats, offsets) with view i's pixels at
+        [offsets[i], offsets[i + 1])."""
         import torch
 
         arr = (N.View * len(views))()
@@ -212,6 +214,7 @@ class Scene:
             arr[i].max_depth = v.get("max_depth", 8)
             arr[i].rr_depth = v.get("rr_depth", 3)
             arr[i].seed = v.get("seed", 0)
+            arr[i].scene = v.get("scene", 0)
             offsets.append(offsets[-1] + v["camera"].width * v["camera"].height)
         npx = offsets[-1]
         if film is None:
@@ -267,6 +270,16 @@ def make_rays(o: np.ndarray, d: np.ndarray, tmax=None) -> np.ndarray:
     r["dx"], r["dy"], r["dz"] = d[:, 0], d[:, 1], d[:, 2]
     r["tmax"] = np.inf if tmax is None else tmax
     return r
+
+
+def merge_scenes(ctx: Context, scenes) -> Scene:
+    """rt_scene_merge: committed scenes of `ctx` as one scene whose render_batch views name their
+    scene by its index in `scenes` (key "scene")."""
+    arr = (ctypes.c_void_p * len(scenes))(*[s.handle.value if hasattr(s.handle, "value") else s.handle
+                                           for s in scenes])
+    h = ctypes.c_void_p()
+    N.check(N.lib().rt_scene_merge(ctx.handle, ctypes.cast(arr, ctypes.c_void_p), len(scenes), ctypes.byref(h)))
+    return Scene(ctx, handle=h)
 
 
 def material(type_, color=(0.8, 0.8, 0.8), intensity=0.0, eta=(1.5, 1.5, 1.5), k=(0.0, 0.0, 0.0),

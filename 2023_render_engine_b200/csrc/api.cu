@@ -121,6 +121,8 @@ rtb::SceneView rt_scene::view() const
     v.ntri = (uint32_t)(tri9.size() / 9);
     v.nspheres = (uint32_t)spheres.size();
     v.nnodes = (uint32_t)nnodes;
+    v.subs = merged ? d_subs.as<SubScene>() : nullptr;
+    v.nsubs = merged ? (uint32_t)subs.size() : 0u;
     return v;
 }
 
@@ -223,6 +225,7 @@ int rt_scene_add_mesh(rt_scene *s, const float *xyz, uint32_t nv, const uint32_t
                       int transparent, uint32_t *first_tri)
 {
     if (!s || (!xyz && nv) || (!idx && ntri)) return fail(RT_ERR_INVALID, "rt_scene_add_mesh: null argument");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_add_mesh: not available on a merged scene");
     if ((normals == nullptr) != (nidx == nullptr)) return fail(RT_ERR_INVALID, "rt_scene_add_mesh: normals need nidx");
     uint64_t base = s->tri9.size() / 9;
     if (base + ntri >= 0x40000000ull) return fail(RT_ERR_CAPACITY, "rt_scene_add_mesh: more than 2^30 triangles");
@@ -254,6 +257,7 @@ int rt_scene_add_sphere(rt_scene *s, const float o2w[16], const float w2o[16], f
                         int32_t shape_id, int transparent, uint32_t *index)
 {
     if (!s || !o2w || !w2o) return fail(RT_ERR_INVALID, "rt_scene_add_sphere: null argument");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_add_sphere: not available on a merged scene");
     if (!(radius > 0)) return fail(RT_ERR_INVALID, "rt_scene_add_sphere: radius must be positive");
     SphereRecord r{};
     std::memcpy(r.w2o, w2o, sizeof(r.w2o));
@@ -271,6 +275,7 @@ int rt_scene_add_sphere(rt_scene *s, const float o2w[16], const float w2o[16], f
 int rt_scene_set_build(rt_scene *s, uint32_t mode)
 {
     if (!s) return fail(RT_ERR_INVALID, "rt_scene_set_build: null scene");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_build: not available on a merged scene");
     if (mode != RT_BUILD_DEVICE && mode != RT_BUILD_HOST) return fail(RT_ERR_INVALID, "rt_scene_set_build: bad mode");
     s->build_mode = mode;
     return RT_OK;
@@ -279,6 +284,7 @@ int rt_scene_set_build(rt_scene *s, uint32_t mode)
 int rt_scene_commit(rt_scene *s)
 {
     if (!s) return fail(RT_ERR_INVALID, "rt_scene_commit: null scene");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_commit: not available on a merged scene");
     RTB_CUDA(cudaSetDevice(s->ctx->device));
     cudaStream_t st = s->ctx->stream;
     auto t0 = std::chrono::steady_clock::now();
@@ -369,6 +375,7 @@ int rt_scene_stats_get(rt_scene *s, rt_scene_stats *out)
 static int trace_common(rt_scene *s, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags)
 {
     if (!s) return fail(RT_ERR_INVALID, "rt_trace_closest: null scene");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_trace_closest: not available on a merged scene");
     if (!s->committed) return fail(RT_ERR_STATE, "rt_trace_closest: scene not committed");
     if (n && (!rays || !hits)) return fail(RT_ERR_INVALID, "rt_trace_closest: null buffer");
     if (n >= 0x80000000ull) return fail(RT_ERR_INVALID, "rt_trace_closest: at most 2^31-1 rays per call");
@@ -417,6 +424,7 @@ static int trace_any_common(rt_scene *s, const rt_ray *rays, uint64_t n, void *o
                             const char *who)
 {
     if (!s) return fail(RT_ERR_INVALID, std::string(who) + ": null scene");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, std::string(who) + ": not available on a merged scene");
     if (!s->committed) return fail(RT_ERR_STATE, std::string(who) + ": scene not committed");
     if (n && (!rays || !out)) return fail(RT_ERR_INVALID, std::string(who) + ": null buffer");
     if (n >= 0x80000000ull) return fail(RT_ERR_INVALID, std::string(who) + ": at most 2^31-1 rays per call");

@@ -53,6 +53,7 @@ using namespace rtb;
 extern "C" int rt_trace_closest_noalloc(rt_scene *s, const rt_ray *rays, uint64_t n, rt_hit *hits, uint32_t flags)
 {
     if (!s) return fail(RT_ERR_INVALID, "rt_trace_closest_noalloc: null scene");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_trace_closest_noalloc: not available on a merged scene");
     if (!s->committed) return fail(RT_ERR_STATE, "rt_trace_closest_noalloc: scene not committed");
     if (n && (!rays || !hits)) return fail(RT_ERR_INVALID, "rt_trace_closest_noalloc: null buffer");
     if (n > kNoAllocMaxRays)

@@ -503,6 +503,7 @@ int rt_photons_trace(rt_scene *s, uint64_t n, uint32_t max_depth, uint32_t rr_de
                      rt_photon_map **out, rt_photon_trace_stats *stats)
 {
     if (!s || !out) return fail(RT_ERR_INVALID, "rt_photons_trace: null argument");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_photons_trace: not available on a merged scene");
     if (!s->committed) return fail(RT_ERR_STATE, "rt_photons_trace: scene not committed");
     if (n == 0 || n >= (1ull << 31)) return fail(RT_ERR_INVALID, "rt_photons_trace: n must be in [1, 2^31)");
     if (max_depth == 0 || max_depth > 255) return fail(RT_ERR_INVALID, "rt_photons_trace: max_depth in [1, 255]");

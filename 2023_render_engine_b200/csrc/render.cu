@@ -139,7 +139,8 @@ __device__ void start_path(const RenderView &rv, const Buffers &bf, int b, uint3
     ray.dz = d.z;
     ray.flags = 0;
     reinterpret_cast<float4 *>(bf.rays[b])[2 * q] = make_float4(ray.ox, ray.oy, ray.oz, ray.tmax);
-    reinterpret_cast<float4 *>(bf.rays[b])[2 * q + 1] = make_float4(ray.dx, ray.dy, ray.dz, 0.f);
+    // the last word carries the view's scene (merged scenes; 0 otherwise)
+    reinterpret_cast<float4 *>(bf.rays[b])[2 * q + 1] = make_float4(ray.dx, ray.dy, ray.dz, __uint_as_float(vw.scene));
     bf.st0[b][q] = make_float4(1.f, 1.f, 1.f, 0.f);
     bf.st1[b][q] = make_float4(0.f, 0.f, 0.f, __uint_as_float(rv.view_pixel0[vi] + pix));
     bf.st2[b][q] = make_uint4((uint32_t)r.state, (uint32_t)(r.state >> 32), j, kCameraRay | kRecBits);
@@ -170,14 +171,17 @@ __global__ void __launch_bounds__(kB) k_start(RenderView rv, Buffers bf)
 // shadow. Used for point lights in compat mode; area-light samples must be blocked by
 // glass so that their MIS pairing with BSDF-sampled emitter hits stays unbiased.
 // rec: the guide record the contribution also belongs to (kRecNone: none).
+// The shadow ray's last word: bit 0 skip_transparent, bits 1..22 the guide record, bits 24..31
+// the path's scene (merged scenes).
+constexpr uint32_t kShadowSceneShift = 24;
 __device__ __forceinline__ void push_shadow(const Buffers &bf, V3 o, V3 d, float tmax, V3 contrib, uint32_t target,
-                                            bool skip_transparent, uint32_t rec = kRecNone)
+                                            bool skip_transparent, uint32_t sub, uint32_t rec = kRecNone)
 {
     uint32_t i = append(bf.cnt + 2);
     if (i >= bf.scap) return;
     reinterpret_cast<float4 *>(bf.srays)[2 * i] = make_float4(o.x, o.y, o.z, tmax);
-    reinterpret_cast<float4 *>(bf.srays)[2 * i + 1] =
-        make_float4(d.x, d.y, d.z, __uint_as_float((rec << 1) | (skip_transparent ? 1u : 0u)));
+    reinterpret_cast<float4 *>(bf.srays)[2 * i + 1] = make_float4(
+        d.x, d.y, d.z, __uint_as_float((sub << kShadowSceneShift) | (rec << 1) | (skip_transparent ? 1u : 0u)));
     bf.scontrib[i] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(target));
 }
 
@@ -289,7 +293,9 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
     const uint32_t q = bf.perm ? __ldg(bf.perm + i) : i;  // the queue slot this thread shades
     const int nxt = cur ^ 1;
     const bool compat = (rv.flags & RT_RENDER_COMPAT) != 0;
-    const bool nee_area = (rv.flags & RT_RENDER_NEE_AREA) != 0 && rv.nemit > 0;
+    const uint32_t sub = rv.sv.subs ? __float_as_uint(__ldg(reinterpret_cast<const float *>(bf.rays[cur]) + 8 * q + 7)) : 0u;
+    const SceneLights lights = scene_lights(rv, sub);
+    const bool nee_area = (rv.flags & RT_RENDER_NEE_AREA) != 0 && lights.ne > 0;
     const bool photon_mode = (rv.flags & RT_RENDER_PHOTON_MAP) != 0;
     const bool hybrid = (rv.flags & RT_RENDER_HYBRID) != 0;
     const bool subsurface = (rv.flags & RT_RENDER_SUBSURFACE) != 0;
@@ -352,7 +358,7 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
         if (!is_black(Le)) {
             float w = 1.f;
             if (nee_area && bs.type == RT_MAT_LIGHT && depth > 0 && !(flags & kLastSpecular) && sf.emissive_tri) {
-                float pl = emitter_pdf(rv, Le, h.t * h.t, sf.area_cos);
+                float pl = emitter_pdf(lights.etotal, Le, h.t * h.t, sf.area_cos);
                 w = (last_pdf * last_pdf) / (last_pdf * last_pdf + pl * pl);
             }
             L = L + beta_in * Le * w;
@@ -456,7 +462,7 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
             if (subsurface && bs.type == RT_MAT_SUBSURFACE && (flags & kCameraRay))
                 push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherSubsurface, rec_in, bs.color);
             if (hybrid) push_gather(bf, sf, wo_w, beta_in * dscale, target, kGatherDensity, rec_in, bs.color);
-            for (uint32_t li = 0; li < rv.nplights; li++) {  // Scene::estimateAllDirectLights, PointLight
+            for (uint32_t li = lights.pl0; li < lights.pl0 + lights.npl; li++) {  // Scene::estimateAllDirectLights
                 float4 lp = rv.plights[2 * li], li4 = rv.plights[2 * li + 1];
                 V3 tol = v3(lp.x, lp.y, lp.z) - sf.p;
                 float dist2 = dot(tol, tol), dist = sqrtf(dist2);
@@ -473,13 +479,13 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
                 float w = compat ? 1.0f / (1.0f + pb * pb) : 1.0f;  // powerHeuristic(1,1,1,pdf), Scene.cu:331
                 V3 c = beta_in * fl * Li * (w * dscale);
                 V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
-                push_shadow(bf, so, wl, dist, c, target, compat, rec_in);
+                push_shadow(bf, so, wl, dist, c, target, compat, sub, rec_in);
             }
             if (nee_area) {
                 float u0 = pcg_float(rng), u1 = pcg_float(rng), u2 = pcg_float(rng);
                 // pick an emitter by area * luminance
-                float x = u0 * rv.emit_total;
-                uint32_t lo = 0, hi = rv.nemit - 1;
+                float x = u0 * lights.etotal;
+                uint32_t lo = lights.e0, hi = lights.e0 + lights.ne - 1;
                 while (lo < hi) {
                     uint32_t mid = (lo + hi) >> 1;
                     if (rv.emit_cdf[mid] <= x)
@@ -501,7 +507,7 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
                 float cosl = fabsf(dot(nl, wl));
                 const rt_material &em = rv.mats[min(rv.tri_mat[etri], rv.nmats - 1)];
                 V3 Lel = v3(em.color[0], em.color[1], em.color[2]) * em.intensity;
-                float pl = emitter_pdf(rv, Lel, dist2, cosl);
+                float pl = emitter_pdf(lights.etotal, Lel, dist2, cosl);
                 if (pl > 0 && dot(wl, sf.n) > 0) {
                     V3 wls = v3(dot(wl, t), dot(wl, bvec), dot(wl, sf.n));
                     float pb;
@@ -513,7 +519,7 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
                         float w = (pl * pl) / (pl * pl + pb * pb);
                         V3 c = beta_in * fl * Lel * (w * dscale / pl);
                         V3 so = spawn_origin(sf.p, sf.n, sf.perr, wl);
-                        push_shadow(bf, so, wl, dist * (1.0f - 1e-4f), c, target, false, rec_in);
+                        push_shadow(bf, so, wl, dist * (1.0f - 1e-4f), c, target, false, sub, rec_in);
                     }
                 }
             }
@@ -524,7 +530,8 @@ __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView r
     if (cont) {
         const uint32_t qn = target;
         reinterpret_cast<float4 *>(bf.rays[nxt])[2 * qn] = make_float4(next_o.x, next_o.y, next_o.z, INFINITY);
-        reinterpret_cast<float4 *>(bf.rays[nxt])[2 * qn + 1] = make_float4(next_d.x, next_d.y, next_d.z, 0.f);
+        reinterpret_cast<float4 *>(bf.rays[nxt])[2 * qn + 1] =
+            make_float4(next_d.x, next_d.y, next_d.z, __uint_as_float(sub));
         bf.st0[nxt][qn] = make_float4(beta.x, beta.y, beta.z, next_pdf);
         bf.st1[nxt][qn] = make_float4(L.x, L.y, L.z, __uint_as_float(pix));
         bf.st2[nxt][qn] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), s2.z, next_flags);
@@ -546,7 +553,8 @@ __global__ void __launch_bounds__(kB, RTB_TRAV_MIN_BLOCKS) k_shadow(RenderView r
         [&](uint32_t i, Trav &T) {
             const float4 r0 = reinterpret_cast<const float4 *>(bf.srays)[2 * i];
             const float4 r1 = reinterpret_cast<const float4 *>(bf.srays)[2 * i + 1];
-            trav_init(T, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w);
+            const uint32_t sub = __float_as_uint(r1.w) >> kShadowSceneShift;
+            trav_init(T, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w, scene_root(rv.sv, sub));
             T.shadow = (__float_as_uint(r1.w) & 1u) != 0;
         },
         [&](uint32_t i, Trav &T) {
@@ -556,7 +564,10 @@ __global__ void __launch_bounds__(kB, RTB_TRAV_MIN_BLOCKS) k_shadow(RenderView r
                 float t = tmax;
                 int32_t prim = -1;
                 float b1 = 0, b2 = 0;
-                intersect_spheres(rv.sv, T.w.ox, T.w.oy, T.w.oz, T.dx, T.dy, T.dz, tmax, T.shadow, t, prim, b1, b2);
+                const uint32_t sub =
+                    __float_as_uint(reinterpret_cast<const float4 *>(bf.srays)[2 * i + 1].w) >> kShadowSceneShift;
+                intersect_spheres(rv.sv, sub, T.w.ox, T.w.oy, T.w.oz, T.dx, T.dy, T.dz, tmax, T.shadow, t, prim, b1,
+                                  b2);
                 occ = prim >= 0 && t < tmax;
             }
             if (occ) return;
@@ -750,6 +761,7 @@ extern "C" {
 int rt_scene_set_materials(rt_scene *s, const rt_material *table, uint32_t n)
 {
     if (!s || (!table && n)) return fail(RT_ERR_INVALID, "rt_scene_set_materials: null argument");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_materials: not available on a merged scene");
     for (uint32_t i = 0; i < n; i++)
         if (table[i].type > RT_MAT_PLASTIC) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_materials: unknown type");
     s->materials.assign(table, table + n);
@@ -760,6 +772,7 @@ int rt_scene_set_materials(rt_scene *s, const rt_material *table, uint32_t n)
 int rt_scene_set_triangle_materials(rt_scene *s, uint32_t first, uint32_t n, const uint32_t *mats)
 {
     if (!s || (!mats && n)) return fail(RT_ERR_INVALID, "rt_scene_set_triangle_materials: null argument");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_triangle_materials: not available on a merged scene");
     if ((uint64_t)first + n > s->tri_material.size())
         return fail(RT_ERR_INVALID, "rt_scene_set_triangle_materials: range out of bounds");
     std::memcpy(s->tri_material.data() + first, mats, 4ull * n);
@@ -770,6 +783,7 @@ int rt_scene_set_triangle_materials(rt_scene *s, uint32_t first, uint32_t n, con
 int rt_render_set_photon_map(rt_scene *s, rt_photon_map *m, uint32_t k, float radius)
 {
     if (!s) return fail(RT_ERR_INVALID, "rt_render_set_photon_map: null scene");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_render_set_photon_map: not available on a merged scene");
     if (m && (k == 0 || k > kKnnMaxK)) return fail(RT_ERR_INVALID, "rt_render_set_photon_map: k must be in [1, 128]");
     s->pmap = m;
     s->pm_k = k;
@@ -780,6 +794,7 @@ int rt_render_set_photon_map(rt_scene *s, rt_photon_map *m, uint32_t k, float ra
 int rt_scene_add_texture(rt_scene *s, const float *rgb, uint32_t width, uint32_t height, uint32_t *id)
 {
     if (!s || !rgb || !id) return fail(RT_ERR_INVALID, "rt_scene_add_texture: null argument");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_add_texture: not available on a merged scene");
     if (width == 0 || height == 0 || width >= (1u << 24) || height >= (1u << 24) ||
         (uint64_t)width * height >= (1ull << 32))
         return fail(RT_ERR_INVALID, "rt_scene_add_texture: size must be in [1, 2^24) per axis, < 2^32 texels");
@@ -799,6 +814,7 @@ int rt_scene_add_texture(rt_scene *s, const float *rgb, uint32_t width, uint32_t
 int rt_scene_set_triangle_uvs(rt_scene *s, uint32_t first, uint32_t n, const float *uv)
 {
     if (!s || (!uv && n)) return fail(RT_ERR_INVALID, "rt_scene_set_triangle_uvs: null argument");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_set_triangle_uvs: not available on a merged scene");
     const uint64_t ntri = s->tri9.size() / 9;
     if ((uint64_t)first + n > ntri) return fail(RT_ERR_INVALID, "rt_scene_set_triangle_uvs: range out of bounds");
     if (s->tri_uv.size() < 6 * ntri) {
@@ -837,6 +853,7 @@ int rt_texture_lookup(rt_scene *s, uint32_t id, const float *uv, uint64_t n, flo
 int rt_scene_add_point_light(rt_scene *s, const float pos[3], const float rgb[3], float intensity)
 {
     if (!s || !pos || !rgb) return fail(RT_ERR_INVALID, "rt_scene_add_point_light: null argument");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_add_point_light: not available on a merged scene");
     s->plights.push_back(make_float4(pos[0], pos[1], pos[2], 0.f));
     s->plights.push_back(make_float4(rgb[0] * intensity, rgb[1] * intensity, rgb[2] * intensity, 0.f));
     s->plight_rgbi.push_back({rgb[0], rgb[1], rgb[2], intensity});
@@ -926,7 +943,16 @@ int upload_render_data(rt_scene *s)
     std::vector<uint32_t> etri;
     std::vector<float> cdf;
     double acc = 0;
+    uint32_t sub = 0;  // merged scene: emitters are gathered per scene, each cdf from 0
     for (uint32_t t = 0; t < n; t++) {
+        if (s->merged) {
+            while (sub + 1 < s->sub_tri0.size() && t >= s->sub_tri0[sub + 1]) {
+                s->subs[sub].etotal = (float)acc;
+                sub++;
+                s->subs[sub].e0 = (uint32_t)etri.size();
+                acc = 0;
+            }
+        }
         const rt_material &m = s->materials[s->tri_material[t]];
         if (m.type != RT_MAT_LIGHT) continue;
         const float *p = s->tri9.data() + 9ull * t;
@@ -943,6 +969,17 @@ int upload_render_data(rt_scene *s)
     }
     s->emit_total = (float)acc;
     s->nemit = (uint32_t)etri.size();
+    if (s->merged) {
+        for (uint32_t k = sub + 1; k < s->subs.size(); k++) s->subs[k].e0 = (uint32_t)etri.size();  // trailing empty scenes
+        s->subs[sub].etotal = (float)acc;
+        for (size_t k = 0; k < s->subs.size(); k++) {
+            const uint32_t e1 = k + 1 < s->subs.size() ? s->subs[k + 1].e0 : (uint32_t)etri.size();
+            s->subs[k].ne = e1 - s->subs[k].e0;
+            if (s->subs[k].ne == 0) s->subs[k].etotal = 0.f;
+        }
+        s->subs[0].e0 = 0;
+        RTB_CHECK(s->d_subs.upload(s->subs.data(), s->subs.size() * sizeof(SubScene), st));
+    }
     if (!etri.empty()) {
         RTB_CHECK(s->d_emit_tri.upload(etri.data(), 4ull * etri.size(), st));
         RTB_CHECK(s->d_emit_cdf.upload(cdf.data(), 4ull * cdf.size(), st));
@@ -989,6 +1026,15 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     const std::string name(who);
     if (!s || !views || nviews == 0 || !sum_rgb || !count) return fail(RT_ERR_INVALID, name + ": null argument");
     if (!s->committed) return fail(RT_ERR_STATE, name + ": scene not committed");
+    if (s->merged) {
+        if (flags & (RT_RENDER_EXACT_TRACE | RT_RENDER_PHOTON_MAP | RT_RENDER_SUBSURFACE | RT_RENDER_HYBRID))
+            return fail(RT_ERR_UNSUPPORTED, name + ": a merged scene renders without photon maps or exact tracing");
+        for (uint32_t i = 0; i < nviews; i++)
+            if (views[i].scene >= s->subs.size()) return fail(RT_ERR_INVALID, name + ": view scene index out of range");
+    } else {
+        for (uint32_t i = 0; i < nviews; i++)
+            if (views[i].scene != 0) return fail(RT_ERR_INVALID, name + ": view scene index without a merged scene");
+    }
     std::vector<uint64_t> sample0(nviews + 1, 0);
     std::vector<uint32_t> pixel0(nviews + 1, 0);
     uint32_t depth_max = 0;

@@ -126,6 +126,18 @@ struct alignas(16) SphereRecord {
     float o2w[16];
 };
 
+// One scene of a merged scene (rt_scene_merge): where its BVH8 root lies in the merged node
+// array, and its ranges of spheres, emissive triangles and point lights. A path carries the
+// index of its scene in the last word of its rays.
+constexpr uint32_t kNoRoot = 0xFFFFFFFFu;  // a scene without triangles
+struct SubScene {
+    uint32_t root;       // node index of its BVH8 root, or kNoRoot
+    uint32_t sph0, nsph;  // its spheres
+    uint32_t e0, ne;      // its emitters in emit_tri / emit_cdf (the cdf restarts at 0 per scene)
+    float etotal;         // sum over its emitters of area * luminance
+    uint32_t pl0, npl;    // its point lights
+};
+
 // Device view used by the kernels.
 struct SceneView {
     const Bvh8Node *nodes;
@@ -139,6 +151,8 @@ struct SceneView {
     uint32_t nspheres;
     uint32_t nnodes;
     uint32_t root_is_leaf;  // scene with a single leaf (ntri <= 3): node 0 still describes it
+    const SubScene *subs;   // merged scene: per-scene roots and ranges (null: one scene, root 0)
+    uint32_t nsubs;
 };
 
 // ------------------------------------------------------------ host build
@@ -279,6 +293,12 @@ struct rt_scene {
     uint64_t last_rays = 0, last_fallback = 0;
     rtb::DevBuf h2d_rays, d2h_hits;  // device staging for the host-buffer entry points
     rtb::DevBuf any_hits;            // closest hits behind rt_trace_any's reference-exact decision
+    // merged scene (rt_scene_merge): its scenes' roots and ranges and where each one's
+    // triangles start (emitters are gathered per scene at upload)
+    bool merged = false;
+    std::vector<rtb::SubScene> subs;
+    std::vector<uint32_t> sub_tri0;  // nsubs + 1 entries
+    rtb::DevBuf d_subs;
     // rendering
     std::vector<rt_material> materials;
     std::vector<float4> plights;  // 2 per light: position, rgb * intensity

@@ -450,11 +450,27 @@ __device__ __forceinline__ V3 bsdf_sample(const Bsdf &b, V3 wo, Pcg &r, bool com
     }
 }
 
-__device__ __forceinline__ float emitter_pdf(const RenderView &rv, V3 Le, float dist2, float cosl)
+// Emitters and point lights next-event estimation draws from for a path of scene `sub`
+// (all of them in a plain scene; the scene's own in a merged scene).
+struct SceneLights {
+    uint32_t e0, ne;  // emitters [e0, e0 + ne) of emit_tri / emit_cdf
+    float etotal;     // their sum of area * luminance (the cdf's last value)
+    uint32_t pl0, npl;
+};
+__device__ __forceinline__ SceneLights scene_lights(const RenderView &rv, uint32_t sub)
+{
+    if (rv.sv.subs) {
+        const SubScene &ss = rv.sv.subs[min(sub, rv.sv.nsubs - 1)];
+        return SceneLights{ss.e0, ss.ne, ss.etotal, ss.pl0, ss.npl};
+    }
+    return SceneLights{0u, rv.nemit, rv.emit_total, 0u, rv.nplights};
+}
+
+__device__ __forceinline__ float emitter_pdf(float emit_total, V3 Le, float dist2, float cosl)
 {
     // p(select tri) / area = luminance(Le) / total; solid-angle conversion dist^2 / |cos|
-    if (!(cosl > 0) || rv.emit_total <= 0) return 0.f;
-    return luminance(Le) / rv.emit_total * dist2 / cosl;
+    if (!(cosl > 0) || emit_total <= 0) return 0.f;
+    return luminance(Le) / emit_total * dist2 / cosl;
 }
 
 

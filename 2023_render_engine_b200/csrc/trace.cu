@@ -29,16 +29,19 @@ constexpr int kBlock = 128;
 
 // Decides, for a finished ray, whether the kernel's answer provably equals the reference's
 // (see the file comment) and writes the hit, or queues the ray for k_trace_exact.
-__device__ __forceinline__ void closest_epilogue(const SceneView &v, uint64_t i, const Trav &T, uint32_t flags,
-                                                 rt_hit *__restrict__ hits, uint32_t *__restrict__ queue,
-                                                 uint32_t queue_cap, uint32_t *__restrict__ counters)
+// A merged scene (rt_scene_merge) has no reference-order tree: its rays are traced in the fast
+// mode, and a ray whose walk ran out of stack keeps the hit found so far (status word set).
+__device__ __forceinline__ void closest_epilogue(const SceneView &v, uint64_t i, uint32_t sub, const Trav &T,
+                                                 uint32_t flags, rt_hit *__restrict__ hits,
+                                                 uint32_t *__restrict__ queue, uint32_t queue_cap,
+                                                 uint32_t *__restrict__ counters)
 {
     const bool shadow = (flags & RT_TRACE_SHADOW) != 0;
     const Best &best = T.best;
     const float ox = T.w.ox, oy = T.w.oy, oz = T.w.oz, tmax = T.w.tmax;
     bool exact_needed = false, replay = false;
     if (!T.ok) {
-        exact_needed = replay = true;
+        exact_needed = replay = v.subs == nullptr;
         atomicCAS(counters + 1, 0u, (uint32_t)DEV_STACK_OVERFLOW);
     } else if (!(flags & RT_TRACE_FAST) && best.prim >= 0) {
         if (best.minblock < best.t) {
@@ -66,8 +69,14 @@ __device__ __forceinline__ void closest_epilogue(const SceneView &v, uint64_t i,
     float t = best.prim >= 0 ? best.t : INFINITY;
     int32_t prim = best.prim;
     float b1 = best.b1, b2 = best.b2;
-    intersect_spheres(v, ox, oy, oz, T.dx, T.dy, T.dz, tmax, shadow, t, prim, b1, b2);
+    intersect_spheres(v, sub, ox, oy, oz, T.dx, T.dy, T.dz, tmax, shadow, t, prim, b1, b2);
     reinterpret_cast<float4 *>(hits)[i] = make_float4(t, __int_as_float(prim), b1, b2);
+}
+
+// Scene index a ray carries in its last word (merged scenes only; 0 otherwise).
+__device__ __forceinline__ uint32_t ray_scene(const SceneView &v, const rt_ray *rays, uint64_t i)
+{
+    return v.subs ? __float_as_uint(__ldg(reinterpret_cast<const float *>(rays) + 8 * i + 7)) : 0u;
 }
 
 // Persistent closest-hit kernel: warps fetch rays from counters[3] until all n are done.
@@ -83,10 +92,13 @@ __global__ void __launch_bounds__(kBlock, RTB_TRAV_MIN_BLOCKS) k_trace_closest(S
         [&](uint32_t i, Trav &T) {
             float4 ra, rb;
             load_ray(rays, i, ra, rb);
-            trav_init(T, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, (flags & kTraceUnbounded) ? INFINITY : ra.w);
+            const uint32_t root = scene_root(v, v.subs ? __float_as_uint(rb.w) : 0u);
+            trav_init(T, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, (flags & kTraceUnbounded) ? INFINITY : ra.w, root);
             T.shadow = shadow;
         },
-        [&](uint32_t i, Trav &T) { closest_epilogue(v, i, T, flags, hits, queue, queue_cap, counters); });
+        [&](uint32_t i, Trav &T) {
+            closest_epilogue(v, i, ray_scene(v, rays, i), T, flags, hits, queue, queue_cap, counters);
+        });
 }
 
 __global__ void __launch_bounds__(kBlock) k_trace_exact(SceneView v, const rt_ray *__restrict__ rays,
@@ -131,7 +143,7 @@ __global__ void __launch_bounds__(kBlock) k_trace_exact(SceneView v, const rt_ra
             atomicAdd(counters + 2, 1u);
         }
         if (prim < 0) t = INFINITY;
-        intersect_spheres(v, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w, shadow, t, prim, b1, b2);
+        intersect_spheres(v, 0u, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w, shadow, t, prim, b1, b2);
         reinterpret_cast<float4 *>(hits)[i] = make_float4(t, __int_as_float(prim), b1, b2);
     }
 }
@@ -158,7 +170,7 @@ __global__ void __launch_bounds__(kBlock) k_trace_any(SceneView v, const rt_ray 
             float t = ra.w;
             int32_t prim = -1;
             float b1 = 0, b2 = 0;
-            intersect_spheres(v, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w, shadow, t, prim, b1, b2);
+            intersect_spheres(v, 0u, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w, shadow, t, prim, b1, b2);
             occ = prim >= 0 && t < ra.w;
         }
     }

@@ -94,8 +94,28 @@ struct Trav {
     uint2 st[kStack];  // node index, entry distance bits: one 8-byte local access per push / pop
 };
 
+// BVH8 root of scene `sub` (0 for a plain scene) and its spheres [s0, s0 + ns).
+__device__ __forceinline__ uint32_t scene_root(const SceneView &v, uint32_t sub)
+{
+    if (v.subs) return v.subs[min(sub, v.nsubs - 1)].root;
+    return v.ntri ? 0u : kNoRoot;
+}
+__device__ __forceinline__ void scene_spheres(const SceneView &v, uint32_t sub, uint32_t &s0, uint32_t &ns)
+{
+    if (v.subs) {
+        const SubScene &ss = v.subs[min(sub, v.nsubs - 1)];
+        s0 = ss.sph0;
+        ns = ss.nsph;
+    } else {
+        s0 = 0;
+        ns = v.nspheres;
+    }
+}
+
+// root: the BVH8 node the walk starts at (kNoRoot: the scene has no triangles; the walk is
+// skipped).
 __device__ __forceinline__ void trav_init(Trav &T, float ox, float oy, float oz, float dx, float dy, float dz,
-                                          float tmax)
+                                          float tmax, uint32_t root)
 {
     T.w = make_watertight(ox, oy, oz, dx, dy, dz, tmax);
     T.dx = dx;
@@ -107,7 +127,7 @@ __device__ __forceinline__ void trav_init(Trav &T, float ox, float oy, float oz,
     T.oix = -ox * T.ix;
     T.oiy = -oy * T.iy;
     T.oiz = -oz * T.iz;
-    T.cur = 0;
+    T.cur = root;
     T.sp = 0;
     T.steps = 0;
     T.ok = true;
@@ -217,11 +237,12 @@ __device__ __forceinline__ bool traverse_bvh8(const SceneView &v, const Watertig
                                               bool shadow, bool anyhit, Best &best)
 {
     Trav T;
-    trav_init(T, w.ox, w.oy, w.oz, dx, dy, dz, w.tmax);
+    trav_init(T, w.ox, w.oy, w.oz, dx, dy, dz, w.tmax, scene_root(v, 0));
     T.shadow = shadow;
     T.best = best;
-    while (!trav_step(v, T, anyhit)) {
-    }
+    if (T.cur != kNoRoot)
+        while (!trav_step(v, T, anyhit)) {
+        }
     best = T.best;
     return T.ok;
 }
@@ -256,7 +277,7 @@ __device__ __forceinline__ void persistent_traverse(const SceneView &v, uint32_t
         }
         if (__all_sync(0xFFFFFFFFu, ray == 0xFFFFFFFFu)) break;
         if (ray != 0xFFFFFFFFu) {
-            if (v.ntri == 0 || trav_step(v, T, anyhit)) {
+            if (T.cur == kNoRoot || trav_step(v, T, anyhit)) {
                 finish(ray, T);
                 ray = 0xFFFFFFFFu;
             }
@@ -264,11 +285,14 @@ __device__ __forceinline__ void persistent_traverse(const SceneView &v, uint32_t
     }
 }
 
-__device__ __forceinline__ void intersect_spheres(const SceneView &v, float ox, float oy, float oz, float dx, float dy,
-                                              float dz, float tmax, bool shadow, float &t, int32_t &prim, float &b1,
-                                              float &b2)
+// Scene::intersects' loop over the analytic shapes (Scene.cu:141-146) of scene `sub`.
+__device__ __forceinline__ void intersect_spheres(const SceneView &v, uint32_t sub, float ox, float oy, float oz,
+                                                  float dx, float dy, float dz, float tmax, bool shadow, float &t,
+                                                  int32_t &prim, float &b1, float &b2)
 {
-    for (uint32_t s = 0; s < v.nspheres; s++) {
+    uint32_t s0, ns;
+    scene_spheres(v, sub, s0, ns);
+    for (uint32_t s = s0; s < s0 + ns; s++) {
         const SphereRecord &sr = v.spheres[s];
         if (shadow && (sr.flags & 1u)) continue;
         float ts;

@@ -338,7 +338,8 @@ RT_API int rt_render(rt_scene *scene, const rt_camera *camera, const rt_render_o
 typedef struct rt_view {
     rt_camera camera;
     uint32_t spp, sample_offset, max_depth, rr_depth, seed;
-    uint32_t reserved[3];
+    uint32_t scene; /* the view's scene in a merged scene (rt_scene_merge: its index in the list); 0 otherwise */
+    uint32_t reserved[2];
 } rt_view;
 
 /* Many views of one scene in one wavefront (new in this build: the reference renders one
@@ -350,6 +351,16 @@ typedef struct rt_view {
  * options. flags: RT_RENDER_* for all views; max_paths: queue capacity (0: 4M). */
 RT_API int rt_render_batch(rt_scene *scene, const rt_view *views, uint32_t nviews, uint32_t flags, uint32_t max_paths,
                            float *sum_rgb, uint32_t *count, double *sum64, rt_render_stats *stats);
+
+/* Several committed scenes of one context as one scene for rendering (new in this build; the
+ * reference renders one scene per PathTracerIntegrator::render call, PathTracerIntegrator.cu:
+ * 140-210). rt_render_batch on the result renders views of all of them in one wavefront: a
+ * view's `scene` field is the index of its scene in `scenes`, and its paths see only that
+ * scene's geometry, materials, textures and lights. Each scene keeps its own BVH (copied, with
+ * its indices moved); the sources stay valid and independent. A merged scene is for rendering
+ * only: it is not modified, traced with rt_trace_*, or rendered with photon maps or
+ * RT_RENDER_EXACT_TRACE (RT_ERR_UNSUPPORTED). At most 256 scenes. Free with rt_scene_destroy. */
+RT_API int rt_scene_merge(rt_context *ctx, rt_scene *const *scenes, uint32_t n, rt_scene **out);
 
 /* Material sort of the wavefront (new in this build; the reference shades its samples in pixel
  * order, pathTracing.cu:284-414): before each wave is shaded, every chunk of 2^chunk_log2 queue

@@ -69,3 +69,55 @@ def test_batch_rejects_bad_views(core, gpu_ctx):
         sc.render_batch([dict(camera=cam, spp=0)])
     with pytest.raises(Exception):
         sc.render_batch([])
+
+
+def _textured_floor(core, ctx):
+    """A textured Lambertian quad under a point light and a quad emitter (texture ids, uvs and
+    point lights of a scene that is not the first of a merge)."""
+    sc = core.Scene(ctx)
+    tex = np.random.default_rng(1).uniform(0.1, 1.0, (4, 4, 3)).astype(np.float32)
+    tid = sc.add_texture(tex)
+    sc.set_materials([core.material(N.RT_MAT_LAMBERTIAN, color=(0.9, 0.8, 0.7), texture=tid),
+                      core.material(N.RT_MAT_LIGHT, color=(1, 1, 1), intensity=8.0)])
+    floor = np.array([[-2, 0, -2], [2, 0, -2], [2, 0, 2], [-2, 0, 2]], np.float32)
+    light = np.array([[-0.5, 1.5, -0.5], [-0.5, 1.5, 0.5], [0.5, 1.5, 0.5], [0.5, 1.5, -0.5]], np.float32)
+    q = np.array([[0, 2, 1], [0, 3, 2]], np.uint32)
+    first = sc.add_mesh(floor, q, material=0, shape_id=0)
+    sc.set_triangle_uvs(first, np.array([[0, 0, 1, 1, 1, 0], [0, 0, 0, 1, 1, 1]], np.float32))
+    sc.add_mesh(light, q, material=1, shape_id=1)
+    sc.add_point_light((0.5, 1.0, 0.5), (1, 0.9, 0.8), 2.0)
+    sc.commit()
+    return sc
+
+
+def test_merged_scenes_render_like_each_scene(core, gpu_ctx):
+    """rt_scene_merge: views of three scenes (the Cornell box with its spheres and area light, a
+    small BVH-stress mesh with per-block GGX, a textured floor with a point light) in one
+    wavefront give every view the image rt_render_batch of its own scene gives it."""
+    cfgs = importlib.import_module("2023_render_engine_b200.configs")
+    s0, cam0, _ = cfgs.build_config0(gpu_ctx, 40, 32)
+    s1, cam1, _ = cfgs.build_config1(gpu_ctx, 48, 24, subdiv=3)
+    s2 = _textured_floor(core, gpu_ctx)
+    cam2 = core.look_at_camera((0, 1.2, 3.0), (0, 0, 0), (0, 1, 0), 50.0, 32, 32)
+    per_scene = [(s0, [dict(camera=cam0, spp=4, max_depth=8, seed=1), dict(camera=cam0, spp=2, max_depth=5, seed=2)]),
+                 (s1, [dict(camera=cam1, spp=3, max_depth=12, seed=3)]),
+                 (s2, [dict(camera=cam2, spp=4, max_depth=6, seed=4), dict(camera=cam2, spp=1, max_depth=3, seed=5)])]
+    flags = N.RT_RENDER_NEE_AREA
+    want, rays = [], 0
+    for sc, views in per_scene:
+        film, st, off = sc.render_batch(views, flags=flags, fp64=True, max_paths=1 << 14)
+        m = core.film_mean(film)
+        want += [m[off[i]:off[i + 1]] for i in range(len(views))]
+        rays += st["extension_rays"] + st["shadow_rays"]
+    merged = core.merge_scenes(gpu_ctx, [s0, s1, s2])
+    views = [dict(v, scene=k) for k, (_, vs) in enumerate(per_scene) for v in vs]
+    film, st, off = merged.render_batch(views, flags=flags, fp64=True, max_paths=1 << 14)
+    m = core.film_mean(film)
+    assert st["extension_rays"] + st["shadow_rays"] == rays
+    for i in range(len(views)):
+        assert np.allclose(m[off[i]:off[i + 1]], want[i], rtol=1e-5, atol=1e-6), i
+    with pytest.raises(N.RtError):  # a merged scene is not traced or modified
+        merged.add_point_light((0, 0, 0), (1, 1, 1), 1.0)
+    with pytest.raises(N.RtError):
+        merged.render_batch([dict(camera=cam0, spp=1, scene=3)])
+    merged.close()
