@@ -130,6 +130,7 @@ SIGNATURES = {
     "rt_scene_destroy": [_P],
     "rt_scene_add_mesh": [_P, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _I32, _INT, ctypes.POINTER(_U32)],
     "rt_scene_add_sphere": [_P, _P, _P, _F32, _U32, _I32, _INT, ctypes.POINTER(_U32)],
+    "rt_scene_add_plane": [_P, _P, _P, _U32, _I32, _INT, ctypes.POINTER(_U32)],
     "rt_scene_commit": [_P],
     "rt_scene_set_build": [_P, _U32],
     "rt_material_eval": [_P, _P, _P, ctypes.c_uint64, _P, _P],

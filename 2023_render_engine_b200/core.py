@@ -67,6 +67,17 @@ class Scene:
                                           int(transparent), ctypes.byref(first)))
         return first.value
 
+    def add_plane(self, object_to_world, world_to_object, material: int = 0, shape_id: int = 0,
+                  transparent: bool = False) -> int:
+        """rt_scene_add_plane: the unit square of the plane's object space (Plane.cu); returns its
+        shape index (shared with spheres, in the order they are added)."""
+        o2w = np.ascontiguousarray(object_to_world, dtype=np.float32).reshape(16)
+        w2o = np.ascontiguousarray(world_to_object, dtype=np.float32).reshape(16)
+        idx = ctypes.c_uint32()
+        N.check(N.lib().rt_scene_add_plane(self.handle, _ptr(o2w), _ptr(w2o), material, shape_id, int(transparent),
+                                           ctypes.byref(idx)))
+        return idx.value
+
     def add_sphere(self, object_to_world, world_to_object, radius: float, material: int = 0, shape_id: int = 0,
                    transparent: bool = False) -> int:
         o2w = np.ascontiguousarray(object_to_world, dtype=np.float32).reshape(16)

@@ -272,6 +272,24 @@ int rt_scene_add_sphere(rt_scene *s, const float o2w[16], const float w2o[16], f
     return RT_OK;
 }
 
+int rt_scene_add_plane(rt_scene *s, const float o2w[16], const float w2o[16], uint32_t material, int32_t shape_id,
+                       int transparent, uint32_t *index)
+{
+    if (!s || !o2w || !w2o) return fail(RT_ERR_INVALID, "rt_scene_add_plane: null argument");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_scene_add_plane: not available on a merged scene");
+    SphereRecord r{};
+    std::memcpy(r.w2o, w2o, sizeof(r.w2o));
+    std::memcpy(r.o2w, o2w, sizeof(r.o2w));
+    r.radius = 0.f;
+    r.material = material;
+    r.shape_id = shape_id;
+    r.flags = kShapePlane | (transparent ? 3u : 0u);
+    if (index) *index = (uint32_t)s->spheres.size();
+    s->spheres.push_back(r);
+    s->committed = false;
+    return RT_OK;
+}
+
 int rt_scene_set_build(rt_scene *s, uint32_t mode)
 {
     if (!s) return fail(RT_ERR_INVALID, "rt_scene_set_build: null scene");

@@ -231,4 +231,61 @@ __device__ __forceinline__ bool sphere_test(const float *m, float radius, float 
     return true;
 }
 
+// The world -> object transform of a ray as Transform::operator()(const Ray &) does it
+// (Transform.cu:216-237): origin with its error bound, direction, origin moved to the edge of
+// the bound (dt along the direction) and the limit reduced by dt. po / pd: object-space
+// origin and direction, tm the reduced limit.
+__device__ __forceinline__ void ray_to_object(const float *m, float ox, float oy, float oz, float dx, float dy, float dz,
+                                              float tmax, float po[3], float pd[3], float &tm)
+{
+    const float eb3 = error_bound(3);
+    float oe[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const float *row = m + 4 * r;
+        oe[r] = fmul(fadd(fadd(fadd(fabsf(fmul(row[0], ox)), fabsf(fmul(row[1], oy))), fabsf(fmul(row[2], oz))),
+                          fabsf(row[3])),
+                     eb3);
+        po[r] = fadd(fadd(fadd(fmul(row[0], ox), fmul(row[1], oy)), fmul(row[2], oz)), row[3]);
+        pd[r] = fadd(fadd(fmul(row[0], dx), fmul(row[1], dy)), fmul(row[2], dz));
+    }
+    const float wp = fadd(fadd(fadd(fmul(m[12], ox), fmul(m[13], oy)), fmul(m[14], oz)), m[15]);
+    const float invw = fdiv(1.0f, wp);
+#pragma unroll
+    for (int r = 0; r < 3; r++) po[r] = fmul(invw, po[r]);
+    const float ls = fadd(fadd(fmul(pd[0], pd[0]), fmul(pd[1], pd[1])), fmul(pd[2], pd[2]));
+    tm = tmax;
+    if (ls > 0) {
+        const float dt =
+            fdiv(fadd(fadd(fmul(fabsf(pd[0]), oe[0]), fmul(fabsf(pd[1]), oe[1])), fmul(fabsf(pd[2]), oe[2])), ls);
+#pragma unroll
+        for (int r = 0; r < 3; r++) po[r] = fadd(po[r], fmul(pd[r], dt));
+        tm = fsub(tm, dt);
+    }
+}
+
+// Plane::intersects (shapes/Plane.cu:127-170): the ray in the plane's object space (its unit
+// square [0,1]^2 at z = 0), skipped when |d.z| <= FLOAT_ERROR_MARGIN (1e-7, compared in double
+// as the reference's double literal makes it); the hit point o - (o.z / d.z) d; the offset
+// Ray::getOffset takes from the x components alone ((p.x - o.x) / d.x, so a ray whose
+// object-space x direction is 0 never hits, Ray.cu:69-72); accepted when 0 < offset <= the
+// world ray's limit and the point lies in the square. Returns the offset in tOut; uv: the
+// object-space (x, y) (the surface point, Plane.cu:80-82).
+__device__ __forceinline__ bool plane_test(const float *m, float ox, float oy, float oz, float dx, float dy, float dz,
+                                           float tmax, float &tOut, float &u, float &v)
+{
+    float po[3], pd[3], tm;
+    ray_to_object(m, ox, oy, oz, dx, dy, dz, tmax, po, pd, tm);
+    if (!((double)fabsf(pd[2]) > 1e-7)) return false;
+    const float s = fdiv(po[2], pd[2]);
+    const float hx = fsub(po[0], fmul(s, pd[0])), hy = fsub(po[1], fmul(s, pd[1]));
+    const float off = fmul(fsub(hx, po[0]), fdiv(1.0f, pd[0]));
+    if (off <= 0.f || off > tmax || hx < 0.f || hx > 1.f || hy < 0.f || hy > 1.f) return false;
+    if (!(off == off)) return false;  // NaN offsets fail the reference's offset < hitOffset test
+    tOut = off;
+    u = hx;
+    v = hy;
+    return true;
+}
+
 }  // namespace rtb

@@ -116,13 +116,16 @@ struct alignas(16) TriRecord {
     float4 v2;  // w: flags
 };
 
-// Sphere as the reference stores it: world->object matrix (rows 0..3) and radius.
+// Analytic shape as the reference stores it: world->object matrix (rows 0..3), radius
+// (spheres) and object->world matrix. A plane (kShapePlane) is the unit square [0,1]^2 of its
+// object space (shapes/Plane.cu).
+constexpr uint32_t kShapePlane = 4u;  // SphereRecord.flags: the record is a Plane
 struct alignas(16) SphereRecord {
     float w2o[16];
     float radius;
     uint32_t material;
     int32_t shape_id;
-    uint32_t flags;  // bit 0: transparent to shadow rays
+    uint32_t flags;  // bit 0: transparent to shadow rays; bit 1: transparent as added; kShapePlane
     float o2w[16];
 };
 

@@ -107,6 +107,29 @@ __device__ __forceinline__ Surface surface_at(const RenderView &rv, const rt_hit
     Surface s;
     if (h.prim & RT_PRIM_SHAPE) {
         const SphereRecord &sr = rv.sv.spheres[h.prim & ~RT_PRIM_SHAPE];
+        if (sr.flags & kShapePlane) {
+            // Plane::intersect (Plane.cu:62-122): the object-space hit (x, y, 0) the trace reports
+            // in (b1, b2) carried to world space; the normal (0, 0, 1) turned against the ray; the
+            // reference's fixed object-space error bound 1e-4 carried by the transform
+            const float *m = sr.o2w;
+            const V3 lp = v3(h.b1, h.b2, 0.f);
+            s.p = xform_point(m, lp);
+            V3 n = normalize(v3(sr.w2o[8], sr.w2o[9], sr.w2o[10]));
+            if (dot(n, d) > 0) n = -n;
+            s.n = n;
+            const float eb3 = error_bound(3);
+            const V3 rows = v3(fabsf(m[0]) + fabsf(m[1]) + fabsf(m[2]), fabsf(m[4]) + fabsf(m[5]) + fabsf(m[6]),
+                               fabsf(m[8]) + fabsf(m[9]) + fabsf(m[10]));
+            const V3 mag = v3(fabsf(m[0] * lp.x) + fabsf(m[1] * lp.y) + fabsf(m[3]),
+                              fabsf(m[4] * lp.x) + fabsf(m[5] * lp.y) + fabsf(m[7]),
+                              fabsf(m[8] * lp.x) + fabsf(m[9] * lp.y) + fabsf(m[11]));
+            s.perr = rows * (1e-4f * (1.f + eb3)) + mag * eb3;
+            s.mat = sr.material;
+            s.shape = sr.shape_id;
+            s.emissive_tri = false;
+            s.area_cos = 0.f;
+            return s;
+        }
         V3 c = v3(sr.o2w[3], sr.o2w[7], sr.o2w[11]);
         V3 p = o + d * h.t;
         V3 n = normalize(p - c);
@@ -175,6 +198,7 @@ __device__ __forceinline__ V3 tex_color(const RenderView &rv, uint32_t id, float
 __device__ __forceinline__ float2 surface_uv(const RenderView &rv, const rt_hit &h, const Surface &s)
 {
     if (h.prim & RT_PRIM_SHAPE) {
+        if (rv.sv.spheres[h.prim & ~RT_PRIM_SHAPE].flags & kShapePlane) return make_float2(h.b1, h.b2);  // Plane.cu:82
         const float *m = rv.sv.spheres[h.prim & ~RT_PRIM_SHAPE].w2o;
         const float x = m[0] * s.p.x + m[1] * s.p.y + m[2] * s.p.z + m[3];
         const float y = m[4] * s.p.x + m[5] * s.p.y + m[6] * s.p.z + m[7];

@@ -295,12 +295,14 @@ __device__ __forceinline__ void intersect_spheres(const SceneView &v, uint32_t s
     for (uint32_t s = s0; s < s0 + ns; s++) {
         const SphereRecord &sr = v.spheres[s];
         if (shadow && (sr.flags & 1u)) continue;
-        float ts;
-        if (sphere_test(sr.w2o, sr.radius, ox, oy, oz, dx, dy, dz, tmax, ts) && ts < t) {
+        float ts, pu = 0.f, pv = 0.f;
+        const bool hit = (sr.flags & kShapePlane) ? plane_test(sr.w2o, ox, oy, oz, dx, dy, dz, tmax, ts, pu, pv)
+                                                  : sphere_test(sr.w2o, sr.radius, ox, oy, oz, dx, dy, dz, tmax, ts);
+        if (hit && ts < t) {
             t = ts;
             prim = RT_PRIM_SHAPE | (int32_t)s;
-            b1 = 0.f;
-            b2 = 0.f;
+            b1 = pu;  // a plane hit reports its object-space (x, y); 0 for spheres
+            b2 = pv;
         }
     }
 }

@@ -83,6 +83,15 @@ RT_API int rt_scene_add_sphere(rt_scene *scene, const float object_to_world[16],
                         float radius, uint32_t material, int32_t shape_id, int transparent,
                         uint32_t *index);
 
+/* Appends a Plane (shapes/Plane.cu): the unit square [0,1]^2 at z = 0 of its object space, with
+ * the reference's object<->world matrices (row-major 4x4: the base change of
+ * Plane(bottomLeftCorner, axisX, axisY, normal), Plane.cu:26-50, and its inverse). Its hits are
+ * Plane::intersects' arithmetic (Plane.cu:127-170) and are reported as prim = RT_PRIM_SHAPE | index
+ * with the object-space (x, y) in the hit's b1, b2; planes and spheres share one index space in
+ * the order they were added, as the reference's shape list does (Scene.cu:141-146). */
+RT_API int rt_scene_add_plane(rt_scene *scene, const float object_to_world[16], const float world_to_object[16],
+                              uint32_t material, int32_t shape_id, int transparent, uint32_t *index);
+
 /* Builds the acceleration structures: the 8-wide compressed BVH used for traversal
  * and the reference-order tree (BVH::BVH, cuda_libraries/BVH.cu:314-341) whose
  * static order breaks exact distance ties like the reference does. Replaces
@@ -128,7 +137,7 @@ typedef struct rt_ray {
 } rt_ray;
 
 /* 16-byte hit: distance, primitive (global triangle id, RT_PRIM_SHAPE|shape, or -1),
- * scaled barycentrics b1, b2 of a triangle hit (0 for shapes). */
+ * scaled barycentrics b1, b2 of a triangle hit, a plane's object-space (x, y), 0 for spheres. */
 typedef struct rt_hit {
     float t;
     int32_t prim;

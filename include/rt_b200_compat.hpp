@@ -52,6 +52,7 @@ struct SphereAccess : public Sphere {
 };
 struct PlaneAccess : public Plane {
     using Plane::objectToWorld;
+    using Plane::worldToObject;
 };
 struct LightMaterialAccess : public LightMaterial {
     using LightMaterial::color;
@@ -398,25 +399,12 @@ private:
             compat_detail::matrix16(a->worldToObject, w2o);
             check(rt_scene_add_sphere(scene_, o2w, w2o, (float)a->sph_radius, mat, index, transparent, nullptr));
         } else if (const auto *pl = dynamic_cast<const Plane *>(s)) {
-            // the unit square of the plane's object space (Plane.cu:85-90), as two triangles
+            // the reference's own plane: its matrices and Plane::intersects' arithmetic
             const auto *a = static_cast<const compat_detail::PlaneAccess *>(pl);
-            float xyz[12];
-            const Point3f corners[4] = {Point3f(0, 0, 0), Point3f(1, 0, 0), Point3f(1, 1, 0), Point3f(0, 1, 0)};
-            for (int c = 0; c < 4; c++) {
-                const Point3f w = a->objectToWorld(corners[c]);
-                xyz[3 * c] = (float)w.x;
-                xyz[3 * c + 1] = (float)w.y;
-                xyz[3 * c + 2] = (float)w.z;
-            }
-            const uint32_t idx[6] = {0, 1, 2, 0, 2, 3};
-            const uint32_t first = (uint32_t)tri_material_.size();
-            check(rt_scene_add_mesh(scene_, xyz, 4, idx, 2, nullptr, 0, nullptr, mat, index, transparent, nullptr));
-            tri_material_.push_back(mat);
-            tri_material_.push_back(mat);
-            // the plane's surface point is its object-space (x, y) (Plane.cu:82): the corners'
-            // coordinates, blended barycentrically, give the same point
-            const float uv[12] = {0, 0, 1, 0, 1, 1, 0, 0, 1, 1, 0, 1};
-            check(rt_scene_set_triangle_uvs(scene_, first, 2, uv));
+            float o2w[16], w2o[16];
+            compat_detail::matrix16(a->objectToWorld, o2w);
+            compat_detail::matrix16(a->worldToObject, w2o);
+            check(rt_scene_add_plane(scene_, o2w, w2o, mat, index, transparent, nullptr));
         } else {
             check_unsupported(std::string("shape class ") + typeid(*s).name());
         }

@@ -93,6 +93,11 @@ class RefOracle:
         L.refo_spheres_free.argtypes = [P]
         L.refo_sphere_matrices.argtypes = [P, U32, P, P]
         L.refo_spheres_intersect.argtypes = [P, P, P, U64, I, P, P, I]
+        L.refo_planes_build.restype = P
+        L.refo_planes_build.argtypes = [P, P, U32]
+        L.refo_planes_free.argtypes = [P]
+        L.refo_plane_matrices.argtypes = [P, U32, P, P]
+        L.refo_planes_intersect.argtypes = [P, P, P, U64, I, P, P, I]
         L.refo_kdtree_build.restype = P
         L.refo_kdtree_build.argtypes = [P, P, U64]
         L.refo_kdtree_free.argtypes = [P]
@@ -190,6 +195,39 @@ class RefSpheres:
         t = np.zeros(o.shape[0], np.float32)
         self.o.L.refo_spheres_intersect(self.h, o.ctypes.data, d.ctypes.data, o.shape[0], int(shadow), ids.ctypes.data,
                                         t.ctypes.data, threads)
+        return ids, t
+
+
+class RefPlanes:
+    """The reference's Plane shapes (Plane(bottomLeftCorner, axisX, axisY, normal)), their
+    matrices and Plane::intersects in Scene::intersects' shape-loop order."""
+
+    def __init__(self, o: RefOracle, planes12, glass=None):
+        self.o = o
+        p = _np(planes12, np.float32).reshape(-1, 12)
+        g = None if glass is None else _np(glass, np.uint8)
+        self.n = p.shape[0]
+        self.h = o.L.refo_planes_build(p.ctypes.data, None if g is None else g.ctypes.data, self.n)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.o.L.refo_planes_free(self.h)
+            self.h = None
+
+    def matrices(self, i):
+        o2w, w2o = np.zeros(16, np.float32), np.zeros(16, np.float32)
+        self.o.L.refo_plane_matrices(self.h, i, o2w.ctypes.data, w2o.ctypes.data)
+        return o2w.reshape(4, 4), w2o.reshape(4, 4)
+
+    def intersect(self, o, d, t_init=None, shadow=False, threads=8):
+        """(ids, t): the last plane that lowered the running offset (starting at t_init), -1: none."""
+        o = _np(o, np.float32).reshape(-1, 3)
+        d = _np(d, np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        t = np.full(n, np.inf, np.float32) if t_init is None else _np(t_init, np.float32).copy()
+        ids = np.zeros(n, np.int32)
+        self.o.L.refo_planes_intersect(self.h, o.ctypes.data, d.ctypes.data, n, int(shadow), ids.ctypes.data,
+                                       t.ctypes.data, threads)
         return ids, t
 
 

@@ -56,6 +56,7 @@
 #define swap ref_swap_
 #include "cuda_libraries/BVH.cu"
 #include "shapes/Sphere.cu"
+#include "shapes/Plane.cu"
 #include "cuda_libraries/kdtree.h"
 #include "materials/LambertianMaterial.cu"
 #include "materials/GlassMaterial.cu"
@@ -305,6 +306,71 @@ REFO_API void refo_spheres_intersect(void *h, const float *o, const float *d, ui
             if (s->spheres[j]->intersects(r, off, checkShadow != 0)) id = (int)j;
         outId[i] = id;
         outT[i] = off;
+    });
+}
+
+namespace {
+struct RefPlanes {
+    std::vector<Plane *> planes;
+    std::vector<Material *> materials;
+    ~RefPlanes()
+    {
+        for (auto *p : planes) delete p;
+        for (auto *m : materials) delete m;
+    }
+};
+}  // namespace
+
+// Planes built with the reference's Plane(bottomLeftCorner, axisX, axisY, normal) constructor
+// (Plane.cu:26-50), 12 floats each; glass=1 makes one transparent for shadow rays.
+REFO_API void *refo_planes_build(const float *p12, const uint8_t *glass, uint32_t n)
+{
+    RefPlanes *s = new RefPlanes();
+    for (uint32_t i = 0; i < n; i++) {
+        const float *p = p12 + 12 * i;
+        Plane *pl = new Plane(Point3f(p[0], p[1], p[2]), Vector3f(p[3], p[4], p[5]), Vector3f(p[6], p[7], p[8]),
+                              Vector3f(p[9], p[10], p[11]));
+        Material *m = (glass && glass[i]) ? (Material *)new GlassMaterial(Spectrum(1.0))
+                                          : (Material *)new LambertianMaterial(Spectrum(0.8));
+        pl->setMaterial(m);
+        s->planes.push_back(pl);
+        s->materials.push_back(m);
+    }
+    return s;
+}
+
+REFO_API void refo_planes_free(void *h) { delete static_cast<RefPlanes *>(h); }
+
+// Both matrices the reference stores for plane i (row-major 4x4, objectToWorld then worldToObject).
+REFO_API void refo_plane_matrices(void *h, uint32_t i, float *o2w, float *w2o)
+{
+    struct Peek : public Plane {
+        using Plane::objectToWorld;
+        using Plane::worldToObject;
+    };
+    Peek *p = static_cast<Peek *>(static_cast<RefPlanes *>(h)->planes[i]);
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) {
+            o2w[4 * r + c] = p->objectToWorld.m[r][c];
+            w2o[4 * r + c] = p->worldToObject.m[r][c];
+        }
+}
+
+// Scene::intersects' shape loop (Scene.cu:141-146) over these planes, starting from the offset
+// in t_inout (INFINITY, or a triangle hit's offset): each Plane::intersects that lowers the
+// running offset replaces the hit. outId: the last plane that did (-1: none).
+REFO_API void refo_planes_intersect(void *h, const float *o, const float *d, uint64_t n, int checkShadow,
+                                    int32_t *outId, float *t_inout, int nthreads)
+{
+    RefPlanes *s = static_cast<RefPlanes *>(h);
+    parallel_for(n, nthreads, [&](uint64_t i) {
+        Ray r = make_ray(o + 3 * i, d + 3 * i, INFINITY);
+        Float off = t_inout[i];
+        int id = -1;
+        for (size_t j = 0; j < s->planes.size(); j++)
+            if (s->planes[j]->intersects(r, off, checkShadow != 0)) id = (int)j;
+        outId[i] = id;
+        t_inout[i] = off;
     });
 }
 

@@ -93,6 +93,52 @@ def test_statistical_parity_with_reference_integrator(core, gpu_ctx, tmp_path):
     assert rel < 0.01
 
 
+def test_analytic_planes_match_the_reference_integrator(core, gpu_ctx, refo, tmp_path):
+    """The same box with its walls as analytic planes (rt_scene_add_plane with the reference's
+    own Plane matrices and Plane::intersects arithmetic) instead of triangles: the per-tile
+    z-test against the reference integrator as above."""
+    from oracle import bindings
+
+    try:
+        ref = bindings.RefRender()
+    except FileNotFoundError as e:
+        pytest.skip(str(e))
+    path = tmp_path / "box.obejota"
+    path.write_text(OBEJOTA)
+    runs = 8
+    ref_imgs = []
+    for _ in range(runs):
+        img, c2w, r2c = ref.render(path, PLANES, KD)
+        ref_imgs.append(img)
+    w, h, spp, depth = ref.width, ref.height, ref.spp, ref.depth
+    rp = bindings.RefPlanes(refo, PLANES)
+    sc = core.Scene(gpu_ctx)
+    sc.set_materials([core.material(N.RT_MAT_LAMBERTIAN, color=k) for k in KD])
+    for i in range(len(PLANES)):
+        o2w, w2o = rp.matrices(i)
+        sc.add_plane(o2w, w2o, material=i, shape_id=i)
+    sc.add_point_light(*LIGHT)
+    sc.commit()
+    cam = N.Camera()
+    cam.camera_to_world[:] = [float(x) for x in c2w.reshape(-1)]
+    cam.raster_to_camera[:] = [float(x) for x in r2c.reshape(-1)]
+    cam.lens_radius, cam.focal_distance, cam.width, cam.height = 0.0, 0.0, w, h
+    my_imgs = []
+    for r in range(runs):
+        film, _ = sc.render(cam, spp=spp, max_depth=depth, rr_depth=3, seed=900 + r, flags=N.RT_RENDER_COMPAT,
+                            fp64=True)
+        my_imgs.append(core.film_mean(film))
+    R = np.stack([tiles(i, w, h) for i in ref_imgs])
+    M = np.stack([tiles(i, w, h) for i in my_imgs])
+    se = np.sqrt(R.var(axis=0, ddof=1) / runs + M.var(axis=0, ddof=1) / runs)
+    z = (M.mean(0) - R.mean(0)) / np.maximum(se, 1e-12)
+    zs = z[se > 0]
+    assert np.abs(zs).mean() < 1.2
+    assert (np.abs(zs) > 4).mean() < 0.01
+    assert abs(zs.mean()) < 0.25
+    assert abs(M.mean() - R.mean()) / R.mean() < 0.01
+
+
 def test_compat_layer_is_a_drop_in_for_the_reference_integrator(tmp_path):
     """The same reference objects (its Plane, LambertianMaterial, loadObejota camera, film and
     point light) through include/rt_b200_compat.hpp — rtb::Scene::build and

@@ -333,3 +333,69 @@ def test_trace_any_empty_and_invalid(core, gpu_ctx):
     bits = torch.zeros(2, dtype=torch.int32, device="cuda")
     with pytest.raises(N.RtError):  # a bit mask must be 4-byte aligned
         N.check(N.lib().rt_trace_any_bits(sc.handle, rd.data_ptr(), 1, bits.data_ptr() + 2, 0))
+
+
+def plane_cases():
+    """Planes as the reference constructs them (corner, axisX, axisY, normal): unit squares, a
+    2.7 x 2.2 one (the reference truncates axis lengths to integers, Plane.cu:32-33), a tilted one
+    and a glass one (transparent to shadow rays)."""
+    return np.array([
+        [0.5, -0.5, -0.5, 0, 1, 0, 0, 0, 1, -0.5, 0, 0],
+        [-0.5, -0.5, 0.5, 1, 0, 0, 0, 1, 0, 0, 0, -0.5],
+        [-1.3, -1.1, -0.9, 2.7, 0, 0, 0, 0, 2.2, 0, 1, 0],
+        [-0.4, 0.3, -0.2, 0.8, 0.6, 0, -0.36, 0.48, 0.8, 0.48, -0.64, 0.6],
+        [-0.5, -0.5, -0.1, 1, 0, 0, 0, 1, 0, 0, 0, 1]], np.float32)
+
+
+def plane_rays(n, seed):
+    """Random rays, rays aimed at the squares' interiors and edges, rays with no x component
+    (the reference's offset divides by it: those never hit, Ray.cu:69-72) and grazing rays."""
+    o, d = S.random_rays(n, seed=seed, lo=-1.5, hi=1.5)
+    rng = np.random.default_rng(seed)
+    k = n // 4
+    d[:k, 0] = 0.0                                    # no x component
+    d[k:2 * k, 2] = rng.uniform(-1e-6, 1e-6, k)         # grazing the z = const planes
+    tgt = rng.uniform(-0.6, 0.6, (k, 3)).astype(np.float32)
+    tgt[:, 2] = np.round(tgt[:, 2] * 2) / 2             # edges and corners of the unit squares
+    d[2 * k:3 * k] = tgt - o[2 * k:3 * k]
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return o.astype(np.float32), d.astype(np.float32)
+
+
+def test_planes_match_reference(core, gpu_ctx, refo):
+    """rt_scene_add_plane: closest hits of analytic planes equal the reference's own
+    Plane::intersects (ids and offsets bit for bit), alone and behind a triangle mesh, in the
+    order Scene::intersects tests them (Scene.cu:130-146), shadow mode included."""
+    from oracle import bindings
+
+    P = plane_cases()
+    glass = np.array([0, 0, 0, 0, 1], np.uint8)
+    rp = bindings.RefPlanes(refo, P, glass)
+    o, d = plane_rays(40000, seed=21)
+    for with_mesh in (False, True):
+        sc = core.Scene(gpu_ctx)
+        if with_mesh:
+            v, f = cases.soup(3000, 5, size=0.15)
+            sc.add_mesh(v, f)
+        for j in range(len(P)):
+            o2w, w2o = rp.matrices(j)
+            N.check(N.lib().rt_scene_add_plane(sc.handle, o2w.ctypes.data, w2o.ctypes.data, 0, j, int(glass[j]), None))
+        sc.commit()
+        for shadow in (False, True):
+            t0 = None
+            tri = np.full(len(o), -1, np.int32)
+            if with_mesh:
+                rb = refo.bvh(v, f, np.zeros(f.shape[0], np.uint8))
+                tri = rb.intersect(o, d, shadow=shadow)
+                t0 = np.where(tri >= 0, rb.hit_t(tri, o, d), np.inf).astype(np.float32)
+            pid, pt = rp.intersect(o, d, t_init=t0, shadow=shadow)
+            want = np.where(pid >= 0, N.RT_PRIM_SHAPE | pid, tri)
+            ids, t, h = trace_gpu(sc, o, d, flags=N.RT_TRACE_SHADOW if shadow else 0)
+            assert np.array_equal(ids, want), (with_mesh, shadow, int((ids != want).sum()))
+            hit = want >= 0
+            assert np.array_equal(t[hit], pt[hit] if not with_mesh else np.where(pid >= 0, pt, t0)[hit])
+            plane_hits = (want >= 0) & (want >= N.RT_PRIM_SHAPE)
+            assert plane_hits.mean() > 0.1
+            # a plane hit reports its object-space (x, y) in the unit square
+            assert np.all((h["b1"][plane_hits] >= 0) & (h["b1"][plane_hits] <= 1))
+        sc.close()
