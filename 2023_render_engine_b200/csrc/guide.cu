@@ -282,6 +282,418 @@ __global__ void __launch_bounds__(128) k_guide_wgrad(const __half *xt, const __h
     }
 }
 
+// ------------------------------------------------------------------ training on tcgen05
+//
+// k_guide_train_tc: the forward and backward passes of 128-row tiles on the 5th-generation tensor
+// cores, two independent 128-thread groups per CTA sharing one copy of the weights in shared
+// memory. Per layer one thread issues tcgen05.mma (M = 128 rows, FP16 operands in K-major core
+// matrices, FP32 accumulator in the group's 64 TMEM columns) and commits to the group's
+// mbarrier; every thread then reads its own row back (tcgen05.ld), applies bias and ReLU (forward)
+// or the ReLU mask (backward) and writes the next operand. The forward operand is W_l^T (the
+// inference staging); the backward operand is W_l itself, restaged once per CTA. Each thread
+// keeps its row's ReLU signs as bit masks, so only two operand buffers per group are needed.
+// Every layer input X_l and output gradient G_l is also written feature-major (planes of Bp rows)
+// for the weight gradient.
+constexpr int kFbGroups = 2;
+constexpr int kFbWb = 50432;  // backward weights W_1..W_4 (64 rows of out_l halves), 8 KB slots
+__host__ __device__ constexpr int fb_wb(int l) { return kFbWb + (l - 1) * 8192; }
+constexpr int kFbGroup0 = kFbWb + 4 * 8192;
+constexpr int kFbBufA = 128 * kGuideIn * 2;  // X_0 (144 halves per row); later X_2, X_4, G_3, G_1
+constexpr int kFbBufB = 128 * 64 * 2;        // X_1, X_3, G_4, G_2
+constexpr int kFbGroupBytes = kFbBufA + kFbBufB;
+constexpr int kFbBar = kFbGroup0 + kFbGroups * kFbGroupBytes;
+constexpr int kFbSmem = kFbBar + 8 * kFbGroups + 16;
+constexpr int kFbTmemCols = 64 * kFbGroups;
+static_assert(kTcBias + 4 * (4 * 64 + 48) <= kFbWb && kFbGroup0 % 128 == 0 && kFbBar % 8 == 0, "train layout");
+static_assert(kFbSmem <= 227 * 1024, "training shared memory");
+
+// one M = 128 pass of layer operands: D[tmem] = A (kc_a chunks per row) * B^T over `ksteps`
+// K = 16 steps, issued by the calling thread and committed to `bar`
+__device__ __forceinline__ void fb_mma(uint32_t tmem, uint32_t a0, uint32_t kca, uint32_t b0, uint32_t kcb, int ksteps,
+                                       int n, uint64_t *bar)
+{
+    const uint32_t idesc = umma_idesc_f16(128, n);
+    for (int s = 0; s < ksteps; s++)
+        umma_f16(tmem, umma_desc(a0 + 256u * s, 128u, 128u * kca), umma_desc(b0 + 256u * s, 128u, 128u * kcb), idesc,
+                 s > 0 ? 1u : 0u);
+    umma_commit(bar);
+}
+
+// FP16 pair of a row to the feature-major planes: dst[f * Bp + row], dst[(f + 1) * Bp + row]
+__device__ __forceinline__ void plane_store2(__half *dst, uint64_t Bp, int f, uint64_t row, uint32_t h2)
+{
+    const __half2 v = *reinterpret_cast<const __half2 *>(&h2);
+    dst[(uint64_t)f * Bp + row] = __low2half(v);
+    dst[(uint64_t)(f + 1) * Bp + row] = __high2half(v);
+}
+
+__global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uint4 *img, TrainArgs A)
+{
+    extern __shared__ __align__(128) unsigned char fb_smem[];
+    unsigned char *sm = fb_smem;
+    __shared__ double wsum;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int grp = tid >> 7, gt = tid & 127;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kFbBar) + grp;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kFbBar + 8 * kFbGroups);
+    const unsigned char *ib = reinterpret_cast<const unsigned char *>(img);
+    // forward weights (W_l^T) and biases, as the inference kernel stages them
+#pragma unroll 1
+    for (int l = 0; l < kGuideLayers; l++) {
+        const int kc = guide_in(l) / 8, nrows = guide_out(l);
+        for (int i = tid; i < nrows * kc; i += blockDim.x) {
+            const int r = i / kc, c = i - r * kc;
+            *reinterpret_cast<uint4 *>(sm + tc_w(l) + tc_chunk(r, c, kc)) =
+                *reinterpret_cast<const uint4 *>(ib + 2 * (guide_iw(l) + r * guide_stride(l)) + 16 * c);
+        }
+    }
+    for (int i = tid; i < (4 * 64 + 48) / 4; i += blockDim.x)
+        reinterpret_cast<uint4 *>(sm + kTcBias)[i] = reinterpret_cast<const uint4 *>(ib + kGuideImgBias)[i];
+    // backward weights W_l (l = 1..4): row i (input), chunk c = outputs 8c .. 8c + 7
+    const __half *ih = reinterpret_cast<const __half *>(img);
+#pragma unroll 1
+    for (int l = 1; l < kGuideLayers; l++) {
+        const int kc = guide_out(l) / 8;
+        for (int i = tid; i < 64 * kc; i += blockDim.x) {
+            const int r = i / kc, c = i - r * kc;
+            uint32_t w[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const __half lo = ih[guide_iw(l) + (8 * c + 2 * j) * guide_stride(l) + r];
+                const __half hi = ih[guide_iw(l) + (8 * c + 2 * j + 1) * guide_stride(l) + r];
+                w[j] = pack_h2(lo, hi);
+            }
+            *reinterpret_cast<uint4 *>(sm + fb_wb(l) + tc_chunk(r, c, kc)) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+    if (tid < 32) {
+        double sw = 0.0;
+        for (int i = tid; i < kWsumBlocks; i += 32) sw += A.wpart[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sw += __shfl_xor_sync(0xffffffffu, sw, o);
+        if (tid == 0) wsum = sw;
+    }
+    if (gt == 0) mbar_init(bar, 1);
+    __syncwarp();
+    if (warp == 0) tmem_alloc(tslot, kFbTmemCols);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot + (uint32_t)(64 * grp);
+    const uint32_t tlane = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    const uint32_t bar_id = 1u + (uint32_t)grp;
+    const float *bias = reinterpret_cast<const float *>(sm + kTcBias);
+    unsigned char *bufA = sm + kFbGroup0 + grp * kFbGroupBytes, *bufB = bufA + kFbBufA;
+    const uint32_t aA = smem_u32(bufA), aB = smem_u32(bufB);
+    const float wmean = A.B ? (float)(wsum / (double)A.B) : 0.f;
+    const float winv = wmean > 0.f ? 1.f / wmean : 0.f;
+    const uint64_t Bp = A.Bpad;
+    float lsum = 0.f;
+    uint32_t phase = 0;
+    bool failed = false;
+    // waits for this group's MMA batch; false (for the whole group) when a wait ran out
+    auto wait_mma = [&]() -> bool {
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar, phase, kUmmaWaitPolls));
+        phase ^= 1u;
+        tc_fence_after();
+        return !group_sync_or(bar_id, !ok);
+    };
+    // the operand just written becomes visible to the tensor core; thread 0 of the group issues
+    auto issue = [&](uint32_t a0, uint32_t kca, uint32_t b0, uint32_t kcb, int ksteps, int n) {
+        fence_async_smem();
+        tc_fence_before();
+        group_sync_or(bar_id, false);
+        if (gt == 0) {
+            tc_fence_after();
+            fb_mma(tmem, a0, kca, b0, kcb, ksteps, n, bar);
+        }
+    };
+    const uint32_t stride = gridDim.x * kFbGroups;
+    for (uint64_t tile = (uint64_t)blockIdx.x * kFbGroups + grp; !failed && tile * 128 < Bp; tile += stride) {
+        const uint64_t row = tile * 128 + gt;
+        const bool in_b = row < A.B, in_p = row < Bp;
+        float q[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) q[i] = in_b ? A.q[9 * row + i] : 0.f;
+        {
+            __half2 e[72];
+            guide_encode(0, q, A.box, e);
+            guide_encode(1, q, A.box, e);
+#pragma unroll
+            for (int c = 0; c < kGuideIn / 8; c++)
+                *reinterpret_cast<uint4 *>(bufA + tc_chunk(gt, c, kGuideIn / 8)) =
+                    *reinterpret_cast<const uint4 *>(&e[4 * c]);
+            if (in_p)
+#pragma unroll 4
+                for (int j = 0; j < 72; j++)
+                    plane_store2(A.xt, Bp, 2 * j, row, *reinterpret_cast<const uint32_t *>(&e[j]));
+        }
+        // forward: X_0 (A) -> X_1 (B) -> X_2 (A) -> X_3 (B) -> X_4 (A) -> outputs
+        uint32_t mask[4][2];
+#pragma unroll 1
+        for (int l = 0; l < kGuideLayers - 1 && !failed; l++) {
+            const uint32_t src = (l & 1) ? aB : aA;
+            unsigned char *dst = (l & 1) ? bufA : bufB;
+            issue(src, guide_in(l) / 8, smem_u32(sm + tc_w(l)), guide_in(l) / 8, guide_in(l) / 16, 64);
+            if (!wait_mma()) {
+                failed = true;
+                break;
+            }
+            const float *b = bias + guide_ib(l);
+            uint32_t m0 = 0, m1 = 0;
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                float v[16];
+                tmem_ld16(tlane + 16u * h, v);
+                uint32_t w[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    w[j] = relu_half2(v[2 * j] + b[16 * h + 2 * j], v[2 * j + 1] + b[16 * h + 2 * j + 1]);
+                    const __half2 hv = *reinterpret_cast<const __half2 *>(&w[j]);
+                    const uint32_t bits = (__low2float(hv) > 0.f ? 1u : 0u) | (__high2float(hv) > 0.f ? 2u : 0u);
+                    const int f = 16 * h + 2 * j;
+                    if (f < 32)
+                        m0 |= bits << f;
+                    else
+                        m1 |= bits << (f - 32);
+                    if (in_p) plane_store2(A.xt + (uint64_t)guide_xoff(l + 1) * Bp, Bp, f, row, w[j]);
+                }
+                *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h, 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+                *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h + 1, 8)) = make_uint4(w[4], w[5], w[6], w[7]);
+            }
+            mask[l][0] = m0;
+            mask[l][1] = m1;
+        }
+        if (failed) break;
+        issue(aA, 8, smem_u32(sm + tc_w(4)), 8, 4, kGuideOut);
+        if (!wait_mma()) {
+            failed = true;
+            break;
+        }
+        {
+            float o[kGuideOut];
+#pragma unroll
+            for (int h = 0; h < kGuideOut / 16; h++) tmem_ld16(tlane + 16u * h, o + 16 * h);
+            const float *b = bias + guide_ib(4);
+#pragma unroll
+            for (int j = 0; j < kGuideOut; j++) o[j] += b[j];
+            float dout[kGuideOut];
+            if (in_b) {
+                const float wt = fminf(A.w[row] * winv, kGuideWeightClip);
+                const V3 wi = v3(A.dir[3 * row], A.dir[3 * row + 1], A.dir[3 * row + 2]);
+                lsum += guide_loss_grad(o, wi, A.pdf[row], wt, dout);
+            } else {
+#pragma unroll
+                for (int j = 0; j < kGuideOut; j++) dout[j] = 0.f;
+            }
+            uint32_t w[kGuideOut / 2];
+#pragma unroll
+            for (int j = 0; j < kGuideOut / 2; j++) {
+                const __half2 hv =
+                    __floats2half2_rn(dout[2 * j] * (1.f / kGuideGradScale), dout[2 * j + 1] * (1.f / kGuideGradScale));
+                w[j] = *reinterpret_cast<const uint32_t *>(&hv);
+                if (in_p) plane_store2(A.gt + (uint64_t)guide_goff(4) * Bp, Bp, 2 * j, row, w[j]);
+            }
+#pragma unroll
+            for (int c = 0; c < kGuideOut / 8; c++)
+                *reinterpret_cast<uint4 *>(bufB + tc_chunk(gt, c, kGuideOut / 8)) =
+                    make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+        }
+        // backward: G_4 (B) -> G_3 (A) -> G_2 (B) -> G_1 (A) -> G_0 (planes only)
+#pragma unroll 1
+        for (int l = kGuideLayers - 1; l >= 1 && !failed; l--) {
+            const uint32_t src = (l & 1) ? aA : aB;  // l = 4: G_4 in B; 3: G_3 in A; ...
+            unsigned char *dst = (l & 1) ? bufB : bufA;
+            const int kco = guide_out(l) / 8;
+            issue(src, kco, smem_u32(sm + fb_wb(l)), kco, guide_out(l) / 16, 64);
+            if (!wait_mma()) {
+                failed = true;
+                break;
+            }
+            const uint32_t m0 = mask[l - 1][0], m1 = mask[l - 1][1];
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                float v[16];
+                tmem_ld16(tlane + 16u * h, v);
+                uint32_t w[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const int f = 16 * h + 2 * j;
+                    const uint32_t bits = f < 32 ? (m0 >> f) : (m1 >> (f - 32));
+                    const __half2 hv = __floats2half2_rn((bits & 1u) ? v[2 * j] : 0.f, (bits & 2u) ? v[2 * j + 1] : 0.f);
+                    w[j] = *reinterpret_cast<const uint32_t *>(&hv);
+                    if (in_p) plane_store2(A.gt + (uint64_t)guide_goff(l - 1) * Bp, Bp, f, row, w[j]);
+                }
+                if (l > 1) {
+                    *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h, 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+                    *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h + 1, 8)) = make_uint4(w[4], w[5], w[6], w[7]);
+                }
+            }
+        }
+    }
+    if (failed) {
+        if (gt == 0) atomicOr(reinterpret_cast<uint32_t *>(A.scal) + 2, 2u);  // tensor-core wait ran out
+        mbar_wait_bounded(bar, phase ^ 1u, kUmmaWaitPolls);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    if (lane == 0 && lsum != 0.f) atomicAdd(A.scal + 1, lsum);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) {
+        __syncwarp();
+        tmem_dealloc(*tslot, kFbTmemCols);
+    }
+}
+
+// k_guide_wgrad_tc: dW_l^T = G_l^T X_l over a chunk of rows, all five layers, on tcgen05. The
+// feature-major planes are K-major operands with the rows as K: A = G_l^T (M = 128 lanes, the
+// out_l valid ones first; the rest of the tile is the next layer's rows or unused bytes, whose
+// products land in TMEM lanes nobody reads), B = X_l^T (N = in_l). Stages of 64 rows are loaded
+// into one of two shared-memory buffers while the tensor core works on the other; the five
+// accumulators (144 + 4 x 64 TMEM columns) stay in TMEM for the whole chunk, which then writes
+// its FP32 partial dW in the master layout.
+constexpr uint32_t kTcWgradChunk = 2048;  // rows per CTA
+constexpr int kWgStageA = 5 * 8192 + 8192;         // G^T tiles: layer l at l * 8 KB (64 valid rows)
+constexpr int kWgStageB = 18 * 1024 + 4 * 8192;    // X^T tiles: layer 0 (144 rows), layers 1-4 (64)
+constexpr int kWgStage = kWgStageA + kWgStageB;
+constexpr int kWgBar = 2 * kWgStage;
+constexpr int kWgSmem = kWgBar + 16 + 16;
+constexpr int kWgTmemCols = 512;
+static_assert(kWgSmem <= 227 * 1024, "weight-gradient shared memory");
+__host__ __device__ constexpr int wg_b(int l) { return kWgStageA + (l == 0 ? 0 : 18 * 1024 + (l - 1) * 8192); }
+__host__ __device__ constexpr int wg_col(int l) { return l == 0 ? 0 : kGuideIn + (l - 1) * 64; }
+
+__global__ void __launch_bounds__(128, 1) k_guide_wgrad_tc(const __half *xt, const __half *gt, uint64_t Bp,
+                                                           float *partial, float *scal)
+{
+    extern __shared__ __align__(128) unsigned char wg_smem[];
+    unsigned char *sm = wg_smem;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kWgBar);  // one per buffer
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kWgBar + 16);
+    const uint64_t r0 = (uint64_t)blockIdx.x * kTcWgradChunk;
+    const uint64_t r1 = r0 + kTcWgradChunk < Bp ? r0 + kTcWgradChunk : Bp;
+    const int nstages = (int)((r1 - r0) / 64);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+    }
+    __syncwarp();
+    if (warp == 0) tmem_alloc(tslot, kWgTmemCols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    uint32_t phase[2] = {0u, 0u};
+    bool failed = false;
+    for (int s = 0; s < nstages && !failed; s++) {
+        const int b = s & 1;
+        unsigned char *buf = sm + b * kWgStage;
+        if (s >= 2) {  // the MMAs of stage s - 2 read this buffer
+            const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar + b, phase[b], kUmmaWaitPolls));
+            phase[b] ^= 1u;
+            failed = __syncthreads_or(!ok) != 0;
+            if (failed) break;
+        }
+        const uint64_t rs = r0 + 64ull * s;
+        // G^T: 304 features x 8 chunks of 8 rows; X^T: 400 features x 8 chunks
+        for (int i = tid; i < kGuideGFeatures * 8; i += 128) {
+            const int f = i >> 3, c = i & 7;
+            const int l = f < 4 * kGuideHidden ? f / kGuideHidden : 4, fl = f - guide_goff(l);
+            *reinterpret_cast<uint4 *>(buf + l * 8192 + tc_chunk(fl, c, 8)) =
+                __ldg(reinterpret_cast<const uint4 *>(gt + (uint64_t)f * Bp + rs) + c);
+        }
+        for (int i = tid; i < kGuideXFeatures * 8; i += 128) {
+            const int f = i >> 3, c = i & 7;
+            const int l = f < kGuideIn ? 0 : 1 + (f - kGuideIn) / kGuideHidden, fl = f - guide_xoff(l);
+            *reinterpret_cast<uint4 *>(buf + wg_b(l) + tc_chunk(fl, c, 8)) =
+                __ldg(reinterpret_cast<const uint4 *>(xt + (uint64_t)f * Bp + rs) + c);
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t base = smem_u32(buf);
+#pragma unroll 1
+            for (int l = 0; l < kGuideLayers; l++) {
+                const uint32_t idesc = umma_idesc_f16(128, guide_in(l));
+                for (int k = 0; k < 4; k++)
+                    umma_f16(tmem + (uint32_t)wg_col(l), umma_desc(base + l * 8192 + 256u * k, 128u, 1024u),
+                             umma_desc(base + wg_b(l) + 256u * k, 128u, 1024u), idesc, (s > 0 || k > 0) ? 1u : 0u);
+            }
+            umma_commit(bar + b);
+        }
+    }
+    // the last batch of each buffer
+    for (int b = 0; b < 2 && !failed; b++) {
+        const int last = nstages - 1 - ((nstages - 1 - b) & 1);  // latest stage that used buffer b
+        if (last < 0 || last < nstages - 2) continue;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar + b, phase[b], kUmmaWaitPolls));
+        phase[b] ^= 1u;
+        failed = __syncthreads_or(!ok) != 0;
+    }
+    tc_fence_after();
+    float *part = partial + (uint64_t)blockIdx.x * kGuideParamCount;
+    if (!failed && warp < 2) {  // TMEM lanes 0..63: the output features
+        const int o = 32 * warp + (tid & 31);
+        const uint32_t tl = tmem + ((uint32_t)(32 * warp) << 16);
+#pragma unroll 1
+        for (int l = 0; l < kGuideLayers; l++) {
+            const int nin = guide_in(l), out = guide_out(l);
+            for (int c0 = 0; c0 < nin; c0 += 16) {
+                float v[16];
+                tmem_ld16(tl + (uint32_t)(wg_col(l) + c0), v);
+                if (o < out)
+#pragma unroll
+                    for (int j = 0; j < 16; j++) part[guide_pw(l) + (c0 + j) * out + o] = v[j];
+            }
+        }
+    }
+    if (failed) {
+        if (tid == 0) atomicOr(reinterpret_cast<uint32_t *>(scal) + 2, 2u);
+        for (int b = 0; b < 2; b++) mbar_wait_bounded(bar + b, phase[b], kUmmaWaitPolls);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) {
+        __syncwarp();
+        tmem_dealloc(tmem, kWgTmemCols);
+    }
+}
+
+// db_l = sum of G_l over the chunk's rows (feature-major planes), one warp per 8 features
+__global__ void __launch_bounds__(256) k_guide_bias_grad(const __half *gt, uint64_t Bp, float *partial)
+{
+    const uint64_t r0 = (uint64_t)blockIdx.x * kTcWgradChunk;
+    const uint64_t r1 = r0 + kTcWgradChunk < Bp ? r0 + kTcWgradChunk : Bp;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *part = partial + (uint64_t)blockIdx.x * kGuideParamCount;
+    for (int f = blockIdx.y * 64 + warp; f < kGuideGFeatures && f < (int)blockIdx.y * 64 + 64; f += 8) {
+        const uint4 *g4 = reinterpret_cast<const uint4 *>(gt + (uint64_t)f * Bp + r0);
+        float s = 0.f;
+        for (uint64_t i = lane; i < (r1 - r0) / 8; i += 32) {
+            const uint4 v = __ldg(g4 + i);
+            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float2 h = __half22float2(*reinterpret_cast<const __half2 *>(&w[k]));
+                s += h.x + h.y;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            const int l = f < 4 * kGuideHidden ? f / kGuideHidden : 4;
+            part[guide_pb(l) + (f - guide_goff(l))] = s;
+        }
+    }
+}
+
 // partial sums of the sample weights (double, fixed order); block 0 also clears the loss
 // sum and the non-finite flag of this step
 __global__ void __launch_bounds__(256) k_guide_wsum(const float *w, uint64_t B, double *part, float *scal)
@@ -494,8 +906,8 @@ int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf,
         if (grad_host) std::memset(grad_host, 0, 4ull * kGuideParamCount);
         return RT_OK;
     }
-    const uint64_t Bp = (B + 31) / 32 * 32;
-    const uint32_t nchunks = (uint32_t)((Bp + kWgradChunk - 1) / kWgradChunk);
+    const uint64_t Bp = (B + 127) / 128 * 128;  // whole 128-row tiles
+    const uint32_t nchunks = (uint32_t)((Bp + kTcWgradChunk - 1) / kTcWgradChunk);
     RTB_CHECK(g->xt.reserve(2ull * kGuideXFeatures * Bp));
     RTB_CHECK(g->gt.reserve(2ull * kGuideGFeatures * Bp));
     RTB_CHECK(g->partial.reserve(4ull * kGuideParamCount * nchunks));
@@ -507,17 +919,21 @@ int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf,
     k_guide_wsum<<<kWsumBlocks, 256, 0, st>>>(w, B, wpart, scal);
     RTB_CUDA(cudaGetLastError());
     if (!(device_slot(SLOT_SMEM_ATTRS) & SMEM_GUIDE_TRAIN)) {
-        RTB_CUDA(cudaFuncSetAttribute(k_guide_train_fb, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem));
+        RTB_CUDA(cudaFuncSetAttribute(k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kFbSmem));
+        RTB_CUDA(cudaFuncSetAttribute(k_guide_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem));
         or_device_slot(SLOT_SMEM_ATTRS, SMEM_GUIDE_TRAIN);
     }
     TrainArgs a{q, dir, pdf, w, B, Bp, g->xt.as<__half>(), g->gt.as<__half>(), scal, wpart, guide_box(g)};
-    const uint64_t tiles = Bp / 16;
+    const uint64_t tiles = Bp / 128;
     const unsigned grid =
-        (unsigned)std::min<uint64_t>((tiles + kTrainWarps - 1) / kTrainWarps, (uint64_t)std::max(g->ctx->sm_count, 1));
-    k_guide_train_fb<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(g->img.as<uint4>(), a);
+        (unsigned)std::min<uint64_t>((tiles + kFbGroups - 1) / kFbGroups, (uint64_t)std::max(g->ctx->sm_count, 1));
+    k_guide_train_tc<<<grid, 128 * kFbGroups, kFbSmem, st>>>(g->img.as<uint4>(), a);
     RTB_CUDA(cudaGetLastError());
-    k_guide_wgrad<<<dim3(nchunks, (kWgradItems + 3) / 4), 128, 0, st>>>(g->xt.as<__half>(), g->gt.as<__half>(), Bp,
-                                                                   g->partial.as<float>());
+    k_guide_wgrad_tc<<<nchunks, 128, kWgSmem, st>>>(g->xt.as<__half>(), g->gt.as<__half>(), Bp, g->partial.as<float>(),
+                                                    scal);
+    RTB_CUDA(cudaGetLastError());
+    k_guide_bias_grad<<<dim3(nchunks, (kGuideGFeatures + 63) / 64), 256, 0, st>>>(g->gt.as<__half>(), Bp,
+                                                                              g->partial.as<float>());
     RTB_CUDA(cudaGetLastError());
     const unsigned pblocks = (kGuideParamCount + 255) / 256;
     k_guide_reduce<<<pblocks, 256, 0, st>>>(g->partial.as<float>(), nchunks, kGuideGradScale / (float)B,
@@ -540,6 +956,8 @@ int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf,
         if (grad_host)
             RTB_CUDA(cudaMemcpyAsync(grad_host, g->grad.ptr, 4ull * kGuideParamCount, cudaMemcpyDeviceToHost, st));
         RTB_CUDA(cudaStreamSynchronize(st));
+        if (static_cast<const uint32_t *>(g->host_scal)[2] & 2u)
+            return fail(RT_ERR_TIMEOUT, "guide training: a tensor-core completion wait timed out");
         if (loss_out) *loss_out = static_cast<const float *>(g->host_scal)[1] / (float)B;
     }
     return RT_OK;

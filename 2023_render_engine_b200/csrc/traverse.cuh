@@ -30,11 +30,44 @@ struct Best {
 
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xFFu; }
 
+// L2 residency of the scene against the streamed rays and hits. With RTB_TRAV_L2HINT the node and
+// triangle-record loads carry an evict-last cache policy and the ray loads are evict-first
+// (streaming): a call over more rays than L2 holds then re-reads the scene less.
+#ifdef RTB_TRAV_L2HINT
+__device__ __forceinline__ uint64_t scene_policy()
+{
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint4 ld_scene(const uint4 *ptr)
+{
+    uint4 r;
+    asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+        : "l"(ptr), "l"(scene_policy()));
+    return r;
+}
+__device__ __forceinline__ float4 ld_scene(const float4 *ptr)
+{
+    float4 r;
+    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+        : "l"(ptr), "l"(scene_policy()));
+    return r;
+}
+__device__ __forceinline__ float4 ld_stream(const float4 *ptr) { return __ldcs(ptr); }
+#else
+__device__ __forceinline__ uint4 ld_scene(const uint4 *ptr) { return __ldg(ptr); }
+__device__ __forceinline__ float4 ld_scene(const float4 *ptr) { return __ldg(ptr); }
+__device__ __forceinline__ float4 ld_stream(const float4 *ptr) { return __ldg(ptr); }
+#endif
+
 __device__ __forceinline__ void load_ray(const rt_ray *rays, uint64_t i, float4 &a, float4 &b)
 {
     const float4 *r4 = reinterpret_cast<const float4 *>(rays);
-    a = __ldg(r4 + 2 * i);
-    b = __ldg(r4 + 2 * i + 1);
+    a = ld_stream(r4 + 2 * i);
+    b = ld_stream(r4 + 2 * i + 1);
 }
 
 // Tests one triangle record against the running best; see the file comment for the rule.
@@ -42,7 +75,7 @@ __device__ __forceinline__ void test_triangle(const WatertightRay &w, const TriR
                                               bool shadow, Best &best)
 {
     const float4 *p = reinterpret_cast<const float4 *>(tris + rec);
-    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    float4 a = ld_scene(p), b = ld_scene(p + 1), c = ld_scene(p + 2);
     if (shadow && (__float_as_uint(c.w) & 1u)) return;
     TriHit h;
     if (!watertight_test(w, a, b, c, h)) return;
@@ -147,7 +180,8 @@ __device__ __forceinline__ bool trav_step(const SceneView &v, Trav &T, bool anyh
         return true;
     }
     const uint4 *np = reinterpret_cast<const uint4 *>(v.nodes + T.cur);
-    const uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
+    const uint4 n0 = ld_scene(np), n1 = ld_scene(np + 1), n2 = ld_scene(np + 2), n3 = ld_scene(np + 3),
+                n4 = ld_scene(np + 4);
     const float sx = __uint_as_float((n0.w & 0xFFu) << 23);
     const float sy = __uint_as_float(((n0.w >> 8) & 0xFFu) << 23);
     const float sz = __uint_as_float(((n0.w >> 16) & 0xFFu) << 23);
