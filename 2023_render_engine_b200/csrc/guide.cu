@@ -1,12 +1,13 @@
 // Path-guide network: training on the tensor cores and the rt_guide_* entry points.
 //
-// One training step on B samples (rows padded to a multiple of 16):
+// One training step on B samples (rows padded to a multiple of 128), all contractions on the
+// 5th-generation tensor cores (tcgen05.mma, accumulators in TMEM):
 //   k_guide_wsum      partial sums of the sample weights (their mean normalises the loss)
-//   k_guide_train_fb  per 16-row warp tile: encode, forward (activations kept in shared
-//                     memory), loss gradient per row, backward through the 5 layers; writes
-//                     every layer's input and output gradient transposed (feature-major) so
-//                     the weight gradient is a plain tensor-core contraction over rows
-//   k_guide_wgrad     dW_l = X_l^T G_l and db_l = sum G_l per chunk of rows (FP32 partials)
+//   k_guide_train_tc  per 128-row tile: encode, forward, loss gradient per row, backward
+//                     through the 5 layers; writes every layer's input and output gradient
+//                     feature-major, so the weight gradient is a contraction over rows
+//   k_guide_wgrad_tc  dW_l = X_l^T G_l per chunk of rows (FP32 partials), all layers at once
+//   k_guide_bias_grad db_l = sum G_l per chunk of rows
 //   k_guide_reduce    sum of the chunk partials in a fixed order (deterministic gradient)
 //   k_guide_adam      Adam on the FP32 master weights; refreshes the FP16 image
 #include <cuda_fp16.h>
@@ -23,13 +24,6 @@ namespace rtb {
 
 namespace {
 
-constexpr int kTrainWarps = 8;  // 16 rows per warp
-constexpr int kTrainX0 = 0, kTrainH = 16 * 152 * 2, kTrainD = kTrainH + 4 * 16 * 72 * 2, kTrainO = kTrainD + 16 * 56 * 2;
-constexpr int kTrainWarpBytes = kTrainO + 16 * 49 * 4;
-constexpr int kTrainSmem = kGuideImgBytes + kTrainWarps * kTrainWarpBytes;
-static_assert(kTrainSmem <= 227 * 1024, "training kernel shared memory");
-constexpr uint32_t kWgradChunk = 1024;  // rows per weight-gradient block
-constexpr int kWgradItems = 28;         // 25 input-feature tiles + 3 bias groups
 constexpr int kWsumBlocks = 128;
 constexpr float kAdamB1 = 0.9f, kAdamB2 = 0.99f, kAdamEps = 1e-8f;
 
@@ -37,45 +31,6 @@ __device__ __forceinline__ uint32_t pack_h2(__half a, __half b)
 {
     __half2 h = __halves2half2(a, b);
     return *reinterpret_cast<uint32_t *>(&h);
-}
-
-// 16 rows x W features (stride S halves) -> feature-major planes dst[f * Bpad + row0 + r]
-template <int W, int S>
-__device__ __forceinline__ void store_t(const __half *buf, __half *dst, uint64_t Bpad, uint64_t row0, int lane)
-{
-#pragma unroll
-    for (int c = 2 * lane; c < W; c += 64) {
-        uint32_t lo[8], hi[8];
-#pragma unroll
-        for (int p = 0; p < 8; p++) {
-            const __half2 v0 = *reinterpret_cast<const __half2 *>(buf + (2 * p) * S + c);
-            const __half2 v1 = *reinterpret_cast<const __half2 *>(buf + (2 * p + 1) * S + c);
-            lo[p] = pack_h2(__low2half(v0), __low2half(v1));
-            hi[p] = pack_h2(__high2half(v0), __high2half(v1));
-        }
-        uint4 *d0 = reinterpret_cast<uint4 *>(dst + (uint64_t)c * Bpad + row0);
-        uint4 *d1 = reinterpret_cast<uint4 *>(dst + (uint64_t)(c + 1) * Bpad + row0);
-        d0[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-        d0[1] = make_uint4(lo[4], lo[5], lo[6], lo[7]);
-        d1[0] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-        d1[1] = make_uint4(hi[4], hi[5], hi[6], hi[7]);
-    }
-}
-
-// G_{l-1} = acc * [H > 0], written over H (same positions, so no lane reads another's)
-template <int N, int S>
-__device__ __forceinline__ void mask_store(const float (&acc)[1][N / 8][4], __half *H, int lane)
-{
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int nt = 0; nt < N / 8; nt++) {
-        const int n = nt * 8 + 2 * t;
-        __half2 *p0 = reinterpret_cast<__half2 *>(H + g * S + n);
-        __half2 *p1 = reinterpret_cast<__half2 *>(H + (g + 8) * S + n);
-        const float2 h0 = __half22float2(*p0), h1 = __half22float2(*p1);
-        *p0 = __floats2half2_rn(h0.x > 0.f ? acc[0][nt][0] : 0.f, h0.y > 0.f ? acc[0][nt][1] : 0.f);
-        *p1 = __floats2half2_rn(h1.x > 0.f ? acc[0][nt][2] : 0.f, h1.y > 0.f ? acc[0][nt][3] : 0.f);
-    }
 }
 
 struct TrainArgs {
@@ -86,201 +41,6 @@ struct TrainArgs {
     const double *wpart;  // kWsumBlocks partial sums of the weights
     GuideBox box;
 };
-
-__global__ void __launch_bounds__(kTrainWarps * 32, 1) k_guide_train_fb(const uint4 *img, TrainArgs A)
-{
-    extern __shared__ uint4 train_smem[];
-    __shared__ double wsum;
-    for (int i = threadIdx.x; i < kGuideImgBytes / 16; i += blockDim.x) train_smem[i] = img[i];
-    if (threadIdx.x < 32) {
-        double s = 0.0;
-        for (int i = threadIdx.x; i < kWsumBlocks; i += 32) s += A.wpart[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (threadIdx.x == 0) wsum = s;
-    }
-    __syncthreads();
-    unsigned char *sm = reinterpret_cast<unsigned char *>(train_smem);
-    const __half *W = reinterpret_cast<const __half *>(sm);
-    const float *bias = reinterpret_cast<const float *>(sm + kGuideImgBias);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char *wb = sm + kGuideImgBytes + warp * kTrainWarpBytes;
-    __half *X0 = reinterpret_cast<__half *>(wb + kTrainX0);
-    __half *H1 = reinterpret_cast<__half *>(wb + kTrainH);
-    __half *H2 = H1 + 16 * 72, *H3 = H2 + 16 * 72, *H4 = H3 + 16 * 72;
-    __half *D = reinterpret_cast<__half *>(wb + kTrainD);
-    float *O = reinterpret_cast<float *>(wb + kTrainO);
-    const float wmean = A.B ? (float)(wsum / (double)A.B) : 0.f;
-    const float winv = wmean > 0.f ? 1.f / wmean : 0.f;
-    const uint64_t Bp = A.Bpad;
-    float lsum = 0.f;
-    for (uint64_t tile = (uint64_t)blockIdx.x * kTrainWarps + warp; tile * 16 < Bp;
-         tile += (uint64_t)gridDim.x * kTrainWarps) {
-        const uint64_t row0 = tile * 16;
-        {
-            const uint64_t r = row0 + (lane & 15);
-            float q[9];
-#pragma unroll
-            for (int i = 0; i < 9; i++) q[i] = r < A.B ? A.q[9 * r + i] : 0.f;
-            guide_encode(lane >> 4, q, A.box, reinterpret_cast<__half2 *>(X0 + (lane & 15) * 152));
-        }
-        __syncwarp();
-        store_t<kGuideIn, 152>(X0, A.xt + (uint64_t)guide_xoff(0) * Bp, Bp, row0, lane);
-        {
-            float acc[1][8][4];
-            guide_gemm<1, kGuideIn, 64, 152, 152>(acc, X0, W + guide_iw(0), lane);
-            guide_store_hidden<1, 64, 72>(acc, bias + guide_ib(0), H1, lane);
-            __syncwarp();
-            store_t<64, 72>(H1, A.xt + (uint64_t)guide_xoff(1) * Bp, Bp, row0, lane);
-            guide_gemm<1, 64, 64, 72, 72>(acc, H1, W + guide_iw(1), lane);
-            guide_store_hidden<1, 64, 72>(acc, bias + guide_ib(1), H2, lane);
-            __syncwarp();
-            store_t<64, 72>(H2, A.xt + (uint64_t)guide_xoff(2) * Bp, Bp, row0, lane);
-            guide_gemm<1, 64, 64, 72, 72>(acc, H2, W + guide_iw(2), lane);
-            guide_store_hidden<1, 64, 72>(acc, bias + guide_ib(2), H3, lane);
-            __syncwarp();
-            store_t<64, 72>(H3, A.xt + (uint64_t)guide_xoff(3) * Bp, Bp, row0, lane);
-            guide_gemm<1, 64, 64, 72, 72>(acc, H3, W + guide_iw(3), lane);
-            guide_store_hidden<1, 64, 72>(acc, bias + guide_ib(3), H4, lane);
-            __syncwarp();
-            store_t<64, 72>(H4, A.xt + (uint64_t)guide_xoff(4) * Bp, Bp, row0, lane);
-        }
-        {
-            float acc[1][6][4];
-            guide_gemm<1, 64, kGuideOut, 72, 72>(acc, H4, W + guide_iw(4), lane);
-            guide_store_out<1, kGuideOut, 49>(acc, bias + guide_ib(4), O, lane);
-        }
-        __syncwarp();
-        if (lane < 16) {
-            const uint64_t r = row0 + lane;
-            float dout[kGuideOut];
-            if (r < A.B) {
-                const float wt = fminf(A.w[r] * winv, kGuideWeightClip);
-                const V3 wi = v3(A.dir[3 * r], A.dir[3 * r + 1], A.dir[3 * r + 2]);
-                lsum += guide_loss_grad(O + lane * 49, wi, A.pdf[r], wt, dout);
-            } else {
-#pragma unroll
-                for (int i = 0; i < kGuideOut; i++) dout[i] = 0.f;
-            }
-            __half2 *drow = reinterpret_cast<__half2 *>(D + lane * 56);
-#pragma unroll
-            for (int i = 0; i < kGuideOut / 2; i++)
-                drow[i] = __floats2half2_rn(dout[2 * i] * (1.f / kGuideGradScale), dout[2 * i + 1] * (1.f / kGuideGradScale));
-        }
-        __syncwarp();
-        store_t<kGuideOut, 56>(D, A.gt + (uint64_t)guide_goff(4) * Bp, Bp, row0, lane);
-        {
-            float acc[1][8][4];
-            guide_gemm_bt<1, kGuideOut, 64, 56, 72>(acc, D, W + guide_iw(4), lane);
-            mask_store<64, 72>(acc, H4, lane);  // G3
-            __syncwarp();
-            store_t<64, 72>(H4, A.gt + (uint64_t)guide_goff(3) * Bp, Bp, row0, lane);
-            guide_gemm_bt<1, 64, 64, 72, 72>(acc, H4, W + guide_iw(3), lane);
-            mask_store<64, 72>(acc, H3, lane);  // G2
-            __syncwarp();
-            store_t<64, 72>(H3, A.gt + (uint64_t)guide_goff(2) * Bp, Bp, row0, lane);
-            guide_gemm_bt<1, 64, 64, 72, 72>(acc, H3, W + guide_iw(2), lane);
-            mask_store<64, 72>(acc, H2, lane);  // G1
-            __syncwarp();
-            store_t<64, 72>(H2, A.gt + (uint64_t)guide_goff(1) * Bp, Bp, row0, lane);
-            guide_gemm_bt<1, 64, 64, 72, 72>(acc, H2, W + guide_iw(1), lane);
-            mask_store<64, 72>(acc, H1, lane);  // G0
-            __syncwarp();
-            store_t<64, 72>(H1, A.gt + (uint64_t)guide_goff(0) * Bp, Bp, row0, lane);
-        }
-        __syncwarp();
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-    if (lane == 0 && lsum != 0.f) atomicAdd(A.scal + 1, lsum);
-}
-
-// dW (16 input features x NT*8 outputs) over rows [r0, r1), r0 and r1 multiples of 32.
-// The reduction runs over rows, so their order inside a 32-row block is free: logical k-slots
-// {2t, 2t+1, 2t+8, 2t+9} of the two m16n8k16 steps map to rows 8t .. 8t+7, which lets every
-// lane fetch its A and B fragments with one 16-byte load per feature plane.
-template <int NT>
-__device__ __forceinline__ void wgrad_tile(const __half *X, const __half *G, uint64_t Bp, int mt, uint64_t r0,
-                                           uint64_t r1, float *dW, int out, int lane)
-{
-    const int g = lane >> 2, t = lane & 3;
-    float acc[NT][4];
-#pragma unroll
-    for (int n = 0; n < NT; n++)
-#pragma unroll
-        for (int i = 0; i < 4; i++) acc[n][i] = 0.f;
-    const uint4 *xa = reinterpret_cast<const uint4 *>(X + (uint64_t)(mt * 16 + g) * Bp);
-    const uint4 *xb = reinterpret_cast<const uint4 *>(X + (uint64_t)(mt * 16 + g + 8) * Bp);
-    const uint4 *gb[NT];
-#pragma unroll
-    for (int n = 0; n < NT; n++) gb[n] = reinterpret_cast<const uint4 *>(G + (uint64_t)(n * 8 + g) * Bp);
-#pragma unroll 2
-    for (uint64_t r = r0; r < r1; r += 32) {
-        const uint64_t i = (r >> 3) + t;
-        const uint4 a = __ldg(xa + i), b = __ldg(xb + i);
-        const uint32_t a0[4] = {a.x, b.x, a.y, b.y}, a1[4] = {a.z, b.z, a.w, b.w};
-#pragma unroll
-        for (int n = 0; n < NT; n++) {
-            const uint4 v = __ldg(gb[n] + i);
-            mma16816(acc[n], a0, v.x, v.y);
-            mma16816(acc[n], a1, v.z, v.w);
-        }
-    }
-    const int m = mt * 16 + g;
-#pragma unroll
-    for (int n = 0; n < NT; n++) {
-        const int c = n * 8 + 2 * t;
-        dW[m * out + c] = acc[n][0];
-        dW[m * out + c + 1] = acc[n][1];
-        dW[(m + 8) * out + c] = acc[n][2];
-        dW[(m + 8) * out + c + 1] = acc[n][3];
-    }
-}
-
-// One warp per work item and chunk of rows: items 0..24 are the layers' 16-feature input
-// tiles (9 for layer 0, 4 for each other layer), items 25..27 the bias sums (a third of the
-// 304 output features each). Grid: (chunks, 7) blocks of 4 warps.
-__global__ void __launch_bounds__(128) k_guide_wgrad(const __half *xt, const __half *gt, uint64_t Bp, float *partial)
-{
-    const uint32_t c = blockIdx.x;
-    const int item = blockIdx.y * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (item >= kWgradItems) return;
-    const uint64_t r0 = (uint64_t)c * kWgradChunk;
-    const uint64_t r1 = r0 + kWgradChunk < Bp ? r0 + kWgradChunk : Bp;
-    float *part = partial + (uint64_t)c * kGuideParamCount;
-    if (item < 25) {
-        const int l = item < 9 ? 0 : 1 + (item - 9) / 4;
-        const int mt = item < 9 ? item : (item - 9) % 4;
-        const __half *X = xt + (uint64_t)guide_xoff(l) * Bp;
-        const __half *G = gt + (uint64_t)guide_goff(l) * Bp;
-        if (l == kGuideLayers - 1)
-            wgrad_tile<6>(X, G, Bp, mt, r0, r1, part + guide_pw(l), kGuideOut, lane);
-        else
-            wgrad_tile<8>(X, G, Bp, mt, r0, r1, part + guide_pw(l), kGuideHidden, lane);
-        return;
-    }
-    constexpr int kPer = (kGuideGFeatures + 2) / 3;
-    const int f0 = (item - 25) * kPer, f1 = f0 + kPer < kGuideGFeatures ? f0 + kPer : kGuideGFeatures;
-    for (int f = f0; f < f1; f++) {
-        const uint4 *g4 = reinterpret_cast<const uint4 *>(gt + (uint64_t)f * Bp + r0);
-        float s = 0.f;
-        for (uint64_t i = lane; i < (r1 - r0) / 8; i += 32) {
-            const uint4 v = __ldg(g4 + i);
-            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const float2 h = __half22float2(*reinterpret_cast<const __half2 *>(&w[k]));
-                s += h.x + h.y;
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) {
-            const int ll = f < 4 * kGuideHidden ? f / kGuideHidden : 4;
-            part[guide_pb(ll) + (f - guide_goff(ll))] = s;
-        }
-    }
-}
 
 // ------------------------------------------------------------------ training on tcgen05
 //
@@ -319,12 +79,24 @@ __device__ __forceinline__ void fb_mma(uint32_t tmem, uint32_t a0, uint32_t kca,
     umma_commit(bar);
 }
 
-// FP16 pair of a row to the feature-major planes: dst[f * Bp + row], dst[(f + 1) * Bp + row]
-__device__ __forceinline__ void plane_store2(__half *dst, uint64_t Bp, int f, uint64_t row, uint32_t h2)
+// The group's 128-row operand tile (kc chunks of 8 halves per row, core-matrix layout) to the
+// feature-major planes dst[f * Bp + row0 + r] for features f < nfeat: each 16-byte store holds
+// one feature of 8 consecutive rows (read from the 8 rows of one core matrix).
+__device__ __forceinline__ void tile_to_planes(const unsigned char *tile, int kc, int nfeat, __half *dst, uint64_t Bp,
+                                               uint64_t row0, int gt)
 {
-    const __half2 v = *reinterpret_cast<const __half2 *>(&h2);
-    dst[(uint64_t)f * Bp + row] = __low2half(v);
-    dst[(uint64_t)(f + 1) * Bp + row] = __high2half(v);
+    for (int i = gt; i < nfeat * 16; i += 128) {
+        const int f = i >> 4, rg = i & 15;  // feature, group of 8 rows
+        const unsigned char *src = tile + tc_chunk((uint32_t)(8 * rg), (uint32_t)(f >> 3), (uint32_t)kc) + 2 * (f & 7);
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const __half lo = *reinterpret_cast<const __half *>(src + 32 * j);
+            const __half hi = *reinterpret_cast<const __half *>(src + 32 * j + 16);
+            w[j] = pack_h2(lo, hi);
+        }
+        *reinterpret_cast<uint4 *>(dst + (uint64_t)f * Bp + row0 + 8 * rg) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
 }
 
 __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uint4 *img, TrainArgs A)
@@ -399,8 +171,10 @@ __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uin
         tc_fence_after();
         return !group_sync_or(bar_id, !ok);
     };
-    // the operand just written becomes visible to the tensor core; thread 0 of the group issues
-    auto issue = [&](uint32_t a0, uint32_t kca, uint32_t b0, uint32_t kcb, int ksteps, int n) {
+    // the operand just written becomes visible to the tensor core; thread 0 of the group issues,
+    // then the group copies the operand to its feature-major planes while the MMA runs
+    auto issue = [&](uint32_t a0, uint32_t kca, uint32_t b0, uint32_t kcb, int ksteps, int n, const unsigned char *tile,
+                     int nfeat, __half *planes, uint64_t row0) {
         fence_async_smem();
         tc_fence_before();
         group_sync_or(bar_id, false);
@@ -408,6 +182,7 @@ __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uin
             tc_fence_after();
             fb_mma(tmem, a0, kca, b0, kcb, ksteps, n, bar);
         }
+        tile_to_planes(tile, (int)kca, nfeat, planes, Bp, row0, gt);
     };
     const uint32_t stride = gridDim.x * kFbGroups;
     for (uint64_t tile = (uint64_t)blockIdx.x * kFbGroups + grp; !failed && tile * 128 < Bp; tile += stride) {
@@ -424,18 +199,16 @@ __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uin
             for (int c = 0; c < kGuideIn / 8; c++)
                 *reinterpret_cast<uint4 *>(bufA + tc_chunk(gt, c, kGuideIn / 8)) =
                     *reinterpret_cast<const uint4 *>(&e[4 * c]);
-            if (in_p)
-#pragma unroll 4
-                for (int j = 0; j < 72; j++)
-                    plane_store2(A.xt, Bp, 2 * j, row, *reinterpret_cast<const uint32_t *>(&e[j]));
         }
+        const uint64_t row0 = tile * 128;
         // forward: X_0 (A) -> X_1 (B) -> X_2 (A) -> X_3 (B) -> X_4 (A) -> outputs
         uint32_t mask[4][2];
 #pragma unroll 1
         for (int l = 0; l < kGuideLayers - 1 && !failed; l++) {
             const uint32_t src = (l & 1) ? aB : aA;
             unsigned char *dst = (l & 1) ? bufA : bufB;
-            issue(src, guide_in(l) / 8, smem_u32(sm + tc_w(l)), guide_in(l) / 8, guide_in(l) / 16, 64);
+            issue(src, guide_in(l) / 8, smem_u32(sm + tc_w(l)), guide_in(l) / 8, guide_in(l) / 16, 64,
+                  (l & 1) ? bufB : bufA, guide_in(l), A.xt + (uint64_t)guide_xoff(l) * Bp, row0);
             if (!wait_mma()) {
                 failed = true;
                 break;
@@ -457,7 +230,6 @@ __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uin
                         m0 |= bits << f;
                     else
                         m1 |= bits << (f - 32);
-                    if (in_p) plane_store2(A.xt + (uint64_t)guide_xoff(l + 1) * Bp, Bp, f, row, w[j]);
                 }
                 *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h, 8)) = make_uint4(w[0], w[1], w[2], w[3]);
                 *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h + 1, 8)) = make_uint4(w[4], w[5], w[6], w[7]);
@@ -466,7 +238,8 @@ __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uin
             mask[l][1] = m1;
         }
         if (failed) break;
-        issue(aA, 8, smem_u32(sm + tc_w(4)), 8, 4, kGuideOut);
+        issue(aA, 8, smem_u32(sm + tc_w(4)), 8, 4, kGuideOut, bufA, kGuideHidden, A.xt + (uint64_t)guide_xoff(4) * Bp,
+              row0);
         if (!wait_mma()) {
             failed = true;
             break;
@@ -493,7 +266,6 @@ __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uin
                 const __half2 hv =
                     __floats2half2_rn(dout[2 * j] * (1.f / kGuideGradScale), dout[2 * j + 1] * (1.f / kGuideGradScale));
                 w[j] = *reinterpret_cast<const uint32_t *>(&hv);
-                if (in_p) plane_store2(A.gt + (uint64_t)guide_goff(4) * Bp, Bp, 2 * j, row, w[j]);
             }
 #pragma unroll
             for (int c = 0; c < kGuideOut / 8; c++)
@@ -506,7 +278,8 @@ __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uin
             const uint32_t src = (l & 1) ? aA : aB;  // l = 4: G_4 in B; 3: G_3 in A; ...
             unsigned char *dst = (l & 1) ? bufB : bufA;
             const int kco = guide_out(l) / 8;
-            issue(src, kco, smem_u32(sm + fb_wb(l)), kco, guide_out(l) / 16, 64);
+            issue(src, kco, smem_u32(sm + fb_wb(l)), kco, guide_out(l) / 16, 64, (l & 1) ? bufA : bufB, guide_out(l),
+                  A.gt + (uint64_t)guide_goff(l) * Bp, row0);
             if (!wait_mma()) {
                 failed = true;
                 break;
@@ -523,12 +296,13 @@ __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uin
                     const uint32_t bits = f < 32 ? (m0 >> f) : (m1 >> (f - 32));
                     const __half2 hv = __floats2half2_rn((bits & 1u) ? v[2 * j] : 0.f, (bits & 2u) ? v[2 * j + 1] : 0.f);
                     w[j] = *reinterpret_cast<const uint32_t *>(&hv);
-                    if (in_p) plane_store2(A.gt + (uint64_t)guide_goff(l - 1) * Bp, Bp, f, row, w[j]);
                 }
-                if (l > 1) {
-                    *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h, 8)) = make_uint4(w[0], w[1], w[2], w[3]);
-                    *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h + 1, 8)) = make_uint4(w[4], w[5], w[6], w[7]);
-                }
+                *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h, 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+                *reinterpret_cast<uint4 *>(dst + tc_chunk(gt, 2 * h + 1, 8)) = make_uint4(w[4], w[5], w[6], w[7]);
+            }
+            if (l == 1) {  // G_0 feeds no further product: only its planes
+                group_sync_or(bar_id, false);
+                tile_to_planes(dst, 8, kGuideHidden, A.gt, Bp, row0, gt);
             }
         }
     }
@@ -555,7 +329,12 @@ __global__ void __launch_bounds__(128 * kFbGroups, 1) k_guide_train_tc(const uin
 // into one of two shared-memory buffers while the tensor core works on the other; the five
 // accumulators (144 + 4 x 64 TMEM columns) stay in TMEM for the whole chunk, which then writes
 // its FP32 partial dW in the master layout.
-constexpr uint32_t kTcWgradChunk = 2048;  // rows per CTA
+// rows per CTA: a multiple of 64 chosen per step so the chunks about cover the SMs once
+__host__ __device__ inline uint64_t wgrad_chunk(uint64_t Bp, uint32_t sms)
+{
+    const uint64_t c = (Bp / (sms ? sms : 1) + 63) / 64 * 64;
+    return c < 256 ? 256 : c;
+}
 constexpr int kWgStageA = 5 * 8192 + 8192;         // G^T tiles: layer l at l * 8 KB (64 valid rows)
 constexpr int kWgStageB = 18 * 1024 + 4 * 8192;    // X^T tiles: layer 0 (144 rows), layers 1-4 (64)
 constexpr int kWgStage = kWgStageA + kWgStageB;
@@ -567,15 +346,15 @@ __host__ __device__ constexpr int wg_b(int l) { return kWgStageA + (l == 0 ? 0 :
 __host__ __device__ constexpr int wg_col(int l) { return l == 0 ? 0 : kGuideIn + (l - 1) * 64; }
 
 __global__ void __launch_bounds__(128, 1) k_guide_wgrad_tc(const __half *xt, const __half *gt, uint64_t Bp,
-                                                           float *partial, float *scal)
+                                                           uint64_t chunk, float *partial, float *scal)
 {
     extern __shared__ __align__(128) unsigned char wg_smem[];
     unsigned char *sm = wg_smem;
     const int tid = threadIdx.x, warp = tid >> 5;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kWgBar);  // one per buffer
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kWgBar + 16);
-    const uint64_t r0 = (uint64_t)blockIdx.x * kTcWgradChunk;
-    const uint64_t r1 = r0 + kTcWgradChunk < Bp ? r0 + kTcWgradChunk : Bp;
+    const uint64_t r0 = (uint64_t)blockIdx.x * chunk;
+    const uint64_t r1 = r0 + chunk < Bp ? r0 + chunk : Bp;
     const int nstages = (int)((r1 - r0) / 64);
     if (tid == 0) {
         mbar_init(bar, 1);
@@ -667,10 +446,10 @@ __global__ void __launch_bounds__(128, 1) k_guide_wgrad_tc(const __half *xt, con
 }
 
 // db_l = sum of G_l over the chunk's rows (feature-major planes), one warp per 8 features
-__global__ void __launch_bounds__(256) k_guide_bias_grad(const __half *gt, uint64_t Bp, float *partial)
+__global__ void __launch_bounds__(256) k_guide_bias_grad(const __half *gt, uint64_t Bp, uint64_t chunk, float *partial)
 {
-    const uint64_t r0 = (uint64_t)blockIdx.x * kTcWgradChunk;
-    const uint64_t r1 = r0 + kTcWgradChunk < Bp ? r0 + kTcWgradChunk : Bp;
+    const uint64_t r0 = (uint64_t)blockIdx.x * chunk;
+    const uint64_t r1 = r0 + chunk < Bp ? r0 + chunk : Bp;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *part = partial + (uint64_t)blockIdx.x * kGuideParamCount;
     for (int f = blockIdx.y * 64 + warp; f < kGuideGFeatures && f < (int)blockIdx.y * 64 + 64; f += 8) {
@@ -907,7 +686,8 @@ int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf,
         return RT_OK;
     }
     const uint64_t Bp = (B + 127) / 128 * 128;  // whole 128-row tiles
-    const uint32_t nchunks = (uint32_t)((Bp + kTcWgradChunk - 1) / kTcWgradChunk);
+    const uint64_t chunk = wgrad_chunk(Bp, (uint32_t)std::max(g->ctx->sm_count, 1));
+    const uint32_t nchunks = (uint32_t)((Bp + chunk - 1) / chunk);
     RTB_CHECK(g->xt.reserve(2ull * kGuideXFeatures * Bp));
     RTB_CHECK(g->gt.reserve(2ull * kGuideGFeatures * Bp));
     RTB_CHECK(g->partial.reserve(4ull * kGuideParamCount * nchunks));
@@ -929,10 +709,10 @@ int guide_train(rt_guide *g, const float *q, const float *dir, const float *pdf,
         (unsigned)std::min<uint64_t>((tiles + kFbGroups - 1) / kFbGroups, (uint64_t)std::max(g->ctx->sm_count, 1));
     k_guide_train_tc<<<grid, 128 * kFbGroups, kFbSmem, st>>>(g->img.as<uint4>(), a);
     RTB_CUDA(cudaGetLastError());
-    k_guide_wgrad_tc<<<nchunks, 128, kWgSmem, st>>>(g->xt.as<__half>(), g->gt.as<__half>(), Bp, g->partial.as<float>(),
-                                                    scal);
+    k_guide_wgrad_tc<<<nchunks, 128, kWgSmem, st>>>(g->xt.as<__half>(), g->gt.as<__half>(), Bp, chunk,
+                                                    g->partial.as<float>(), scal);
     RTB_CUDA(cudaGetLastError());
-    k_guide_bias_grad<<<dim3(nchunks, (kGuideGFeatures + 63) / 64), 256, 0, st>>>(g->gt.as<__half>(), Bp,
+    k_guide_bias_grad<<<dim3(nchunks, (kGuideGFeatures + 63) / 64), 256, 0, st>>>(g->gt.as<__half>(), Bp, chunk,
                                                                               g->partial.as<float>());
     RTB_CUDA(cudaGetLastError());
     const unsigned pblocks = (kGuideParamCount + 255) / 256;

@@ -3,8 +3,8 @@
 // importance-sampling proposal, combined with BSDF sampling by one-sample MIS.
 //
 // Network: 144 encoded inputs -> 4 hidden layers of 64 (ReLU) -> 48 outputs, FP16 weights and
-// activations on the tensor cores with FP32 accumulation (inference: tcgen05.mma with TMEM
-// accumulators; training: mma.sync m16n8k16), FP32 master weights.
+// activations on the 5th-generation tensor cores (tcgen05.mma, FP32 accumulators in TMEM) for
+// inference and training, FP32 master weights.
 // Input encoding of a shading point (position p, shading normal n, outgoing direction wo):
 //   [0, 72)    p normalised to the guide's box (u in [0, 1]), per axis 12 frequency bands:
 //              sin, cos(2^(k/2) pi u), k = 0..11 (half-octave steps: the finest band resolves
@@ -46,7 +46,7 @@ __host__ __device__ constexpr int guide_pb(int l) { return guide_pw(l) + guide_i
 static_assert(guide_pb(4) + 48 == kGuideParamCount, "parameter count");
 
 // FP16 weight image (the shared-memory copy, loaded with 16-byte copies): W_l transposed,
-// out_l rows of stride guide_stride(l) halves (padding keeps ldmatrix conflict-free), then
+// out_l rows of stride guide_stride(l) halves (the kernels restage them as core matrices), then
 // the FP32 biases (64 per hidden layer, 48 for the output layer).
 __host__ __device__ constexpr int guide_stride(int l) { return l == 0 ? 152 : 72; }
 __host__ __device__ constexpr int guide_iw(int l)
@@ -95,129 +95,6 @@ struct GuideBox {
 struct rt_guide;
 namespace rtb {
 GuideBox guide_box(const rt_guide *g);  // position encoding domain of a guide
-
-// ------------------------------------------------------------------ tensor-core helpers
-
-__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
-{
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void *p)
-{
-    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
-
-__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const void *p)
-{
-    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
-
-// acc[MT x 16 rows][N] = A[MT*16 rows][K] (stride SA) * W, W^T stored [N][SW] (forward layers)
-template <int MT, int K, int N, int SA, int SW>
-__device__ __forceinline__ void guide_gemm(float (&acc)[MT][N / 8][4], const __half *A, const __half *Wt, int lane)
-{
-#pragma unroll
-    for (int m = 0; m < MT; m++)
-#pragma unroll
-        for (int n = 0; n < N / 8; n++)
-#pragma unroll
-            for (int i = 0; i < 4; i++) acc[m][n][i] = 0.f;
-#pragma unroll
-    for (int ks = 0; ks < K / 16; ks++) {
-        uint32_t a[MT][4];
-#pragma unroll
-        for (int m = 0; m < MT; m++)
-            ldsm_x4(a[m], A + (m * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * SA + ks * 16 + (lane >> 4) * 8);
-#pragma unroll
-        for (int np = 0; np < N / 16; np++) {
-            uint32_t b[4];
-            ldsm_x4(b, Wt + (np * 16 + (lane & 7) + (lane >> 4) * 8) * SW + ks * 16 + ((lane >> 3) & 1) * 8);
-#pragma unroll
-            for (int m = 0; m < MT; m++) {
-                mma16816(acc[m][2 * np], a[m], b[0], b[1]);
-                mma16816(acc[m][2 * np + 1], a[m], b[2], b[3]);
-            }
-        }
-    }
-}
-
-// acc[MT x 16 rows][N] = G[rows][K] (stride SA) * W_l^T, with W_l^T stored [K][SW]
-// (backward: K = the layer's outputs, N = its inputs)
-template <int MT, int K, int N, int SA, int SW>
-__device__ __forceinline__ void guide_gemm_bt(float (&acc)[MT][N / 8][4], const __half *A, const __half *Wt, int lane)
-{
-#pragma unroll
-    for (int m = 0; m < MT; m++)
-#pragma unroll
-        for (int n = 0; n < N / 8; n++)
-#pragma unroll
-            for (int i = 0; i < 4; i++) acc[m][n][i] = 0.f;
-#pragma unroll
-    for (int ks = 0; ks < K / 16; ks++) {
-        uint32_t a[MT][4];
-#pragma unroll
-        for (int m = 0; m < MT; m++)
-            ldsm_x4(a[m], A + (m * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * SA + ks * 16 + (lane >> 4) * 8);
-#pragma unroll
-        for (int np = 0; np < N / 16; np++) {
-            uint32_t b[4];
-            ldsm_x4_t(b, Wt + (ks * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * SW + np * 16 + (lane >> 4) * 8);
-#pragma unroll
-            for (int m = 0; m < MT; m++) {
-                mma16816(acc[m][2 * np], a[m], b[0], b[1]);
-                mma16816(acc[m][2 * np + 1], a[m], b[2], b[3]);
-            }
-        }
-    }
-}
-
-// bias + ReLU, FP16 store (stride SO halves)
-template <int MT, int N, int SO>
-__device__ __forceinline__ void guide_store_hidden(const float (&acc)[MT][N / 8][4], const float *bias, __half *out,
-                                                   int lane)
-{
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int m = 0; m < MT; m++)
-#pragma unroll
-        for (int nt = 0; nt < N / 8; nt++) {
-            const int n = nt * 8 + 2 * t, r = m * 16 + g;
-            const float b0 = bias[n], b1 = bias[n + 1];
-            *reinterpret_cast<__half2 *>(out + r * SO + n) =
-                __floats2half2_rn(fmaxf(acc[m][nt][0] + b0, 0.f), fmaxf(acc[m][nt][1] + b1, 0.f));
-            *reinterpret_cast<__half2 *>(out + (r + 8) * SO + n) =
-                __floats2half2_rn(fmaxf(acc[m][nt][2] + b0, 0.f), fmaxf(acc[m][nt][3] + b1, 0.f));
-        }
-}
-
-// bias, FP32 store (stride SO floats)
-template <int MT, int N, int SO>
-__device__ __forceinline__ void guide_store_out(const float (&acc)[MT][N / 8][4], const float *bias, float *out,
-                                                int lane)
-{
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int m = 0; m < MT; m++)
-#pragma unroll
-        for (int nt = 0; nt < N / 8; nt++) {
-            const int n = nt * 8 + 2 * t, r = m * 16 + g;
-            out[r * SO + n] = acc[m][nt][0] + bias[n];
-            out[r * SO + n + 1] = acc[m][nt][1] + bias[n + 1];
-            out[(r + 8) * SO + n] = acc[m][nt][2] + bias[n];
-            out[(r + 8) * SO + n + 1] = acc[m][nt][3] + bias[n + 1];
-        }
-}
 
 // ------------------------------------------------------------------ encoding
 

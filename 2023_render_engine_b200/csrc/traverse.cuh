@@ -30,38 +30,12 @@ struct Best {
 
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xFFu; }
 
-// L2 residency of the scene against the streamed rays and hits. With RTB_TRAV_L2HINT the node and
-// triangle-record loads carry an evict-last cache policy and the ray loads are evict-first
-// (streaming): a call over more rays than L2 holds then re-reads the scene less.
-#ifdef RTB_TRAV_L2HINT
-__device__ __forceinline__ uint64_t scene_policy()
-{
-    uint64_t p;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-__device__ __forceinline__ uint4 ld_scene(const uint4 *ptr)
-{
-    uint4 r;
-    asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
-        : "l"(ptr), "l"(scene_policy()));
-    return r;
-}
-__device__ __forceinline__ float4 ld_scene(const float4 *ptr)
-{
-    float4 r;
-    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
-        : "l"(ptr), "l"(scene_policy()));
-    return r;
-}
-__device__ __forceinline__ float4 ld_stream(const float4 *ptr) { return __ldcs(ptr); }
-#else
+// Scene records (nodes, triangles) and streamed rays. Evict-last L2 policies on the scene loads
+// with evict-first ray loads were measured against these plain read-only loads: 3207 against 3183
+// Mrays/s on the 2^24 BVH-stress rays, 1821 against 1832 on the render; not kept.
 __device__ __forceinline__ uint4 ld_scene(const uint4 *ptr) { return __ldg(ptr); }
 __device__ __forceinline__ float4 ld_scene(const float4 *ptr) { return __ldg(ptr); }
 __device__ __forceinline__ float4 ld_stream(const float4 *ptr) { return __ldg(ptr); }
-#endif
 
 __device__ __forceinline__ void load_ray(const rt_ray *rays, uint64_t i, float4 &a, float4 &b)
 {
