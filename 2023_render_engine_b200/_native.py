@@ -86,6 +86,7 @@ RT_BUILD_DEVICE, RT_BUILD_HOST = 0, 1
  RT_TONEMAP_GAMMA_CLAMP) = range(6)
 RT_RENDER_SUBSURFACE = 0x20
 RT_RENDER_HYBRID = 0x40
+RT_RENDER_HOST_LOOP = 0x80
 
 
 class PhotonTraceStats(ctypes.Structure):

@@ -1232,7 +1232,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     // cannot be captured) the host loop below runs instead.
     bool device_loop = false;
     const uint32_t wave_cap = (uint32_t)std::min<uint64_t>(max_waves, 0x7FFFFFF0u);
-    if (st != nullptr && st != cudaStreamLegacy) {
+    if (st != nullptr && st != cudaStreamLegacy && !(flags & RT_RENDER_HOST_LOOP)) {
         cudaGraph_t g = nullptr;
         cudaGraphConditionalHandle loop_handle;
         bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&

@@ -44,9 +44,11 @@ WORKLOAD = ("BVH-stress render: 1920x1080, 64 spp, max depth 12, RR after depth 
 TRACE_WORKLOAD = "closest hit of 2^{} seeded rays (origins uniform in [-1,1]^3, directions uniform), reference-exact ids"
 NRAYS = 1 << 24
 ALG_BYTES_PER_RAY = 48  # 32 B ray in + 16 B hit out (queue level)
-# DRAM bytes (read + write) of one k_trace_closest launch of the 2^24-ray call, from one ncu
-# capture of the full-size launch (1 pass, --cache-control none; profiles/k_trace_closest_bvh_stress.md)
-TRACE_TRAFFIC_BYTES_2_24 = 2_457_002_240 + 976_186_368
+# DRAM bytes (read + write) of one k_trace_closest launch of the 2^24-ray call: the mean of the
+# four 2^24-ray launches of one ncu capture of this file's render command (1 pass, --cache-control
+# none; profiles/k_trace_closest_bvh_stress.md), taken at commit 162b555 of the traversal. A
+# change to traverse.cuh or trace.cu needs a new capture.
+TRACE_TRAFFIC_BYTES_2_24 = 2_457_424_064 + 978_677_632
 
 
 def dist_env():
@@ -205,6 +207,50 @@ def reference_render_rate(host, args, S, width, height, spp, runs=1, warmup=0):
             if k >= warmup:
                 out.append(st)
     return out
+
+
+def reference_config4(S, width, height, photons):
+    """The reference's own integrator (host build) on the 4K photon-mapping configuration's scene:
+    RENDER_MODE HYBRID with CHECK_SUBSURFACE_SCATTERING, k = 50 (MAX_NEIGHBOURS), radius 100, the
+    given number of photons, at width x height (the same view), 1 spp, depth 16. Its render call
+    includes its photon pass and kd-tree build (PathTracerIntegrator::render calls
+    generatePhotons). None if the harness is not built."""
+    import tempfile
+
+    from oracle import bindings
+
+    try:
+        R = bindings.RefIntegrator(host=True)
+    except (FileNotFoundError, OSError):
+        return None
+    (tv, tf), (sv, sf), spheres = S.photon_terrain(seed=11, n=1000)
+    v = np.concatenate([tv, sv]).astype(np.float32)
+    f = np.concatenate([tf, sf + tv.shape[0]]).astype(np.uint32)
+    tri_mat = np.concatenate([np.zeros(tf.shape[0], np.uint32), np.full(sf.shape[0], 2, np.uint32)])
+    tri_shape = np.concatenate([np.zeros(tf.shape[0], np.int32), np.ones(sf.shape[0], np.int32)])
+    table = [R.entry(R.LAMBERTIAN, (0.6, 0.55, 0.45)), R.entry(R.DIELECTRIC, (1, 1, 1), value=1.5),
+             R.subsurface_entry((0.9, 0.9, 0.9), (0.04, 0.04, 0.04), 1.3, 40.0, (1.0, 0.8, 0.6),
+                                (0.01, 0.02, 0.05), 0.0)]
+    sph = [(c, r, 1) for c, r in spheres]
+    # the loader negates the y of every position it reads (FileImporting.cu:514-516)
+    scene_file = ("camera\np 0 -2.4 5.6\nlookat 0 0.1 0\nup 0 1 0\ncts 0 0 -0.8\nframeY 0.662742\n"
+                  "\nlightPoint l0\np -1.6 -2.6 1.4\nc 1 1 1\ni 50\n"
+                  "\nlightPoint l1\np 1.8 -3.2 -1.2\nc 1 1 1\ni 50\n")
+    R.config_photons(R.HYBRID, True, photons, 50, 100.0)
+    try:
+        with tempfile.TemporaryDirectory() as td:
+            path = Path(td) / "config4.obejota"
+            path.write_text(scene_file)
+            _, _, _, st = R.render(path, width, height, 1, 16, table, v, f, tri_mat, tri_shape, spheres=sph)
+    finally:
+        R.config_photons(R.PATH_TRACING, False, 100000, 100, 100.0)
+    rays = st["extension_rays"] + st["shadow_rays"]
+    return {"workload": f"the reference's PathTracerIntegrator::render (host build) on the same scene, RENDER_MODE "
+                        f"HYBRID + CHECK_SUBSURFACE_SCATTERING, {photons} photons, k = 50, {width}x{height}, 1 spp, "
+                        f"depth 16; its render call includes its photon pass and kd-tree build",
+            "seconds": st["render_s"], "build_s": st["build_s"], "rays": rays,
+            "mrays_s": rays / st["render_s"] / 1e6, "samples_per_s": width * height / st["render_s"],
+            "cores": os.cpu_count() or 1}
 
 
 def run_reference(args):
@@ -413,7 +459,9 @@ def run_ours(args):
             "count": torch.zeros(H * W, dtype=torch.int32, device="cuda")}
     host_sum = torch.empty(H * W * 3, dtype=torch.float32).pin_memory()
     host_cnt = torch.empty(H * W, dtype=torch.int32).pin_memory()
-    rflags = N.RT_RENDER_NEE_AREA
+    # --host-wave-loop: the host checks the queues after every 4-wave group (a profiling aid: ncu
+    # does not see kernels inside the device loop's conditional graph); the same kernels and rays
+    rflags = N.RT_RENDER_NEE_AREA | (N.RT_RENDER_HOST_LOOP if args.host_wave_loop else 0)
 
     def render_step(seed):
         film["sum"].zero_()
@@ -513,6 +561,8 @@ def run_ours(args):
         photon_sss = PR.measure(ctx, torch, stream, width=args.c4_width, height=args.c4_height, spp=args.c4_spp)
         photon_sss["metric"] = ("Mrays/s, samples/s and photon-map gathers/s of hybrid + subsurface rendering; "
                                 "guided vs plain time to equal noise")
+        if not args.no_cpu_baseline:
+            photon_sss["reference"] = reference_config4(S, args.c4_ref_width, args.c4_ref_height, args.c4_ref_photons)
 
     # ---- the reference's own CUDA traversal on the same rays (baseline, not a target)
     ref_cuda = None
@@ -607,9 +657,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1 << 20)
-    ap.add_argument("--ref-width", type=int, default=480, help="reference integrator sample image width")
-    ap.add_argument("--ref-height", type=int, default=270)
+    ap.add_argument("--ref-width", type=int, default=960, help="reference integrator sample image width")
+    ap.add_argument("--ref-height", type=int, default=540)
     ap.add_argument("--rays-log2", type=int, default=24, help="smaller ray sets for profiler captures")
+    ap.add_argument("--host-wave-loop", action="store_true",
+                    help="render with the host-side wave loop (profiler captures of the render kernels)")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--spp", type=int, default=64)
@@ -619,6 +671,9 @@ def main():
     ap.add_argument("--c4-spp", type=int, default=256, help="config-4 spp per mode (0 skips config 4)")
     ap.add_argument("--c4-width", type=int, default=3840)
     ap.add_argument("--c4-height", type=int, default=2160)
+    ap.add_argument("--c4-ref-width", type=int, default=384, help="reference config-4 sample image width")
+    ap.add_argument("--c4-ref-height", type=int, default=216)
+    ap.add_argument("--c4-ref-photons", type=int, default=1_000_000, help="photons of the reference config-4 sample")
     ap.add_argument("--guide-target", type=float, default=0.01)
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)

@@ -303,6 +303,10 @@ typedef struct rt_camera {
 #define RT_RENDER_COMPAT 0x2u   /* reference estimator quirks (delta-light MIS weight, 0.7/0.3 glass lobes
                                    without pdf, reference Fresnel); off = physically consistent */
 #define RT_RENDER_EXACT_TRACE 0x4u /* reference-exact closest-hit ids for extension rays */
+#define RT_RENDER_HOST_LOOP 0x80u  /* the host checks for completion after every 4-wave group instead of the
+                                      device-side loop (a CUDA graph with a conditional WHILE node); the same
+                                      kernels and samples, for tools that do not see kernels inside
+                                      conditional graphs */
 #define RT_RENDER_SUBSURFACE 0x20u /* CHECK_SUBSURFACE_SCATTERING: at camera-ray hits on RT_MAT_SUBSURFACE add
                                       the dipole photon estimate (rt_photon_subsurface, radius 0.3);
                                       needs the photon map of rt_render_set_photon_map */

@@ -690,8 +690,9 @@ class RefIntegrator:
     on OpenMP: its BVH build and traversal run on the host cores too). host=False:
     libref_integrator_cuda.so, its stock CUDA build (BVH on the GPU, compile.sh flags)."""
 
-    # material kinds of the harness's 12-float table entries
-    LAMBERTIAN, TROWBRIDGE, LIGHT, DIELECTRIC, MIRROR = 0, 1, 2, 3, 4
+    # material kinds of the harness's 16-float table entries
+    LAMBERTIAN, TROWBRIDGE, LIGHT, DIELECTRIC, MIRROR, SUBSURFACE = 0, 1, 2, 3, 4, 5
+    PATH_TRACING, PHOTON_MAPPING, HYBRID = 0, 1, 2
 
     def __init__(self, host: bool = True):
         name = "libref_integrator_host.so" if host else "libref_integrator_cuda.so"
@@ -701,6 +702,8 @@ class RefIntegrator:
         L = ctypes.CDLL(str(path))
         L.refi_error.restype = ctypes.c_char_p
         L.refi_config.argtypes = [I, I, I, I]
+        L.refi_config_photons.argtypes = [I, I, U32, U32, F]
+        L.refi_config_photons.restype = I
         L.refi_render.argtypes = [ctypes.c_char_p, U32, P, U32, P, P, P, U32, P, P, U32, P, P, U32, P, P, P, P, P]
         L.refi_render.restype = I
         L.refi_material_sample.argtypes = [P, P, P, U32, P, P, P]
@@ -714,7 +717,7 @@ class RefIntegrator:
     @staticmethod
     def entry(kind, color=(1, 1, 1), eta=(0, 0, 0), k=(0, 0, 0), roughness=(0, 0), value=0.0):
         """A material table entry: value is the Light intensity or the Dielectric IOR."""
-        e = np.zeros(12, np.float32)
+        e = np.zeros(16, np.float32)
         e[0] = kind
         e[1:4] = color
         if kind == RefIntegrator.TROWBRIDGE:
@@ -723,6 +726,22 @@ class RefIntegrator:
             e[4] = value
         return e
 
+    @staticmethod
+    def subsurface_entry(kd, ks, eta, ns, sigma_s, sigma_a, g):
+        """SSMaterial(0, kd, ks, eta, ns, no texture, opaque, sigma_s, sigma_a, g)."""
+        e = np.zeros(16, np.float32)
+        e[0] = RefIntegrator.SUBSURFACE
+        e[1:4], e[4:7], e[7], e[8] = kd, ks, eta, ns
+        e[9:12], e[12:15], e[15] = sigma_s, sigma_a, g
+        return e
+
+    def config_photons(self, mode, subsurface, photons, neighbours, radius):
+        """RENDER_MODE, CHECK_SUBSURFACE_SCATTERING, N_PHOTON_SAMPLES, MAX_NEIGHBOURS and
+        PHOTON_SEARCH_RADIUS of the reference's render (types.h:51-60)."""
+        if self.L.refi_config_photons(int(mode), int(bool(subsurface)), int(photons), int(neighbours),
+                                      float(radius)) != 0:
+            raise ValueError("bad photon configuration")
+
     def render(self, obejota_path, width, height, spp, depth, materials, verts=None, idx=None, tri_mat=None,
                tri_shape=None, spheres=(), planes=()):
         """Returns (per-pixel mean (h*w, 3), camera_to_world (4, 4), raster_to_camera (4, 4), stats)
@@ -730,7 +749,7 @@ class RefIntegrator:
         material); planes: (12 floats of Plane(corner, axisX, axisY, normal), material)."""
         if self.L.refi_config(width, height, spp, depth) != 0:
             raise ValueError("bad render configuration")
-        mats = _np(np.stack(list(materials)), np.float32).reshape(-1, 12)
+        mats = _np(np.stack(list(materials)), np.float32).reshape(-1, 16)
         if verts is None or idx is None or len(idx) == 0:
             v = np.zeros((1, 3), np.float32)
             f = np.zeros((0, 3), np.uint32)
@@ -756,7 +775,7 @@ class RefIntegrator:
 
     @staticmethod
     def _scene_args(materials, verts, idx, tri_mat, tri_shape, spheres, planes):
-        mats = _np(np.stack(list(materials)), np.float32).reshape(-1, 12)
+        mats = _np(np.stack(list(materials)), np.float32).reshape(-1, 16)
         if verts is None or idx is None or len(idx) == 0:
             v, f = np.zeros((1, 3), np.float32), np.zeros((0, 3), np.uint32)
         else:

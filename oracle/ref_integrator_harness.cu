@@ -82,6 +82,10 @@ namespace refi {
 struct Config {
     int w = 64, h = 64, spp = 4, depth = 8;
     unsigned photons = 100000;  // N_PHOTON_SAMPLES of a photon pass
+    int mode = 0;               // RENDER_MODE: 0 PATH_TRACING, 1 PHOTON_MAPPING, 2 HYBRID
+    bool subsurface = false;    // CHECK_SUBSURFACE_SCATTERING
+    unsigned neighbours = 100;  // MAX_NEIGHBOURS
+    float radius = 100.f;       // PHOTON_SEARCH_RADIUS
 };
 Config g_cfg;
 std::atomic<unsigned long long> g_ext_rays{0}, g_shadow_rays{0};
@@ -111,8 +115,14 @@ int count_shadow(const V &rays, const Rest &...)
 #undef CHECK_SUBSURFACE_SCATTERING
 #undef RENDER_MODE
 #undef N_PHOTON_SAMPLES
+#undef MAX_NEIGHBOURS
+#undef PHOTON_SEARCH_RADIUS
 #ifdef __CUDA_ARCH__
 #define N_PHOTON_SAMPLES 1
+#define MAX_NEIGHBOURS 100
+#define PHOTON_SEARCH_RADIUS 100
+#define CHECK_SUBSURFACE_SCATTERING false
+#define RENDER_MODE PATH_TRACING
 // device pass: the reference's __device__ code that names these is never launched here
 #define resolutionX 640
 #define resolutionY 360
@@ -124,9 +134,11 @@ int count_shadow(const V &rays, const Rest &...)
 #define SAMPLES_PER_PIXEL (refi::g_cfg.spp)
 #define MAX_RAY_RECURSION_DEPTH (refi::g_cfg.depth)
 #define N_PHOTON_SAMPLES (refi::g_cfg.photons)
+#define MAX_NEIGHBOURS (refi::g_cfg.neighbours)
+#define PHOTON_SEARCH_RADIUS (refi::g_cfg.radius)
+#define CHECK_SUBSURFACE_SCATTERING (refi::g_cfg.subsurface)
+#define RENDER_MODE ((RenderMode)refi::g_cfg.mode)
 #endif
-#define CHECK_SUBSURFACE_SCATTERING false
-#define RENDER_MODE PATH_TRACING
 
 // include order of the reference's own mains (cornellBoxGuion.cu:1-22); its BVH first, so
 // that the counting macro below applies to Scene.cu's call sites only
@@ -174,14 +186,19 @@ struct ScenePeek : public Scene {
 };
 thread_local std::string g_error;
 
-// Material table entry: 12 floats.
+// Material table entry: 16 floats.
 //   [0] kind: 0 Lambertian (kd = [1..3]), 1 Trowbridge (kd [1..3], eta [4..6], k [7..9],
 //       roughness x [10], y [11]), 2 Light (color [1..3], intensity [4]), 3 Dielectric
-//       (color [1..3], ior [4]), 4 Mirror (color [1..3])
+//       (color [1..3], ior [4]), 4 Mirror (color [1..3]), 5 SSMaterial (kd [1..3], ks [4..6],
+//       eta [7], ns [8], sigma_s [9..11], sigma_a [12..14], g [15])
+constexpr int kEntry = 16;
 Material *make_material(const float *m)
 {
     const Spectrum c(m[1], m[2], m[3]);
     switch ((int)m[0]) {
+    case 5:
+        return new SSMaterial(Spectrum(0), c, Spectrum(m[4], m[5], m[6]), m[7], m[8], nullptr, false,
+                              Spectrum(m[9], m[10], m[11]), Spectrum(m[12], m[13], m[14]), m[15]);
     case 0:
         return new LambertianMaterial(c);
     case 1:
@@ -213,7 +230,17 @@ REFI_API int refi_host_backend()
 REFI_API int refi_config(int w, int h, int spp, int depth)
 {
     if (w <= 0 || h <= 0 || spp <= 0 || depth <= 0) return 1;
-    refi::g_cfg = refi::Config{w, h, spp, depth};
+    refi::g_cfg.w = w, refi::g_cfg.h = h, refi::g_cfg.spp = spp, refi::g_cfg.depth = depth;
+    return 0;
+}
+
+// The photon-mapping settings of types.h:51-60: RENDER_MODE (0 path tracing, 1 photon mapping,
+// 2 hybrid), CHECK_SUBSURFACE_SCATTERING, N_PHOTON_SAMPLES, MAX_NEIGHBOURS, PHOTON_SEARCH_RADIUS.
+REFI_API int refi_config_photons(int mode, int subsurface, unsigned photons, unsigned neighbours, float radius)
+{
+    if (mode < 0 || mode > 2 || photons == 0 || neighbours == 0) return 1;
+    refi::g_cfg.mode = mode, refi::g_cfg.subsurface = subsurface != 0, refi::g_cfg.photons = photons;
+    refi::g_cfg.neighbours = neighbours, refi::g_cfg.radius = radius;
     return 0;
 }
 
@@ -225,7 +252,7 @@ REFI_API int refi_config(int w, int h, int spp, int depth)
 //   spheres: center xyz + radius per sphere (Sphere(Point3f, Float), Sphere.cu:233) and its
 //            material; planes: 12 floats per plane as Plane(corner, axisX, axisY, normal),
 //            Plane.cu:26-50, and its material;
-//   materials: nmat entries of 12 floats (make_material).
+//   materials: nmat entries of 16 floats (make_material).
 // out_mean: per-pixel mean radiance (the Film's sum / spp), row-major, 3 floats per pixel.
 // out_c2w / out_r2c (nullable): the camera's cameraToWorld and rasterToCamera (row-major).
 // out_stats (nullable): [0] seconds in PathTracerIntegrator::render, [1] extension rays,
@@ -253,7 +280,7 @@ int make_scene_input(SceneInput &in, const char *obejota, uint32_t nv, const flo
                      const uint32_t *plane_mat, uint32_t nmat, const float *materials)
 {
     for (uint32_t i = 0; i < nmat; i++) {
-        in.mats.emplace_back(make_material(materials + 12 * i));
+        in.mats.emplace_back(make_material(materials + kEntry * i));
         if (!in.mats.back()) return g_error = "unknown material kind", 1;
     }
     for (uint32_t i = 0; i < nspheres; i++) {
