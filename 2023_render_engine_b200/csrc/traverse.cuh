@@ -150,6 +150,9 @@ __device__ __forceinline__ void trav_init(Trav &T, float ox, float oy, float oz,
 // order but was slower on the BVH-stress scene: render 1683 / 1714 / 1654 against 1832
 // Mrays/s, 2^24-ray trace ~2900 against 3123, for triangle-step ratios 3 / 2 / 5 (leaves
 // hold at most 3 triangles, so the per-step phase vote costs more than the packing saves).
+// Two smaller rewrites of the box test were slower too (render / trace Mrays/s, against
+// 1837 / 3130): bytes turned into floats through the mantissa of 2^23 (1815 / 3067), and a
+// minimum instead of the sorting network when one interior child is hit (1824 / 3086).
 // Returns true when the ray is done (T.ok = false if the stack or step cap was exceeded).
 __device__ __forceinline__ bool trav_step(const SceneView &v, Trav &T, bool anyhit)
 {
