@@ -13,7 +13,7 @@ import time
 
 from . import _native as N
 
-CAPACITIES = (1 << 23, 1 << 22, 1 << 21, 1 << 20)
+CAPACITIES = (1 << 25, 1 << 24, 1 << 23, 1 << 22, 1 << 21)
 SORT_LOG2 = (0, 8, 10, 12)
 
 

@@ -107,7 +107,10 @@ __host__ __device__ __forceinline__ BBox triangle_box(const float *p, float marg
 
 // SAH rule that turns a subtree of `cnt` triangles (children of nl and nr) into one leaf: a
 // leaf when cnt <= kMaxLeaf and cnt is not above the cost of keeping the split
-// (traversal cost 1, intersection cost 1 per triangle).
+// (traversal cost 1, intersection cost 1 per triangle). 2^24-ray trace on the BVH-stress scene,
+// Mrays/s (BVH8 nodes): 3133 (268,797) for this rule; 3143 (274,795) with leaves of at most 2,
+// 3122 (267,843) at most 4; traversal cost 1.5: ~3016 (191,677), 2: 2994 (183,921), 2 with
+// leaves of at most 4: 2885 (151,352).
 constexpr uint32_t kMaxLeaf = 3;
 __host__ __device__ __forceinline__ bool sah_leaf(uint32_t cnt, float parea, float al, uint32_t nl, float ar, uint32_t nr)
 {
