@@ -66,7 +66,8 @@ def measure(groups, sync, autotune=True, merged=True):
             continue
         cap, trials = autotune_capacity(scene, views, flags, sync) if autotune else (0, [])
         sort_log2, sort_trials = autotune_sort(scene, views, flags, cap, sync) if autotune else (10, [])
-        scene.render_batch(views[:1], flags=flags, max_paths=cap)  # warm
+        # warm at full size: the queues grow to the batch's capacity here, not in the timed call
+        scene.render_batch(views, flags=flags, max_paths=cap)
         t_b, (film, st, off) = _timed(lambda: scene.render_batch(views, flags=flags, max_paths=cap), sync)
         rays = st["extension_rays"] + st["shadow_rays"]
         del film
@@ -111,7 +112,7 @@ def measure_merged(groups, sync, autotune=True):
     try:
         cap, trials = autotune_capacity(merged, views, flags[0], sync) if autotune else (0, [])
         sort_log2, sort_trials = autotune_sort(merged, views, flags[0], cap, sync) if autotune else (10, [])
-        merged.render_batch(views[:1], flags=flags[0], max_paths=cap)  # warm
+        merged.render_batch(views, flags=flags[0], max_paths=cap)  # warm at full size (queue growth)
         t, (film, st, _) = _timed(lambda: merged.render_batch(views, flags=flags[0], max_paths=cap), sync)
         del film
         rays = st["extension_rays"] + st["shadow_rays"]

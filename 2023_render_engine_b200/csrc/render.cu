@@ -239,26 +239,28 @@ __global__ void __launch_bounds__(kSortBlock) k_material_sort(RenderView rv, Buf
     __shared__ uint32_t count[kSortKeys], start[kSortKeys];
     __shared__ uint8_t key[1u << kSortMaxLog2];
     const uint32_t n = min(bf.cnt[cur], bf.cap);
-    const uint32_t c0 = blockIdx.x << log2;
-    if (c0 >= n) return;
-    const uint32_t len = min(1u << log2, n - c0);
-    if (threadIdx.x < kSortKeys) count[threadIdx.x] = 0;
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < len; j += kSortBlock) {
-        const uint32_t k = shade_key(rv, bf, c0 + j);
-        key[j] = (uint8_t)k;
-        atomicAdd(&count[k], 1u);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t acc = 0;
-        for (int k = 0; k < kSortKeys; k++) {
-            start[k] = acc;
-            acc += count[k];
+    // chunks in a grid-stride loop over the resident blocks (c0 is the same for the whole block)
+    for (uint32_t c0 = blockIdx.x << log2; c0 < n; c0 += gridDim.x << log2) {
+        const uint32_t len = min(1u << log2, n - c0);
+        if (threadIdx.x < kSortKeys) count[threadIdx.x] = 0;
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < len; j += kSortBlock) {
+            const uint32_t k = shade_key(rv, bf, c0 + j);
+            key[j] = (uint8_t)k;
+            atomicAdd(&count[k], 1u);
         }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for (int k = 0; k < kSortKeys; k++) {
+                start[k] = acc;
+                acc += count[k];
+            }
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < len; j += kSortBlock) perm[c0 + atomicAdd(&start[key[j]], 1u)] = c0 + j;
+        __syncthreads();  // count, start and key are reused by the next chunk
     }
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < len; j += kSortBlock) perm[c0 + atomicAdd(&start[key[j]], 1u)] = c0 + j;
 }
 
 // End of one 4-wave group of the device-side wave loop: counts the waves and sets the loop's
@@ -284,6 +286,10 @@ __global__ void k_wave_check(uint32_t *cnt, uint64_t total, uint32_t max_waves, 
 #ifndef RTB_SHADE_MIN_BLOCKS
 #define RTB_SHADE_MIN_BLOCKS 8
 #endif
+// One thread per queue position i of the wave (the slot perm[i] when the queue is sorted), on a
+// grid of the queue's capacity. A grid-stride loop over the resident blocks instead nearly
+// doubles the spills at the 64-register bound (708 -> 1300 bytes of spill stores) and was 13%
+// slower on the BVH-stress render (1806 -> 1578 Mrays/s at 2^22 paths).
 __global__ void __launch_bounds__(kB, RTB_SHADE_MIN_BLOCKS) k_shade(RenderView rv, Buffers bf, int cur, GuideView gv)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -658,11 +664,9 @@ __device__ __forceinline__ float record_weight(const GuideRecord &r)
     return s * (1.f / 3.f);
 }
 
-__global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t *count, double *sum64, GuideView gv)
+__device__ __forceinline__ void retire_path(const Buffers &bf, float *sum, uint32_t *count, double *sum64,
+                                            const GuideView &gv, uint32_t i)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = min(bf.cnt[3], bf.cap);
-    if (i >= n) return;
     if (gv.train) {
         // the path is complete: each of its records gets the radiance of everything after it
         uint32_t r = gv.retire_rec[i];
@@ -695,6 +699,15 @@ __global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t 
         atomicAdd(sum64 + 3 * pix + 1, (double)v.y);
         atomicAdd(sum64 + 3 * pix + 2, (double)v.z);
     }
+}
+
+// The wave's retired paths (usually a small part of the capacity) in a grid-stride loop over
+// the resident blocks: a grid of the capacity would spend most of its blocks exiting.
+__global__ void __launch_bounds__(kB) k_retire(Buffers bf, float *sum, uint32_t *count, double *sum64, GuideView gv)
+{
+    const uint32_t n = min(bf.cnt[3], bf.cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        retire_path(bf, sum, count, sum64, gv, i);
 }
 
 // Guide network at the wave's hits (queue slots of buffer `cur`); writes the decoded mixture
@@ -1024,6 +1037,20 @@ namespace {
 // time the persistent traversal kernels spend draining their last rays, wave after wave.
 // BVH-stress render at 1920x1080 x 64 spp (244 B per path), Mrays/s: 1585 / 1806 / 1947 /
 // 2074 / 2130 / 2189 for 2^21 / 2^22 / 2^23 / 2^24 / 2^25 / 2^26 paths.
+// Blocks of `kernel` (block size `block`) resident on the current device at once (cached).
+template <typename Kernel>
+unsigned resident_grid(DeviceSlot slot, Kernel kernel, int block)
+{
+    unsigned r = device_slot(slot);
+    if (!r) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+        r = device_sm_count() * (unsigned)std::max(per_sm, 1);
+        set_device_slot(slot, r);
+    }
+    return r;
+}
+
 uint32_t default_paths(uint32_t flags, uint32_t per_path_shadow)
 {
     uint64_t bytes = 64 + 96 + 16 + 16 + 4;  // rays, path state, hits, retire, shading order
@@ -1156,7 +1183,10 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     bf.gcap = gcap;
     // material sort of the shading order, chunks of 2^sort_log2 queue slots (0: off)
     const uint32_t sort_log2 = s->sort_log2 ? std::min<uint32_t>(std::max<uint32_t>(s->sort_log2, 5u), kSortMaxLog2) : 0u;
-    const unsigned sort_blocks = sort_log2 ? (unsigned)((cap + (1u << sort_log2) - 1) >> sort_log2) : 0u;
+    const unsigned sort_blocks =
+        sort_log2 ? std::min((unsigned)((cap + (1u << sort_log2) - 1) >> sort_log2),
+                             resident_grid(SLOT_SORT_RESIDENT, k_material_sort, kSortBlock))
+                  : 0u;
     if (sort_log2) RTB_CHECK(rs.perm.reserve(4ull * cap));
     bf.perm = sort_log2 ? rs.perm.as<uint32_t>() : nullptr;
     bf.cnt = rs.cnt.as<uint32_t>();
@@ -1176,14 +1206,9 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     RTB_CUDA(cudaEventRecord(e0, st));
     RTB_CUDA(cudaMemsetAsync(bf.cnt, 0, 256, st));
     const unsigned blocks = cap / kB;
-    unsigned shadow_resident = device_slot(SLOT_SHADOW_RESIDENT);
-    if (!shadow_resident) {
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shadow, kB, 0);
-        shadow_resident = device_sm_count() * (unsigned)std::max(per_sm, 1);
-        set_device_slot(SLOT_SHADOW_RESIDENT, shadow_resident);
-    }
-    const unsigned shadow_blocks = std::min<unsigned>(shadow_resident, (scap + kB - 1) / kB);
+    const unsigned retire_blocks = std::min(blocks, resident_grid(SLOT_RETIRE_RESIDENT, k_retire, kB));
+    const unsigned shadow_blocks =
+        std::min<unsigned>(resident_grid(SLOT_SHADOW_RESIDENT, k_shadow, kB), (scap + kB - 1) / kB);
     unsigned gather_resident = device_slot(SLOT_GATHER_RESIDENT);  // persistent gather warps: every resident block
     if (gathers && !gather_resident) {
         int per_sm = 0;
@@ -1232,7 +1257,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
                 k_gather<<<gather_blocks, kGatherBlock, 0, st>>>(rv, bf, pv, cur ^ 1, gv);
                 RTB_CUDA(cudaGetLastError());
             }
-            k_retire<<<blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64, gv);
+            k_retire<<<retire_blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64, gv);
             RTB_CUDA(cudaGetLastError());
             cur ^= 1;
         }

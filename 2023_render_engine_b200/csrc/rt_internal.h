@@ -72,7 +72,9 @@ enum DeviceSlot : int {
     SLOT_SMEM_ATTRS = 3,       // bit mask of kernels whose dynamic shared-memory limit is raised (SMEM_*)
     SLOT_SM_COUNT = 4,         // multiprocessor count
     SLOT_MEM_MIB = 5,          // device memory, MiB
-    SLOT_COUNT = 6
+    SLOT_RETIRE_RESIDENT = 6,  // resident blocks of the render's k_retire
+    SLOT_SORT_RESIDENT = 7,    // resident blocks of the render's k_material_sort
+    SLOT_COUNT = 8
 };
 enum SmemAttr : unsigned { SMEM_RENDER_INFER = 1u, SMEM_GUIDE_TRAIN = 2u, SMEM_GUIDE_EVAL = 4u };
 // Value of `slot` for the current device; 0 until set_device_slot stored one.

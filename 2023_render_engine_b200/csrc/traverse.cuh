@@ -152,7 +152,9 @@ __device__ __forceinline__ void trav_init(Trav &T, float ox, float oy, float oz,
 // hold at most 3 triangles, so the per-step phase vote costs more than the packing saves).
 // Two smaller rewrites of the box test were slower too (render / trace Mrays/s, against
 // 1837 / 3130): bytes turned into floats through the mantissa of 2^23 (1815 / 3067), and a
-// minimum instead of the sorting network when one interior child is hit (1824 / 3086).
+// minimum instead of the sorting network when one interior child is hit (1824 / 3086). Shadow
+// rays (any hit) gain from the near-to-far order too: pushing their children unsorted, or only
+// the nearest first, rendered at 2140 and 2112 against 2228 Mrays/s (2^26 paths).
 // Returns true when the ray is done (T.ok = false if the stack or step cap was exceeded).
 __device__ __forceinline__ bool trav_step(const SceneView &v, Trav &T, bool anyhit)
 {
