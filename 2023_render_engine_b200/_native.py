@@ -18,6 +18,7 @@ LIB_PATH = Path(os.environ["RT_B200_LIB"]) if os.environ.get("RT_B200_LIB") else
 RT_OK = 0
 RT_TRACE_SHADOW = 0x1
 RT_TRACE_FAST = 0x2
+RT_TRACE_COUNT_ANY = 0x4
 RT_PRIM_SHAPE = 0x40000000
 
 STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID", 2: "RT_ERR_CUDA", 3: "RT_ERR_OOM", 4: "RT_ERR_TIMEOUT",
@@ -146,6 +147,7 @@ SIGNATURES = {
     "rt_trace_closest_noalloc": [_P, _P, _U64, _P, _U32],
     "rt_trace_any": [_P, _P, _U64, _P, _U32],
     "rt_trace_any_bits": [_P, _P, _U64, _P, _U32],
+    "rt_trace_counts": [_P, _P, _U64, _U32, _P],
     "rt_trace_stats_get": [_P, ctypes.POINTER(TraceStats)],
     "rt_scene_set_materials": [_P, _P, _U32],
     "rt_scene_set_triangle_materials": [_P, _U32, _U32, _P],

@@ -146,6 +146,14 @@ class Scene:
             n = rays_dev.numel() // 8
         N.check(N.lib().rt_trace_any_bits(self.handle, rays_dev.data_ptr(), n, bits_dev.data_ptr(), flags))
 
+    def trace_counts(self, rays_dev, counts_dev, n: int | None = None, flags: int = 0):
+        """Traversal work per ray: counts_dev (2n int32) gets, for ray i, the BVH8 nodes visited
+        (80 B each) and the triangle records tested (48 B each) by the closest-hit walk, or by
+        the any-hit walk with N.RT_TRACE_COUNT_ANY."""
+        if n is None:
+            n = rays_dev.numel() // 8
+        N.check(N.lib().rt_trace_counts(self.handle, rays_dev.data_ptr(), n, flags, counts_dev.data_ptr()))
+
     # ---- rendering ----
     def set_materials(self, mats):
         arr = (N.Material * len(mats))(*mats)

@@ -495,6 +495,26 @@ int rt_trace_any_bits(rt_scene *s, const rt_ray *rays, uint64_t n, uint32_t *occ
     return trace_any_common(s, rays, n, occluded_bits, true, flags, "rt_trace_any_bits");
 }
 
+int rt_trace_counts(rt_scene *s, const rt_ray *rays, uint64_t n, uint32_t flags, uint32_t *counts)
+{
+    if (!s) return fail(RT_ERR_INVALID, "rt_trace_counts: null scene");
+    if (s->merged) return fail(RT_ERR_UNSUPPORTED, "rt_trace_counts: not available on a merged scene");
+    if (!s->committed) return fail(RT_ERR_STATE, "rt_trace_counts: scene not committed");
+    if (n && (!rays || !counts)) return fail(RT_ERR_INVALID, "rt_trace_counts: null buffer");
+    if (n >= 0x80000000ull) return fail(RT_ERR_INVALID, "rt_trace_counts: at most 2^31-1 rays per call");
+    if ((reinterpret_cast<uintptr_t>(rays) & 15u) || (reinterpret_cast<uintptr_t>(counts) & 7u))
+        return fail(RT_ERR_INVALID, "rt_trace_counts: rays must be 16-byte and counts 8-byte aligned");
+    if (n == 0) return RT_OK;
+    RTB_CUDA(cudaSetDevice(s->ctx->device));
+    cudaStream_t st = s->ctx->stream;
+    RTB_CHECK(launch_trace_counts(s->view(), rays, n, flags & RT_TRACE_SHADOW, (flags & RT_TRACE_COUNT_ANY) != 0,
+                                  counts, s->scratch.counters.as<uint32_t>(), st));
+    uint32_t c[4] = {0, 0, 0, 0};
+    RTB_CUDA(cudaMemcpyAsync(c, s->scratch.counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, st));
+    RTB_CUDA(cudaStreamSynchronize(st));
+    return check_device_status(c[1]);
+}
+
 int rt_trace_stats_get(rt_scene *s, rt_trace_stats *out)
 {
     if (!s || !out) return fail(RT_ERR_INVALID, "rt_trace_stats_get: null argument");

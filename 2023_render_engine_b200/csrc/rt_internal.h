@@ -207,6 +207,8 @@ int launch_occlusion_from_hits(const rt_ray *rays, uint64_t n, const rt_hit *hit
                                cudaStream_t s);
 // Any-hit occlusion of n rays: one byte per ray, or (bits) bit i % 32 of word i / 32 (the last
 // word's bits past n are 0).
+int launch_trace_counts(const SceneView &v, const rt_ray *rays, uint64_t n, uint32_t flags, bool anyhit,
+                        uint32_t *counts, uint32_t *counters, cudaStream_t s);
 int launch_trace_any(const SceneView &v, const rt_ray *rays, uint64_t n, void *out, bool bits, uint32_t flags,
                      uint32_t *counters, cudaStream_t s);
 

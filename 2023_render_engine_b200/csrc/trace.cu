@@ -101,6 +101,29 @@ __global__ void __launch_bounds__(kBlock, RTB_TRAV_MIN_BLOCKS) k_trace_closest(S
         });
 }
 
+// Traversal work per ray (rt_trace_counts): the persistent walk of k_trace_closest without its
+// exactness checks (closest hit) or the any-hit walk of the renderer's shadow rays, writing for
+// ray i the BVH8 nodes it visited and the triangle records it tested.
+__global__ void __launch_bounds__(kBlock, RTB_TRAV_MIN_BLOCKS) k_trace_counts(SceneView v, const rt_ray *__restrict__ rays,
+                                                                             uint64_t n, uint32_t flags, bool anyhit,
+                                                                             uint2 *__restrict__ counts,
+                                                                             uint32_t *__restrict__ counters)
+{
+    const bool shadow = (flags & RT_TRACE_SHADOW) != 0;
+    persistent_traverse<true>(
+        v, (uint32_t)n, counters + 3, anyhit,
+        [&](uint32_t i, Trav &T) {
+            float4 ra, rb;
+            load_ray(rays, i, ra, rb);
+            trav_init(T, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, ra.w, scene_root(v, 0));
+            T.shadow = shadow;
+        },
+        [&](uint32_t i, Trav &T) {
+            if (!T.ok) atomicCAS(counters + 1, 0u, (uint32_t)DEV_STACK_OVERFLOW);
+            counts[i] = make_uint2(T.cur == kNoRoot ? 0u : T.steps, T.tested);
+        });
+}
+
 __global__ void __launch_bounds__(kBlock) k_trace_exact(SceneView v, const rt_ray *__restrict__ rays,
                                                         rt_hit *__restrict__ hits, uint32_t flags,
                                                         const uint32_t *__restrict__ queue, uint32_t queue_cap,
@@ -247,6 +270,18 @@ int launch_trace_closest_dev(const SceneView &v, const rt_ray *rays, const uint3
     k_trace_closest<<<(unsigned)blocks, kBlock, 0, s>>>(v, rays, cap, n_dev, hits, flags, queue, cap, counters);
     RTB_CUDA(cudaGetLastError());
     k_trace_exact<<<exact_blocks(), kBlock, 0, s>>>(v, rays, hits, flags, queue, cap, counters);
+    RTB_CUDA(cudaGetLastError());
+    return RT_OK;
+}
+
+int launch_trace_counts(const SceneView &v, const rt_ray *rays, uint64_t n, uint32_t flags, bool anyhit,
+                        uint32_t *counts, uint32_t *counters, cudaStream_t s)
+{
+    if (n == 0) return RT_OK;
+    RTB_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), s));
+    const uint64_t blocks = std::min<uint64_t>((n + kBlock - 1) / kBlock, persistent_blocks());
+    k_trace_counts<<<(unsigned)blocks, kBlock, 0, s>>>(v, rays, n, flags, anyhit, reinterpret_cast<uint2 *>(counts),
+                                                       counters);
     RTB_CUDA(cudaGetLastError());
     return RT_OK;
 }

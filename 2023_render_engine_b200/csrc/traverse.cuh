@@ -98,6 +98,7 @@ struct Trav {
     bool ok;
     bool shadow;  // checkShadow semantics: transparent primitives are skipped
     Best best;
+    uint32_t tested;  // triangle records tested (counted by the COUNT walk only; steps counts nodes)
     uint2 st[kStack];  // node index, entry distance bits: one 8-byte local access per push / pop
 };
 
@@ -140,6 +141,7 @@ __device__ __forceinline__ void trav_init(Trav &T, float ox, float oy, float oz,
     T.ok = true;
     T.shadow = false;
     T.best = Best{INFINITY, -1, 0u, 0.f, 0.f, INFINITY};
+    T.tested = 0;
 }
 
 // Visits node T.cur: tests its eight quantized child boxes (unrolled), the triangles of the
@@ -156,6 +158,7 @@ __device__ __forceinline__ void trav_init(Trav &T, float ox, float oy, float oz,
 // rays (any hit) gain from the near-to-far order too: pushing their children unsorted, or only
 // the nearest first, rendered at 2140 and 2112 against 2228 Mrays/s (2^26 paths).
 // Returns true when the ray is done (T.ok = false if the stack or step cap was exceeded).
+template <bool COUNT = false>
 __device__ __forceinline__ bool trav_step(const SceneView &v, Trav &T, bool anyhit)
 {
     const bool shadow = T.shadow;
@@ -206,6 +209,7 @@ __device__ __forceinline__ bool trav_step(const SceneView &v, Trav &T, bool anyh
         leafmask &= leafmask - 1;
         const uint32_t meta = byte_of(k < 4 ? meta_lo : meta_hi, k & 3);
         const uint32_t first = tri_base + (meta & 31u), cnt = (meta >> 5) + 1;
+        if (COUNT) T.tested += cnt;
 #pragma unroll 1
         for (uint32_t j = 0; j < cnt; j++) test_triangle(T.w, v.tris, first + j, shadow, T.best);
         if (anyhit && T.best.prim >= 0) return true;
@@ -268,7 +272,8 @@ __device__ __forceinline__ bool traverse_bvh8(const SceneView &v, const Watertig
 // Persistent-warp driver: every lane runs its own ray; a lane whose ray is done fetches the
 // next ray index from *work (one atomic per fetching warp) until n is exhausted.
 // init(i, T) prepares ray i (trav_init + T.shadow), finish(i, T) consumes the result.
-template <typename Init, typename Finish>
+// COUNT: the walk also counts the triangle records it tests (T.tested), for rt_trace_counts.
+template <bool COUNT = false, typename Init, typename Finish>
 __device__ __forceinline__ void persistent_traverse(const SceneView &v, uint32_t n, uint32_t *work, bool anyhit,
                                                     Init init, Finish finish)
 {
@@ -295,7 +300,7 @@ __device__ __forceinline__ void persistent_traverse(const SceneView &v, uint32_t
         }
         if (__all_sync(0xFFFFFFFFu, ray == 0xFFFFFFFFu)) break;
         if (ray != 0xFFFFFFFFu) {
-            if (T.cur == kNoRoot || trav_step(v, T, anyhit)) {
+            if (T.cur == kNoRoot || trav_step<COUNT>(v, T, anyhit)) {
                 finish(ray, T);
                 ray = 0xFFFFFFFFu;
             }

@@ -391,6 +391,46 @@ def measure_guiding(args, core, N, cfgs, ctx, torch):
     }
 
 
+def traversal_work(N, torch, sc, rays_d, n, ms=None, any_hit=False):
+    """Per-ray traversal work from rt_trace_counts: BVH8 nodes visited (80 B each) and triangle
+    records tested (48 B each), their bytes per ray (mean and percentiles) and, given the trace
+    call's time, the rate at which the walk reads node and triangle bytes (L2 or HBM)."""
+    cnt = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+    sc.trace_counts(rays_d, cnt, n, flags=N.RT_TRACE_COUNT_ANY if any_hit else 0)
+    c = cnt.view(n, 2).to(torch.float64)
+    b = 80.0 * c[:, 0] + 48.0 * c[:, 1]
+    srt = torch.sort(b).values
+    pick = lambda q: float(srt[min(n - 1, int(q * n))])
+    out = {"rays": n, "walk": "any hit" if any_hit else "closest hit",
+           "nodes_per_ray": float(c[:, 0].mean()), "triangles_per_ray": float(c[:, 1].mean()),
+           "bytes_per_ray": {"mean": float(b.mean()), "p50": pick(0.5), "p90": pick(0.9), "p99": pick(0.99),
+                             "max": float(srt[-1])}}
+    if ms:
+        out["walk_gbs"] = float(b.sum()) / (ms / 1000) / 1e9
+    del cnt
+    return out
+
+
+def measure_traversal_work(N, torch, core, S, cfgs, ctx, sc1, rays_d, n, ms_trace):
+    """bytes per ray of the walk on fixed ray sets: the 2^24-ray set of the BVH-stress scene
+    (closest and any hit), and 2^20 rays with origins uniform in the bounding box of configs 0, 2
+    and 4 (closest hit)."""
+    res = {"config 1 (BVH stress)": traversal_work(N, torch, sc1, rays_d, n, ms=ms_trace),
+           "config 1 (BVH stress), any hit": traversal_work(N, torch, sc1, rays_d, n, any_hit=True)}
+    boxes = {"config 0 (Cornell box)": (cfgs.build_config0, (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)),
+             "config 2 (guiding room)": (cfgs.build_config2, (-2.0, 0.0, -2.0), (2.0, 2.5, 2.0)),
+             "config 4 (terrain)": (cfgs.build_config4, (-4.0, -0.4, -4.0), (4.0, 1.2, 4.0))}
+    m = 1 << 20
+    for name, (build, lo, hi) in boxes.items():
+        sc = build(ctx)[0]
+        o, d = S.random_rays(m, seed=17, lo=np.array(lo), hi=np.array(hi))
+        r = torch.from_numpy(core.make_rays(o, d).view(np.float32).reshape(-1)).cuda()
+        res[name] = traversal_work(N, torch, sc, r, m)
+        sc.close()
+        del r
+    return res
+
+
 def measure_guide_inference(core, cfgs, ctx, torch, stream, rows):
     """rt_guide_eval on `rows` seeded queries (positions in the guiding room's box, unit normals
     and directions): the network forward on the tensor cores (tcgen05), encoding and output
@@ -525,6 +565,9 @@ def run_ours(args):
     barrier()
     ms_trace = t0.elapsed_time(t1) / args.steps
     fallback = sc.trace_stats()["exact_fallback_rays"]
+    trav_work = None
+    if world == 1 and not args.no_traversal_work:
+        trav_work = measure_traversal_work(N, torch, core, S, cfgs, ctx, sc, rays_d, NRAYS, ms_trace)
 
     # ---- learned guiding: time to RMSE <= target against the FP64 converged render, guided vs
     # plain, on the guiding room (one process only: it is a sequence of dependent passes)
@@ -609,7 +652,9 @@ def run_ours(args):
                             "of a step are the camera and options structs"},
             "trace": {"workload": TRACE_WORKLOAD.format(NRAYS.bit_length() - 1), "value": trace_rate, "unit": "Mrays/s", "ms_per_step": ms_trace,
                       "exact_fallback_rays": int(fallback)},
-            "gpu_launches": int(st_last["waves"]) * 5 + 1,
+            # per frame: 6 kernels a wave (closest hit, its replay, material sort, shade, shadow,
+            # retire), the wave check of each 4-wave group and the first camera rays
+            "gpu_launches": args.steps * (int(st_last["waves"]) * 6 + (int(st_last["waves"]) + 3) // 4 + 1),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": (TRACE_TRAFFIC_BYTES_2_24 / (ms_trace / 1000) / 1e9) if NRAYS == 1 << 24 else None,
@@ -619,6 +664,7 @@ def run_ours(args):
                                  "of the full launch: 4.3x the algorithmic bytes, the scene re-read past L2 and the "
                                  "traversal stacks in local memory; see profiles/"},
             "clocks": clk.summary(),
+            "traversal_work": trav_work,
             "guiding": guiding,
             "guide_inference": guide_inference,
             "reference_cuda": ref_cuda,
@@ -668,6 +714,7 @@ def main():
     ap.add_argument("--guide-ref-spp", type=int, default=4096, help="0 skips the guiding measurement")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip the reference CUDA traversal baseline")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view measurement")
+    ap.add_argument("--no-traversal-work", action="store_true", help="skip the per-ray traversal work counts")
     ap.add_argument("--c4-spp", type=int, default=256, help="config-4 spp per mode (0 skips config 4)")
     ap.add_argument("--c4-width", type=int, default=3840)
     ap.add_argument("--c4-height", type=int, default=2160)

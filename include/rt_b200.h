@@ -147,6 +147,7 @@ typedef struct rt_hit {
 /* Trace flags. */
 #define RT_TRACE_SHADOW 0x1u /* checkShadow semantics: skip transparent primitives */
 #define RT_TRACE_FAST 0x2u   /* skip the reference-order exactness checks */
+#define RT_TRACE_COUNT_ANY 0x4u /* rt_trace_counts: count the any-hit walk instead of the closest-hit one */
 
 /* Closest hit for n rays, device pointers. Replaces BVH::intersectRays
  * (cuda_libraries/BVH.cu:541-584) followed by the analytic-shape loop of
@@ -186,6 +187,15 @@ RT_API int rt_trace_any(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, uin
  * (ceil(n / 32) words, 4-byte aligned; the last word's bits past n are 0). */
 RT_API int rt_trace_any_bits(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, uint32_t *occluded_bits_dev,
                              uint32_t flags);
+
+/* Traversal work per ray, the numerator of a traversal roofline (new in this library; the
+ * reference has no counterpart). Walks the rays as rt_trace_closest does with RT_TRACE_FAST
+ * (or, with RT_TRACE_COUNT_ANY, as rt_trace_any does with RT_TRACE_FAST: the renderer's
+ * shadow rays, stopping at the first hit before tmax) and writes, for ray i,
+ * counts_dev[2i] = BVH8 nodes visited (80 bytes each) and counts_dev[2i+1] = triangle records
+ * tested (48 bytes each). Writes no hits. RT_TRACE_SHADOW: transparent primitives are skipped.
+ * counts_dev: 2n uint32, 8-byte aligned. */
+RT_API int rt_trace_counts(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, uint32_t flags, uint32_t *counts_dev);
 
 /* Counters of the last rt_trace_closest call: rays that took the reference-order
  * exact traversal (distance ties resolved through the reference tree, grazing

@@ -399,3 +399,61 @@ def test_planes_match_reference(core, gpu_ctx, refo):
             # a plane hit reports its object-space (x, y) in the unit square
             assert np.all((h["b1"][plane_hits] >= 0) & (h["b1"][plane_hits] <= 1))
         sc.close()
+
+
+def trace_counts(sc, o, d, tmax=None, flags=0):
+    import torch
+
+    rays = core_make_rays(o, d, tmax)
+    rd = torch.from_numpy(rays.view(np.float32).reshape(-1)).cuda()
+    cd = torch.full((2 * o.shape[0],), -1, dtype=torch.int32, device="cuda")
+    sc.trace_counts(rd, cd, o.shape[0], flags)
+    torch.cuda.synchronize()
+    c = cd.cpu().numpy().reshape(-1, 2)
+    return c[:, 0].copy(), c[:, 1].copy()
+
+
+@pytest.mark.parametrize("key", ["soup1000", "soup20000", "grids"])
+def test_trace_counts_invariants(core, gpu_ctx, key):
+    """rt_trace_counts against what the walk must do: every ray of a non-empty scene visits the
+    root and at most every node; a ray with a triangle hit tested at least one triangle; the
+    any-hit walk is the closest-hit walk stopped at the first hit, so it never counts more and
+    counts the same where nothing is hit; the counts are reproducible."""
+    g = _unpack(np.load(GOLDEN / "trace_small.npz"), key)
+    sc = make_scene(core, gpu_ctx, g["v"], g["f"])
+    nnodes = sc.stats()["bvh8_nodes"]
+    nodes, tris = trace_counts(sc, g["o"], g["d"])
+    assert np.all(nodes >= 1) and np.all(nodes <= nnodes)
+    ids, _, _ = trace_gpu(sc, g["o"], g["d"], flags=N.RT_TRACE_FAST)
+    assert np.all(tris[ids >= 0] >= 1)
+    an, at = trace_counts(sc, g["o"], g["d"], flags=N.RT_TRACE_COUNT_ANY)
+    assert np.all(an <= nodes) and np.all(at <= tris)
+    miss = ids < 0
+    assert np.array_equal(an[miss], nodes[miss]) and np.array_equal(at[miss], tris[miss])
+    assert np.any(an[~miss] < nodes[~miss])  # the any-hit walk does stop early
+    n2, t2 = trace_counts(sc, g["o"], g["d"])
+    assert np.array_equal(n2, nodes) and np.array_equal(t2, tris)
+
+
+def test_trace_counts_small_and_invalid(core, gpu_ctx):
+    import torch
+
+    # one triangle: the walk is the root alone; its leaf is tested when the ray meets its box
+    v = np.array([[-1, -1, 0], [1, -1, 0], [0, 1, 0]], np.float32)
+    sc1 = make_scene(core, gpu_ctx, v, np.array([[0, 1, 2]], np.uint32))
+    # (a ray with a zero direction component sees that axis's slab as unbounded, which keeps
+    # the box test conservative: the second ray is oblique so that it misses the leaf's box)
+    o = np.array([[0, 0, 1], [5, 5, 1], [0, 0, 1]], np.float32)
+    d = np.array([[0, 0, -1], [0.1, 0.1, -1], [0, 0, 1]], np.float32)
+    nodes, tris = trace_counts(sc1, o, d)
+    assert nodes.tolist() == [1, 1, 1] and tris.tolist() == [1, 0, 0]
+    # no triangles: nothing is walked
+    sc0 = make_scene(core, gpu_ctx, np.zeros((0, 3), np.float32), np.zeros((0, 3), np.uint32))
+    nodes, tris = trace_counts(sc0, o, d)
+    assert nodes.tolist() == [0, 0, 0] and tris.tolist() == [0, 0, 0]
+    # zero rays is a no-op; a misaligned count buffer is refused
+    rd = torch.empty(8, dtype=torch.float32, device="cuda")
+    cd = torch.empty(4, dtype=torch.int32, device="cuda")
+    sc1.trace_counts(rd, cd, 0)
+    with pytest.raises(N.RtError):
+        N.check(N.lib().rt_trace_counts(sc1.handle, rd.data_ptr(), 1, 0, cd.data_ptr() + 4))
