@@ -71,10 +71,9 @@ enum DeviceSlot : int {
     SLOT_GATHER_RESIDENT = 2,  // resident blocks of the render's k_gather
     SLOT_SMEM_ATTRS = 3,       // bit mask of kernels whose dynamic shared-memory limit is raised (SMEM_*)
     SLOT_SM_COUNT = 4,         // multiprocessor count
-    SLOT_MEM_MIB = 5,          // device memory, MiB
-    SLOT_RETIRE_RESIDENT = 6,  // resident blocks of the render's k_retire
-    SLOT_SORT_RESIDENT = 7,    // resident blocks of the render's k_material_sort
-    SLOT_COUNT = 8
+    SLOT_RETIRE_RESIDENT = 5,  // resident blocks of the render's k_retire
+    SLOT_SORT_RESIDENT = 6,    // resident blocks of the render's k_material_sort
+    SLOT_COUNT = 7
 };
 enum SmemAttr : unsigned { SMEM_RENDER_INFER = 1u, SMEM_GUIDE_TRAIN = 2u, SMEM_GUIDE_EVAL = 4u };
 // Value of `slot` for the current device; 0 until set_device_slot stored one.
@@ -83,8 +82,6 @@ void set_device_slot(DeviceSlot slot, unsigned value);
 void or_device_slot(DeviceSlot slot, unsigned bits);
 // Multiprocessor count of the current device (cached).
 unsigned device_sm_count();
-// Total memory of the current device in MiB (cached).
-unsigned device_mem_mib();
 
 // Error codes written by kernels into the status word (first failure wins).
 enum DevError : uint32_t {

@@ -372,7 +372,8 @@ typedef struct rt_view {
  * pixel sum over k < i of width_k * height_k in sum_rgb (3 floats per pixel), count and sum64
  * (nullable). A view renders exactly the samples rt_render would give it with the same
  * options. flags: RT_RENDER_* for all views; max_paths: queue capacity (0: automatic, the largest
- * power of two up to 2^26 paths whose buffers fit in an eighth of the device's memory). */
+ * power of two up to 2^26 paths whose buffers fit in the smaller of an eighth of the device's
+ * memory and a quarter of its free memory, never more paths than the call's samples). */
 RT_API int rt_render_batch(rt_scene *scene, const rt_view *views, uint32_t nviews, uint32_t flags, uint32_t max_paths,
                            float *sum_rgb, uint32_t *count, double *sum64, rt_render_stats *stats);
 
