@@ -139,6 +139,8 @@ def measure_guided(scene, flags, views, guide, sync, capacity=0, train_passes=4,
     sync()
     t_train = time.perf_counter() - t0
     scene.set_guide(guide, train=False)
+    # warm at full size: the guided queues (and the per-path mixtures) grow here, not in the timed call
+    scene.render_batch(views, flags=flags | N.RT_RENDER_GUIDE, max_paths=capacity)
     t_g, (film, st, _) = _timed(lambda: scene.render_batch(views, flags=flags | N.RT_RENDER_GUIDE,
                                                            max_paths=capacity), sync)
     rays_g = st["extension_rays"] + st["shadow_rays"]

@@ -58,6 +58,21 @@ unsigned device_sm_count()
     return n;
 }
 
+unsigned device_mem_mib()
+{
+    unsigned m = device_slot(SLOT_MEM_MIB);
+    if (!m) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            (void)cudaGetLastError();
+            total_b = 0;
+        }
+        m = (unsigned)std::max<size_t>(total_b >> 20, 1);
+        set_device_slot(SLOT_MEM_MIB, m);
+    }
+    return m;
+}
+
 int DevBuf::reserve(size_t n)
 {
     if (n <= bytes && ptr) return RT_OK;

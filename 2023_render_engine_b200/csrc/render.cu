@@ -1047,25 +1047,32 @@ unsigned resident_grid(DeviceSlot slot, Kernel kernel, int block)
 }
 
 // Path capacity when the caller gives none: the largest power of two of at most 2^26 paths
-// whose wave buffers fit in the smaller of an eighth of the device's memory and a quarter of
-// what is free now (queues the scene already holds count as free: they are reused). Fewer,
-// larger waves shorten the time the persistent traversal kernels spend draining their last
-// rays, wave after wave. BVH-stress render at 1920x1080 x 64 spp (244 B per path), Mrays/s:
-// 1585 / 1806 / 1947 / 2074 / 2130 / 2189 for 2^21 / 2^22 / 2^23 / 2^24 / 2^25 / 2^26 paths.
-uint32_t default_paths(uint32_t flags, uint32_t per_path_shadow, uint64_t held_paths)
+// whose wave buffers fit in an eighth of the device's memory; when the call needs more queue
+// than the scene holds, also in a quarter of what is free (the queues held count as free, as
+// they are reused), so that several scenes in one process shrink each other's default. The
+// free-memory query runs only when the queues must grow: it is not free (milliseconds with
+// many allocations live). Fewer, larger waves shorten the time the persistent traversal
+// kernels spend draining their last rays, wave after wave. BVH-stress render at 1920x1080 x 64
+// spp (244 B per path), Mrays/s: 1585 / 1806 / 1947 / 2074 / 2130 / 2189 for 2^21 / 2^22 /
+// 2^23 / 2^24 / 2^25 / 2^26 paths.
+uint32_t default_paths(uint32_t flags, uint32_t per_path_shadow, uint64_t held_paths, uint64_t samples)
 {
     uint64_t bytes = 64 + 96 + 16 + 16 + 4;  // rays, path state, hits, retire, shading order
     bytes += 48ull * std::max<uint32_t>(per_path_shadow, 1);
     if (flags & (RT_RENDER_PHOTON_MAP | RT_RENDER_SUBSURFACE | RT_RENDER_HYBRID)) bytes += 2ull * 16 * kGatherWords;
     if (flags & RT_RENDER_GUIDE) bytes += 208 + 4;
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-        (void)cudaGetLastError();
-        free_b = total_b = 0;
-    }
-    const uint64_t budget = std::min<uint64_t>(total_b / 8, (free_b + held_paths * bytes) / 4);
+    const uint64_t total_b = (uint64_t)device_mem_mib() << 20;
     uint32_t cap = 1u << 26;
-    while (cap > (1u << 20) && cap > held_paths && (uint64_t)cap * bytes > budget) cap >>= 1;
+    while (cap > (1u << 20) && (uint64_t)cap * bytes > total_b / 8) cap >>= 1;
+    const uint64_t need = std::min<uint64_t>(cap, std::max<uint64_t>(samples, 1024));
+    if (need <= held_paths) return cap;  // the queues held already cover the call
+    size_t free_b = 0, tb = 0;
+    if (cudaMemGetInfo(&free_b, &tb) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return cap;
+    }
+    const uint64_t budget = (free_b + held_paths * bytes) / 4;
+    while (cap > (1u << 20) && cap > held_paths && std::min<uint64_t>(cap, need) * bytes > budget) cap >>= 1;
     return cap;
 }
 
@@ -1109,7 +1116,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     RTB_CHECK(rs.view_sample0.upload(sample0.data(), 8ull * (nviews + 1), st));
     RTB_CHECK(rs.view_pixel0.upload(pixel0.data(), 4ull * (nviews + 1), st));
     const uint32_t per_path_shadow = (uint32_t)(s->plights.size() / 2) + ((flags & RT_RENDER_NEE_AREA) ? 1 : 0);
-    uint32_t cap = max_paths ? max_paths : default_paths(flags, per_path_shadow, rs.rays[0].bytes / 32);
+    uint32_t cap = max_paths ? max_paths : default_paths(flags, per_path_shadow, rs.rays[0].bytes / 32, total);
     cap = (uint32_t)std::min<uint64_t>(cap, std::max<uint64_t>(total, 1024));
     cap = (cap + kB - 1) / kB * kB;
     const uint32_t scap = std::max<uint32_t>(cap * std::max<uint32_t>(per_path_shadow, 1), kB);

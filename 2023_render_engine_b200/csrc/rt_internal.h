@@ -73,7 +73,8 @@ enum DeviceSlot : int {
     SLOT_SM_COUNT = 4,         // multiprocessor count
     SLOT_RETIRE_RESIDENT = 5,  // resident blocks of the render's k_retire
     SLOT_SORT_RESIDENT = 6,    // resident blocks of the render's k_material_sort
-    SLOT_COUNT = 7
+    SLOT_MEM_MIB = 7,          // device memory, MiB
+    SLOT_COUNT = 8
 };
 enum SmemAttr : unsigned { SMEM_RENDER_INFER = 1u, SMEM_GUIDE_TRAIN = 2u, SMEM_GUIDE_EVAL = 4u };
 // Value of `slot` for the current device; 0 until set_device_slot stored one.
@@ -82,6 +83,8 @@ void set_device_slot(DeviceSlot slot, unsigned value);
 void or_device_slot(DeviceSlot slot, unsigned bits);
 // Multiprocessor count of the current device (cached).
 unsigned device_sm_count();
+// Total memory of the current device in MiB (cached).
+unsigned device_mem_mib();
 
 // Error codes written by kernels into the status word (first failure wins).
 enum DevError : uint32_t {

@@ -60,11 +60,14 @@ def measure(ctx, torch, stream, width=3840, height=2160, spp=None, photons=None,
     sc.render(small, spp=1, max_depth=p["max_depth"], seed=1, flags=fl)
     torch.cuda.synchronize()
 
-    # 1. photon trace
-    ms_trace, (pm, pst) = _event_ms(torch, stream,
-                                    lambda: sc.trace_photons(photons, max_depth=16, seed=seed + 1))
-    out["photon_trace"] = {"ms": ms_trace, "emitted": int(pst["emitted"]), "stored": len(pm),
-                           "rays": int(pst["rays"]), "emitted_per_s": pst["emitted"] / (ms_trace / 1000),
+    # 1. photon trace. The call allocates the new map's buffers before its kernels run; its own
+    # event-timed figure (pst["ms"]) covers the kernels, the outer one the allocations too, which
+    # vary with how much device memory the process already holds
+    ms_call, (pm, pst) = _event_ms(torch, stream, lambda: sc.trace_photons(photons, max_depth=16, seed=seed + 1))
+    ms_trace = pst["ms"]
+    out["photon_trace"] = {"ms": ms_trace, "ms_with_allocation": ms_call, "emitted": int(pst["emitted"]),
+                           "stored": len(pm), "rays": int(pst["rays"]),
+                           "emitted_per_s": pst["emitted"] / (ms_trace / 1000),
                            "Mrays_per_s": pst["rays"] / (ms_trace / 1000) / 1e6}
     # 2. kd-tree (host build over the device photons, then upload)
     t0 = time.perf_counter()
