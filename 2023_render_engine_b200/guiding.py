@@ -104,3 +104,37 @@ def time_to_rmse(scene, camera, ref_mean, target: float, guide=None, pass_spp: i
             scene.set_guide(guide, train=False)
     spp, seconds, e = curve[-1]
     return {"seconds": seconds, "spp": spp, "rmse": e, "reached": state["done"], "curve": curve}
+
+
+def profile_passes(width: int = 1280, height: int = 720, guided_passes: int = 2, pass_spp: int = 4):
+    """The guiding room's schedule with the host-side wave loop, for profiler launch lists (ncu
+    does not list the kernels inside the device loop's conditional graph): the training passes
+    (one spp, then the configured Adam steps), then `guided_passes` pairs of a guided and a plain
+    pass of `pass_spp`. Every render call starts with one k_start launch."""
+    import torch
+
+    from . import configs, core
+
+    torch.cuda.set_device(0)
+    ctx = core.Context(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    sc, cam, _ = configs.build_config2(ctx, width, height)
+    flags = N.RT_RENDER_NEE_AREA | N.RT_RENDER_HOST_LOOP
+    T = configs.GUIDE_TRAINING
+    g = core.Guide(ctx, T["bbox_min"], T["bbox_max"], learning_rate=T["learning_rate"], seed=2,
+                   max_depth=T["max_depth"])
+    sc.set_guide(g, train=True)
+    for i in range(T["train_passes"]):
+        sc.render(cam, spp=1, max_depth=16, rr_depth=3, seed=7 + i, flags=flags | N.RT_RENDER_GUIDE)
+        g.train_records(T["steps_per_pass"], T["batch"], seed=i)
+    sc.set_guide(g, train=False)
+    for k in range(guided_passes):
+        sc.render(cam, spp=pass_spp, max_depth=16, rr_depth=3, seed=100 + k, flags=flags | N.RT_RENDER_GUIDE)
+        sc.render(cam, spp=pass_spp, max_depth=16, rr_depth=3, seed=200 + k, flags=flags)
+    torch.cuda.synchronize()
+
+
+if __name__ == "__main__":
+    profile_passes()
