@@ -162,3 +162,23 @@ def test_device_wave_loop_equals_host_loop(core, gpu_ctx):
     assert sa["extension_rays"] == sb["extension_rays"] and sa["shadow_rays"] == sb["shadow_rays"]
     assert sa["waves"] == sb["waves"] and sa["waves"] > 8
     assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+
+
+def test_path_capacity_leaves_the_image_unchanged(core, gpu_ctx):
+    """The capacity (paths in flight) only decides how many waves a frame takes: every sample
+    keeps its own random stream, so small queues, the automatic capacity (max_paths 0: here
+    all of the frame's samples at once) and a capacity above the samples give the same rays
+    and the same image up to the order of film additions; the retire and sort kernels'
+    grid-stride loops see from one to many chunks per block."""
+    cfgs = importlib.import_module("2023_render_engine_b200.configs")
+    sc, cam, p = cfgs.build_config0(gpu_ctx, 64, 48)
+    flags = N.RT_RENDER_NEE_AREA
+    out = []
+    for cap in (1 << 10, 0, 1 << 20):
+        film, st = sc.render(cam, spp=6, max_depth=8, seed=5, flags=flags, fp64=True, max_paths=cap)
+        out.append((core.film_mean(film), st))
+    (a, sa) = out[0]
+    assert sa["waves"] > out[1][1]["waves"]
+    for b, sb in out[1:]:
+        assert sa["extension_rays"] == sb["extension_rays"] and sa["shadow_rays"] == sb["shadow_rays"]
+        assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
