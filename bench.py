@@ -660,6 +660,12 @@ def run_ours(args):
                          "traffic": (TRACE_TRAFFIC_BYTES_2_24 / (ms_trace / 1000) / 1e9) if NRAYS == 1 << 24 else None,
                          "traffic_bytes_per_launch": TRACE_TRAFFIC_BYTES_2_24 if NRAYS == 1 << 24 else None,
                          "kernel": "k_trace_closest (2^24-ray closest-hit call, 48 B/ray queue-level bytes)",
+                         # what the walk itself reads (nodes x 80 B + triangle records x 48 B per ray, counted
+                         # by rt_trace_counts), over the same launch time: mostly L1 and L2 hits
+                         "walk": ({"bytes_per_ray": trav_work["config 1 (BVH stress)"]["bytes_per_ray"]["mean"],
+                                   "gbs": trav_work["config 1 (BVH stress)"]["walk_gbs"],
+                                   "frac_of_hbm_peak": trav_work["config 1 (BVH stress)"]["walk_gbs"] / peak}
+                                  if trav_work else None),
                          "note": f"peak {peak_kind}; traffic (GB/s over the same launch time) from the ncu capture "
                                  "of the full launch: 4.3x the algorithmic bytes, the scene re-read past L2 and the "
                                  "traversal stacks in local memory; see profiles/"},
