@@ -512,6 +512,8 @@ int rt_trace_counts(rt_scene *s, const rt_ray *rays, uint64_t n, uint32_t flags,
     uint32_t c[4] = {0, 0, 0, 0};
     RTB_CUDA(cudaMemcpyAsync(c, s->scratch.counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, st));
     RTB_CUDA(cudaStreamSynchronize(st));
+    if (c[1] == DEV_STACK_OVERFLOW)
+        return fail(RT_ERR_CAPACITY, "rt_trace_counts: a ray's walk ran out of stack; its counts stop there");
     return check_device_status(c[1]);
 }
 

@@ -119,7 +119,9 @@ __global__ void __launch_bounds__(kBlock, RTB_TRAV_MIN_BLOCKS) k_trace_counts(Sc
             T.shadow = shadow;
         },
         [&](uint32_t i, Trav &T) {
-            if (!T.ok) atomicCAS(counters + 1, 0u, (uint32_t)DEV_STACK_OVERFLOW);
+            if (!T.ok)
+                atomicCAS(counters + 1, 0u,
+                          (uint32_t)(T.steps > v.nnodes + 1 ? DEV_STEP_CAP : DEV_STACK_OVERFLOW));
             counts[i] = make_uint2(T.cur == kNoRoot ? 0u : T.steps, T.tested);
         });
 }

@@ -194,7 +194,8 @@ RT_API int rt_trace_any_bits(rt_scene *scene, const rt_ray *rays_dev, uint64_t n
  * shadow rays, stopping at the first hit before tmax) and writes, for ray i,
  * counts_dev[2i] = BVH8 nodes visited (80 bytes each) and counts_dev[2i+1] = triangle records
  * tested (48 bytes each). Writes no hits. RT_TRACE_SHADOW: transparent primitives are skipped.
- * counts_dev: 2n uint32, 8-byte aligned. */
+ * counts_dev: 2n uint32, 8-byte aligned. RT_ERR_CAPACITY when a ray's walk ran out of stack
+ * (its counts stop there; the other rays' are complete). */
 RT_API int rt_trace_counts(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, uint32_t flags, uint32_t *counts_dev);
 
 /* Counters of the last rt_trace_closest call: rays that took the reference-order
