@@ -46,9 +46,9 @@ NRAYS = 1 << 24
 ALG_BYTES_PER_RAY = 48  # 32 B ray in + 16 B hit out (queue level)
 # DRAM bytes (read + write) of one k_trace_closest launch of the 2^24-ray call: the mean of the
 # four 2^24-ray launches of one ncu capture of this file's render command (1 pass, --cache-control
-# none; profiles/k_trace_closest_bvh_stress.md), taken at commit 162b555 of the traversal. A
-# change to traverse.cuh or trace.cu needs a new capture.
-TRACE_TRAFFIC_BYTES_2_24 = 2_457_424_064 + 978_677_632
+# none; profiles/k_trace_closest_bvh_stress.md), taken at commit 97e6eef of the traversal. A
+# change to traverse.cuh or trace.cu that alters k_trace_closest needs a new capture.
+TRACE_TRAFFIC_BYTES_2_24 = 2_477_571_776 + 1_031_053_120
 
 
 def dist_env():
@@ -667,7 +667,7 @@ def run_ours(args):
                                    "frac_of_hbm_peak": trav_work["config 1 (BVH stress)"]["walk_gbs"] / peak}
                                   if trav_work else None),
                          "note": f"peak {peak_kind}; traffic (GB/s over the same launch time) from the ncu capture "
-                                 "of the full launch: 4.3x the algorithmic bytes, the scene re-read past L2 and the "
+                                 "of the full launch: 4.4x the algorithmic bytes, the scene re-read past L2 and the "
                                  "traversal stacks in local memory; see profiles/"},
             "clocks": clk.summary(),
             "traversal_work": trav_work,
