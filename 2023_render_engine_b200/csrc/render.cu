@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(kSortBlock) k_material_sort(RenderView rv, Buf
 {
     __shared__ uint32_t count[kSortKeys], start[kSortKeys];
     __shared__ uint8_t key[1u << kSortMaxLog2];
+    __shared__ uint32_t wcount[kSortBlock / 32][kSortKeys];
     const uint32_t n = min(bf.cnt[cur], bf.cap);
     // chunks in a grid-stride loop over the resident blocks (c0 is the same for the whole block)
     for (uint32_t c0 = blockIdx.x << log2; c0 < n; c0 += gridDim.x << log2) {
@@ -258,8 +259,34 @@ __global__ void __launch_bounds__(kSortBlock) k_material_sort(RenderView rv, Buf
             }
         }
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < len; j += kSortBlock) perm[c0 + atomicAdd(&start[key[j]], 1u)] = c0 + j;
-        __syncthreads();  // count, start and key are reused by the next chunk
+        // stable scatter: within a key the slots keep their queue order, so that a warp of k_shade
+        // reads nearly consecutive slots of the dominant material (render 2213 against 2190-2205
+        // Mrays/s with the atomic, unordered scatter). Per 256-entry step, a slot's rank among
+        // the same key in its warp (match + popc), then the warps' counts per key scanned in
+        // warp order on top of the key's running start.
+        const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+        for (uint32_t j0 = 0; j0 < len; j0 += kSortBlock) {
+            const uint32_t j = j0 + threadIdx.x;
+            const uint32_t k = j < len ? key[j] : (uint32_t)kSortKeys;  // kSortKeys: no entry
+            if (threadIdx.x < (kSortBlock / 32) * kSortKeys) wcount[threadIdx.x / kSortKeys][threadIdx.x % kSortKeys] = 0;
+            __syncthreads();
+            const unsigned same = __match_any_sync(0xFFFFFFFFu, k);
+            const unsigned below = same & ((1u << lane) - 1u);
+            if (below == 0 && k < (uint32_t)kSortKeys) wcount[warp][k] = __popc(same);
+            __syncthreads();
+            if (threadIdx.x < kSortKeys) {
+                uint32_t acc = start[threadIdx.x];
+                for (int w = 0; w < kSortBlock / 32; w++) {
+                    const uint32_t c = wcount[w][threadIdx.x];
+                    wcount[w][threadIdx.x] = acc;
+                    acc += c;
+                }
+                start[threadIdx.x] = acc;
+            }
+            __syncthreads();
+            if (k < (uint32_t)kSortKeys) perm[c0 + wcount[warp][k] + __popc(below)] = c0 + j;
+            __syncthreads();  // wcount, and after the last step count, start and key, are reused
+        }
     }
 }
 
