@@ -82,6 +82,8 @@ RT_RENDER_COMPAT = 0x2
 RT_RENDER_EXACT_TRACE = 0x4
 RT_RENDER_PHOTON_MAP = 0x8
 RT_RENDER_GUIDE = 0x10
+RT_RENDER_STAGE_TIMES = 0x100
+RENDER_STAGES = ("trace", "guide_inference", "material_sort", "shade", "shadow", "gather", "retire")
 RT_BUILD_DEVICE, RT_BUILD_HOST = 0, 1
 (RT_TONEMAP_EQUALIZE, RT_TONEMAP_REINHARD, RT_TONEMAP_REINHARD_JODIE, RT_TONEMAP_ACES, RT_TONEMAP_UNCHARTED2,
  RT_TONEMAP_GAMMA_CLAMP) = range(6)
@@ -148,6 +150,7 @@ SIGNATURES = {
     "rt_trace_any": [_P, _P, _U64, _P, _U32],
     "rt_trace_any_bits": [_P, _P, _U64, _P, _U32],
     "rt_trace_counts": [_P, _P, _U64, _U32, _P],
+    "rt_render_stage_times": [_P, _P, _U32],
     "rt_trace_stats_get": [_P, ctypes.POINTER(TraceStats)],
     "rt_scene_set_materials": [_P, _P, _U32],
     "rt_scene_set_triangle_materials": [_P, _U32, _U32, _P],

@@ -215,6 +215,12 @@ class Scene:
                                   ctypes.byref(st)))
         return film, {f: getattr(st, f) for f, _ in N.RenderStats._fields_}
 
+    def stage_times(self) -> dict:
+        """Per-stage device milliseconds of the last render made with N.RT_RENDER_STAGE_TIMES."""
+        out = (ctypes.c_double * len(N.RENDER_STAGES))()
+        N.check(N.lib().rt_render_stage_times(self.handle, out, len(N.RENDER_STAGES)))
+        return dict(zip(N.RENDER_STAGES, list(out)))
+
     def render_batch(self, views, flags: int = 0, max_paths: int = 0, film=None, fp64: bool = False):
         """Renders many views of this scene in one wavefront (rt_render_batch).
 

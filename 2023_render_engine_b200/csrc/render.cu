@@ -1274,35 +1274,63 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     const uint32_t trace_flags = (flags & RT_RENDER_EXACT_TRACE) ? 0u : RT_TRACE_FAST;
     uint64_t waves = 0;
     const uint64_t max_waves = (uint64_t)depth_max * (total / std::max<uint32_t>(cap / 4, 1) + 8) + 64;
+    // RT_RENDER_STAGE_TIMES: an event at each stage boundary of each wave of a group (host loop,
+    // no graphs), the elapsed times summed into rs.stage_ms after every group
+    const bool stage_times = (flags & RT_RENDER_STAGE_TIMES) != 0;
+    for (int k = 0; k < RT_RENDER_STAGES; k++) rs.stage_ms[k] = 0.0;
+    struct StageEvents {  // destroyed on every return path
+        cudaEvent_t e[4][RT_RENDER_STAGES + 1] = {};
+        ~StageEvents()
+        {
+            for (auto &row : e)
+                for (cudaEvent_t ev : row)
+                    if (ev) cudaEventDestroy(ev);
+        }
+    } sev;
+    if (stage_times)
+        for (auto &row : sev.e)
+            for (cudaEvent_t &ev : row) RTB_CUDA(cudaEventCreate(&ev));
+    auto mark = [&](int k, int b) -> int {
+        if (stage_times) RTB_CUDA(cudaEventRecord(sev.e[k][b], st));
+        return RT_OK;
+    };
     // One group = 4 waves (cur 0, 1, 0, 1). The first group is launched directly; the rest
     // replay it as a CUDA graph captured from the second group's launches.
     auto wave_group = [&]() -> int {
         int cur = 0;
         for (int k = 0; k < 4; k++) {
+            RTB_CHECK(mark(k, 0));
             RTB_CHECK(launch_trace_closest_dev(rv.sv, bf.rays[cur], bf.cnt + cur, cap, bf.hits, trace_flags,
                                                s->scratch.queue.as<uint32_t>(), s->scratch.counters.as<uint32_t>(),
                                                st));
+            RTB_CHECK(mark(k, 1));
             if (gv.params) {
                 k_guide_infer<<<infer_blocks, kInferWarps * 32, kInferSmem, st>>>(
                     rv, bf, cur, guide->img.as<uint4>(), gbox, guide->params.as<GuideParams>(), gv.max_depth);
                 RTB_CUDA(cudaGetLastError());
             }
+            RTB_CHECK(mark(k, 2));
             RTB_CUDA(cudaMemsetAsync(bf.cnt + ((cur ^ 1)), 0, 4, st));
             RTB_CUDA(cudaMemsetAsync(bf.cnt + 2, 0, 24, st));
             if (sort_log2) {
                 k_material_sort<<<sort_blocks, kSortBlock, 0, st>>>(rv, bf, cur, rs.perm.as<uint32_t>(), sort_log2);
                 RTB_CUDA(cudaGetLastError());
             }
+            RTB_CHECK(mark(k, 3));
             k_shade<<<blocks, kB, 0, st>>>(rv, bf, cur, gv);
             RTB_CUDA(cudaGetLastError());
+            RTB_CHECK(mark(k, 4));
             k_shadow<<<shadow_blocks, kB, 0, st>>>(rv, bf, cur ^ 1, gv);
             RTB_CUDA(cudaGetLastError());
+            RTB_CHECK(mark(k, 5));
             if (gathers) {
                 k_gather<<<gather_blocks, kGatherBlock, 0, st>>>(rv, bf, pv, cur ^ 1, gv);
                 RTB_CUDA(cudaGetLastError());
             }
+            RTB_CHECK(mark(k, 6));
             k_retire<<<retire_blocks, kB, 0, st>>>(bf, sum_rgb, count, sum64, gv);
             RTB_CUDA(cudaGetLastError());
+            RTB_CHECK(mark(k, 7));
             cur ^= 1;
         }
         return RT_OK;
@@ -1318,7 +1346,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     // cannot be captured) the host loop below runs instead.
     bool device_loop = false;
     const uint32_t wave_cap = (uint32_t)std::min<uint64_t>(max_waves, 0x7FFFFFF0u);
-    if (st != nullptr && st != cudaStreamLegacy && !(flags & RT_RENDER_HOST_LOOP)) {
+    if (st != nullptr && st != cudaStreamLegacy && !(flags & (RT_RENDER_HOST_LOOP | RT_RENDER_STAGE_TIMES))) {
         cudaGraph_t g = nullptr;
         cudaGraphConditionalHandle loop_handle;
         bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
@@ -1373,7 +1401,7 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
     for (uint64_t group = 0; !device_loop; group++) {
         int rc = RT_OK;
         // the legacy default stream cannot be captured: there every group is launched directly
-        if (group == 1 && st != nullptr && st != cudaStreamLegacy &&
+        if (group == 1 && !stage_times && st != nullptr && st != cudaStreamLegacy &&
             cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
             rc = wave_group();
             cudaGraph_t g = nullptr;
@@ -1404,6 +1432,15 @@ int render_views(rt_scene *s, const rt_view *views, uint32_t nviews, uint32_t fl
         if (ce != cudaSuccess) {
             release_graph();
             return cuda_status(ce, "wave group");
+        }
+        if (stage_times) {
+            // stage 1 (guide inference) spans boundaries 1-2, stage 2 (sort and counter resets) 2-3, ...
+            for (int k = 0; k < 4; k++)
+                for (int b = 0; b < RT_RENDER_STAGES; b++) {
+                    float t = 0.f;
+                    if (cudaEventElapsedTime(&t, sev.e[k][b], sev.e[k][b + 1]) == cudaSuccess) rs.stage_ms[b] += t;
+                }
+            (void)cudaGetLastError();
         }
         const uint32_t *hc = static_cast<const uint32_t *>(rs.host_cnt);
         uint64_t next_sample;
@@ -1463,6 +1500,14 @@ extern "C" int rt_render_batch(rt_scene *s, const rt_view *views, uint32_t nview
                                float *sum_rgb, uint32_t *count, double *sum64, rt_render_stats *stats)
 {
     return render_views(s, views, nviews, flags, max_paths, sum_rgb, count, sum64, stats, "rt_render_batch");
+}
+
+extern "C" int rt_render_stage_times(rt_scene *s, double *ms_out, uint32_t n)
+{
+    if (!s || (!ms_out && n)) return fail(RT_ERR_INVALID, "rt_render_stage_times: null argument");
+    if (n > RT_RENDER_STAGES) return fail(RT_ERR_INVALID, "rt_render_stage_times: at most RT_RENDER_STAGES values");
+    for (uint32_t k = 0; k < n; k++) ms_out[k] = s->rscratch.stage_ms[k];
+    return RT_OK;
 }
 
 extern "C" int rt_render_set_sort(rt_scene *s, uint32_t chunk_log2)

@@ -218,6 +218,7 @@ struct RenderScratch {
     DevBuf views, view_sample0, view_pixel0;  // the render's views and their prefix sums
     DevBuf perm;  // shading order of the wave (material sort)
     void *host_cnt = nullptr;  // pinned
+    double stage_ms[RT_RENDER_STAGES] = {};  // last render's per-stage time (RT_RENDER_STAGE_TIMES)
     void release();
 };
 

@@ -318,6 +318,9 @@ typedef struct rt_camera {
                                       device-side loop (a CUDA graph with a conditional WHILE node); the same
                                       kernels and samples, for tools that do not see kernels inside
                                       conditional graphs */
+#define RT_RENDER_STAGE_TIMES 0x100u /* time every wavefront stage with CUDA events (read them with
+                                        rt_render_stage_times); implies the host-side loop, launched
+                                        without graphs, so it is slower: a profiling aid */
 #define RT_RENDER_SUBSURFACE 0x20u /* CHECK_SUBSURFACE_SCATTERING: at camera-ray hits on RT_MAT_SUBSURFACE add
                                       the dipole photon estimate (rt_photon_subsurface, radius 0.3);
                                       needs the photon map of rt_render_set_photon_map */
@@ -395,6 +398,14 @@ RT_API int rt_scene_merge(rt_context *ctx, rt_scene *const *scenes, uint32_t n, 
  * 0 turns the sort off; a new scene uses 10. Results do not depend on it. Applies to rt_render
  * and rt_render_batch. */
 RT_API int rt_render_set_sort(rt_scene *scene, uint32_t chunk_log2);
+
+/* Per-stage device time of the scene's last render call made with RT_RENDER_STAGE_TIMES (new; the
+ * reference times whole tiles on the host, PathTracerIntegrator.cu:107-135). ms_out[0..n) gets, in
+ * milliseconds summed over the call's waves: 0 closest-hit trace (with its reference-order replay),
+ * 1 guide inference, 2 material sort, 3 shading, 4 shadow rays, 5 photon-map gathers, 6 film
+ * accumulation. Zeros when the last call did not time its stages. n at most RT_RENDER_STAGES. */
+#define RT_RENDER_STAGES 7
+RT_API int rt_render_stage_times(rt_scene *scene, double *ms_out, uint32_t n);
 
 /* --------------------------------------------------------------- photons */
 

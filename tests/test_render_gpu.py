@@ -182,3 +182,29 @@ def test_path_capacity_leaves_the_image_unchanged(core, gpu_ctx):
     for b, sb in out[1:]:
         assert sa["extension_rays"] == sb["extension_rays"] and sa["shadow_rays"] == sb["shadow_rays"]
         assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+
+
+def test_stage_times(core, gpu_ctx):
+    """RT_RENDER_STAGE_TIMES times every wavefront stage with CUDA events (host loop, no graphs):
+    the same samples as an untimed render, a time for each stage that ran, none for the stages
+    that did not (no guide, no photon map), and a sum within the call's own time."""
+    cfgs = importlib.import_module("2023_render_engine_b200.configs")
+    sc, cam, p = cfgs.build_config0(gpu_ctx, 64, 48)
+    flags = N.RT_RENDER_NEE_AREA
+    ref, st0 = sc.render(cam, spp=4, max_depth=8, seed=9, flags=flags, fp64=True, max_paths=1 << 12)
+    assert all(v == 0.0 for v in sc.stage_times().values())
+    got, st1 = sc.render(cam, spp=4, max_depth=8, seed=9, flags=flags | N.RT_RENDER_STAGE_TIMES, fp64=True,
+                         max_paths=1 << 12)
+    t = sc.stage_times()
+    assert st0["extension_rays"] == st1["extension_rays"] and st0["shadow_rays"] == st1["shadow_rays"]
+    assert np.allclose(core.film_mean(ref), core.film_mean(got), rtol=1e-5, atol=1e-6)
+    for k in ("trace", "material_sort", "shade", "shadow", "retire"):
+        assert t[k] > 0.0
+    # nothing runs between those two pairs of events: only the events' own spacing is timed
+    assert t["gather"] < 0.25 * t["trace"] and t["guide_inference"] < 0.25 * t["trace"]
+    assert sum(t.values()) <= st1["ms"] * 1.001
+    # an untimed render clears them again
+    sc.render(cam, spp=1, max_depth=8, seed=9, flags=flags)
+    assert all(v == 0.0 for v in sc.stage_times().values())
+    with pytest.raises(N.RtError):
+        N.check(N.lib().rt_render_stage_times(sc.handle, None, 1))
