@@ -546,6 +546,14 @@ def run_ours(args):
     barrier()
     ms_e2e = e0.elapsed_time(e1) / args.steps
 
+    # ---- one more frame (untimed) with its stages timed by CUDA events: where the frame goes
+    film["sum"].zero_()
+    film["count"].zero_()
+    _, st_stages = sc.render(cam, spp=args.spp, max_depth=p["max_depth"], rr_depth=p["rr_depth"],
+                             seed=rank_seed(900, rank), flags=rflags | N.RT_RENDER_STAGE_TIMES, film=film)
+    stage_ms = {k: round(v, 3) for k, v in sc.stage_times().items()}
+    stage_ms["frame"] = round(st_stages["ms"], 3)
+
     # ---- closest-hit trace of the 2^24-ray set (dominant kernel, roofline)
     o, d = S.random_rays(NRAYS, seed=7 + rank)
     rays_np = core.make_rays(o, d)
@@ -645,7 +653,8 @@ def run_ours(args):
                         "camera_rays": int(st_last["camera_rays"]), "waves": int(st_last["waves"]),
                         "samples_per_s": samples * world / (ms / 1000),
                         "l2": "scene ~140 MB and path queues ~1 GB per step exceed the 126 MB L2",
-                        "parallelism": f"replicas x{world}"},
+                        "parallelism": f"replicas x{world}",
+                        "stage_ms": stage_ms},
             "e2e": {"value": rate_e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 144 + 32,
                     "d2h_bytes_per_step": W * H * 16,
                     "note": "render call through the C ABI + film read back to pinned host memory; the inputs "
