@@ -124,8 +124,8 @@ def measure_merged(groups, sync, autotune=True):
         merged.close()
 
 
-def measure_guided(scene, flags, views, guide, sync, capacity=0, train_passes=4, steps_per_pass=64,
-                   batch=1 << 16):
+def measure_guided(scene, flags, views, guide, sync, capacity=0, train_passes=4, steps_per_pass=128,
+                   batch=2 * 148 * 128):
     """The views of one scene rendered with the learned guide: `train_passes` one-spp
     recording passes over the whole batch (each followed by `steps_per_pass` training steps),
     then the batch at its own spp with the guide, against the same batch without it."""

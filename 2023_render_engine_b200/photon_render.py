@@ -37,7 +37,7 @@ def _event_ms(torch, stream, fn):
 
 
 def measure(ctx, torch, stream, width=3840, height=2160, spp=None, photons=None, k=None, seed=11,
-            guided=True, train_passes=4, train_steps=64, train_batch=1 << 16, terrain_n=1000):
+            guided=True, train_passes=4, train_steps=128, train_batch=2 * 148 * 128, terrain_n=1000):
     """Runs config 4 once and returns a dict of its timings and rates."""
     spp = spp or 256
     photons = photons or configs.CONFIG4_PHOTONS

@@ -740,8 +740,10 @@ def main():
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)
     ap.add_argument("--guide-train-passes", type=int, default=4)
-    ap.add_argument("--guide-steps", type=int, default=64)
-    ap.add_argument("--guide-batch", type=int, default=1 << 16)
+    ap.add_argument("--guide-steps", type=int, default=128, help="Adam steps per recording pass "
+                    "(configs.GUIDE_TRAINING)")
+    ap.add_argument("--guide-batch", type=int, default=2 * 148 * 128, help="samples per Adam step "
+                    "(configs.GUIDE_TRAINING: one round of the training kernel's tiles on 148 SMs)")
     ap.add_argument("--guide-eval-rows", type=int, default=1 << 21, help="guide inference rows (0 skips)")
     args = ap.parse_args()
     global NRAYS
