@@ -212,9 +212,9 @@ struct PhotonView {
     float radius;
 };
 
-// Material sort: the shading order of a wave. Each block takes one chunk of 2^log2 queue slots
-// and orders it by the kind of surface its ray hit (a miss first, then rt_material_type), by
-// a counting sort in shared memory; k_shade's thread i then shades slot perm[i]. Lanes of a warp
+// Material sort: the shading order of a wave. Each block takes chunks of 2^log2 queue slots
+// and orders each by the kind of surface its ray hit (a miss first, then rt_material_type), by
+// a stable counting sort in shared memory; k_shade's thread i then shades slot perm[i]. Lanes of a warp
 // then mostly run the same BSDF code, while the chunk keeps the state reads of a warp within a
 // few kilobytes. The chunk size is the sort granularity (rt_render_set_sort).
 constexpr int kSortBlock = 256;
