@@ -573,6 +573,17 @@ def run_ours(args):
     barrier()
     ms_trace = t0.elapsed_time(t1) / args.steps
     fallback = sc.trace_stats()["exact_fallback_rays"]
+    # the same rays in RT_TRACE_FAST mode (the renderer's extension rays: no reference-order checks)
+    for _ in range(2):
+        sc.trace_closest(rays_d, hits_d, NRAYS, N.RT_TRACE_FAST)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for _ in range(args.steps):
+        sc.trace_closest(rays_d, hits_d, NRAYS, N.RT_TRACE_FAST)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms_trace_fast = t0.elapsed_time(t1) / args.steps
+    sc.trace_closest(rays_d, hits_d, NRAYS)  # the reference-exact hits again (compared further down)
     trav_work = None
     if world == 1 and not args.no_traversal_work:
         trav_work = measure_traversal_work(N, torch, core, S, cfgs, ctx, sc, rays_d, NRAYS, ms_trace)
@@ -660,7 +671,8 @@ def run_ours(args):
                     "note": "render call through the C ABI + film read back to pinned host memory; the inputs "
                             "of a step are the camera and options structs"},
             "trace": {"workload": TRACE_WORKLOAD.format(NRAYS.bit_length() - 1), "value": trace_rate, "unit": "Mrays/s", "ms_per_step": ms_trace,
-                      "exact_fallback_rays": int(fallback)},
+                      "exact_fallback_rays": int(fallback),
+                      "fast_value": NRAYS * world / (ms_trace_fast / 1000) / 1e6, "fast_ms_per_step": ms_trace_fast},
             # per frame: 6 kernels a wave (closest hit, its replay, material sort, shade, shadow,
             # retire), the wave check of each 4-wave group and the first camera rays
             "gpu_launches": args.steps * (int(st_last["waves"]) * 6 + (int(st_last["waves"]) + 3) // 4 + 1),
