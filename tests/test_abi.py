@@ -47,6 +47,10 @@ def test_abi_version_and_errors_without_gpu():
     # null arguments are rejected before any device work
     assert lib.rt_scene_commit(None) == 1
     assert "null" in N.last_error()
+    assert lib.rt_trace_counts(None, None, 0, 0, None) == 1
+    assert "rt_trace_counts" in N.last_error()
+    assert lib.rt_render_stage_times(None, None, 0) == 1
+    assert "rt_render_stage_times" in N.last_error()
     h = ctypes.c_void_p()
     st = lib.rt_context_create(0, ctypes.byref(h))
     import torch
