@@ -109,7 +109,7 @@ int check_device_status(uint32_t word)
     case DEV_OK:
         return RT_OK;
     case DEV_STACK_OVERFLOW:
-        return fail(RT_ERR_CAPACITY, "traversal stack overflow (a ray was replayed on the reference tree)");
+        return fail(RT_ERR_CAPACITY, "traversal stack overflow: a walk that could not be replayed stopped early");
     case DEV_STEP_CAP:
         return fail(RT_ERR_TIMEOUT, "traversal exceeded its step cap");
     case DEV_QUEUE_OVERFLOW:

@@ -82,7 +82,7 @@ extern "C" int rt_trace_closest_noalloc(rt_scene *s, const rt_ray *rays, uint64_
     case DEV_OK:
         return RT_OK;
     case DEV_STACK_OVERFLOW:
-        return fail(RT_ERR_CAPACITY, "traversal stack overflow (a ray was replayed on the reference tree)");
+        return fail(RT_ERR_CAPACITY, "traversal stack overflow: a walk that could not be replayed stopped early");
     case DEV_QUEUE_OVERFLOW:
         return fail(RT_ERR_CAPACITY, "exact-traversal queue overflow");
     default:

@@ -41,8 +41,11 @@ __device__ __forceinline__ void closest_epilogue(const SceneView &v, uint64_t i,
     const float ox = T.w.ox, oy = T.w.oy, oz = T.w.oz, tmax = T.w.tmax;
     bool exact_needed = false, replay = false;
     if (!T.ok) {
+        // the walk ran out of stack or steps: the reference-order replay gives the exact answer
+        // (its own overflow is reported by k_trace_exact); a merged scene has no reference tree,
+        // so there the status word reports that the hit found so far is kept
         exact_needed = replay = v.subs == nullptr;
-        atomicCAS(counters + 1, 0u, (uint32_t)DEV_STACK_OVERFLOW);
+        if (v.subs) atomicCAS(counters + 1, 0u, (uint32_t)DEV_STACK_OVERFLOW);
     } else if (!(flags & RT_TRACE_FAST) && best.prim >= 0) {
         if (best.minblock < best.t) {
             exact_needed = replay = true;

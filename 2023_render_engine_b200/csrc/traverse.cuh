@@ -9,7 +9,13 @@
 
 namespace rtb {
 
-constexpr int kStack = 48;
+// Entries of a walk's stack (8 bytes each, in local memory). A walk that would need more ends,
+// and its ray is replayed on the reference tree (exact); 32 entries overflowed on dense
+// triangle soups without changing the render's speed.
+#ifndef RTB_KSTACK
+#define RTB_KSTACK 48
+#endif
+constexpr int kStack = RTB_KSTACK;
 
 // Resident blocks of 128 threads per SM the traversal kernels are compiled for (register cap
 // 65536 / (128 * N)): 9 gives 56 registers and 36 warps per SM (measured on the BVH-stress

@@ -200,7 +200,8 @@ RT_API int rt_trace_counts(rt_scene *scene, const rt_ray *rays_dev, uint64_t n, 
 
 /* Counters of the last rt_trace_closest call: rays that took the reference-order
  * exact traversal (distance ties resolved through the reference tree, grazing
- * rays, near-zero offsets). */
+ * rays, near-zero offsets, and walks deeper than the BVH8 stack, which are replayed
+ * there with exact results rather than reported as errors). */
 typedef struct rt_trace_stats {
     uint64_t rays;
     uint64_t exact_fallback_rays;
