@@ -46,9 +46,9 @@ NRAYS = 1 << 24
 ALG_BYTES_PER_RAY = 48  # 32 B ray in + 16 B hit out (queue level)
 # DRAM bytes (read + write) of one k_trace_closest launch of the 2^24-ray call: the mean of the
 # four 2^24-ray launches of one ncu capture of this file's render command (1 pass, --cache-control
-# none; profiles/k_trace_closest_bvh_stress.md), taken at commit 97e6eef of the traversal. A
+# none; profiles/k_trace_closest_bvh_stress.md), taken at commit 39de656 of the traversal. A
 # change to traverse.cuh or trace.cu that alters k_trace_closest needs a new capture.
-TRACE_TRAFFIC_BYTES_2_24 = 2_477_571_776 + 1_031_053_120
+TRACE_TRAFFIC_BYTES_2_24 = 2_479_014_720 + 1_033_936_064
 
 
 def dist_env():
